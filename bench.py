@@ -1,0 +1,293 @@
+"""Throughput benchmark of the FDTD hot path (Gcell-updates/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: Drude nanoparticle lit by a TF/SF plane wave -- 384^3 FP32 cells,
+sphere r = 40 cells (eps_inf = 1, wp = 2 pi c/(8 dx), gamma = wp/50) as a
+Drude ADE current, +x Ez-polarised Gaussian-pulse plane wave through a TF/SF
+box inset 20 cells from a 12-cell CPML, running FP64 DFT at 16 frequencies on
+one x-normal plane.  Synthetic inputs of those shapes (no dataset).  One
+bench step = --tsteps leapfrog time steps (default 100).
+
+Multi-GPU: one process per GPU, each running an independent replica
+(weak scaling, no data-path collective); time = max over ranks.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=384)
+    ap.add_argument("--tsteps", type=int, default=100)
+    ap.add_argument("--engine", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=2)
+    return ap.parse_args()
+
+
+METRIC = "Gcell-updates/s (FP32 forward, Drude sphere + TF/SF + 16-freq DFT plane)"
+UNIT = "Gcell-updates/s"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes(sc):
+    """Algorithmic DRAM bytes of one launch of the H and the E field kernel
+    (each field value read once and written once; absorber and ADE state only
+    where they exist; 1 B material index per E component)."""
+    import numpy as np
+    cfg = sc["cfg"]
+    n = (cfg.nx, cfg.ny, cfg.nz)
+    ncell = n[0] * n[1] * n[2]
+    slab = 0
+    for a in range(3):
+        th = cfg.pml[a][0] + cfg.pml[a][1]
+        slab += th * ncell // n[a]
+    # per slab cell along an axis: 2 E and 2 H components carry a psi (read + write 4 B each)
+    hb = 36 * ncell + 2 * 8 * slab
+    mats, idx = sc["materials"]
+    disp = 0
+    if mats is not None:
+        for c in range(3):
+            for m, mat in enumerate(mats):
+                if mat.npoles > 0:
+                    disp += int((np.asarray(idx[c]) == m).sum())
+    # ADE per dispersive node: Em, Jp, Jm read + write (4 B each) instead of the 1/eps path
+    eb = 36 * ncell + 3 * ncell + 2 * 8 * slab + disp * 24
+    return hb, eb
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    from dtmaxwell4_b200 import Simulation, scenarios, abi
+
+    dev = rank % max(1, torch.cuda.device_count())
+    torch.cuda.set_device(dev)
+    sc = scenarios.drude_sphere_tfsf(n=args.n, steps=args.tsteps * (args.steps + args.warmup + 8))
+    sim = Simulation(sc["cfg"])
+    scenarios.apply(sim, sc)
+    if args.engine:
+        sim.set_engine(args.engine)
+    ncell = sc["cfg"].nx * sc["cfg"].ny * sc["cfg"].nz
+    stream = torch.cuda.ExternalStream(sim.stream_handle())
+    for _ in range(args.warmup):
+        sim.step(args.tsteps)
+    sim.sync()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    l0 = sim.launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        sim.step(args.tsteps)
+    ev1.record(stream)
+    ev1.synchronize()
+    launches = sim.launches() - l0
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    cell_updates = ncell * args.tsteps * args.steps * world
+    value = cell_updates / (ms_max * 1e-3) / 1e9
+    assert sim.check_finite(), "non-finite fields"
+
+    # roofline of the dominant field kernel: per-launch device time with events
+    sim.set_profiling(True)
+    sim.step(max(20, args.tsteps // 5))
+    h_ms, e_ms, cnt = sim.read_profile()
+    sim.set_profiling(False)
+    hb, eb = algorithmic_bytes(sc)
+    peak, peak_kind = measured_peaks()
+    if e_ms >= h_ms:
+        kname, kms, kbytes = "e_kernel", e_ms / cnt, eb
+    else:
+        kname, kms, kbytes = "h_kernel", h_ms / cnt, hb
+    achieved = kbytes / (kms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+            "algorithmic_bytes_per_launch": kbytes, "ms_per_launch": round(kms, 4),
+            "h_ms_per_launch": round(h_ms / cnt, 4), "e_ms_per_launch": round(e_ms / cnt, 4),
+            "step_bytes_per_cell_update": round((hb + eb) / ncell, 2)}
+
+    # end to end through the public API with host buffers: the state lives in
+    # pinned host memory (as the reference's windowed calcStep keeps it in host
+    # RAM); every step uploads the six fields, advances tsteps, downloads them.
+    host = [torch.empty(sc["cfg"].nx, sc["cfg"].ny, sc["cfg"].nz, dtype=torch.float32).pin_memory() for _ in range(6)]
+    arrs = [h.numpy() for h in host]
+    for c in range(6):
+        sim.get_field(c, out=arrs[c])
+    e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e_steps):
+        for c in range(6):
+            sim.set_field(c, arrs[c])
+        sim.step(args.tsteps)
+        for c in range(6):
+            sim.get_field(c, out=arrs[c])
+    e1.record(stream)
+    e1.synchronize()
+    te = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
+    e2e_val = ncell * args.tsteps * e_steps * world / (float(te.item()) * 1e-3) / 1e9
+    nb = 6 * ncell * 4
+    e2e = {"value": round(e2e_val, 3), "unit": UNIT, "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
+           "steps": e_steps}
+    sim.close()
+    return value, ms_max, launches, roof, e2e, clk, sc
+
+
+def cpu_sample(args, n, tsteps):
+    """Time the oracle (FP32 port, all host threads) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from dtmaxwell4_b200 import scenarios
+    sc = scenarios.drude_sphere_tfsf(n=n, steps=tsteps + 8)
+    o = pyoracle.OracleSim(sc["cfg"], "f32")
+    scenarios.apply(o, sc)
+    o.step(1)                       # first step pays for lazy allocations
+    t0 = time.perf_counter()
+    o.step(tsteps)
+    dt = time.perf_counter() - t0
+    ncell = sc["cfg"].nx * sc["cfg"].ny * sc["cfg"].nz
+    o.close()
+    return ncell * tsteps / dt / 1e9, pyoracle.threads(), dt
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        # the reference has no CPU implementation of the path; its CPU arm is
+        # the oracle port (FP32, all host threads), one time step per bench step
+        vals = []
+        for it in range(args.warmup + args.steps):
+            v, cores, dt = cpu_sample(args, args.n, 1)
+            if it >= args.warmup:
+                vals.append(v)
+        value = sum(vals) / len(vals)
+        line = {"metric": METRIC, "value": round(value, 5), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(1e3 * (args.n ** 3) / (value * 1e9), 3),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "impl": "reference",
+                "config": {"workload": "drude_sphere_tfsf %d^3" % args.n, "time_steps_per_step": 1},
+                "cpu_baseline": {"value": round(value, 5), "unit": UNIT, "cores": cores, "kind": "port",
+                                 "sample": "1 time step of the %d^3 workload per bench step" % args.n},
+                "e2e": {"value": round(value, 5), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    if world > 1:
+        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    value, ms, launches, roof, e2e, clk, sc = run_ours(args, rank, world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, dt = cpu_sample(args, args.n, args.cpu_steps)
+        cpu = {"value": round(v, 5), "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": "%d time steps of the %d^3 workload (oracle FP32, %.1f s)" % (args.cpu_steps, args.n, dt)}
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "drude_sphere_tfsf %d^3, %d time steps per step" % (args.n, args.tsteps),
+                           "desc": sc["desc"], "time_steps_per_step": args.tsteps,
+                           "l2": "inputs larger than L2 (%.2f GB of fields)" % (6 * args.n ** 3 * 4 / 1e9),
+                           "parallelism": "replicas%d" % world},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

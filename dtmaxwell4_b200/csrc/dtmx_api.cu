@@ -1,0 +1,802 @@
+// dtmx_api.cu -- host runtime behind the C ABI declared in include/dtmx.h.
+//
+// Owns every device allocation of a simulation context, validates the
+// configuration (the reference's printf+exit checks in GeoParamsHost::set,
+// DTmxw.cu:278-487, become status codes), builds the coefficient tables and
+// launches the per-step kernel sequence on the context's stream.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "dtmx.h"
+#include "dtmx_device.cuh"
+#include "dtmx_aux.cuh"
+
+using namespace dtmx;
+
+struct DftHost {
+  DftDev d;
+  int ncomp;
+  double* omega = nullptr;
+  double2* acc = nullptr;
+};
+
+struct dtmx_ctx {
+  dtmx_config cfg{};
+  int dev = 0;
+  cudaStream_t stream = nullptr;
+  Params P{};
+  int nzp = 0;
+  size_t nstore = 0;            // elements per component array (padded)
+  size_t ncell = 0;             // nx*ny*nz
+  std::vector<void*> allocs;
+  // coefficient tables
+  float* ctab[3][3] = {};
+  // materials
+  MatTable* d_mt = nullptr;
+  MatTable h_mt{};
+  dtmx_material mats[DTMX_MAX_MATERIALS]{};
+  int nmat = 1;
+  uint8_t* d_mat[3] = {};
+  std::vector<uint8_t> h_mat[3];
+  // sources
+  std::vector<PointSrcDev> psrc;
+  PointSrcDev* d_psrc = nullptr;
+  int has_tfsf = 0;
+  dtmx_tfsf tfsf{};
+  TfsfDev T{};
+  double* line_e = nullptr;
+  double* line_h = nullptr;
+  int line_src = 0;
+  // monitors
+  std::vector<ProbeDev> probes;
+  ProbeDev* d_probes = nullptr;
+  float* d_traces = nullptr;
+  int probe_cap = 0;
+  std::vector<DftHost> dfts;
+  // state
+  long long* d_step = nullptr;
+  int* d_flag = nullptr;
+  long long step = 0;
+  long long launches = 0;
+  bool prepared = false;
+  bool profiling = false;
+  cudaEvent_t ev[4] = {};
+  double prof_ms_h = 0, prof_ms_e = 0;
+  long long prof_count = 0;
+  bool prof_pending = false;
+  int engine = 0, tblock = 0;
+  std::string err;
+};
+
+static const char* kErrStr[] = {"ok", "invalid argument", "CUDA error", "out of device memory", "non-finite value",
+                                "device wait timed out", "invalid state", "unsupported", "no CUDA device"};
+
+#define CK(call)                                                                           \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) {                                                               \
+      if (ctx) ctx->err = std::string(#call) + ": " + cudaGetErrorString(e_);              \
+      return e_ == cudaErrorMemoryAllocation ? DTMX_ERR_OOM : DTMX_ERR_CUDA;               \
+    }                                                                                      \
+  } while (0)
+
+static int fail(dtmx_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+template <class T>
+static int dalloc(dtmx_ctx* ctx, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    ctx->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? DTMX_ERR_OOM : DTMX_ERR_CUDA;
+  }
+  e = cudaMemsetAsync(q, 0, std::max<size_t>(count, 1) * sizeof(T), ctx->stream);
+  if (e != cudaSuccess) { ctx->err = cudaGetErrorString(e); return DTMX_ERR_CUDA; }
+  ctx->allocs.push_back(q);
+  *p = (T*)q;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_version(void) { return DTMX_ABI_VERSION; }
+extern "C" const char* dtmx_error_string(int code) {
+  if (code < 0 || code > 8) return "unknown";
+  return kErrStr[code];
+}
+extern "C" const char* dtmx_last_error(const dtmx_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+// ---------------------------------------------------------------- boundaries
+static void setup_grid(dtmx_ctx* ctx) {
+  Grid& g = ctx->P.g;
+  const dtmx_config& c = ctx->cfg;
+  int n[3] = {c.nx, c.ny, c.nz};
+  for (int a = 0; a < 3; a++) g.n[a] = n[a];
+  g.sy = ctx->nzp;
+  g.sx = (long long)c.ny * ctx->nzp;
+  for (int a = 0; a < 3; a++)
+    for (int s = 0; s < 2; s++) { g.btype[a][s] = 0; g.bsE[a][s] = 1; g.bsH[a][s] = 1; }
+  if (c.geometry == DTMX_GEOM_BOX) {
+    for (int a = 0; a < 3; a++) { g.bplane[a][0] = -1; g.bplane[a][1] = 2 * n[a]; }
+  } else {
+    // x: isOutS zero planes (defs.h:40); y: I-kernel free reflection at 0 with H odd
+    // (genAlg.py:166-168) and X-kernel even mirror at 6*Na-3 (genAlg.py:9,36);
+    // z: Vrefl even mirrors at 0 and 2*Nv-1 (defs.h:76-81).
+    g.bplane[0][0] = 3; g.bplane[0][1] = 2 * n[0] - 3;
+    g.btype[1][0] = 1; g.bplane[1][0] = 0; g.bsH[1][0] = -1;
+    g.btype[1][1] = 1; g.bplane[1][1] = 2 * n[1] - 3;
+    g.btype[2][0] = 1; g.bplane[2][0] = 0;
+    g.btype[2][1] = 1; g.bplane[2][1] = 2 * n[2] - 1;
+  }
+  for (int comp = 0; comp < 6; comp++)
+    for (int a = 0; a < 3; a++) {
+      int lo = 0, hi = n[a] - 1;
+      for (; lo <= hi; lo++) {
+        int H = 2 * lo + comp_off(comp, a);
+        if (g.btype[a][0] == 0 ? H > g.bplane[a][0] : H >= g.bplane[a][0]) break;
+      }
+      for (; hi >= lo; hi--) {
+        int H = 2 * hi + comp_off(comp, a);
+        if (g.btype[a][1] == 0 ? H < g.bplane[a][1] : H <= g.bplane[a][1]) break;
+      }
+      g.live_lo[comp][a] = lo;
+      g.live_hi[comp][a] = hi;
+    }
+}
+
+// Reference PMLgamma_func (DTmxw.cu:220-229).
+static double ref_gamma(int i, int N, double dstep, double vmax) {
+  if (i >= N - 3) return 0.0;
+  if (i < 0) i = 0;
+  N -= 3;
+  const double att = 4.0;
+  const double smax = vmax * std::log(10000.0) * ((att + 1.0) / (2.0 * (N * dstep * 0.5)));
+  const double xmax = std::pow(smax, 1.0 / att);
+  const double x = xmax - i * (xmax / N);
+  return std::pow(x, att);
+}
+
+static int setup_absorber(dtmx_ctx* ctx) {
+  const dtmx_config& c = ctx->cfg;
+  Absorb& ab = ctx->P.ab;
+  ab.kind = c.absorber;
+  const int n[3] = {c.nx, c.ny, c.nz};
+  const double d[3] = {c.dx, c.dy, c.dz};
+  std::vector<float> t0[3], t1[3], t2[3];
+  for (int a = 0; a < 3; a++) {
+    const int H = 2 * n[a] + 2;
+    t0[a].assign(H, 1.f); t1[a].assign(H, 0.f); t2[a].assign(H, 1.f);
+    ab.L[a][0] = ab.L[a][1] = 0;
+  }
+  if (c.absorber == DTMX_ABS_CPML) {
+    const double m = c.cpml_m > 0 ? c.cpml_m : 3.0;
+    const double fac = c.cpml_sigma_factor > 0 ? c.cpml_sigma_factor : 1.0;
+    const double kmax = c.cpml_kappa_max >= 1 ? c.cpml_kappa_max : 1.0;
+    const double amax = c.cpml_alpha_max;
+    for (int a = 0; a < 3; a++)
+      for (int s = 0; s < 2; s++) {
+        const int L = c.pml[a][s];
+        ab.L[a][s] = L;
+        if (L <= 0) continue;
+        const double smax = fac * 0.8 * (m + 1.0) / d[a];
+        for (int h = 0; h < 2 * n[a]; h++) {
+          double dep = s == 0 ? (2.0 * L - 1.0 - h) * 0.5 : (h - (2.0 * n[a] - 2.0 * L)) * 0.5;
+          if (dep <= 0) continue;
+          dep = std::min<double>(dep, L);
+          const double r = dep / L;
+          const double sg = smax * std::pow(r, m);
+          const double kp = 1.0 + (kmax - 1.0) * std::pow(r, m);
+          const double al = amax * (1.0 - r);
+          const double b = std::exp(-(sg / kp + al) * c.dt);
+          const double aa = sg > 0 ? sg / (sg * kp + kp * kp * al) * (b - 1.0) : 0.0;
+          t0[a][h] = (float)b; t1[a][h] = (float)aa; t2[a][h] = (float)(1.0 / kp);
+        }
+      }
+  } else if (c.absorber == DTMX_ABS_SPLIT_PML) {
+    // setPMLcoeffs (DTmxw.cu:250-265): K2 = 1/(1+dt/2*gamma), K1 = 2*K2-1
+    const double V = c.spml_vmax;
+    const int KX = 60, KY = 60, KZ = 64;
+    ab.L[0][0] = c.pml[0][0]; ab.L[0][1] = c.pml[0][1];
+    ab.L[1][0] = c.pml[1][0]; ab.L[1][1] = c.pml[1][1];
+    ab.L[2][0] = 0;           ab.L[2][1] = c.pml[2][1];
+    for (int h = 0; h < 2 * n[0] + 2; h++) {
+      int i = -1;
+      if (h < 27) i = h;                               // inPMLsync (defs.h:45)
+      else if (h >= 2 * n[0] - 27) i = h - 2 * n[0] + KX;
+      if (i < 0 || i >= KX) continue;
+      const double k2 = 1.0 / (1.0 + 0.5 * c.dt * ref_gamma(KX / 2 - std::abs(i - KX / 2) - 3, KX / 2 - 3, c.dx, V));
+      t1[0][h] = (float)k2; t0[0][h] = (float)(2.0 * k2 - 1.0);
+    }
+    for (int h = 0; h < 2 * n[1] + 2; h++) {
+      int i = -1;
+      if (h < KY / 2) i = h;
+      else if (h >= 2 * n[1] - KY / 2) i = h - 2 * n[1] + KY;
+      if (i < 0 || i >= KY) continue;
+      const double k2 = 1.0 / (1.0 + 0.5 * c.dt * ref_gamma(i < KY / 2 ? i : KY - i - 3, KY / 2, c.dy, V));
+      t1[1][h] = (float)k2; t0[1][h] = (float)(2.0 * k2 - 1.0);
+    }
+    for (int h = 0; h < 2 * n[2] + 2; h++) {
+      const int i = h - 2 * n[2] + KZ;                 // top face only (DTmxw.cu:262)
+      if (i < KZ / 2 || i >= KZ) continue;
+      const double k2 = 1.0 / (1.0 + 0.5 * c.dt * ref_gamma(KZ - i - 1, KZ / 2, c.dz, V));
+      t1[2][h] = (float)k2; t0[2][h] = (float)(2.0 * k2 - 1.0);
+    }
+  }
+  for (int a = 0; a < 3; a++) {
+    const int H = 2 * n[a] + 2;
+    float* q[3];
+    for (int t = 0; t < 3; t++) {
+      int rc = dalloc(ctx, &q[t], H);
+      if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(q[0], t0[a].data(), H * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(q[1], t1[a].data(), H * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(q[2], t2[a].data(), H * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ab.c0[a] = q[0]; ab.c1[a] = q[1]; ab.c2[a] = q[2];
+    const size_t th = (size_t)(ab.L[a][0] + ab.L[a][1]);
+    for (int s = 0; s < 4; s++) ab.aux[a][s] = nullptr;
+    if (!th || c.absorber == DTMX_ABS_NONE) continue;
+    const size_t cnt = th * (ctx->ncell / (size_t)n[a]);
+    for (int s = 0; s < 4; s++) {
+      int rc = dalloc(ctx, &ab.aux[a][s], cnt);
+      if (rc) return rc;
+    }
+    // sync the coefficient vectors (host memory) before they go out of scope
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DTMX_OK;
+}
+
+static int upload_mattable(dtmx_ctx* ctx) {
+  dtmx_ctx* c = ctx;
+  CK(cudaMemcpyAsync(c->d_mt, &c->h_mt, sizeof(MatTable), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_create(const dtmx_config* cfg, dtmx_ctx** out) {
+  if (!cfg || !out) return DTMX_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return DTMX_ERR_NODEVICE;
+  const dtmx_config& c = *cfg;
+  if (c.nx < 8 || c.ny < 8 || c.nz < 8) return DTMX_ERR_INVALID;
+  if (c.order != 2 && c.order != 4) return DTMX_ERR_INVALID;
+  if (!(c.dx > 0 && c.dy > 0 && c.dz > 0 && c.dt > 0)) return DTMX_ERR_INVALID;
+  // Courant limits: 1 for the Yee stencil, 6/7 for the (27,-1)/24 stencil (DTmxw.cu:332)
+  const double cn = c.dt * std::sqrt(1 / (c.dx * c.dx) + 1 / (c.dy * c.dy) + 1 / (c.dz * c.dz));
+  if (cn > (c.order == 4 ? 6.0 / 7.0 : 1.0)) return DTMX_ERR_INVALID;
+  if (c.geometry != DTMX_GEOM_BOX && c.geometry != DTMX_GEOM_REFERENCE) return DTMX_ERR_INVALID;
+  if (c.absorber == DTMX_ABS_CPML && c.geometry != DTMX_GEOM_BOX) return DTMX_ERR_UNSUPPORTED;
+  if (c.absorber == DTMX_ABS_SPLIT_PML && c.geometry != DTMX_GEOM_REFERENCE) return DTMX_ERR_UNSUPPORTED;
+  if (c.geometry == DTMX_GEOM_REFERENCE && (c.nx % 3 || c.ny % 3)) return DTMX_ERR_INVALID;  // DTmxw.cu:330-331
+  const int n[3] = {c.nx, c.ny, c.nz};
+  for (int a = 0; a < 3; a++)
+    for (int s = 0; s < 2; s++)
+      if (c.pml[a][s] < 0 || c.pml[a][0] + c.pml[a][1] > n[a] - 4) return DTMX_ERR_INVALID;
+
+  dtmx_ctx* ctx = new dtmx_ctx();
+  ctx->cfg = c;
+  if (cudaGetDevice(&ctx->dev) != cudaSuccess) { delete ctx; return DTMX_ERR_CUDA; }
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return DTMX_ERR_CUDA; }
+  ctx->nzp = (c.nz + 31) / 32 * 32;
+  ctx->ncell = (size_t)c.nx * c.ny * c.nz;
+  ctx->nstore = (size_t)c.nx * c.ny * ctx->nzp;
+  setup_grid(ctx);
+  int rc = DTMX_OK;
+  for (int comp = 0; comp < 6 && !rc; comp++) rc = dalloc(ctx, &ctx->P.f[comp], ctx->nstore);
+  if (!rc) rc = setup_absorber(ctx);
+  if (!rc) rc = dalloc(ctx, &ctx->d_mt, 1);
+  if (!rc) rc = dalloc(ctx, &ctx->d_step, 1);
+  if (!rc) rc = dalloc(ctx, &ctx->d_flag, 1);
+  if (rc) { *out = ctx; return rc; }
+  ctx->P.cdt[0] = (float)(c.dt / c.dx); ctx->P.cdt[1] = (float)(c.dt / c.dy); ctx->P.cdt[2] = (float)(c.dt / c.dz);
+  // default material 0: vacuum
+  dtmx_material vac{};
+  vac.eps[0] = vac.eps[1] = vac.eps[2] = 1.0;
+  ctx->mats[0] = vac;
+  for (int comp = 0; comp < 3; comp++) ctx->h_mt.inv_eps[0][comp] = 1.f;
+  ctx->P.mt = ctx->d_mt;
+  rc = upload_mattable(ctx);
+  if (rc) { *out = ctx; return rc; }
+  ctx->probe_cap = c.probe_capacity > 0 ? c.probe_capacity : 4096;
+  *out = ctx;
+  return DTMX_OK;
+}
+
+extern "C" void dtmx_destroy(dtmx_ctx* ctx) {
+  if (!ctx) return;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (void* p : ctx->allocs) cudaFree(p);
+  for (auto& d : ctx->dfts) { cudaFree(d.omega); cudaFree(d.acc); }
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+// ---------------------------------------------------------------- materials
+// DispStruct::set (dispersion.cpp:41-82), coefficients in double then stored in float.
+static void disp_coeffs(const dtmx_material& M, double dt, MatTable& t, int mi) {
+  double alpha[MAXPOLE], ksi[MAXPOLE], zetp[MAXPOLE], zetm[MAXPOLE], zet[MAXPOLE];
+  double zms = 0, zps = 0, zs = 0;
+  for (int i = 0; i < M.npoles; i++) {
+    const double Deps = M.pole[i][0], wp = M.pole[i][1], gp = M.pole[i][2], gp_ = M.pole[i][3];
+    const double a0 = Deps * wp * wp, a1 = Deps * gp_;
+    const double b0 = M.pole_kind[i] == DTMX_POLE_DRUDE ? 0.0 : wp * wp, b1 = 2 * gp;
+    alpha[i] = (4 - 2 * b0 * dt * dt) / (b1 * dt + 2);
+    ksi[i] = (b1 * dt - 2) / (b1 * dt + 2);
+    zetp[i] = (a0 * dt * dt + 2 * a1 * dt) / (b1 * dt + 2);
+    zetm[i] = (-a0 * dt * dt + 2 * a1 * dt) / (b1 * dt + 2);
+    zet[i] = -(4 * a1 * dt) / (b1 * dt + 2);
+    zms += zetm[i]; zps += zetp[i]; zs += zet[i];
+  }
+  const double den = 2 * M.eps_inf + M.sigma * dt + zps;
+  const double C1 = -zms / den, C2 = (2 * M.eps_inf - M.sigma * dt - zs) / den, C3 = 2 * dt / den;
+  for (int xc = 0; xc < 3; xc++) {
+    for (int i = 0; i < M.npoles; i++) {
+      t.kJ[mi][xc][i][0] = (float)alpha[i]; t.kJ[mi][xc][i][1] = (float)ksi[i];
+      t.kJ[mi][xc][i][2] = (float)(zetp[i] / dt); t.kJ[mi][xc][i][3] = (float)(zetm[i] / dt);
+      t.kJ[mi][xc][i][4] = (float)(zet[i] / dt);
+      t.kEJ[mi][xc][i][0] = (float)(C3 * 0.5 * (1 + alpha[i])); t.kEJ[mi][xc][i][1] = (float)(C3 * 0.5 * ksi[i]);
+    }
+    t.kE[mi][xc][0] = (float)C1; t.kE[mi][xc][1] = (float)C2; t.kE[mi][xc][2] = (float)(C3 / dt);
+  }
+}
+
+static inline size_t store_index(const dtmx_ctx* ctx, int i, int j, int k) {
+  return ((size_t)i * ctx->cfg.ny + j) * ctx->nzp + k;
+}
+
+extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int nmat, const uint8_t* idx_x,
+                                  const uint8_t* idx_y, const uint8_t* idx_z) {
+  if (!ctx || !table || nmat < 1 || nmat > DTMX_MAX_MATERIALS || !idx_x) return fail(ctx, DTMX_ERR_INVALID, "bad material arguments");
+  if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "materials must be set before the first step");
+  const uint8_t* src[3] = {idx_x, idx_y ? idx_y : idx_x, idx_z ? idx_z : idx_x};
+  for (int m = 0; m < nmat; m++) {
+    const dtmx_material& M = table[m];
+    if (M.npoles < 0 || M.npoles > DTMX_MAX_POLES) return fail(ctx, DTMX_ERR_INVALID, "npoles out of range");
+    if (M.npoles > 0 && !(M.eps_inf > 0)) return fail(ctx, DTMX_ERR_INVALID, "dispersive material needs eps_inf > 0");
+    if (M.npoles == 0 && !(M.eps[0] > 0 && M.eps[1] > 0 && M.eps[2] > 0)) return fail(ctx, DTMX_ERR_INVALID, "eps must be > 0");
+    if (M.gyro_wp != 0) return fail(ctx, DTMX_ERR_UNSUPPORTED, "gyrotropic materials are not supported by this build");
+  }
+  MatTable& t = ctx->h_mt;
+  memset(&t, 0, sizeof(t));
+  for (int m = 0; m < nmat; m++) {
+    ctx->mats[m] = table[m];
+    t.npoles[m] = table[m].npoles;
+    for (int c = 0; c < 3; c++) t.inv_eps[m][c] = table[m].npoles > 0 ? 0.f : (float)(1.0 / table[m].eps[c]);
+    if (table[m].npoles > 0) disp_coeffs(table[m], ctx->cfg.dt, t, m);
+  }
+  ctx->nmat = nmat;
+  const dtmx_config& c = ctx->cfg;
+  int lo[3] = {c.nx, c.ny, c.nz}, hi[3] = {-1, -1, -1};
+  for (int comp = 0; comp < 3; comp++) {
+    ctx->h_mat[comp].assign(ctx->nstore, 0);
+    for (int i = 0; i < c.nx; i++)
+      for (int j = 0; j < c.ny; j++) {
+        const uint8_t* row = src[comp] + ((size_t)i * c.ny + j) * c.nz;
+        uint8_t* dst = ctx->h_mat[comp].data() + store_index(ctx, i, j, 0);
+        for (int k = 0; k < c.nz; k++) {
+          const uint8_t m = row[k];
+          if (m >= nmat) return fail(ctx, DTMX_ERR_INVALID, "material index out of range");
+          dst[k] = m;
+          if (table[m].npoles > 0) {
+            const int v[3] = {i, j, k};
+            for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], v[a]); hi[a] = std::max(hi[a], v[a]); }
+          }
+        }
+      }
+    if (!ctx->d_mat[comp]) {
+      int rc = dalloc(ctx, &ctx->d_mat[comp], ctx->nstore);
+      if (rc) return rc;
+    }
+    CK(cudaMemcpyAsync(ctx->d_mat[comp], ctx->h_mat[comp].data(), ctx->nstore, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->P.mat[comp] = ctx->d_mat[comp];
+  }
+  int rc = upload_mattable(ctx);
+  if (rc) return rc;
+  Ade& A = ctx->P.ade;
+  if (hi[0] >= 0) {
+    size_t na = 1;
+    for (int a = 0; a < 3; a++) { A.lo[a] = lo[a]; A.n[a] = hi[a] - lo[a] + 1; na *= A.n[a]; }
+    int maxp = 0;
+    for (int m = 0; m < nmat; m++) maxp = std::max(maxp, table[m].npoles);
+    for (int comp = 0; comp < 3; comp++) {
+      if ((rc = dalloc(ctx, &A.Em[comp], na))) return rc;
+      for (int q = 0; q < maxp; q++) {
+        if ((rc = dalloc(ctx, &A.Jp[comp][q], na))) return rc;
+        if ((rc = dalloc(ctx, &A.Jm[comp][q], na))) return rc;
+      }
+    }
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DTMX_OK;
+}
+
+static bool node_live(const dtmx_ctx* ctx, int comp, int i, int j, int k) {
+  const Grid& g = ctx->P.g;
+  return i >= g.live_lo[comp][0] && i <= g.live_hi[comp][0] && j >= g.live_lo[comp][1] && j <= g.live_hi[comp][1] &&
+         k >= g.live_lo[comp][2] && k <= g.live_hi[comp][2];
+}
+
+extern "C" int dtmx_add_point_source(dtmx_ctx* ctx, const dtmx_point_source* s) {
+  if (!ctx || !s || s->comp < 0 || s->comp > 2) return fail(ctx, DTMX_ERR_INVALID, "bad point source");
+  if (!node_live(ctx, s->comp, s->i, s->j, s->k)) return fail(ctx, DTMX_ERR_INVALID, "point source outside the live domain");
+  if (!(s->tau > 0)) return fail(ctx, DTMX_ERR_INVALID, "point source tau must be > 0");
+  if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "sources must be added before the first step");
+  PointSrcDev d;
+  d.comp = s->comp;
+  d.id = (long long)store_index(ctx, s->i, s->j, s->k);
+  d.amp = s->amp; d.f0 = s->f0; d.tau = s->tau; d.t0 = s->t0;
+  ctx->psrc.push_back(d);
+  return DTMX_OK;
+}
+
+// inSF along one axis with the reference's float arithmetic (signal.hpp:153-160)
+static void sf_range(double dstep, double bm, double bp, int hmax, int* lo, int* hi) {
+  const float bmf = (float)bm, bpf = (float)bp, df = (float)dstep;
+  *lo = 1; *hi = 0;
+  bool first = true;
+  for (int h = -8; h <= hmax + 8; h++) {
+    const float sv = (float)((double)h * 0.5 * (double)df);
+    if (sv > bmf && sv < bpf) { if (first) { *lo = h; first = false; } *hi = h; }
+  }
+}
+
+extern "C" int dtmx_set_tfsf(dtmx_ctx* ctx, const dtmx_tfsf* s) {
+  if (!ctx || !s || (s->kind != DTMX_TFSF_DIPOLE && s->kind != DTMX_TFSF_PLANE_X)) return fail(ctx, DTMX_ERR_INVALID, "bad TF/SF source");
+  if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "TF/SF source must be set before the first step");
+  const dtmx_config& c = ctx->cfg;
+  TfsfDev& T = ctx->T;
+  T = TfsfDev{};
+  const double d[3] = {c.dx, c.dy, c.dz};
+  const int n[3] = {c.nx, c.ny, c.nz};
+  for (int a = 0; a < 3; a++) {
+    sf_range(d[a], s->box_lo[a], s->box_hi[a], 2 * n[a], &T.lo[a], &T.hi[a]);
+    if (T.lo[a] > T.hi[a]) return fail(ctx, DTMX_ERR_INVALID, "TF/SF box contains no node");
+    // the correction shell (3 half cells around the surface) must stay inside the
+    // live domain and clear of the absorber
+    const int clo = (T.lo[a] - 4) / 2 - 1, chi = (T.hi[a] + 4) / 2 + 1;
+    const int alo = c.absorber == DTMX_ABS_NONE ? 0 : ctx->P.ab.L[a][0];
+    const int ahi = c.absorber == DTMX_ABS_NONE ? 0 : ctx->P.ab.L[a][1];
+    int llo = 0, lhi = n[a] - 1;
+    for (int comp = 0; comp < 6; comp++) { llo = std::max(llo, ctx->P.g.live_lo[comp][a]); lhi = std::min(lhi, ctx->P.g.live_hi[comp][a]); }
+    if (clo < std::max(alo, llo) + 1 || chi > std::min(n[a] - 1 - ahi, lhi) - 1)
+      return fail(ctx, DTMX_ERR_INVALID, "TF/SF box too close to the boundary or absorber");
+  }
+  T.active_cfg = 1;
+  T.kind = s->kind;
+  for (int a = 0; a < 3; a++) { T.ctr[a] = (s->box_lo[a] + s->box_hi[a]) * 0.5; T.hd[a] = d[a] * 0.5; }
+  T.dt = c.dt; T.c = s->c; T.w = s->w; T.kenv = s->kenv; T.tstop = s->tstop;
+  T.ntime = s->ntime > 0 ? s->ntime : 1;
+  // shell regions: expanded box E minus inner box I, as 6 disjoint slabs
+  int e[3][2], in_[3][2];
+  bool has_inner = true;
+  for (int a = 0; a < 3; a++) {
+    e[a][0] = (int)std::floor((T.lo[a] - 4) / 2.0);
+    e[a][1] = (int)std::floor((T.hi[a] + 4) / 2.0);
+    in_[a][0] = e[a][0] + 5;
+    in_[a][1] = e[a][1] - 5;
+    if (in_[a][0] > in_[a][1]) has_inner = false;
+  }
+  T.nreg = 0;
+  auto add = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
+    if (x0 > x1 || y0 > y1 || z0 > z1) return;
+    int r = T.nreg++;
+    T.reg[r][0][0] = x0; T.reg[r][0][1] = x1; T.reg[r][1][0] = y0; T.reg[r][1][1] = y1; T.reg[r][2][0] = z0; T.reg[r][2][1] = z1;
+    T.reg_cells[r] = (long long)(x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1);
+  };
+  if (!has_inner) {
+    add(e[0][0], e[0][1], e[1][0], e[1][1], e[2][0], e[2][1]);
+  } else {
+    add(e[0][0], in_[0][0] - 1, e[1][0], e[1][1], e[2][0], e[2][1]);
+    add(in_[0][1] + 1, e[0][1], e[1][0], e[1][1], e[2][0], e[2][1]);
+    add(in_[0][0], in_[0][1], e[1][0], in_[1][0] - 1, e[2][0], e[2][1]);
+    add(in_[0][0], in_[0][1], in_[1][1] + 1, e[1][1], e[2][0], e[2][1]);
+    add(in_[0][0], in_[0][1], in_[1][0], in_[1][1], e[2][0], in_[2][0] - 1);
+    add(in_[0][0], in_[0][1], in_[1][0], in_[1][1], in_[2][1] + 1, e[2][1]);
+  }
+  if (s->kind == DTMX_TFSF_PLANE_X) {
+    T.line_M = 4096;
+    T.line_n = c.nx + 2 * T.line_M;
+    int rc;
+    if (!ctx->line_e) {
+      if ((rc = dalloc(ctx, &ctx->line_e, T.line_n))) return rc;
+      if ((rc = dalloc(ctx, &ctx->line_h, T.line_n))) return rc;
+    }
+    T.line_e = ctx->line_e; T.line_h = ctx->line_h;
+    ctx->line_src = (T.lo[0] - 1) / 2 - 10 + T.line_M;
+  }
+  ctx->tfsf = *s;
+  ctx->has_tfsf = 1;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_add_probe(dtmx_ctx* ctx, int comp, int i, int j, int k, int mode, int* id_out) {
+  if (!ctx || comp < 0 || comp > 5 || (mode != DTMX_PROBE_NODE && mode != DTMX_PROBE_REFERENCE)) return fail(ctx, DTMX_ERR_INVALID, "bad probe");
+  if (i < 0 || i >= ctx->cfg.nx || j < 0 || j >= ctx->cfg.ny || k < 0 || k >= ctx->cfg.nz) return fail(ctx, DTMX_ERR_INVALID, "probe outside the grid");
+  if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "probes must be added before the first step");
+  ProbeDev p{comp, i, j, k, mode};
+  ctx->probes.push_back(p);
+  if (id_out) *id_out = (int)ctx->probes.size() - 1;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_read_probes(dtmx_ctx* ctx, float* out, int max_samples, int* nsamples) {
+  if (!ctx || !out || max_samples < 0) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
+  const int every = ctx->cfg.probe_every > 0 ? ctx->cfg.probe_every : 1;
+  const long long have = std::min<long long>(ctx->step / every, ctx->probe_cap);
+  const int ns = (int)std::min<long long>(have, max_samples);
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ns > 0 && !ctx->probes.empty())
+    CK(cudaMemcpy2D(out, (size_t)max_samples * 4, ctx->d_traces, (size_t)ctx->probe_cap * 4, (size_t)ns * 4,
+                    ctx->probes.size(), cudaMemcpyDeviceToHost));
+  if (nsamples) *nsamples = ns;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_add_dft_plane(dtmx_ctx* ctx, int axis, int index, int comp_mask, int nfreq, const double* omegas, int* id_out) {
+  if (!ctx || axis < 0 || axis > 2 || nfreq < 1 || nfreq > 64 || !omegas || (comp_mask & ~63) || !comp_mask)
+    return fail(ctx, DTMX_ERR_INVALID, "bad DFT plane");
+  const int n[3] = {ctx->cfg.nx, ctx->cfg.ny, ctx->cfg.nz};
+  if (index < 0 || index >= n[axis]) return fail(ctx, DTMX_ERR_INVALID, "DFT plane index out of range");
+  if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "DFT planes must be added before the first step");
+  DftHost h;
+  h.d.axis = axis; h.d.index = index; h.d.comp_mask = comp_mask; h.d.nfreq = nfreq;
+  h.d.n1 = n[axis == 0 ? 1 : 0];
+  h.d.n2 = n[axis == 2 ? 1 : 2];
+  h.ncomp = __builtin_popcount(comp_mask);
+  const size_t nacc = (size_t)h.ncomp * nfreq * h.d.n1 * h.d.n2;
+  if (cudaMalloc(&h.omega, nfreq * sizeof(double)) != cudaSuccess) return fail(ctx, DTMX_ERR_OOM, "DFT allocation");
+  if (cudaMalloc(&h.acc, nacc * sizeof(double2)) != cudaSuccess) { cudaFree(h.omega); return fail(ctx, DTMX_ERR_OOM, "DFT allocation"); }
+  CK(cudaMemsetAsync(h.acc, 0, nacc * sizeof(double2), ctx->stream));
+  CK(cudaMemcpyAsync(h.omega, omegas, nfreq * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  h.d.omega = h.omega; h.d.acc = h.acc;
+  ctx->dfts.push_back(h);
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (id_out) *id_out = (int)ctx->dfts.size() - 1;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_read_dft(dtmx_ctx* ctx, int id, double* out, size_t out_len) {
+  if (!ctx || id < 0 || id >= (int)ctx->dfts.size() || !out) return fail(ctx, DTMX_ERR_INVALID, "bad DFT id");
+  const DftHost& h = ctx->dfts[id];
+  const size_t n = (size_t)h.ncomp * h.d.nfreq * h.d.n1 * h.d.n2 * 2;
+  if (out_len < n) return fail(ctx, DTMX_ERR_INVALID, "output buffer too small");
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(out, h.acc, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return DTMX_OK;
+}
+
+// ---------------------------------------------------------------- stepping
+static int xchunk_for(const dtmx_ctx* ctx) {
+  const dtmx_config& c = ctx->cfg;
+  const long long tiles = (long long)((c.nz + TZ - 1) / TZ) * ((c.ny + TY - 1) / TY);
+  const long long target = 148LL * 8 * 3;   // about three waves of 8 CTAs per SM
+  long long chunks = std::max<long long>(1, (target + tiles - 1) / tiles);
+  long long xc = (c.nx + chunks - 1) / chunks;
+  return (int)std::max<long long>(4, xc);
+}
+
+static int launch_step(dtmx_ctx* ctx) {
+  const dtmx_config& c = ctx->cfg;
+  Params P = ctx->P;
+  P.x0 = 0; P.x1 = c.nx;
+  P.xchunk = xchunk_for(ctx);
+  const dim3 blk(TZ, TY);
+  const dim3 grd((c.nz + TZ - 1) / TZ, (c.ny + TY - 1) / TY, (c.nx + P.xchunk - 1) / P.xchunk);
+  const bool o4 = c.order == 4;
+  cudaStream_t st = ctx->stream;
+  const bool pw = ctx->has_tfsf && ctx->tfsf.kind == DTMX_TFSF_PLANE_X;
+  long long nl = 0;
+  if (ctx->profiling) cudaEventRecord(ctx->ev[0], st);
+  if (o4) h_kernel<4><<<grd, blk, 0, st>>>(P); else h_kernel<2><<<grd, blk, 0, st>>>(P);
+  if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
+  nl++;
+  dim3 tgrid;
+  if (ctx->has_tfsf) {
+    long long mx = 0;
+    for (int r = 0; r < ctx->T.nreg; r++) mx = std::max(mx, ctx->T.reg_cells[r]);
+    tgrid = dim3((unsigned)((mx + 255) / 256), ctx->T.nreg);
+    if (o4) tfsf_kernel<4><<<tgrid, 256, 0, st>>>(P, ctx->T, ctx->d_step, 1);
+    else tfsf_kernel<2><<<tgrid, 256, 0, st>>>(P, ctx->T, ctx->d_step, 1);
+    nl++;
+  }
+  const double r1 = c.dt / c.dx;
+  if (pw) {
+    if (o4) line_h_kernel<4><<<8, 256, 0, st>>>(ctx->line_e, ctx->line_h, ctx->T.line_n, r1);
+    else line_h_kernel<2><<<8, 256, 0, st>>>(ctx->line_e, ctx->line_h, ctx->T.line_n, r1);
+    nl++;
+  }
+  if (ctx->profiling) cudaEventRecord(ctx->ev[2], st);
+  if (o4) e_kernel<4><<<grd, blk, 0, st>>>(P); else e_kernel<2><<<grd, blk, 0, st>>>(P);
+  if (ctx->profiling) {
+    cudaEventRecord(ctx->ev[3], st);
+    // read back this step's two kernel durations (keeps the events reusable)
+    cudaEventSynchronize(ctx->ev[3]);
+    float a = 0, b = 0;
+    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&b, ctx->ev[2], ctx->ev[3]);
+    ctx->prof_ms_h += a; ctx->prof_ms_e += b; ctx->prof_count++;
+  }
+  nl++;
+  if (!ctx->psrc.empty()) {
+    point_source_kernel<<<((int)ctx->psrc.size() + 63) / 64, 64, 0, st>>>(P, ctx->d_psrc, (int)ctx->psrc.size(), ctx->d_step, c.dt);
+    nl++;
+  }
+  if (ctx->has_tfsf) {
+    if (o4) tfsf_kernel<4><<<tgrid, 256, 0, st>>>(P, ctx->T, ctx->d_step, 0);
+    else tfsf_kernel<2><<<tgrid, 256, 0, st>>>(P, ctx->T, ctx->d_step, 0);
+    nl++;
+  }
+  if (pw) {
+    const dtmx_tfsf& s = ctx->tfsf;
+    if (o4) line_e_kernel<4><<<8, 256, 0, st>>>(ctx->line_e, ctx->line_h, ctx->T.line_n, r1, ctx->line_src, ctx->d_step, c.dt, s.amp, s.f0, s.tau, s.t0);
+    else line_e_kernel<2><<<8, 256, 0, st>>>(ctx->line_e, ctx->line_h, ctx->T.line_n, r1, ctx->line_src, ctx->d_step, c.dt, s.amp, s.f0, s.tau, s.t0);
+    nl++;
+  }
+  if (!ctx->probes.empty()) {
+    const int every = c.probe_every > 0 ? c.probe_every : 1;
+    probe_kernel<<<((int)ctx->probes.size() + 127) / 128, 128, 0, st>>>(P, ctx->d_probes, (int)ctx->probes.size(), ctx->d_traces,
+                                                                       ctx->probe_cap, ctx->d_step, every);
+    nl++;
+  }
+  for (auto& d : ctx->dfts) {
+    const long long npts = (long long)d.d.n1 * d.d.n2;
+    dft_kernel<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(P, d.d, ctx->d_step, c.dt);
+    nl++;
+  }
+  advance_step_kernel<<<1, 1, 0, st>>>(ctx->d_step);
+  nl++;
+  ctx->launches += nl;
+  return DTMX_OK;
+}
+
+// First-step preparation: upload the source and probe lists, allocate the
+// probe traces and check the TF/SF shell against the materials.
+static int prepare(dtmx_ctx* ctx) {
+  if (ctx->prepared) return DTMX_OK;
+  int rc;
+  if (!ctx->psrc.empty()) {
+    if ((rc = dalloc(ctx, &ctx->d_psrc, ctx->psrc.size()))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_psrc, ctx->psrc.data(), ctx->psrc.size() * sizeof(PointSrcDev), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (!ctx->probes.empty()) {
+    if ((rc = dalloc(ctx, &ctx->d_probes, ctx->probes.size()))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_probes, ctx->probes.data(), ctx->probes.size() * sizeof(ProbeDev), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = dalloc(ctx, &ctx->d_traces, ctx->probes.size() * (size_t)ctx->probe_cap))) return rc;
+  }
+  if (ctx->has_tfsf && ctx->h_mat[0].size()) {
+    const TfsfDev& T = ctx->T;
+    for (int r = 0; r < T.nreg; r++)
+      for (int i = T.reg[r][0][0]; i <= T.reg[r][0][1]; i++)
+        for (int j = T.reg[r][1][0]; j <= T.reg[r][1][1]; j++)
+          for (int k = T.reg[r][2][0]; k <= T.reg[r][2][1]; k++)
+            for (int comp = 0; comp < 3; comp++)
+              if (ctx->mats[ctx->h_mat[comp][store_index(ctx, i, j, k)]].npoles > 0)
+                return fail(ctx, DTMX_ERR_UNSUPPORTED, "dispersive material on the TF/SF surface");
+  }
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->prepared = true;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
+  if (!ctx || nsteps < 0) return fail(ctx, DTMX_ERR_INVALID, "bad step count");
+  int rc0 = prepare(ctx);
+  if (rc0) return rc0;
+  for (int s = 0; s < nsteps; s++) {
+    int rc = launch_step(ctx);
+    if (rc) return rc;
+    ctx->step++;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ctx, DTMX_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_sync(dtmx_ctx* ctx) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_get_step(const dtmx_ctx* ctx, int64_t* n) {
+  if (!ctx || !n) return DTMX_ERR_INVALID;
+  *n = ctx->step;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_get_field(dtmx_ctx* ctx, int comp, float* host_out) {
+  if (!ctx || comp < 0 || comp > 5 || !host_out) return fail(ctx, DTMX_ERR_INVALID, "bad field request");
+  const dtmx_config& c = ctx->cfg;
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy2D(host_out, (size_t)c.nz * 4, ctx->P.f[comp], (size_t)ctx->nzp * 4, (size_t)c.nz * 4,
+                  (size_t)c.nx * c.ny, cudaMemcpyDeviceToHost));
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_set_field(dtmx_ctx* ctx, int comp, const float* host_in) {
+  if (!ctx || comp < 0 || comp > 5 || !host_in) return fail(ctx, DTMX_ERR_INVALID, "bad field request");
+  const dtmx_config& c = ctx->cfg;
+  CK(cudaMemcpy2DAsync(ctx->P.f[comp], (size_t)ctx->nzp * 4, host_in, (size_t)c.nz * 4, (size_t)c.nz * 4,
+                       (size_t)c.nx * c.ny, cudaMemcpyHostToDevice, ctx->stream));
+  // non-live nodes are held at zero
+  mask_nonlive_kernel<<<148 * 4, 256, 0, ctx->stream>>>(ctx->P, comp, (long long)ctx->ncell);
+  ctx->launches++;
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_field_device_ptr(dtmx_ctx* ctx, int comp, void** dptr, int64_t strides[3]) {
+  if (!ctx || comp < 0 || comp > 5 || !dptr) return fail(ctx, DTMX_ERR_INVALID, "bad field request");
+  *dptr = ctx->P.f[comp];
+  if (strides) { strides[0] = ctx->P.g.sx; strides[1] = ctx->P.g.sy; strides[2] = 1; }
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_check_finite(dtmx_ctx* ctx) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
+  for (int comp = 0; comp < 6; comp++) {
+    nonfinite_kernel<<<148 * 4, 256, 0, ctx->stream>>>(ctx->P, comp, (long long)ctx->ncell, ctx->d_flag);
+    ctx->launches++;
+  }
+  int flag = 0;
+  CK(cudaMemcpyAsync(&flag, ctx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return flag ? fail(ctx, DTMX_ERR_NONFINITE, "non-finite field value") : DTMX_OK;
+}
+
+extern "C" int dtmx_kernel_launches(const dtmx_ctx* ctx, int64_t* n) {
+  if (!ctx || !n) return DTMX_ERR_INVALID;
+  *n = ctx->launches;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block) {
+  if (!ctx || engine < 0 || engine > 2 || time_block < 0) return fail(ctx, DTMX_ERR_INVALID, "bad engine");
+  if (engine == 2) return fail(ctx, DTMX_ERR_UNSUPPORTED, "wavefront engine not built");
+  ctx->engine = engine; ctx->tblock = time_block;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_get_stream(dtmx_ctx* ctx, void** stream) {
+  if (!ctx || !stream) return DTMX_ERR_INVALID;
+  *stream = (void*)ctx->stream;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_set_profiling(dtmx_ctx* ctx, int enable) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  if (enable && !ctx->ev[0])
+    for (int q = 0; q < 4; q++) CK(cudaEventCreate(&ctx->ev[q]));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->profiling = enable != 0;
+  ctx->prof_ms_h = ctx->prof_ms_e = 0;
+  ctx->prof_count = 0;
+  ctx->prof_pending = false;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_read_profile(dtmx_ctx* ctx, double* ms_h, double* ms_e, int64_t* count) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (ms_h) *ms_h = ctx->prof_ms_h;
+  if (ms_e) *ms_e = ctx->prof_ms_e;
+  if (count) *count = ctx->prof_count;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_abi_sizes(int64_t out[4]) {
+  if (!out) return DTMX_ERR_INVALID;
+  out[0] = sizeof(dtmx_config); out[1] = sizeof(dtmx_material);
+  out[2] = sizeof(dtmx_point_source); out[3] = sizeof(dtmx_tfsf);
+  return DTMX_OK;
+}

@@ -1,0 +1,292 @@
+// dtmx_aux.cuh -- per-step side kernels: TF/SF surface corrections, the 1-D
+// incident line of the plane-wave source, soft point sources, probes, running
+// DFT and the device step counter.
+#pragma once
+#include "dtmx_device.cuh"
+
+namespace dtmx {
+
+struct TfsfDev {
+  int active_cfg;            // a TF/SF source is configured
+  int kind;                  // 0 dipole, 1 plane +x
+  int lo[3], hi[3];          // inside-box half-coordinate ranges (inclusive)
+  double ctr[3];             // dipole position (box centre, physical)
+  double hd[3];              // half cell sizes dx/2, dy/2, dz/2
+  double dt, c, w, kenv, tstop;
+  int ntime;
+  const double* line_e; const double* line_h; int line_M, line_n;
+  int nreg;
+  int reg[6][3][2];          // disjoint cell regions covering the box surface shell
+  long long reg_cells[6];
+};
+
+__device__ __forceinline__ bool tfsf_on(const TfsfDev& t, long long n) {
+  if (t.tstop <= 0) return true;
+  const long long is = n / t.ntime;
+  return (double)(is + 1) * t.ntime * t.dt < t.tstop;
+}
+
+__device__ __forceinline__ bool in_box(const TfsfDev& t, int X, int Y, int Z) {
+  return X >= t.lo[0] && X <= t.hi[0] && Y >= t.lo[1] && Y <= t.hi[1] && Z >= t.lo[2] && Z <= t.hi[2];
+}
+
+// Field of a z-oriented Hertzian dipole with a Hann-windowed sine moment,
+// reference DipoleTFSF (signal.hpp:51-97), evaluated in double precision.
+__device__ double dipole_field(const TfsfDev& t, int comp, int X, int Y, int Z, double tt) {
+  const double nx = X * t.hd[0] - t.ctr[0], ny = Y * t.hd[1] - t.ctr[1], nz = Z * t.hd[2] - t.ctr[2];
+  const double R = sqrt(nx * nx + ny * ny + nz * nz);
+  const double time = tt * t.dt, c = t.c, w = t.w, ke = t.kenv;
+  const double ph = w * time - w / c * R;
+  double s, co, sk, ck;
+  sincos(ph, &s, &co);
+  sincos(ph * ke, &sk, &ck);
+  double d = s * 0.5 * (1.0 - ck);
+  double ds = w * co * 0.5 - 0.5 * w * co * ck + 0.5 * s * w * ke * sk;
+  double dss = -w * w * s * 0.5 + 0.5 * w * w * s * ck + w * co * w * ke * sk + 0.5 * s * w * ke * w * ke * ck;
+  if (ph * ke < 0.0 || ph * ke > 2.0 * M_PI) { d = 0; ds = 0; dss = 0; }
+  const double u0 = nx / R, u1 = ny / R, u2 = nz / R;
+  if (comp < 3) {
+    // (dss z^ x n) x n  +  3 (ds.n) n - ds  +  3 (d.n) n - d   with moments along z
+    const double a0 = -dss * u1, a1 = dss * u0;
+    const double cr[3] = {a1 * u2, -a0 * u2, a0 * u1 - a1 * u0};
+    const double uu[3] = {u0, u1, u2};
+    const double dz = comp == 2 ? 1.0 : 0.0;
+    return c * (cr[comp] / (c * c * R) + (3.0 * ds * u2 * uu[comp] - ds * dz) / (c * R * R) +
+                (3.0 * d * u2 * uu[comp] - d * dz) / (R * R * R));
+  }
+  const int q = comp - 3;
+  const double b1 = q == 0 ? -dss * u1 : q == 1 ? dss * u0 : 0.0;
+  const double b2 = q == 0 ? -ds * u1 : q == 1 ? ds * u0 : 0.0;
+  return b1 / (c * c * R) + b2 / (c * R * R);
+}
+
+__device__ __forceinline__ double incident(const TfsfDev& t, int g, int X, int Y, int Z, double tt) {
+  if (t.kind == 0) return dipole_field(t, g, X, Y, Z, tt);
+  if (g == 2) { const int m = ((X - 1) >> 1) + t.line_M; return (m >= 0 && m < t.line_n) ? t.line_e[m] : 0.0; }
+  if (g == 4) { const int m = (X >> 1) + t.line_M; return (m >= 0 && m < t.line_n) ? t.line_h[m] : 0.0; }
+  return 0.0;
+}
+
+// curl terms of component c: {axis, source component} for (+) and (-) terms
+__device__ __forceinline__ void curl_terms(int c, int& a0, int& g0, int& a1, int& g1) {
+  switch (c) {
+    case 0: a0 = 1; g0 = 5; a1 = 2; g1 = 4; break;
+    case 1: a0 = 2; g0 = 3; a1 = 0; g1 = 5; break;
+    case 2: a0 = 0; g0 = 4; a1 = 1; g1 = 3; break;
+    case 3: a0 = 1; g0 = 2; a1 = 2; g1 = 1; break;
+    case 4: a0 = 2; g0 = 0; a1 = 0; g1 = 2; break;
+    default: a0 = 0; g0 = 1; a1 = 1; g1 = 0; break;
+  }
+}
+
+// TF/SF correction of one half step (genAlg.py:209-234): a tap that crosses
+// the box surface gets +inc when the updated node is outside and the tap
+// inside, -inc in the opposite case.  The update is linear in the taps, so
+// the correction is added after the bulk update as dt/d * D(corrections).
+template <int ORDER>
+__global__ void tfsf_kernel(Params p, TfsfDev t, const long long* d_step, int isH) {
+  const long long n = *d_step;
+  if (!tfsf_on(t, n)) return;
+  const int r = blockIdx.y;
+  const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (r >= t.nreg || cell >= t.reg_cells[r]) return;
+  const int ex = t.reg[r][0][1] - t.reg[r][0][0] + 1, ey = t.reg[r][1][1] - t.reg[r][1][0] + 1,
+            ez = t.reg[r][2][1] - t.reg[r][2][0] + 1;
+  (void)ex;
+  const int i = t.reg[r][0][0] + (int)(cell / ((long long)ey * ez));
+  const int j = t.reg[r][1][0] + (int)((cell / ez) % ey);
+  const int k = t.reg[r][2][0] + (int)(cell % ez);
+  const double tt = isH ? (double)n : (double)n + 0.5;
+  const int cbeg = isH ? 3 : 0;
+  const int t0 = isH ? -2 : -1;
+  for (int c = cbeg; c < cbeg + 3; c++) {
+    if (!is_live(p.g, c, i, j, k)) continue;
+    const int idx[3] = {i, j, k};
+    const int Xs[3] = {2 * i + comp_off(c, 0), 2 * j + comp_off(c, 1), 2 * k + comp_off(c, 2)};
+    const bool self_in = in_box(t, Xs[0], Xs[1], Xs[2]);
+    int ax[2], gs[2];
+    curl_terms(c, ax[0], gs[0], ax[1], gs[1]);
+    float total = 0.f;
+    bool any = false;
+    for (int term = 0; term < 2; term++) {
+      const int a = ax[term], g = gs[term];
+      float v[4];
+      bool hit = false;
+      for (int q = 0; q < 4; q++) {
+        v[q] = 0.f;
+        if (ORDER == 2 && (q == 0 || q == 3)) continue;
+        int m[3] = {idx[0], idx[1], idx[2]};
+        m[a] += t0 + q;
+        const int TX = 2 * m[0] + comp_off(g, 0), TY_ = 2 * m[1] + comp_off(g, 1), TZ_ = 2 * m[2] + comp_off(g, 2);
+        const bool tin = in_box(t, TX, TY_, TZ_);
+        if (tin != self_in) {
+          const double inc = incident(t, g, TX, TY_, TZ_, tt);
+          v[q] = (float)(self_in ? -inc : inc);
+          hit = true;
+        }
+      }
+      if (!hit) continue;
+      any = true;
+      float sg = term == 0 ? 1.f : -1.f;
+      if (isH) sg = -sg;
+      total += sg * p.cdt[a] * dstencil<ORDER>(v[0], v[1], v[2], v[3]);
+    }
+    if (!any) continue;
+    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+    if (!isH) {
+      const int mi = p.mat[c] ? (int)p.mat[c][id] : 0;
+      total *= p.mt->inv_eps[mi][c];
+    }
+    p.f[c][id] += total;
+  }
+}
+
+// 1-D incident line (Ez at odd X, Hy at even X), same stencil and time step.
+template <int ORDER>
+__global__ void line_h_kernel(double* e, double* h, int n, double r) {
+  for (int m = threadIdx.x + blockIdx.x * blockDim.x; m < n; m += blockDim.x * gridDim.x) {
+    const double e0 = e[m], em1 = m >= 1 ? e[m - 1] : 0.0;
+    double d;
+    if (ORDER == 4) {
+      const double ep1 = m + 1 < n ? e[m + 1] : 0.0, em2 = m >= 2 ? e[m - 2] : 0.0;
+      d = (27.0 * (e0 - em1) - (ep1 - em2)) / 24.0;
+    } else {
+      d = e0 - em1;
+    }
+    h[m] += r * d;
+  }
+}
+template <int ORDER>
+__global__ void line_e_kernel(double* e, const double* h, int n, double r, int src, const long long* d_step,
+                              double dt, double amp, double f0, double tau, double t0) {
+  const double ts = ((double)(*d_step) + 0.5) * dt - t0;
+  for (int m = threadIdx.x + blockIdx.x * blockDim.x; m < n; m += blockDim.x * gridDim.x) {
+    const double h0 = h[m], hp1 = m + 1 < n ? h[m + 1] : 0.0;
+    double d;
+    if (ORDER == 4) {
+      const double hp2 = m + 2 < n ? h[m + 2] : 0.0, hm1 = m >= 1 ? h[m - 1] : 0.0;
+      d = (27.0 * (hp1 - h0) - (hp2 - hm1)) / 24.0;
+    } else {
+      d = hp1 - h0;
+    }
+    double v = e[m] + r * d;
+    if (m == src) v += amp * sin(2.0 * M_PI * f0 * ts) * exp(-(ts / tau) * (ts / tau));
+    e[m] = v;
+  }
+}
+
+struct PointSrcDev {
+  int comp; long long id; double amp, f0, tau, t0;
+};
+
+__global__ void point_source_kernel(Params p, const PointSrcDev* s, int ns, const long long* d_step, double dt) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= ns) return;
+  const double u = ((double)(*d_step) + 0.5) * dt - s[q].t0;
+  const double v = s[q].amp * sin(2.0 * M_PI * s[q].f0 * u) * exp(-(u / s[q].tau) * (u / s[q].tau));
+  p.f[s[q].comp][s[q].id] += (float)v;
+}
+
+struct ProbeDev { int comp, i, j, k, mode; };
+
+__device__ __forceinline__ float probe_get(const Params& p, int c, int i, int j, int k) {
+  if (i < 0 || i >= p.g.n[0] || j < 0 || j >= p.g.n[1] || k < 0 || k >= p.g.n[2]) return 0.f;
+  return p.f[c][(long long)i * p.g.sx + (long long)j * p.g.sy + k];
+}
+
+// Reference Sensor::write averaging (sensor.h:51-83); for Hz the reference's
+// second point is never assigned and reads a zero node outside the domain.
+__global__ void probe_kernel(Params p, const ProbeDev* pr, int np, float* traces, int cap, const long long* d_step,
+                             int every) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long s = *d_step + 1;
+  if (q >= np || (s % every) != 0) return;
+  const long long sample = s / every - 1;
+  if (sample >= cap) return;
+  const ProbeDev d = pr[q];
+  const int c = d.comp, x = d.i, y = d.j, z = d.k;
+  float v;
+  if (d.mode == 0) {
+    v = probe_get(p, c, x, y, z);
+  } else {
+    const int zM = z == 0 ? z + 1 : z - 1;
+    switch (c) {
+      case 0: v = 0.25f * (probe_get(p, c, x, y - 1, zM) + probe_get(p, c, x, y - 1, z) + probe_get(p, c, x, y, zM) + probe_get(p, c, x, y, z)); break;
+      case 1: v = 0.25f * (probe_get(p, c, x - 1, y, zM) + probe_get(p, c, x - 1, y, z) + probe_get(p, c, x, y, zM) + probe_get(p, c, x, y, z)); break;
+      case 2: v = 0.25f * (probe_get(p, c, x - 1, y - 1, z) + probe_get(p, c, x - 1, y, z) + probe_get(p, c, x, y - 1, z) + probe_get(p, c, x, y, z)); break;
+      case 3: v = 0.5f * (probe_get(p, c, x - 1, y, z) + probe_get(p, c, x, y, z)); break;
+      case 4: v = 0.5f * (probe_get(p, c, x, y - 1, z) + probe_get(p, c, x, y, z)); break;
+      default: v = 0.5f * probe_get(p, c, x, y, zM); break;
+    }
+  }
+  traces[(long long)q * cap + sample] = v;
+}
+
+struct DftDev {
+  int axis, index, comp_mask, nfreq, n1, n2;
+  const double* omega;
+  double2* acc;             // [ncomp][nfreq][n1*n2]
+};
+
+// Running DFT with FP64 accumulators: acc += f(t) exp(-i w t) dt, t = s*dt for E,
+// (s-1/2)*dt for H, s = steps completed.
+__global__ void dft_kernel(Params p, DftDev d, const long long* d_step, double dt) {
+  __shared__ double2 phE[64], phH[64];
+  const long long s = *d_step + 1;
+  for (int f = threadIdx.x; f < d.nfreq; f += blockDim.x) {
+    double sn, cs;
+    sincos(d.omega[f] * (double)s * dt, &sn, &cs);
+    phE[f] = make_double2(cs * dt, -sn * dt);
+    sincos(d.omega[f] * ((double)s - 0.5) * dt, &sn, &cs);
+    phH[f] = make_double2(cs * dt, -sn * dt);
+  }
+  __syncthreads();
+  const long long npts = (long long)d.n1 * d.n2;
+  const long long pt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (pt >= npts) return;
+  const int u = (int)(pt / d.n2), v = (int)(pt % d.n2);
+  int i, j, k;
+  if (d.axis == 0) { i = d.index; j = u; k = v; }
+  else if (d.axis == 1) { i = u; j = d.index; k = v; }
+  else { i = u; j = v; k = d.index; }
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+  int ci = 0;
+  for (int c = 0; c < 6; c++) {
+    if (!(d.comp_mask & (1 << c))) continue;
+    const double val = p.f[c][id];
+    const double2* ph = c < 3 ? phE : phH;
+    double2* acc = d.acc + (long long)ci * d.nfreq * npts + pt;
+    for (int f = 0; f < d.nfreq; f++) {
+      double2 a = acc[(long long)f * npts];
+      a.x += val * ph[f].x;
+      a.y += val * ph[f].y;
+      acc[(long long)f * npts] = a;
+    }
+    ci++;
+  }
+}
+
+__global__ void mask_nonlive_kernel(Params p, int comp, long long ncell) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(q % p.g.n[2]);
+    const long long r = q / p.g.n[2];
+    const int j = (int)(r % p.g.n[1]);
+    const int i = (int)(r / p.g.n[1]);
+    if (!is_live(p.g, comp, i, j, k)) p.f[comp][(long long)i * p.g.sx + (long long)j * p.g.sy + k] = 0.f;
+  }
+}
+
+__global__ void advance_step_kernel(long long* d_step) { *d_step += 1; }
+
+__global__ void nonfinite_kernel(Params p, int comp, long long ncell, int* flag) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(q % p.g.n[2]);
+    const long long r = q / p.g.n[2];
+    const int j = (int)(r % p.g.n[1]);
+    const int i = (int)(r / p.g.n[1]);
+    const float v = p.f[comp][(long long)i * p.g.sx + (long long)j * p.g.sy + k];
+    if (!isfinite(v)) { atomicExch(flag, 1); return; }
+  }
+}
+
+}  // namespace dtmx

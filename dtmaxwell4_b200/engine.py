@@ -1,0 +1,225 @@
+"""Python host API over the CUDA engine's C ABI (libdtmx.so, include/dtmx.h).
+
+There is no CPU fallback: if the shared library or a CUDA device is missing,
+constructing a Simulation raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdtmx.so")
+_lib = None
+
+# every symbol declared in include/dtmx.h
+EXPORTS = (
+    "dtmx_version", "dtmx_error_string", "dtmx_create", "dtmx_destroy", "dtmx_last_error",
+    "dtmx_set_materials", "dtmx_add_point_source", "dtmx_set_tfsf", "dtmx_add_probe",
+    "dtmx_read_probes", "dtmx_add_dft_plane", "dtmx_read_dft", "dtmx_step", "dtmx_sync",
+    "dtmx_get_step", "dtmx_get_field", "dtmx_set_field", "dtmx_field_device_ptr",
+    "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_get_stream",
+    "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes",
+)
+
+
+class DtmxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("dtmx error %d (%s): %s" % (code, _errstr(code), msg))
+        self.code = code
+
+
+def load():
+    """Load libdtmx.so (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError("libdtmx.so not built: run `python -m dtmaxwell4_b200.build` (%s)" % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    vp, ip = C.c_void_p, C.c_int
+    L.dtmx_version.restype = ip
+    L.dtmx_error_string.restype = C.c_char_p
+    L.dtmx_error_string.argtypes = [ip]
+    L.dtmx_create.argtypes = [C.POINTER(abi.Config), C.POINTER(vp)]
+    L.dtmx_destroy.argtypes = [vp]
+    L.dtmx_destroy.restype = None
+    L.dtmx_last_error.argtypes = [vp]
+    L.dtmx_last_error.restype = C.c_char_p
+    L.dtmx_set_materials.argtypes = [vp, C.POINTER(abi.Material), ip, vp, vp, vp]
+    L.dtmx_add_point_source.argtypes = [vp, C.POINTER(abi.PointSource)]
+    L.dtmx_set_tfsf.argtypes = [vp, C.POINTER(abi.TFSF)]
+    L.dtmx_add_probe.argtypes = [vp, ip, ip, ip, ip, ip, C.POINTER(ip)]
+    L.dtmx_read_probes.argtypes = [vp, vp, ip, C.POINTER(ip)]
+    L.dtmx_add_dft_plane.argtypes = [vp, ip, ip, ip, ip, vp, C.POINTER(ip)]
+    L.dtmx_read_dft.argtypes = [vp, ip, vp, C.c_size_t]
+    L.dtmx_step.argtypes = [vp, ip]
+    L.dtmx_sync.argtypes = [vp]
+    L.dtmx_get_step.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.dtmx_get_field.argtypes = [vp, ip, vp]
+    L.dtmx_set_field.argtypes = [vp, ip, vp]
+    L.dtmx_field_device_ptr.argtypes = [vp, ip, C.POINTER(vp), C.POINTER(C.c_int64)]
+    L.dtmx_check_finite.argtypes = [vp]
+    L.dtmx_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.dtmx_set_engine.argtypes = [vp, ip, ip]
+    L.dtmx_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.dtmx_set_profiling.argtypes = [vp, ip]
+    L.dtmx_read_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    L.dtmx_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
+    _lib = L
+    return L
+
+
+def _errstr(code):
+    try:
+        return load().dtmx_error_string(code).decode()
+    except OSError:
+        return "?"
+
+
+class Simulation:
+    """One FDTD simulation context on the current CUDA device."""
+
+    def __init__(self, cfg):
+        self._L = load()
+        self.cfg = cfg
+        h = C.c_void_p()
+        rc = self._L.dtmx_create(C.byref(cfg), C.byref(h))
+        if rc != abi.OK:
+            msg = self._L.dtmx_last_error(h).decode() if h.value else ""
+            if h.value:
+                self._L.dtmx_destroy(h)
+            raise DtmxError(rc, msg or "dtmx_create rejected the configuration")
+        self._h = h
+        self.shape = (cfg.nx, cfg.ny, cfg.nz)
+        self._dft = []
+        self._nprobes = 0
+
+    def _ck(self, rc):
+        if rc != abi.OK:
+            raise DtmxError(rc, self._L.dtmx_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self._L.dtmx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- set-up
+    def set_materials(self, table, idx_x, idx_y=None, idx_z=None):
+        arr = (abi.Material * len(table))(*table)
+        keep = [np.ascontiguousarray(a, dtype=np.uint8).reshape(-1) if a is not None else None for a in (idx_x, idx_y, idx_z)]
+        for a in keep:
+            if a is not None and a.size != self.cfg.nx * self.cfg.ny * self.cfg.nz:
+                raise ValueError("material index array has the wrong size")
+        ptrs = [a.ctypes.data if a is not None else None for a in keep]
+        self._ck(self._L.dtmx_set_materials(self._h, arr, len(table), *ptrs))
+
+    def add_point_source(self, src):
+        self._ck(self._L.dtmx_add_point_source(self._h, C.byref(src)))
+
+    def set_tfsf(self, t):
+        self._ck(self._L.dtmx_set_tfsf(self._h, C.byref(t)))
+
+    def add_probe(self, comp, i, j, k, mode=abi.PROBE_NODE):
+        pid = C.c_int(-1)
+        self._ck(self._L.dtmx_add_probe(self._h, comp, i, j, k, mode, C.byref(pid)))
+        self._nprobes += 1
+        return pid.value
+
+    def add_dft_plane(self, axis, index, comp_mask, omegas):
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        did = C.c_int(-1)
+        self._ck(self._L.dtmx_add_dft_plane(self._h, axis, index, comp_mask, len(om), om.ctypes.data, C.byref(did)))
+        n = list(self.shape)
+        del n[axis]
+        self._dft.append((bin(comp_mask).count("1"), len(om), n[0], n[1]))
+        return did.value
+
+    def set_engine(self, engine, time_block=0):
+        self._ck(self._L.dtmx_set_engine(self._h, engine, time_block))
+
+    # ---- run
+    def step(self, n):
+        self._ck(self._L.dtmx_step(self._h, int(n)))
+
+    def sync(self):
+        self._ck(self._L.dtmx_sync(self._h))
+
+    @property
+    def nstep(self):
+        v = C.c_int64()
+        self._ck(self._L.dtmx_get_step(self._h, C.byref(v)))
+        return v.value
+
+    def launches(self):
+        v = C.c_int64()
+        self._ck(self._L.dtmx_kernel_launches(self._h, C.byref(v)))
+        return v.value
+
+    def check_finite(self):
+        rc = self._L.dtmx_check_finite(self._h)
+        if rc == abi.ERR_NONFINITE:
+            return False
+        self._ck(rc)
+        return True
+
+    # ---- data
+    def get_field(self, comp, out=None):
+        if out is None:
+            out = np.empty(self.shape, dtype=np.float32)
+        assert out.dtype == np.float32 and out.flags.c_contiguous and out.shape == self.shape
+        self._ck(self._L.dtmx_get_field(self._h, comp, out.ctypes.data))
+        return out
+
+    def set_field(self, comp, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float32)
+        assert a.shape == self.shape
+        self._ck(self._L.dtmx_set_field(self._h, comp, a.ctypes.data))
+
+    def read_probes(self, max_samples=None):
+        if max_samples is None:
+            max_samples = max(1, self.cfg.probe_capacity or 4096)
+        out = np.zeros((max(self._nprobes, 1), max_samples), dtype=np.float32)
+        ns = C.c_int(0)
+        self._ck(self._L.dtmx_read_probes(self._h, out.ctypes.data, max_samples, C.byref(ns)))
+        return out[: self._nprobes, : ns.value]
+
+    def read_dft(self, did):
+        ncomp, nf, n1, n2 = self._dft[did]
+        out = np.zeros((ncomp, nf, n1, n2, 2), dtype=np.float64)
+        self._ck(self._L.dtmx_read_dft(self._h, did, out.ctypes.data, out.size))
+        return out[..., 0] + 1j * out[..., 1]
+
+    def stream_handle(self):
+        """cudaStream_t of the context (for torch.cuda.ExternalStream)."""
+        v = C.c_void_p()
+        self._ck(self._L.dtmx_get_stream(self._h, C.byref(v)))
+        return v.value
+
+    def set_profiling(self, on=True):
+        self._ck(self._L.dtmx_set_profiling(self._h, 1 if on else 0))
+
+    def read_profile(self):
+        a, b, n = C.c_double(), C.c_double(), C.c_int64()
+        self._ck(self._L.dtmx_read_profile(self._h, C.byref(a), C.byref(b), C.byref(n)))
+        return a.value, b.value, n.value
+
+
+def abi_sizes():
+    out = (C.c_int64 * 4)()
+    load().dtmx_abi_sizes(out)
+    return tuple(out)

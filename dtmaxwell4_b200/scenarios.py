@@ -1,0 +1,122 @@
+"""Scenario builders: a scenario is a plain dict (config, materials, sources,
+probes, DFT planes) applied to any object with the Simulation call surface.
+
+Workloads (all in c = 1 units with dx = 1 cell unless stated):
+
+* point_dipole_sphere -- vacuum box, centred dielectric sphere, soft Ez point
+  source with a Gaussian-modulated sine, CPML on all faces, Ez/Hx traces at
+  seeded random probe points (128^3, lambda0 = 20 cells, Courant 0.5, 10-cell
+  CPML, sphere r = 20 cells eps = 4, 1000 steps at full size).
+* drude_sphere_tfsf -- Drude sphere (eps_inf = 1, wp = 2 pi c/(8 dx),
+  gamma = wp/50) lit by a +x, Ez-polarised Gaussian-pulse plane wave through a
+  TF/SF box inset 20 cells from a 12-cell CPML; running DFT at 16 frequencies
+  over the pulse's -20 dB band on one x-normal plane (384^3, 4000 steps at
+  full size).
+"""
+import math
+
+import numpy as np
+
+from . import abi
+
+
+def gauss_sine_params(lambda0_cells, dx=1.0, periods=3.0):
+    """f0 = c/lambda0; amplitude-envelope FWHM = periods*T0, so
+    tau = periods*T0/(2 sqrt(ln 2)); t0 = 4 tau."""
+    f0 = 1.0 / (lambda0_cells * dx)
+    T0 = 1.0 / f0
+    tau = periods * T0 / (2.0 * math.sqrt(math.log(2.0)))
+    return f0, tau, 4.0 * tau
+
+
+def sphere_mask(n, center, radius, comp):
+    """Boolean mask of the nodes of E component comp inside a sphere (cells)."""
+    nx, ny, nz = n
+    off = [(0, 1, 1), (1, 0, 1), (1, 1, 0)][comp]
+    x = (np.arange(nx) + 0.5 * off[0])[:, None, None]
+    y = (np.arange(ny) + 0.5 * off[1])[None, :, None]
+    z = (np.arange(nz) + 0.5 * off[2])[None, None, :]
+    return (x - center[0]) ** 2 + (y - center[1]) ** 2 + (z - center[2]) ** 2 <= radius ** 2
+
+
+def point_dipole_sphere(n=128, steps=1000, pml=10, radius=None, eps=4.0, order=2, courant=0.5, nprobes=8,
+                        lambda0=20.0, seed=0):
+    nx = ny = nz = n if isinstance(n, int) else None
+    if not isinstance(n, int):
+        nx, ny, nz = n
+    radius = radius if radius is not None else 20.0 * min(nx, ny, nz) / 128.0
+    cfg = abi.make_config(nx, ny, nz, dx=1.0, courant=courant, order=order, pml=pml, probe_capacity=steps + 8)
+    ctr = (nx / 2.0, ny / 2.0, nz / 2.0)
+    idx = [sphere_mask((nx, ny, nz), ctr, radius, c).astype(np.uint8) for c in range(3)]
+    mats = [abi.make_material(1.0), abi.make_material(eps)]
+    f0, tau, t0 = gauss_sine_params(lambda0)
+    src = abi.PointSource(comp=abi.EZ, i=nx // 2, j=ny // 2, k=nz // 2, waveform=abi.WAVE_GAUSS_SINE,
+                          amp=1.0, f0=f0, tau=tau, t0=t0)
+    rng = np.random.default_rng(seed)
+    lo, hi = pml + 1, np.array([nx, ny, nz]) - pml - 2
+    pts = rng.integers(lo, hi + 1, size=(nprobes, 3))
+    probes = []
+    for p in pts:
+        probes.append((abi.EZ, int(p[0]), int(p[1]), int(p[2]), abi.PROBE_NODE))
+        probes.append((abi.HX, int(p[0]), int(p[1]), int(p[2]), abi.PROBE_NODE))
+    return dict(name="point_dipole_sphere", cfg=cfg, materials=(mats, idx), point_sources=[src], tfsf=None,
+                probes=probes, dft=[], steps=steps,
+                desc="%dx%dx%d, dx=lambda0/%g, Courant %g, order %d, %d-cell CPML, sphere r=%g eps=%g, soft Ez dipole"
+                     % (nx, ny, nz, lambda0, courant, order, pml, radius, eps))
+
+
+def drude_sphere_tfsf(n=384, steps=4000, pml=12, inset=20, radius=None, order=2, courant=0.5, lambda0=20.0,
+                      nfreq=16, dft_plane=None):
+    nx = ny = nz = n if isinstance(n, int) else None
+    if not isinstance(n, int):
+        nx, ny, nz = n
+    radius = radius if radius is not None else 40.0 * min(nx, ny, nz) / 384.0
+    cfg = abi.make_config(nx, ny, nz, dx=1.0, courant=courant, order=order, pml=pml, probe_capacity=steps + 8)
+    ctr = (nx / 2.0, ny / 2.0, nz / 2.0)
+    wp = 2.0 * math.pi / 8.0          # 2 pi c / (8 dx)
+    gamma = wp / 50.0
+    # reference LorenzDisp::setDrude(Deps, wp, gp, gp_): b1 = 2 gp = gamma
+    drude = abi.make_material(1.0, poles=[(abi.POLE_DRUDE, 1.0, wp, gamma / 2.0, 0.0)], eps_inf=1.0)
+    mats = [abi.make_material(1.0), drude]
+    idx = [sphere_mask((nx, ny, nz), ctr, radius, c).astype(np.uint8) for c in range(3)]
+    f0, tau, t0 = gauss_sine_params(lambda0)
+    t = abi.TFSF()
+    t.kind = abi.TFSF_PLANE_X
+    for a, m in enumerate((nx, ny, nz)):
+        t.box_lo[a] = float(pml + inset)
+        t.box_hi[a] = float(m - pml - inset)
+    t.amp, t.f0, t.tau, t.t0 = 1.0, f0, tau, t0
+    t.tstop = 0.0
+    t.ntime = 1
+    # -20 dB band of the Gaussian envelope exp(-(t/tau)^2): |f-f0| <= sqrt(ln 10)/(pi tau)
+    df = math.sqrt(math.log(10.0)) / (math.pi * tau)
+    freqs = np.linspace(f0 - df, f0 + df, nfreq)
+    omegas = 2.0 * math.pi * freqs
+    xplane = dft_plane if dft_plane is not None else nx - pml - inset // 2
+    dft = [(0, xplane, (1 << abi.EY) | (1 << abi.EZ) | (1 << abi.HY) | (1 << abi.HZ), omegas)]
+    c = (nx // 2, ny // 2, nz // 2)
+    probes = [(abi.EZ, c[0] + int(radius) + 4, c[1], c[2], abi.PROBE_NODE),
+              (abi.EZ, pml + inset // 2, c[1], c[2], abi.PROBE_NODE),
+              (abi.HY, c[0], c[1], c[2], abi.PROBE_NODE)]
+    return dict(name="drude_sphere_tfsf", cfg=cfg, materials=(mats, idx), point_sources=[], tfsf=t, probes=probes,
+                dft=dft, steps=steps,
+                desc="%dx%dx%d Drude sphere r=%g (wp=2pi/8, gamma=wp/50), TF/SF +x Ez plane wave lambda0=%g, "
+                     "%d-cell CPML, box inset %d, %d-freq DFT plane x=%d" % (nx, ny, nz, radius, lambda0, pml,
+                                                                             inset, nfreq, xplane))
+
+
+def apply(sim, sc):
+    """Apply a scenario dict to a Simulation (or any object with its surface)."""
+    mats, idx = sc["materials"]
+    if mats is not None:
+        sim.set_materials(mats, idx[0], idx[1], idx[2])
+    for s in sc["point_sources"]:
+        sim.add_point_source(s)
+    if sc["tfsf"] is not None:
+        sim.set_tfsf(sc["tfsf"])
+    for (c, i, j, k, m) in sc["probes"]:
+        sim.add_probe(c, i, j, k, m)
+    ids = []
+    for (axis, index, mask, om) in sc["dft"]:
+        ids.append(sim.add_dft_plane(axis, index, mask, om))
+    return ids

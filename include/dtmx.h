@@ -1,0 +1,238 @@
+/*
+ * dtmx.h -- C ABI of the B200-native DiamondTorre-style FDTD engine.
+ *
+ * Plain C, plain pointers and sizes; no exceptions cross this boundary and
+ * every entry point returns a status code (DTMX_OK or DTMX_ERR_*), where the
+ * reference printed a message and called exit() (params.h:130-136,
+ * DTmxw.cu:281-336).
+ *
+ * Units follow the reference: c = 1 (eps0 = mu0 = 1); E is advanced by
+ * curl(H)*dt/eps and H by -curl(E)*dt (defs.h:11-13, genAlg.py:182-301).
+ *
+ * Lattice.  Cell (i,j,k) of an nx*ny*nz grid carries six nodes whose
+ * coordinates in half-cell units (X,Y,Z) are
+ *     Ex (2i, 2j+1, 2k+1)   Ey (2i+1, 2j, 2k+1)   Ez (2i+1, 2j+1, 2k)
+ *     Hx (2i+1, 2j, 2k)     Hy (2i, 2j+1, 2k)     Hz (2i, 2j, 2k+1)
+ * which is the reference's V (=E, two odd coordinates) / T (=H, one odd
+ * coordinate) lattice (genAlg.py:24, DTmxw.cu:77-83).  Host arrays exchanged
+ * through this ABI are dense nx*ny*nz float arrays, z fastest (index
+ * (i*ny + j)*nz + k).
+ *
+ * Threading: one context per host thread; calls on one context must be
+ * serialised by the caller.  Kernels run asynchronously on the context's
+ * own CUDA stream; read-back calls synchronise that stream.
+ */
+#ifndef DTMX_H
+#define DTMX_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DTMX_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  DTMX_OK = 0,
+  DTMX_ERR_INVALID = 1,      /* bad argument / configuration (Courant, sizes, ...) */
+  DTMX_ERR_CUDA = 2,         /* CUDA runtime error (message in dtmx_last_error) */
+  DTMX_ERR_OOM = 3,          /* device allocation failed */
+  DTMX_ERR_NONFINITE = 4,    /* NaN/Inf found by dtmx_check_finite */
+  DTMX_ERR_TIMEOUT = 5,      /* a bounded device wait gave up (flag set by a kernel) */
+  DTMX_ERR_STATE = 6,        /* call not valid in the current state */
+  DTMX_ERR_UNSUPPORTED = 7,  /* combination not implemented */
+  DTMX_ERR_NODEVICE = 8      /* no CUDA device visible */
+};
+
+/* ---- field components -------------------------------------------------- */
+enum { DTMX_EX = 0, DTMX_EY = 1, DTMX_EZ = 2, DTMX_HX = 3, DTMX_HY = 4, DTMX_HZ = 5 };
+
+/* ---- geometry / boundary modes ----------------------------------------- */
+enum {
+  /* Plain box: every node of the nx*ny*nz array is updated, the field is
+   * zero outside the array (PEC-like outer wall behind the absorber). */
+  DTMX_GEOM_BOX = 0,
+  /* The reference's domain (window.hpp:126-145, defs.h:39-81, genAlg.py:8-10,
+   * 166-168,199-201): nx = 3*Np, ny = 3*Na, nz = Nv cells; nodes with
+   * X <= 3 or X >= 2*nx-3 are held at zero (isOutS); Y < 0 mirrors Y -> -Y
+   * with H odd and E even (I-kernel free reflection); Y > 2*ny-3 mirrors
+   * evenly about Y = 2*ny-3 (X-kernel); Z mirrors evenly about Z = 0 and
+   * Z = 2*nz-1 (Vrefl). */
+  DTMX_GEOM_REFERENCE = 1
+};
+
+enum {
+  DTMX_ABS_NONE = 0,
+  DTMX_ABS_CPML = 1,       /* convolutional PML (Roden-Gedney), DTMX_GEOM_BOX only */
+  DTMX_ABS_SPLIT_PML = 2   /* Berenger split-field PML with the reference grading
+                              (DTmxw.cu:220-265, genAlg.py:117-148), GEOM_REFERENCE only */
+};
+
+typedef struct dtmx_config {
+  int nx, ny, nz;            /* cells */
+  double dx, dy, dz, dt;     /* grid steps and time step (c = 1) */
+  int order;                 /* 2 (Yee) or 4 (reference (27,-1)/24 stencil, defs.h:3-13) */
+  int geometry;              /* DTMX_GEOM_* */
+  int absorber;              /* DTMX_ABS_* */
+  int pml[3][2];             /* absorber thickness in cells, [axis][lo,hi]; 0 = none on that face */
+  /* CPML grading: sigma = sigma_max*(d/L)^m, kappa = 1+(kappa_max-1)(d/L)^m,
+   * alpha = alpha_max*(1-d/L); sigma_max = cpml_sigma_factor*0.8*(m+1)/d_axis.
+   * Zero values select m=3, factor=1, kappa_max=1, alpha_max=0. */
+  double cpml_m, cpml_sigma_factor, cpml_kappa_max, cpml_alpha_max;
+  /* Split-PML grading: reference TFSFsrc.V_max (signal.hpp:191-199 sets it to c). */
+  double spml_vmax;
+  /* Probe samples are recorded after every probe_every-th step (reference:
+   * once per calcStep of Ntime steps, diamond.cu:473-475).  0 = every step. */
+  int probe_every;
+  /* Capacity of the probe trace buffer in samples per probe (0 = 4096). */
+  int probe_capacity;
+  int reserved[8];
+} dtmx_config;
+
+/* ---- materials ----------------------------------------------------------- */
+enum { DTMX_POLE_LORENTZ = 0, DTMX_POLE_DRUDE = 1 };
+#define DTMX_MAX_POLES 2
+#define DTMX_MAX_MATERIALS 64
+
+typedef struct dtmx_material {
+  /* Non-dispersive part: E update coefficient 1/eps per axis (CoffStruct
+   * depsXX/YY/ZZ, defs.h:88-118). */
+  double eps[3];
+  /* Dispersive part (DispStruct::set, dispersion.cpp:41-82): active when
+   * npoles > 0; then eps_inf and sigma are used and eps[] is ignored in the
+   * cell, as the reference's ISDISP branch bypasses coffV (genAlg.py:258,319). */
+  int npoles;
+  int pole_kind[DTMX_MAX_POLES];        /* DTMX_POLE_LORENTZ / DTMX_POLE_DRUDE */
+  double pole[DTMX_MAX_POLES][4];       /* Deps, wp, gp, gp_ (LorenzDisp::set/setDrude) */
+  double eps_inf;
+  double sigma;
+  /* Gyrotropic magnetised-Drude current (no reference counterpart: the
+   * reference's Gyration() is disabled, genAlg.py:303-304): plasma frequency,
+   * collision rate and cyclotron frequency (bias along +z).  Active when
+   * gyro_wp != 0; mutually exclusive with npoles > 0. */
+  double gyro_wp, gyro_gamma, gyro_wc;
+  double reserved[4];
+} dtmx_material;
+
+/* ---- sources --------------------------------------------------------------- */
+enum {
+  DTMX_WAVE_GAUSS_SINE = 0   /* amp*sin(2*pi*f0*(t-t0))*exp(-((t-t0)/tau)^2) */
+};
+
+typedef struct dtmx_point_source {
+  int comp;                  /* DTMX_EX..DTMX_EZ: soft source added to that E node */
+  int i, j, k;
+  int waveform;
+  double amp, f0, tau, t0;
+} dtmx_point_source;
+
+enum {
+  DTMX_TFSF_DIPOLE = 0,      /* analytic z-dipole field, reference DipoleTFSF (signal.hpp:51-97) */
+  DTMX_TFSF_PLANE_X = 1      /* +x propagating, Ez-polarised plane wave from a 1-D auxiliary grid */
+};
+
+typedef struct dtmx_tfsf {
+  int kind;
+  /* Total-field box in physical units (reference TFSFsrc Box{M,P}{s,a,v});
+   * a node is inside when strictly between both faces on every axis, with
+   * the reference's single-precision position arithmetic (inSF, signal.hpp:153-160). */
+  double box_lo[3], box_hi[3];
+  /* Dipole parameters (TFSFsrc::set, signal.hpp:99-115): */
+  double c, w, kenv;
+  /* Corrections are applied while (floor(n/ntime)+1)*ntime*dt < tstop
+   * (window.hpp:125-132); tstop <= 0 means always. ntime 0 means 1. */
+  double tstop;
+  int ntime;
+  /* Plane wave (kind DTMX_TFSF_PLANE_X): Ez_inc(x,t) from a 1-D line driven by
+   * amp*sin(2*pi*f0*(t-t0))*exp(-((t-t0)/tau)^2) at the line's left end. */
+  double amp, f0, tau, t0;
+  double reserved[4];
+} dtmx_tfsf;
+
+/* ---- probes ---------------------------------------------------------------- */
+enum {
+  DTMX_PROBE_NODE = 0,       /* the single node of the component at cell (i,j,k) */
+  DTMX_PROBE_REFERENCE = 1   /* reference Sensor averaging: 4 E nodes / 2 H nodes
+                                around cell point (x,y,z) (sensor.h:51-83) */
+};
+
+/* ---- context --------------------------------------------------------------- */
+typedef struct dtmx_ctx dtmx_ctx;
+
+int  dtmx_version(void);
+const char* dtmx_error_string(int code);
+
+/* Validate cfg and allocate device state on the current CUDA device.
+ * Replaces GeoParamsHost::set + init_index (DTmxw.cu:278-487, 502-561). */
+int  dtmx_create(const dtmx_config* cfg, dtmx_ctx** out);
+void dtmx_destroy(dtmx_ctx* ctx);
+const char* dtmx_last_error(const dtmx_ctx* ctx);
+
+/* Material table and per-component material index arrays (nx*ny*nz uint8,
+ * z fastest); idx_y/idx_z may be NULL to reuse idx_x.  Replaces
+ * init_material + the coffs/DispCoffs __constant__ tables (DTmxw.cu:604-706). */
+int  dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int nmat,
+                        const uint8_t* idx_x, const uint8_t* idx_y, const uint8_t* idx_z);
+
+int  dtmx_add_point_source(dtmx_ctx* ctx, const dtmx_point_source* src);
+/* One TF/SF source per context (reference __constant__ TFSFsrc src, signal.hpp:11). */
+int  dtmx_set_tfsf(dtmx_ctx* ctx, const dtmx_tfsf* src);
+
+/* Probes (reference Sensor, sensor.h:6-84).  Coordinates are cell indices. */
+int  dtmx_add_probe(dtmx_ctx* ctx, int comp, int i, int j, int k, int mode, int* id_out);
+/* Copies traces into out[probe*max_samples + s]; *nsamples gets the count. */
+int  dtmx_read_probes(dtmx_ctx* ctx, float* out, int max_samples, int* nsamples);
+
+/* Running DFT on the plane {axis = index}; comp_mask bit c selects component c.
+ * FP64 complex accumulators sum f(t_n) * exp(-i*omega*t_n) * dt, with t_n the
+ * component's own time level (E at n*dt, H at (n-1/2)*dt after step n). */
+int  dtmx_add_dft_plane(dtmx_ctx* ctx, int axis, int index, int comp_mask,
+                        int nfreq, const double* omegas, int* id_out);
+/* out: [ncomp_selected][nfreq][plane points][2] doubles, plane points in
+ * (slow, fast) order of the two remaining axes. */
+int  dtmx_read_dft(dtmx_ctx* ctx, int id, double* out, size_t out_len);
+
+/* Advance nsteps leapfrog steps (H half step then E half step each,
+ * genAlg.py:420-501).  Asynchronous on the context stream.  Replaces
+ * calcStep (diamond.cu:335-506), which advanced Ntime steps per call. */
+int  dtmx_step(dtmx_ctx* ctx, int nsteps);
+int  dtmx_sync(dtmx_ctx* ctx);
+int  dtmx_get_step(const dtmx_ctx* ctx, int64_t* n);
+
+/* Field access (host buffers, nx*ny*nz floats, z fastest). */
+int  dtmx_get_field(dtmx_ctx* ctx, int comp, float* host_out);
+int  dtmx_set_field(dtmx_ctx* ctx, int comp, const float* host_in);
+/* Device pointer of a component and its element strides (x, y, z). */
+int  dtmx_field_device_ptr(dtmx_ctx* ctx, int comp, void** dptr, int64_t strides[3]);
+
+/* Host-side NaN/Inf check of the probe traces and a device reduction over E;
+ * returns DTMX_ERR_NONFINITE if any is found. */
+int  dtmx_check_finite(dtmx_ctx* ctx);
+
+/* Number of kernels this context has launched so far. */
+int  dtmx_kernel_launches(const dtmx_ctx* ctx, int64_t* n);
+
+/* The context's CUDA stream (cudaStream_t), for event timing by the caller. */
+int  dtmx_get_stream(dtmx_ctx* ctx, void** stream);
+
+/* Per-kernel device timing: when enabled, CUDA events bracket the H and E
+ * field kernels; dtmx_read_profile returns their summed milliseconds and the
+ * number of timed launches of each since profiling was enabled. */
+int  dtmx_set_profiling(dtmx_ctx* ctx, int enable);
+int  dtmx_read_profile(dtmx_ctx* ctx, double* ms_h, double* ms_e, int64_t* count);
+
+/* sizeof of the ABI structs, in the order config, material, point_source,
+ * tfsf (for binding checks). */
+int  dtmx_abi_sizes(int64_t out[4]);
+
+/* Engine choice for dtmx_step: 0 = auto, 1 = one launch per half step,
+ * 2 = L2-resident wavefront (several time steps per launch). */
+int  dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DTMX_H */

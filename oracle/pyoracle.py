@@ -1,0 +1,130 @@
+"""ctypes binding of the CPU oracle (oracle/fdtd_oracle.c).
+
+Test infrastructure only: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline legs of bench.py.  The product package never imports it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from dtmaxwell4_b200 import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = C.CDLL(_LIB)
+        for pfx in ("orc64_", "orc32_"):
+            g = lambda n: getattr(L, pfx + n)
+            g("create").restype = C.c_void_p
+            g("create").argtypes = [C.POINTER(abi.Config)]
+            g("destroy").argtypes = [C.c_void_p]
+            g("set_materials").argtypes = [C.c_void_p, C.POINTER(abi.Material), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+            g("add_point_source").argtypes = [C.c_void_p, C.POINTER(abi.PointSource)]
+            g("set_tfsf").argtypes = [C.c_void_p, C.POINTER(abi.TFSF)]
+            g("add_probe").argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+            g("add_dft_plane").argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+            g("step").argtypes = [C.c_void_p, C.c_int]
+            g("get_field").argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+            g("set_field").argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+            g("read_probes").argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+            g("read_dft").argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+        _lib = L
+    return _lib
+
+
+class OracleSim:
+    """Same call surface as dtmaxwell4_b200.Simulation, on the CPU oracle."""
+
+    def __init__(self, cfg, precision="f64"):
+        self._p = "orc64_" if precision == "f64" else "orc32_"
+        self._L = lib()
+        self.cfg = cfg
+        self._h = self._f("create")(C.byref(cfg))
+        if not self._h:
+            raise ValueError("oracle rejected the configuration")
+        self.shape = (cfg.nx, cfg.ny, cfg.nz)
+        self._dft = []
+        self._nprobes = 0
+
+    def _f(self, n):
+        return getattr(self._L, self._p + n)
+
+    def close(self):
+        if self._h:
+            self._f("destroy")(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def set_materials(self, table, idx_x, idx_y=None, idx_z=None):
+        arr = (abi.Material * len(table))(*table)
+        keep = [np.ascontiguousarray(a, dtype=np.uint8) if a is not None else None for a in (idx_x, idx_y, idx_z)]
+        ptrs = [a.ctypes.data if a is not None else None for a in keep]
+        rc = self._f("set_materials")(self._h, arr, len(table), *ptrs)
+        if rc:
+            raise ValueError("set_materials rc=%d" % rc)
+
+    def add_point_source(self, src):
+        self._f("add_point_source")(self._h, C.byref(src))
+
+    def set_tfsf(self, t):
+        self._f("set_tfsf")(self._h, C.byref(t))
+
+    def add_probe(self, comp, i, j, k, mode=abi.PROBE_NODE):
+        pid = self._f("add_probe")(self._h, comp, i, j, k, mode)
+        if pid < 0:
+            raise ValueError("add_probe failed")
+        self._nprobes += 1
+        return pid
+
+    def add_dft_plane(self, axis, index, comp_mask, omegas):
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        did = self._f("add_dft_plane")(self._h, axis, index, comp_mask, len(om), om.ctypes.data)
+        n = list(self.shape)
+        del n[axis]
+        ncomp = bin(comp_mask).count("1")
+        self._dft.append((ncomp, len(om), n[0], n[1]))
+        return did
+
+    def step(self, n):
+        self._f("step")(self._h, int(n))
+
+    def get_field(self, comp):
+        out = np.empty(self.shape, dtype=np.float64)
+        self._f("get_field")(self._h, comp, out.ctypes.data)
+        return out
+
+    def set_field(self, comp, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        self._f("set_field")(self._h, comp, a.ctypes.data)
+
+    def read_probes(self, max_samples=100000):
+        out = np.zeros((max(self._nprobes, 1), max_samples), dtype=np.float64)
+        ns = C.c_int(0)
+        self._f("read_probes")(self._h, out.ctypes.data, max_samples, C.byref(ns))
+        return out[: self._nprobes, : ns.value]
+
+    def read_dft(self, did):
+        ncomp, nf, n1, n2 = self._dft[did]
+        out = np.zeros((ncomp, nf, n1, n2, 2), dtype=np.float64)
+        rc = self._f("read_dft")(self._h, did, out.ctypes.data, out.size)
+        if rc:
+            raise ValueError("read_dft rc=%d" % rc)
+        return out[..., 0] + 1j * out[..., 1]
+
+
+def threads():
+    return lib().orc64_threads()

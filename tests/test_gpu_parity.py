@@ -1,0 +1,176 @@
+"""CUDA engine vs the FP64 CPU oracle on the same seeded inputs (small sizes).
+
+Tolerance: relative L2 error of FP32 GPU results against the FP64 oracle
+<= 1e-5 on probe traces and full fields (the path's stated bound).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _pair(sc, precision="f64"):
+    import pyoracle
+    from dtmaxwell4_b200 import Simulation, scenarios
+    g = Simulation(sc["cfg"])
+    o = pyoracle.OracleSim(sc["cfg"], precision)
+    gid = scenarios.apply(g, sc)
+    oid = scenarios.apply(o, sc)
+    return g, o, gid, oid
+
+
+def _compare_fields(g, o, comps=range(6), tol=TOL):
+    errs = {}
+    for c in comps:
+        errs[c] = rel_l2(g.get_field(c), o.get_field(c))
+    assert max(errs.values()) <= tol, errs
+    return errs
+
+
+@pytest.mark.parametrize("order,courant", [(2, 0.5), (4, 0.4)])
+def test_point_dipole_sphere(order, courant):
+    from dtmaxwell4_b200 import scenarios
+    sc = scenarios.point_dipole_sphere(n=40, steps=300, pml=8, radius=8, order=order, courant=courant, lambda0=10.0)
+    g, o, _, _ = _pair(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    tg, to = g.read_probes(), o.read_probes(400)
+    assert tg.shape == to.shape == (16, 300)
+    for p in range(tg.shape[0]):
+        assert rel_l2(tg[p], to[p]) <= TOL, (p, rel_l2(tg[p], to[p]))
+    _compare_fields(g, o)
+    assert g.check_finite()
+
+
+def test_drude_sphere_plane_tfsf_dft():
+    from dtmaxwell4_b200 import scenarios
+    sc = scenarios.drude_sphere_tfsf(n=48, steps=260, pml=8, inset=6, radius=7, lambda0=10.0, nfreq=4)
+    g, o, gid, oid = _pair(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    _compare_fields(g, o)
+    tg, to = g.read_probes(), o.read_probes(400)
+    for p in range(tg.shape[0]):
+        assert rel_l2(tg[p], to[p]) <= TOL
+    dg, do = g.read_dft(gid[0]), o.read_dft(oid[0])
+    assert rel_l2(dg.view(np.float64), do.view(np.float64)) <= TOL
+
+
+def test_tfsf_scattered_region_is_quiet():
+    """Plane wave in vacuum: the scattered-field region stays orders of magnitude
+    below the total-field region (1-D line and 3-D grid share the stencil)."""
+    from dtmaxwell4_b200 import Simulation, abi, scenarios
+    sc = scenarios.drude_sphere_tfsf(n=48, steps=200, pml=8, inset=6, radius=7, lambda0=10.0, nfreq=2)
+    sc["materials"] = (None, None)
+    g = Simulation(sc["cfg"])
+    scenarios.apply(g, sc)
+    g.step(200)
+    ez = g.get_field(abi.EZ)
+    lo, hi = 8 + 6, 48 - 8 - 6
+    inside = np.abs(ez[lo + 2:hi - 2, lo + 2:hi - 2, lo + 2:hi - 2]).max()
+    outside = np.abs(ez[lo - 3, lo + 2:hi - 2, lo + 2:hi - 2]).max()
+    assert inside > 1e-2
+    assert outside < 1e-4 * inside, (outside, inside)
+
+
+def _reference_scenario(steps, order=4):
+    """Small DTMX_GEOM_REFERENCE case: split PML, dipole TF/SF box, a Drude
+    layer at the bottom, sensors with the reference averaging."""
+    from dtmaxwell4_b200 import abi
+    Np, Na, Nv = 16, 16, 48
+    nx, ny, nz = 3 * Np, 3 * Na, Nv
+    ds = 0.005
+    cfg = abi.make_config(nx, ny, nz, dx=ds, dt=0.002, order=order, geometry=abi.GEOM_REFERENCE,
+                          absorber=abi.ABS_SPLIT_PML, pml=((15, 15), (15, 15), (0, 16)), spml_vmax=1.0 / 1.75,
+                          probe_capacity=steps + 8)
+    cL = 1.0 / 1.75
+    lam = 0.5 * cL
+    t = abi.TFSF()
+    t.kind = abi.TFSF_DIPOLE
+    ctr = (nx / 2 * ds, ny / 2 * ds, 20 * ds)
+    for a in range(3):
+        t.box_lo[a] = ctr[a] - 5 * ds
+        t.box_hi[a] = ctr[a] + 5 * ds
+    t.c = cL
+    t.w = cL * 2 * math.pi / lam
+    t.kenv = 0.3
+    t.tstop = 0.0
+    t.ntime = 1
+    mats = [abi.make_material(1.75 ** 2),
+            abi.make_material(1.0, poles=[(abi.POLE_DRUDE, 1.0, 136.66 / 3.0, 2.69e13 / 2 / 3e14, 0.0)], eps_inf=1.0),
+            abi.make_material(1.8 ** 2)]
+    idx = np.zeros((nx, ny, nz), np.uint8)
+    idx[:, :, :8] = 1
+    idx[:, :, 8:11] = 2
+    probes = []
+    for xo in (0, 3, 6, 9):
+        for c in range(6):
+            probes.append((c, nx // 2 + xo, ny // 2, 20, abi.PROBE_REFERENCE))
+    return dict(name="reference_small", cfg=cfg, materials=(mats, [idx, idx, idx]), point_sources=[], tfsf=t,
+                probes=probes, dft=[], steps=steps)
+
+
+@pytest.mark.parametrize("order", [4, 2])
+def test_reference_geometry_split_pml_dipole(order):
+    sc = _reference_scenario(240, order)
+    g, o, _, _ = _pair(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    _compare_fields(g, o)
+    tg, to = g.read_probes(), o.read_probes(400)
+    worst = max(rel_l2(tg[p], to[p]) for p in range(tg.shape[0]) if np.abs(to[p]).max() > 0)
+    assert worst <= TOL, worst
+
+
+def test_fp32_oracle_agreement_is_tighter():
+    """Against the FP32 build of the oracle the difference is rounding order only."""
+    from dtmaxwell4_b200 import scenarios
+    sc = scenarios.point_dipole_sphere(n=32, steps=120, pml=6, radius=6, order=4, courant=0.4, lambda0=10.0)
+    g, o, _, _ = _pair(sc, "f32")
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    _compare_fields(g, o, tol=2e-6)
+
+
+def test_step_chunking_is_invariant():
+    """n steps in one call == the same steps split over several calls (bit-exact)."""
+    from dtmaxwell4_b200 import Simulation, abi, scenarios
+    sc = scenarios.point_dipole_sphere(n=32, steps=60, pml=6, radius=6, order=4, courant=0.4, lambda0=10.0)
+    a, b = Simulation(sc["cfg"]), Simulation(sc["cfg"])
+    scenarios.apply(a, sc)
+    scenarios.apply(b, sc)
+    a.step(60)
+    for _ in range(6):
+        b.step(10)
+    for c in range(6):
+        assert np.array_equal(a.get_field(c), b.get_field(c))
+
+
+def test_set_get_field_roundtrip_and_masking():
+    from dtmaxwell4_b200 import Simulation, abi
+    cfg = abi.make_config(24, 24, 24, dx=0.005, dt=0.002, order=4, geometry=abi.GEOM_REFERENCE,
+                          absorber=abi.ABS_NONE, pml=0)
+    g = Simulation(cfg)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((24, 24, 24)).astype(np.float32)
+    g.set_field(abi.EX, x)
+    y = g.get_field(abi.EX)
+    # Ex lives at X = 2i: held at zero for X <= 3 and X >= 2*24-3
+    assert np.all(y[:2] == 0) and np.all(y[23:] == 0)
+    assert np.array_equal(y[2:23], x[2:23])
+
+
+def test_invalid_configs_fail_loudly():
+    from dtmaxwell4_b200 import DtmxError, Simulation, abi
+    with pytest.raises(DtmxError):
+        Simulation(abi.make_config(32, 32, 32, courant=0.7, order=2))       # Courant > 1/sqrt(3)
+    with pytest.raises(DtmxError):
+        Simulation(abi.make_config(32, 32, 32, dt=0.5, order=4))           # > 6/7 limit
+    with pytest.raises(DtmxError):
+        Simulation(abi.make_config(32, 32, 32, geometry=abi.GEOM_REFERENCE, absorber=abi.ABS_CPML))
