@@ -11,6 +11,8 @@
 #include <vector>
 #include <algorithm>
 
+#include <cudaTypedefs.h>
+
 #include "dtmx.h"
 #include "dtmx_device.cuh"
 #include "dtmx_aux.cuh"
@@ -69,6 +71,8 @@ struct dtmx_ctx {
   long long prof_count = 0;
   bool prof_pending = false;
   int engine = 0, tblock = 0;
+  TmaMaps maps{};
+  int* d_err = nullptr;
   std::string err;
 };
 
@@ -147,6 +151,63 @@ static void setup_grid(dtmx_ctx* ctx) {
       g.live_lo[comp][a] = lo;
       g.live_hi[comp][a] = hi;
     }
+  for (int a = 0; a < 3; a++) {
+    g.all_lo[a] = 0; g.all_hi[a] = n[a] - 1;
+    for (int comp = 0; comp < 6; comp++) {
+      g.all_lo[a] = std::max(g.all_lo[a], g.live_lo[comp][a]);
+      g.all_hi[a] = std::min(g.all_hi[a], g.live_hi[comp][a]);
+    }
+    // a zero side never needs the boundary mapping: in-array non-live cells
+    // hold zero and out-of-array boxes are zero-filled by the TMA unit
+    g.safe_lo[a] = g.btype[a][0] == 0 ? -(1 << 28) : g.all_lo[a];
+    g.safe_hi[a] = g.btype[a][1] == 0 ? (1 << 28) : g.all_hi[a];
+  }
+}
+
+// ---------------------------------------------------------------- TMA descriptors
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* q = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &q, cudaEnableDefault, &qr) == cudaSuccess &&
+        qr == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)q;
+  }
+  return fn;
+}
+
+// 3-D map over a padded field (or material) array: dims (nz, ny, nx), box (bz, by, 1)
+static int make_map(dtmx_ctx* ctx, CUtensorMap* map, void* base, bool bytes, int bz, int by) {
+  auto fn = encode_fn();
+  if (!fn) return fail(ctx, DTMX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  const dtmx_config& c = ctx->cfg;
+  const size_t es = bytes ? 1 : 4;
+  cuuint64_t dims[3] = {(cuuint64_t)c.nz, (cuuint64_t)c.ny, (cuuint64_t)c.nx};
+  cuuint64_t strides[2] = {(cuuint64_t)ctx->nzp * es, (cuuint64_t)ctx->nzp * c.ny * es};
+  cuuint32_t box[3] = {(cuuint32_t)bz, (cuuint32_t)by, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(map, bytes ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box,
+                  estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ctx, DTMX_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return DTMX_OK;
+}
+
+static int build_maps(dtmx_ctx* ctx) {
+  const int R = ctx->cfg.order / 2;
+  // source tiles: A and C components carry R (below) + R-1 (above) halo rows for
+  // the H step and R-1 + R for the E step; B components no halo rows
+  const int rows_h = TYT + 2 * R - 1, rows_e = TYT + 2 * R - 1;
+  const int rows[6] = {rows_h, TYT, rows_h, rows_e, TYT, rows_e};
+  int rc;
+  for (int comp = 0; comp < 6; comp++) {
+    if ((rc = make_map(ctx, &ctx->maps.src[comp], ctx->P.f[comp], false, TW_ROW, rows[comp]))) return rc;
+    if ((rc = make_map(ctx, &ctx->maps.own[comp], ctx->P.f[comp], false, TZ, TYT))) return rc;
+  }
+  for (int comp = 0; comp < 3; comp++)
+    if ((rc = make_map(ctx, &ctx->maps.mat[comp], ctx->d_mat[comp], true, TZ, TYT))) return rc;
+  return DTMX_OK;
 }
 
 // Reference PMLgamma_func (DTmxw.cu:220-229).
@@ -198,7 +259,9 @@ static int setup_absorber(dtmx_ctx* ctx) {
         }
       }
   } else if (c.absorber == DTMX_ABS_SPLIT_PML) {
-    // setPMLcoeffs (DTmxw.cu:250-265): K2 = 1/(1+dt/2*gamma), K1 = 2*K2-1
+    // setPMLcoeffs (DTmxw.cu:250-265): K2 = 1/(1+dt/2*gamma), K1 = 2*K2-1;
+    // K1 = K2 = 1 where gamma = 0
+    for (int a = 0; a < 3; a++) t1[a].assign(2 * n[a] + 2, 1.f);
     const double V = c.spml_vmax;
     const int KX = 60, KY = 60, KZ = 64;
     ab.L[0][0] = c.pml[0][0]; ab.L[0][1] = c.pml[0][1];
@@ -290,12 +353,18 @@ extern "C" int dtmx_create(const dtmx_config* cfg, dtmx_ctx** out) {
   ctx->nstore = (size_t)c.nx * c.ny * ctx->nzp;
   setup_grid(ctx);
   int rc = DTMX_OK;
-  for (int comp = 0; comp < 6 && !rc; comp++) rc = dalloc(ctx, &ctx->P.f[comp], ctx->nstore);
+  // 64 floats of slack: aligned 16-byte tile rows may read up to 3 floats past the last node
+  for (int comp = 0; comp < 6 && !rc; comp++) rc = dalloc(ctx, &ctx->P.f[comp], ctx->nstore + 64);
   if (!rc) rc = setup_absorber(ctx);
   if (!rc) rc = dalloc(ctx, &ctx->d_mt, 1);
   if (!rc) rc = dalloc(ctx, &ctx->d_step, 1);
   if (!rc) rc = dalloc(ctx, &ctx->d_flag, 1);
+  if (!rc) rc = dalloc(ctx, &ctx->d_err, 1);
+  for (int comp = 0; comp < 3 && !rc; comp++) rc = dalloc(ctx, &ctx->d_mat[comp], ctx->nstore + 64);
+  if (!rc) rc = build_maps(ctx);
   if (rc) { *out = ctx; return rc; }
+  ctx->P.err = ctx->d_err;
+  for (int comp = 0; comp < 3; comp++) ctx->P.mat[comp] = ctx->d_mat[comp];
   ctx->P.cdt[0] = (float)(c.dt / c.dx); ctx->P.cdt[1] = (float)(c.dt / c.dy); ctx->P.cdt[2] = (float)(c.dt / c.dz);
   // default material 0: vacuum
   dtmx_material vac{};
@@ -391,10 +460,6 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
           }
         }
       }
-    if (!ctx->d_mat[comp]) {
-      int rc = dalloc(ctx, &ctx->d_mat[comp], ctx->nstore);
-      if (rc) return rc;
-    }
     CK(cudaMemcpyAsync(ctx->d_mat[comp], ctx->h_mat[comp].data(), ctx->nstore, cudaMemcpyHostToDevice, ctx->stream));
     ctx->P.mat[comp] = ctx->d_mat[comp];
   }
@@ -577,26 +642,39 @@ extern "C" int dtmx_read_dft(dtmx_ctx* ctx, int id, double* out, size_t out_len)
 // ---------------------------------------------------------------- stepping
 static int xchunk_for(const dtmx_ctx* ctx) {
   const dtmx_config& c = ctx->cfg;
-  const long long tiles = (long long)((c.nz + TZ - 1) / TZ) * ((c.ny + TY - 1) / TY);
+  const long long tiles = (long long)((c.nz + TZ - 1) / TZ) * ((c.ny + TYT - 1) / TYT);
   const long long target = 148LL * 8 * 3;   // about three waves of 8 CTAs per SM
   long long chunks = std::max<long long>(1, (target + tiles - 1) / tiles);
   long long xc = (c.nx + chunks - 1) / chunks;
   return (int)std::max<long long>(4, xc);
 }
 
+static int set_kernel_attributes() {
+  static bool done = false;
+  if (done) return 0;
+  cudaFuncSetAttribute(h_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Pipe<2, true>::SMEM_BYTES);
+  cudaFuncSetAttribute(h_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Pipe<4, true>::SMEM_BYTES);
+  cudaFuncSetAttribute(e_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Pipe<2, false>::SMEM_BYTES);
+  cudaFuncSetAttribute(e_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Pipe<4, false>::SMEM_BYTES);
+  done = true;
+  return 0;
+}
+
 static int launch_step(dtmx_ctx* ctx) {
+  set_kernel_attributes();
   const dtmx_config& c = ctx->cfg;
   Params P = ctx->P;
   P.x0 = 0; P.x1 = c.nx;
   P.xchunk = xchunk_for(ctx);
-  const dim3 blk(TZ, TY);
-  const dim3 grd((c.nz + TZ - 1) / TZ, (c.ny + TY - 1) / TY, (c.nx + P.xchunk - 1) / P.xchunk);
+  const dim3 blk(TZ, TW);
+  const dim3 grd((c.nz + TZ - 1) / TZ, (c.ny + TYT - 1) / TYT, (c.nx + P.xchunk - 1) / P.xchunk);
   const bool o4 = c.order == 4;
   cudaStream_t st = ctx->stream;
   const bool pw = ctx->has_tfsf && ctx->tfsf.kind == DTMX_TFSF_PLANE_X;
   long long nl = 0;
   if (ctx->profiling) cudaEventRecord(ctx->ev[0], st);
-  if (o4) h_kernel<4><<<grd, blk, 0, st>>>(P); else h_kernel<2><<<grd, blk, 0, st>>>(P);
+  if (o4) h_kernel<4><<<grd, blk, Pipe<4, true>::SMEM_BYTES, st>>>(P, ctx->maps);
+  else h_kernel<2><<<grd, blk, Pipe<2, true>::SMEM_BYTES, st>>>(P, ctx->maps);
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
   nl++;
   dim3 tgrid;
@@ -615,7 +693,8 @@ static int launch_step(dtmx_ctx* ctx) {
     nl++;
   }
   if (ctx->profiling) cudaEventRecord(ctx->ev[2], st);
-  if (o4) e_kernel<4><<<grd, blk, 0, st>>>(P); else e_kernel<2><<<grd, blk, 0, st>>>(P);
+  if (o4) e_kernel<4><<<grd, blk, Pipe<4, false>::SMEM_BYTES, st>>>(P, ctx->maps);
+  else e_kernel<2><<<grd, blk, Pipe<2, false>::SMEM_BYTES, st>>>(P, ctx->maps);
   if (ctx->profiling) {
     cudaEventRecord(ctx->ev[3], st);
     // read back this step's two kernel durations (keeps the events reusable)

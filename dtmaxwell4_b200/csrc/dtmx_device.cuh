@@ -1,11 +1,13 @@
-// dtmx_device.cuh -- device-side data structures and kernels of the FDTD engine.
+// dtmx_device.cuh -- device-side data structures and per-plane field updates.
 //
-// One half step (all three H components, or all three E components) is one
-// streaming kernel: a CTA owns a (z,y) tile of TZ x TY nodes and marches
-// along x, keeping the x taps of the derivative in a register queue and the
-// y/z taps of the current plane in shared memory.  Absorber (CPML or the
-// reference split-field PML), material coefficients and the Drude/Lorentz ADE
-// (reference countDisp) are fused into the same pass.
+// The unit of work is one (z,y) tile of one x-plane: TZ = 32 nodes along z
+// (one warp, coalesced 128-byte rows) by TYT = 16 nodes along y (8 warps, two
+// rows per thread).  The y/z taps of the derivatives come from shared-memory
+// copies of the neighbouring field's plane tile; the x taps come from the
+// caller (a register queue when a CTA streams along x, direct loads in the
+// wavefront engine).  Absorber (CPML or the reference split-field PML),
+// material coefficients and the Drude/Lorentz ADE (reference countDisp) are
+// applied in the same pass.
 //
 // Update equations (reference generator genAlg.py:182-301, defs.h:3-13):
 //   H -= dt * curl E,  E += dt/eps * curl H  (c = 1),
@@ -14,13 +16,16 @@
 // H nodes take taps at index offsets -2..+1, E nodes at -1..+2.
 #pragma once
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace dtmx {
 
-constexpr int TZ = 32;     // tile extent along z (one warp)
-constexpr int TY = 8;      // tile extent along y (warps per CTA)
-constexpr int NTHR = TZ * TY;
+constexpr int TZ = 32;          // tile extent along z (one warp)
+constexpr int TW = 8;           // warps per CTA
+constexpr int RY = 2;           // y rows per thread
+constexpr int TYT = TW * RY;    // tile extent along y
+constexpr int NTHR = TZ * TW;
 constexpr int MAXMAT = 64;
 constexpr int MAXPOLE = 2;
 
@@ -31,6 +36,8 @@ struct Grid {
   int n[3];
   long long sx, sy;          // element strides of x and y (z stride 1)
   int live_lo[6][3], live_hi[6][3];
+  int all_lo[3], all_hi[3];  // index range live for every component
+  int safe_lo[3], safe_hi[3];// index range whose taps need no mirror mapping (zero sides unbounded)
   int btype[3][2], bplane[3][2];
   int bsE[3][2], bsH[3][2];
 };
@@ -67,8 +74,17 @@ struct Params {
   const uint8_t* mat[3];     // per E component material index (nullptr -> material 0)
   const MatTable* mt;
   Ade ade;
-  int x0, x1;                // planes [x0, x1) processed by this launch
+  int x0, x1;                // planes [x0, x1) processed by a streaming launch
   int xchunk;                // planes per CTA along x
+  int* err;                  // device error word (bounded waits that gave up)
+};
+
+// TMA descriptors of one context: source tiles (40 z x rows y x 1 plane),
+// own-value tiles (32 x 16 x 1) of every component and material tiles.
+struct TmaMaps {
+  CUtensorMap src[6];
+  CUtensorMap own[6];
+  CUtensorMap mat[3];
 };
 
 // storage slot of component c for derivative axis a (-1: c has no derivative along a)
@@ -78,28 +94,34 @@ __host__ __device__ __forceinline__ int slot_of(int c, int a) {
   return S[c][a];
 }
 
+// Loads: LD = 0 read-only path (field not written during the launch),
+// LD = 1 L2-coherent path (written by other CTAs of the same launch).
+template <int LD>
+__device__ __forceinline__ float ldf(const float* q) { return LD ? __ldcg(q) : __ldg(q); }
+
 // Map index v of component c along axis a to the stored index, applying the
 // boundary rule outside the live range; returns -1 when the value is zero.
 __device__ __forceinline__ int map_idx(const Grid& g, int c, int a, int v, float& sgn) {
-  int lo = g.live_lo[c][a], hi = g.live_hi[c][a];
+  const int lo = g.live_lo[c][a], hi = g.live_hi[c][a];
   if (v >= lo && v <= hi) return v;
-  int side = v < lo ? 0 : 1;
+  const int side = v < lo ? 0 : 1;
   if (g.btype[a][side] == 0) return (v >= 0 && v < g.n[a]) ? v : -1;   // non-live cells hold zero
-  int o = comp_off(c, a);
-  int h2 = 2 * g.bplane[a][side] - (2 * v + o);
-  int v2 = (h2 - o) >> 1;
+  const int o = comp_off(c, a);
+  const int h2 = 2 * g.bplane[a][side] - (2 * v + o);
+  const int v2 = (h2 - o) >> 1;
   sgn *= (float)((c < 3) ? g.bsE[a][side] : g.bsH[a][side]);
   if (v2 < lo || v2 > hi) return -1;
   return v2;
 }
 
+template <int LD>
 __device__ __forceinline__ float fetch(const Params& p, int c, int i, int j, int k) {
   float s = 1.f;
-  int ii = map_idx(p.g, c, 0, i, s);
-  int jj = map_idx(p.g, c, 1, j, s);
-  int kk = map_idx(p.g, c, 2, k, s);
+  const int ii = map_idx(p.g, c, 0, i, s);
+  const int jj = map_idx(p.g, c, 1, j, s);
+  const int kk = map_idx(p.g, c, 2, k, s);
   if ((ii | jj | kk) < 0) return 0.f;
-  return s * __ldg(p.f[c] + ii * p.g.sx + jj * p.g.sy + kk);
+  return s * ldf<LD>(p.f[c] + ii * p.g.sx + jj * p.g.sy + kk);
 }
 
 template <int ORDER>
@@ -111,6 +133,10 @@ __device__ __forceinline__ float dstencil(float v0, float v1, float v2, float v3
 __device__ __forceinline__ bool is_live(const Grid& g, int c, int i, int j, int k) {
   return i >= g.live_lo[c][0] && i <= g.live_hi[c][0] && j >= g.live_lo[c][1] && j <= g.live_hi[c][1] &&
          k >= g.live_lo[c][2] && k <= g.live_hi[c][2];
+}
+
+__device__ __forceinline__ bool in_slab(const Params& p, int a, int v) {
+  return v < p.ab.L[a][0] || v >= p.g.n[a] - p.ab.L[a][1];
 }
 
 __device__ __forceinline__ long long slab_index(const Params& p, int a, int i, int j, int k) {
@@ -127,21 +153,18 @@ __device__ __forceinline__ long long slab_index(const Params& p, int a, int i, i
   return ((long long)i * p.g.n[1] + j) * th + cs;
 }
 
-// Apply the absorber to component c at cell (i,j,k): dif[a] are the signed,
-// scaled derivative terms; returns the new value given the old value F.
-__device__ __forceinline__ float absorb_update(const Params& p, int c, int i, int j, int k, const float dif[3], float F) {
-  if (p.ab.kind == 0) return F + dif[0] + dif[1] + dif[2];
+// Absorber update of component c at cell (i,j,k), which lies in at least one
+// absorber slab: dif[a] are the signed, scaled derivative terms; returns the
+// new value given the old value F.
+__device__ __forceinline__ float absorb_update(const Params& p, int c, int i, int j, int k, const float* dif, float F) {
   long long si[3];
-  bool any = false;
   const int idx[3] = {i, j, k};
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     si[a] = -1;
     if (slot_of(c, a) < 0 || (p.ab.L[a][0] + p.ab.L[a][1]) == 0) continue;
     si[a] = slab_index(p, a, i, j, k);
-    any |= si[a] >= 0;
   }
-  if (!any) return F + dif[0] + dif[1] + dif[2];
   if (p.ab.kind == 1) {
     float add = 0.f;
 #pragma unroll
@@ -179,199 +202,268 @@ __device__ __forceinline__ float absorb_update(const Params& p, int c, int i, in
   return rest + tot;
 }
 
-// Shared-memory tile of one component of plane i with halo (ZL,ZH) in z and (YL,YH) in y.
-template <int ZL, int ZH, int YL, int YH>
+// ---- asynchronous global -> shared copies (16-byte, L2 only: coherent with
+// writes made by other CTAs of the same launch)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Shared-memory copy of one component's plane tile: rows of TW_ROW floats
+// covering z in [k0-4, k0+36) (16-byte aligned), with YL/YH halo rows in y.
+constexpr int ZO = 4;                 // z offset of node k0 inside a row
+constexpr int TW_ROW = TZ + 2 * ZO;   // 40 floats = 10 x 16 bytes
+template <int YL, int YH>
 struct Tile {
-  static constexpr int W = TZ + ZL + ZH;
-  static constexpr int H = TY + YL + YH;
-  static constexpr int N = W * H;
-  __device__ static void load(float* sm, const Params& p, int c, int i, int j0, int k0, int tid) {
-    for (int e = tid; e < N; e += NTHR) {
-      const int zz = e % W, yy = e / W;
-      sm[e] = fetch(p, c, i, j0 - YL + yy, k0 - ZL + zz);
+  static constexpr int H = TYT + YL + YH;
+  static constexpr int NV = TW_ROW * H;                 // floats written by a load
+  static constexpr int N = (NV + 31) / 32 * 32;         // footprint, 128-byte multiple
+  // fast: every element is an in-array interior value -> async 16-byte copies
+  __device__ static void load_async(float* sm, const Params& p, int c, int i, int j0, int k0) {
+    const float* base = p.f[c] + (long long)i * p.g.sx + (long long)(j0 - YL) * p.g.sy + (k0 - ZO);
+    const int tid = threadIdx.y * TZ + threadIdx.x;
+    for (int q = tid; q < H * (TW_ROW / 4); q += NTHR) {
+      const int r = q / (TW_ROW / 4), col = q - r * (TW_ROW / 4);
+      cp_async16(sm + r * TW_ROW + col * 4, base + (long long)r * p.g.sy + col * 4);
     }
   }
-  __device__ static float at(const float* sm, int ty, int tz, int dy, int dz) {
-    return sm[(ty + YL + dy) * W + (tz + ZL + dz)];
+  // boundary tiles: element-wise with the boundary rules (z halo of 2 each side)
+  template <int LD>
+  __device__ static void load_slow(float* sm, const Params& p, int c, int i, int j0, int k0) {
+    const int lane = threadIdx.x, w = threadIdx.y;
+    for (int r = w; r < H; r += TW) {
+      const int j = j0 - YL + r;
+      sm[r * TW_ROW + ZO + lane] = fetch<LD>(p, c, i, j, k0 + lane);
+      if (lane < 2 * ZO) {
+        const int dz = lane < ZO ? lane - ZO : TZ + lane - ZO;   // -4..-1 and 32..35
+        sm[r * TW_ROW + ZO + dz] = fetch<LD>(p, c, i, j, k0 + dz);
+      }
+    }
+  }
+  // (y, z) tile-local node coordinates, (dy, dz) tap offsets
+  __device__ static float at(const float* sm, int y, int z, int dy, int dz) {
+    return sm[(y + YL + dy) * TW_ROW + (z + ZO + dz)];
   }
 };
 
+// fast-path test: all taps of the tile at plane i are live for every component
+__device__ __forceinline__ bool tile_interior(const Grid& g, int i, int j0, int k0) {
+  return i - 2 >= g.all_lo[0] && i + 2 <= g.all_hi[0] && j0 - 2 >= g.all_lo[1] && j0 + TYT + 1 <= g.all_hi[1] &&
+         k0 - 2 >= g.all_lo[2] && k0 + TZ + 1 <= g.all_hi[2];
+}
+
+// The three source-component tiles of one plane (one pipeline stage).
+template <int ORDER, bool ISH>
+struct Stage {
+  static constexpr int R = ORDER / 2;
+  static constexpr int YL = ISH ? R : R - 1, YH = ISH ? R - 1 : R;
+  using TA = Tile<YL, YH>;                     // Ex (H step) / Hx (E step): y and z taps
+  using TB = Tile<0, 0>;                       // Ey / Hy: z taps and own value
+  using TC = Tile<YL, YH>;                     // Ez / Hz: y taps and own value
+  static constexpr int N = TA::N + TB::N + TC::N;
+  static constexpr int c0 = ISH ? 0 : 3;       // first source component
+  template <int LD>
+  __device__ static void load(float* sm, const Params& p, int i, int j0, int k0, bool fast) {
+    if (fast) {
+      TA::load_async(sm, p, c0, i, j0, k0);
+      TB::load_async(sm + TA::N, p, c0 + 1, i, j0, k0);
+      TC::load_async(sm + TA::N + TB::N, p, c0 + 2, i, j0, k0);
+    } else {
+      TA::template load_slow<LD>(sm, p, c0, i, j0, k0);
+      TB::template load_slow<LD>(sm + TA::N, p, c0 + 1, i, j0, k0);
+      TC::template load_slow<LD>(sm + TA::N + TB::N, p, c0 + 2, i, j0, k0);
+    }
+  }
+  __device__ static float own_b(const float* sm, int y, int z) { return TB::at(sm + TA::N, y, z, 0, 0); }
+  __device__ static float own_c(const float* sm, int y, int z) { return TC::at(sm + TA::N + TB::N, y, z, 0, 0); }
+};
+
+// Per-thread absorber context of one node: which slabs hold it.
+__device__ __forceinline__ bool node_in_absorber(const Params& p, bool inx, int j, int k) {
+  return p.ab.kind != 0 && (inx || in_slab(p, 1, j) || in_slab(p, 2, k));
+}
+
 // ---------------------------------------------------------------- H half step
 // Hx -= dt (dy Ez - dz Ey),  Hy -= dt (dz Ex - dx Ez),  Hz -= dt (dx Ey - dy Ex)
-template <int ORDER>
-__global__ void __launch_bounds__(NTHR) h_kernel(Params p) {
-  constexpr int R = ORDER / 2;                 // taps below: 2R-? ; H taps -R..R-1
-  using TEx = Tile<R, R - 1, R, R - 1>;        // dy and dz taps of Ex
-  using TEy = Tile<R, R - 1, 0, 0>;            // dz taps of Ey
-  using TEz = Tile<0, 0, R, R - 1>;            // dy taps of Ez
-  __shared__ float sEx[TEx::N], sEy[TEy::N], sEz[TEz::N];
-  const int tz = threadIdx.x, ty = threadIdx.y, tid = ty * TZ + tz;
-  const int k0 = blockIdx.x * TZ, j0 = blockIdx.y * TY;
-  const int k = k0 + tz, j = j0 + ty;
-  const int xa = p.x0 + blockIdx.z * p.xchunk;
-  const int xb = min(xa + p.xchunk, p.x1);
-  const bool in = (j < p.g.n[1]) && (k < p.g.n[2]);
-  // register queues of Ey, Ez along x: q[0..3] = planes i-2..i+1 (order 4), i-1..i (order 2)
-  float qy[4], qz[4];
-#pragma unroll
-  for (int q = 0; q < 3; q++) {
-    qy[q + 1] = in ? fetch(p, 1, xa - 2 + q, j, k) : 0.f;
-    qz[q + 1] = in ? fetch(p, 2, xa - 2 + q, j, k) : 0.f;
-  }
+// qy[r][0..3], qz[r][0..3]: Ey, Ez of the thread's node r at planes i-2..i+1.
+// own-value tile: 3 components x TYT rows x TZ floats; material tile: 3 x TYT x TZ bytes
+constexpr int OWN_N = TYT * TZ;
+__device__ __forceinline__ float own_at(const float* so, int c, int y, int z) { return so[c * OWN_N + y * TZ + z]; }
+__device__ __forceinline__ int mat_at(const uint8_t* sm, int c, int y, int z) { return sm[c * OWN_N + y * TZ + z]; }
+
+template <int ORDER, int LD>
+__device__ __forceinline__ void h_plane(const Params& p, int i, int j0, int k0, const float* sm, const float (&qy)[RY][4],
+                                        const float (&qz)[RY][4], bool fast, const float* so) {
+  using S = Stage<ORDER, true>;
+  const float* sEx = sm;
+  const float* sEy = sEx + S::TA::N;
+  const float* sEz = sEy + S::TB::N;
+  const int tz = threadIdx.x, w = threadIdx.y;
   const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
-  for (int i = xa; i < xb; i++) {
+  const bool inx = p.ab.kind != 0 && in_slab(p, 0, i);
+  const long long pbase = (long long)i * p.g.sx;
 #pragma unroll
-    for (int q = 0; q < 3; q++) { qy[q] = qy[q + 1]; qz[q] = qz[q + 1]; }
-    qy[3] = in ? fetch(p, 1, i + 1, j, k) : 0.f;
-    qz[3] = in ? fetch(p, 2, i + 1, j, k) : 0.f;
-    TEx::load(sEx, p, 0, i, j0, k0, tid);
-    TEy::load(sEy, p, 1, i, j0, k0, tid);
-    TEz::load(sEz, p, 2, i, j0, k0, tid);
-    __syncthreads();
-    if (in) {
-      // taps v0..v3 at offsets -2..+1 (order 4) ; order 2 uses v1, v2 = offsets -1, 0
-      float a0, a1, a2, a3;
-      // ---- Hx
-      if (is_live(p.g, 3, i, j, k)) {
-        a0 = ORDER == 4 ? TEz::at(sEz, ty, tz, -2, 0) : 0.f; a1 = TEz::at(sEz, ty, tz, -1, 0);
-        a2 = TEz::at(sEz, ty, tz, 0, 0); a3 = ORDER == 4 ? TEz::at(sEz, ty, tz, 1, 0) : 0.f;
-        const float dyEz = dstencil<ORDER>(a0, a1, a2, a3);
-        a0 = ORDER == 4 ? TEy::at(sEy, ty, tz, 0, -2) : 0.f; a1 = TEy::at(sEy, ty, tz, 0, -1);
-        a2 = TEy::at(sEy, ty, tz, 0, 0); a3 = ORDER == 4 ? TEy::at(sEy, ty, tz, 0, 1) : 0.f;
-        const float dzEy = dstencil<ORDER>(a0, a1, a2, a3);
-        float dif[3] = {0.f, -cy * dyEz, cz * dzEy};
-        float* ph = p.f[3] + i * p.g.sx + j * p.g.sy + k;
-        *ph = absorb_update(p, 3, i, j, k, dif, *ph);
-      }
-      // ---- Hy
-      if (is_live(p.g, 4, i, j, k)) {
-        a0 = ORDER == 4 ? TEx::at(sEx, ty, tz, 0, -2) : 0.f; a1 = TEx::at(sEx, ty, tz, 0, -1);
-        a2 = TEx::at(sEx, ty, tz, 0, 0); a3 = ORDER == 4 ? TEx::at(sEx, ty, tz, 0, 1) : 0.f;
-        const float dzEx = dstencil<ORDER>(a0, a1, a2, a3);
-        const float dxEz = dstencil<ORDER>(qz[0], qz[1], qz[2], qz[3]);
-        float dif[3] = {cx * dxEz, 0.f, -cz * dzEx};
-        float* ph = p.f[4] + i * p.g.sx + j * p.g.sy + k;
-        *ph = absorb_update(p, 4, i, j, k, dif, *ph);
-      }
-      // ---- Hz
-      if (is_live(p.g, 5, i, j, k)) {
-        const float dxEy = dstencil<ORDER>(qy[0], qy[1], qy[2], qy[3]);
-        a0 = ORDER == 4 ? TEx::at(sEx, ty, tz, -2, 0) : 0.f; a1 = TEx::at(sEx, ty, tz, -1, 0);
-        a2 = TEx::at(sEx, ty, tz, 0, 0); a3 = ORDER == 4 ? TEx::at(sEx, ty, tz, 1, 0) : 0.f;
-        const float dyEx = dstencil<ORDER>(a0, a1, a2, a3);
-        float dif[3] = {-cx * dxEy, cy * dyEx, 0.f};
-        float* ph = p.f[5] + i * p.g.sx + j * p.g.sy + k;
-        *ph = absorb_update(p, 5, i, j, k, dif, *ph);
-      }
+  for (int r = 0; r < RY; r++) {
+    const int y = w + TW * r;
+    const int j = j0 + y, k = k0 + tz;
+    if (!fast && (j >= p.g.n[1] || k >= p.g.n[2])) continue;
+    const long long off = pbase + (long long)j * p.g.sy + k;
+    const bool ab = node_in_absorber(p, inx, j, k);
+    float a0, a1, a2, a3;
+    // ---- Hx
+    if (fast || is_live(p.g, 3, i, j, k)) {
+      a0 = ORDER == 4 ? S::TC::at(sEz, y, tz, -2, 0) : 0.f; a1 = S::TC::at(sEz, y, tz, -1, 0);
+      a2 = S::TC::at(sEz, y, tz, 0, 0); a3 = ORDER == 4 ? S::TC::at(sEz, y, tz, 1, 0) : 0.f;
+      const float dyEz = dstencil<ORDER>(a0, a1, a2, a3);
+      a0 = ORDER == 4 ? S::TB::at(sEy, y, tz, 0, -2) : 0.f; a1 = S::TB::at(sEy, y, tz, 0, -1);
+      a2 = S::TB::at(sEy, y, tz, 0, 0); a3 = ORDER == 4 ? S::TB::at(sEy, y, tz, 0, 1) : 0.f;
+      const float dzEy = dstencil<ORDER>(a0, a1, a2, a3);
+      const float dif[3] = {0.f, -cy * dyEz, cz * dzEy};
+      const float F0 = own_at(so, 0, y, tz);
+      p.f[3][off] = ab ? absorb_update(p, 3, i, j, k, dif, F0) : F0 + dif[0] + dif[1] + dif[2];
     }
-    __syncthreads();
+    // ---- Hy
+    if (fast || is_live(p.g, 4, i, j, k)) {
+      a0 = ORDER == 4 ? S::TA::at(sEx, y, tz, 0, -2) : 0.f; a1 = S::TA::at(sEx, y, tz, 0, -1);
+      a2 = S::TA::at(sEx, y, tz, 0, 0); a3 = ORDER == 4 ? S::TA::at(sEx, y, tz, 0, 1) : 0.f;
+      const float dzEx = dstencil<ORDER>(a0, a1, a2, a3);
+      const float dxEz = dstencil<ORDER>(qz[r][0], qz[r][1], qz[r][2], qz[r][3]);
+      const float dif[3] = {cx * dxEz, 0.f, -cz * dzEx};
+      const float F1 = own_at(so, 1, y, tz);
+      p.f[4][off] = ab ? absorb_update(p, 4, i, j, k, dif, F1) : F1 + dif[0] + dif[1] + dif[2];
+    }
+    // ---- Hz
+    if (fast || is_live(p.g, 5, i, j, k)) {
+      const float dxEy = dstencil<ORDER>(qy[r][0], qy[r][1], qy[r][2], qy[r][3]);
+      a0 = ORDER == 4 ? S::TA::at(sEx, y, tz, -2, 0) : 0.f; a1 = S::TA::at(sEx, y, tz, -1, 0);
+      a2 = S::TA::at(sEx, y, tz, 0, 0); a3 = ORDER == 4 ? S::TA::at(sEx, y, tz, 1, 0) : 0.f;
+      const float dyEx = dstencil<ORDER>(a0, a1, a2, a3);
+      const float dif[3] = {-cx * dxEy, cy * dyEx, 0.f};
+      const float F2 = own_at(so, 2, y, tz);
+      p.f[5][off] = ab ? absorb_update(p, 5, i, j, k, dif, F2) : F2 + dif[0] + dif[1] + dif[2];
+    }
   }
 }
 
 // ---------------------------------------------------------------- E half step
 // ADE branch restates countDisp (dispersion.cpp:85-99).
-__device__ __forceinline__ float e_node(const Params& p, int c, int i, int j, int k, float dif[3], float F) {
-  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
-  const int m = p.mat[c] ? (int)__ldg(p.mat[c] + id) : 0;
+__device__ __forceinline__ float ade_update(const Params& p, int c, int m, int np, long long ai, float rot, float F) {
   const MatTable& mt = *p.mt;
-  const int np = mt.npoles[m];
+  const float Em = p.ade.Em[c][ai];
+  const float Etmp = F;
+  float sum = 0.f;
+  float jp[MAXPOLE], jm[MAXPOLE];
+  for (int q = 0; q < np; q++) {
+    jp[q] = p.ade.Jp[c][q][ai]; jm[q] = p.ade.Jm[c][q][ai];
+    sum += __ldg(&mt.kEJ[m][c][q][0]) * jp[q] + __ldg(&mt.kEJ[m][c][q][1]) * jm[q];
+  }
+  const float Ep = __ldg(&mt.kE[m][c][0]) * Em + __ldg(&mt.kE[m][c][1]) * F + __ldg(&mt.kE[m][c][2]) * rot - sum;
+  for (int q = 0; q < np; q++) {
+    p.ade.Jp[c][q][ai] = __ldg(&mt.kJ[m][c][q][0]) * jp[q] + __ldg(&mt.kJ[m][c][q][1]) * jm[q] +
+                         __ldg(&mt.kJ[m][c][q][2]) * Ep + __ldg(&mt.kJ[m][c][q][3]) * Em +
+                         __ldg(&mt.kJ[m][c][q][4]) * Etmp;
+    p.ade.Jm[c][q][ai] = jp[q];
+  }
+  p.ade.Em[c][ai] = Etmp;
+  return Ep;
+}
+
+// Material coefficients used on the common path, staged in shared memory.
+struct MatShared {
+  float inv_eps[MAXMAT][3];
+  int npoles[MAXMAT];
+};
+
+__device__ __forceinline__ void load_matshared(MatShared& ms, const Params& p) {
+  const int tid = threadIdx.y * TZ + threadIdx.x;
+  for (int q = tid; q < MAXMAT * 3; q += NTHR) (&ms.inv_eps[0][0])[q] = __ldg(&p.mt->inv_eps[0][0] + q);
+  for (int q = tid; q < MAXMAT; q += NTHR) ms.npoles[q] = __ldg(&p.mt->npoles[q]);
+}
+
+__device__ __forceinline__ float e_node(const Params& p, const MatShared& ms, int c, int m, int i, int j, int k, bool ab,
+                                        float (&dif)[3], float F) {
+  const int np = ms.npoles[m];
   if (np > 0) {
     const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
     if (bi >= 0 && bi < p.ade.n[0] && bj >= 0 && bj < p.ade.n[1] && bk >= 0 && bk < p.ade.n[2]) {
       const long long ai = ((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk;
-      const float rot = dif[0] + dif[1] + dif[2];
-      float Ep = F;
-      const float Em = p.ade.Em[c][ai];
-      const float Etmp = Ep;
-      float sum = 0.f;
-      float jp[MAXPOLE], jm[MAXPOLE];
-      for (int q = 0; q < np; q++) {
-        jp[q] = p.ade.Jp[c][q][ai]; jm[q] = p.ade.Jm[c][q][ai];
-        sum += mt.kEJ[m][c][q][0] * jp[q] + mt.kEJ[m][c][q][1] * jm[q];
-      }
-      Ep = mt.kE[m][c][0] * Em + mt.kE[m][c][1] * Ep + mt.kE[m][c][2] * rot - sum;
-      for (int q = 0; q < np; q++) {
-        p.ade.Jp[c][q][ai] = mt.kJ[m][c][q][0] * jp[q] + mt.kJ[m][c][q][1] * jm[q] + mt.kJ[m][c][q][2] * Ep +
-                             mt.kJ[m][c][q][3] * Em + mt.kJ[m][c][q][4] * Etmp;
-        p.ade.Jm[c][q][ai] = jp[q];
-      }
-      p.ade.Em[c][ai] = Etmp;
-      return Ep;
+      return ade_update(p, c, m, np, ai, dif[0] + dif[1] + dif[2], F);
     }
   }
-  const float ie = mt.inv_eps[m][c];
+  const float ie = ms.inv_eps[m][c];
   dif[0] *= ie; dif[1] *= ie; dif[2] *= ie;
-  return absorb_update(p, c, i, j, k, dif, F);
+  return ab ? absorb_update(p, c, i, j, k, dif, F) : F + dif[0] + dif[1] + dif[2];
 }
 
 // Ex += dt/eps (dy Hz - dz Hy), Ey += dt/eps (dz Hx - dx Hz), Ez += dt/eps (dx Hy - dy Hx)
-template <int ORDER>
-__global__ void __launch_bounds__(NTHR) e_kernel(Params p) {
-  constexpr int R = ORDER / 2;                 // E taps -(R-1)..R  -> halo R-1 below, R above
-  using THx = Tile<R - 1, R, R - 1, R>;        // dz and dy taps of Hx
-  using THy = Tile<R - 1, R, 0, 0>;            // dz taps of Hy
-  using THz = Tile<0, 0, R - 1, R>;            // dy taps of Hz
-  __shared__ float sHx[THx::N], sHy[THy::N], sHz[THz::N];
-  const int tz = threadIdx.x, ty = threadIdx.y, tid = ty * TZ + tz;
-  const int k0 = blockIdx.x * TZ, j0 = blockIdx.y * TY;
-  const int k = k0 + tz, j = j0 + ty;
-  const int xa = p.x0 + blockIdx.z * p.xchunk;
-  const int xb = min(xa + p.xchunk, p.x1);
-  const bool in = (j < p.g.n[1]) && (k < p.g.n[2]);
-  // q[0..3] = planes i-1..i+2
-  float qy[4], qz[4];
-#pragma unroll
-  for (int q = 0; q < 3; q++) {
-    qy[q + 1] = in ? fetch(p, 4, xa - 1 + q, j, k) : 0.f;
-    qz[q + 1] = in ? fetch(p, 5, xa - 1 + q, j, k) : 0.f;
-  }
+// qy[r][0..3], qz[r][0..3]: Hy, Hz of the thread's node r at planes i-1..i+2.
+template <int ORDER, int LD>
+__device__ __forceinline__ void e_plane(const Params& p, int i, int j0, int k0, const float* sm, const float (&qy)[RY][4],
+                                        const float (&qz)[RY][4], bool fast, const float* so, const uint8_t* smat,
+                                        const MatShared& ms) {
+  using S = Stage<ORDER, false>;
+  const float* sHx = sm;
+  const float* sHy = sHx + S::TA::N;
+  const float* sHz = sHy + S::TB::N;
+  const int tz = threadIdx.x, w = threadIdx.y;
   const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
-  for (int i = xa; i < xb; i++) {
+  const bool inx = p.ab.kind != 0 && in_slab(p, 0, i);
+  const long long pbase = (long long)i * p.g.sx;
 #pragma unroll
-    for (int q = 0; q < 3; q++) { qy[q] = qy[q + 1]; qz[q] = qz[q + 1]; }
-    qy[3] = in ? fetch(p, 4, i + 2, j, k) : 0.f;
-    qz[3] = in ? fetch(p, 5, i + 2, j, k) : 0.f;
-    THx::load(sHx, p, 3, i, j0, k0, tid);
-    THy::load(sHy, p, 4, i, j0, k0, tid);
-    THz::load(sHz, p, 5, i, j0, k0, tid);
-    __syncthreads();
-    if (in) {
-      float a0, a1, a2, a3;
-      // ---- Ex
-      if (is_live(p.g, 0, i, j, k)) {
-        a0 = ORDER == 4 ? THz::at(sHz, ty, tz, -1, 0) : 0.f; a1 = THz::at(sHz, ty, tz, 0, 0);
-        a2 = THz::at(sHz, ty, tz, 1, 0); a3 = ORDER == 4 ? THz::at(sHz, ty, tz, 2, 0) : 0.f;
-        const float dyHz = dstencil<ORDER>(a0, a1, a2, a3);
-        a0 = ORDER == 4 ? THy::at(sHy, ty, tz, 0, -1) : 0.f; a1 = THy::at(sHy, ty, tz, 0, 0);
-        a2 = THy::at(sHy, ty, tz, 0, 1); a3 = ORDER == 4 ? THy::at(sHy, ty, tz, 0, 2) : 0.f;
-        const float dzHy = dstencil<ORDER>(a0, a1, a2, a3);
-        float dif[3] = {0.f, cy * dyHz, -cz * dzHy};
-        float* pe = p.f[0] + i * p.g.sx + j * p.g.sy + k;
-        *pe = e_node(p, 0, i, j, k, dif, *pe);
-      }
-      // ---- Ey
-      if (is_live(p.g, 1, i, j, k)) {
-        a0 = ORDER == 4 ? THx::at(sHx, ty, tz, 0, -1) : 0.f; a1 = THx::at(sHx, ty, tz, 0, 0);
-        a2 = THx::at(sHx, ty, tz, 0, 1); a3 = ORDER == 4 ? THx::at(sHx, ty, tz, 0, 2) : 0.f;
-        const float dzHx = dstencil<ORDER>(a0, a1, a2, a3);
-        const float dxHz = dstencil<ORDER>(qz[0], qz[1], qz[2], qz[3]);
-        float dif[3] = {-cx * dxHz, 0.f, cz * dzHx};
-        float* pe = p.f[1] + i * p.g.sx + j * p.g.sy + k;
-        *pe = e_node(p, 1, i, j, k, dif, *pe);
-      }
-      // ---- Ez
-      if (is_live(p.g, 2, i, j, k)) {
-        const float dxHy = dstencil<ORDER>(qy[0], qy[1], qy[2], qy[3]);
-        a0 = ORDER == 4 ? THx::at(sHx, ty, tz, -1, 0) : 0.f; a1 = THx::at(sHx, ty, tz, 0, 0);
-        a2 = THx::at(sHx, ty, tz, 1, 0); a3 = ORDER == 4 ? THx::at(sHx, ty, tz, 2, 0) : 0.f;
-        const float dyHx = dstencil<ORDER>(a0, a1, a2, a3);
-        float dif[3] = {cx * dxHy, -cy * dyHx, 0.f};
-        float* pe = p.f[2] + i * p.g.sx + j * p.g.sy + k;
-        *pe = e_node(p, 2, i, j, k, dif, *pe);
-      }
+  for (int r = 0; r < RY; r++) {
+    const int y = w + TW * r;
+    const int j = j0 + y, k = k0 + tz;
+    if (!fast && (j >= p.g.n[1] || k >= p.g.n[2])) continue;
+    const long long off = pbase + (long long)j * p.g.sy + k;
+    const bool ab = node_in_absorber(p, inx, j, k);
+    float a0, a1, a2, a3;
+    // ---- Ex
+    if (fast || is_live(p.g, 0, i, j, k)) {
+      a0 = ORDER == 4 ? S::TC::at(sHz, y, tz, -1, 0) : 0.f; a1 = S::TC::at(sHz, y, tz, 0, 0);
+      a2 = S::TC::at(sHz, y, tz, 1, 0); a3 = ORDER == 4 ? S::TC::at(sHz, y, tz, 2, 0) : 0.f;
+      const float dyHz = dstencil<ORDER>(a0, a1, a2, a3);
+      a0 = ORDER == 4 ? S::TB::at(sHy, y, tz, 0, -1) : 0.f; a1 = S::TB::at(sHy, y, tz, 0, 0);
+      a2 = S::TB::at(sHy, y, tz, 0, 1); a3 = ORDER == 4 ? S::TB::at(sHy, y, tz, 0, 2) : 0.f;
+      const float dzHy = dstencil<ORDER>(a0, a1, a2, a3);
+      float dif[3] = {0.f, cy * dyHz, -cz * dzHy};
+      p.f[0][off] = e_node(p, ms, 0, mat_at(smat, 0, y, tz), i, j, k, ab, dif, own_at(so, 0, y, tz));
     }
-    __syncthreads();
+    // ---- Ey
+    if (fast || is_live(p.g, 1, i, j, k)) {
+      a0 = ORDER == 4 ? S::TA::at(sHx, y, tz, 0, -1) : 0.f; a1 = S::TA::at(sHx, y, tz, 0, 0);
+      a2 = S::TA::at(sHx, y, tz, 0, 1); a3 = ORDER == 4 ? S::TA::at(sHx, y, tz, 0, 2) : 0.f;
+      const float dzHx = dstencil<ORDER>(a0, a1, a2, a3);
+      const float dxHz = dstencil<ORDER>(qz[r][0], qz[r][1], qz[r][2], qz[r][3]);
+      float dif[3] = {-cx * dxHz, 0.f, cz * dzHx};
+      p.f[1][off] = e_node(p, ms, 1, mat_at(smat, 1, y, tz), i, j, k, ab, dif, own_at(so, 1, y, tz));
+    }
+    // ---- Ez
+    if (fast || is_live(p.g, 2, i, j, k)) {
+      const float dxHy = dstencil<ORDER>(qy[r][0], qy[r][1], qy[r][2], qy[r][3]);
+      a0 = ORDER == 4 ? S::TA::at(sHx, y, tz, -1, 0) : 0.f; a1 = S::TA::at(sHx, y, tz, 0, 0);
+      a2 = S::TA::at(sHx, y, tz, 1, 0); a3 = ORDER == 4 ? S::TA::at(sHx, y, tz, 2, 0) : 0.f;
+      const float dyHx = dstencil<ORDER>(a0, a1, a2, a3);
+      float dif[3] = {cx * dxHy, -cy * dyHx, 0.f};
+      p.f[2][off] = e_node(p, ms, 2, mat_at(smat, 2, y, tz), i, j, k, ab, dif, own_at(so, 2, y, tz));
+    }
+  }
+}
+
+// x taps of the thread's nodes: component c at plane ip (fast: direct load)
+template <int LD>
+__device__ __forceinline__ void load_xtaps(const Params& p, int c, int ip, int j0, int k0, bool fast, float (&out)[RY]) {
+  const int tz = threadIdx.x, w = threadIdx.y;
+#pragma unroll
+  for (int r = 0; r < RY; r++) {
+    const int j = j0 + w + TW * r, k = k0 + tz;
+    if (fast) out[r] = ldf<LD>(p.f[c] + (long long)ip * p.g.sx + (long long)j * p.g.sy + k);
+    else out[r] = (j < p.g.n[1] && k < p.g.n[2]) ? fetch<LD>(p, c, ip, j, k) : 0.f;
   }
 }
 
 }  // namespace dtmx
+
+#include "dtmx_stream.cuh"

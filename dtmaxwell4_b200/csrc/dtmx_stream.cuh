@@ -1,0 +1,204 @@
+// dtmx_stream.cuh -- TMA-fed streaming kernels (one launch per half step).
+//
+// A CTA owns one (z,y) tile column and an x chunk.  For every plane it needs
+// the three source-field tiles (with y/z halo), the own values of the three
+// updated components and, for the E step, their material indices.  One
+// elected thread fetches all of them with cp.async.bulk.tensor (TMA, no
+// multicast) into a ring of NST shared-memory stages, LEAD planes ahead of
+// the plane being updated; completion is tracked per stage by an mbarrier
+// with a transaction count.  Out-of-array boxes are zero-filled by the TMA
+// unit, which is exactly the zero-outside boundary; planes whose taps reach a
+// mirror boundary are staged element-wise with the boundary rules instead.
+#pragma once
+#include "dtmx_device.cuh"
+
+namespace dtmx {
+
+__device__ __forceinline__ unsigned smem_u32(const void* q) { return (unsigned)__cvta_generic_to_shared(q); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred pp;\n mbarrier.try_wait.parity.shared::cta.b64 pp, [%1], %2;\n selp.u32 %0, 1, 0, pp;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after ~2^26 polls, records the failure in *err and returns.
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+  for (long long it = 0; !mbar_test(bar, parity); it++) {
+    if (it > (1LL << 26)) {
+      if (err) atomicExch(err, 1);
+      return;
+    }
+  }
+}
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
+
+template <int ORDER, bool ISH>
+struct Pipe {
+  using S = Stage<ORDER, ISH>;
+  static constexpr int OFF_A = 0;
+  static constexpr int OFF_B = S::TA::N;
+  static constexpr int OFF_C = OFF_B + S::TB::N;
+  static constexpr int OFF_OWN = OFF_C + S::TC::N;
+  static constexpr int OFF_MAT = OFF_OWN + 3 * OWN_N;
+  static constexpr int STAGE = OFF_MAT + (ISH ? 0 : 3 * OWN_N / 4);   // floats, multiple of 32
+  static constexpr unsigned BYTES = (S::TA::NV + S::TB::NV + S::TC::NV + 3 * OWN_N) * 4 + (ISH ? 0 : 3 * OWN_N);
+  // planes beyond i needed by plane i (x taps): H step order 4: +1; E step: +2 (order 4) / +1 (order 2)
+  static constexpr int AHEAD = ISH ? (ORDER == 4 ? 1 : 0) : (ORDER == 4 ? 2 : 1);
+  static constexpr int BEHIND = ISH ? (ORDER == 4 ? 2 : 1) : (ORDER == 4 ? 1 : 0);
+  static constexpr int LEAD = 2;                       // planes in flight beyond the resident ones
+  static constexpr int NST = AHEAD + 1 + LEAD;
+  static constexpr int BASE = ISH ? 2 : 1;             // queue slot of plane i (dstencil taps v0..v3)
+  static constexpr size_t SMEM_BYTES = (size_t)NST * STAGE * 4 + sizeof(MatShared) + NST * 8 + 128;
+};
+
+// Stage plane ip into stage buffer st (all threads call; uniform fast flag).
+template <int ORDER, bool ISH, int LD>
+__device__ __forceinline__ void stage_plane(const Params& p, const TmaMaps& m, float* st, uint64_t* bar, int ip, int j0,
+                                            int k0, bool fast) {
+  using P = Pipe<ORDER, ISH>;
+  using S = typename P::S;
+  const int c0 = ISH ? 0 : 3;       // source components
+  const int cf = ISH ? 3 : 0;       // updated components
+  const int tid = threadIdx.y * TZ + threadIdx.x;
+  if (fast) {
+    if (tid == 0) {
+      mbar_arrive_expect_tx(bar, P::BYTES);
+      tma_load_3d(st + P::OFF_A, &m.src[c0], k0 - ZO, j0 - S::YL, ip, bar);
+      tma_load_3d(st + P::OFF_B, &m.src[c0 + 1], k0 - ZO, j0, ip, bar);
+      tma_load_3d(st + P::OFF_C, &m.src[c0 + 2], k0 - ZO, j0 - S::YL, ip, bar);
+#pragma unroll
+      for (int c = 0; c < 3; c++) tma_load_3d(st + P::OFF_OWN + c * OWN_N, &m.own[cf + c], k0, j0, ip, bar);
+      if (!ISH)
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+          tma_load_3d(reinterpret_cast<uint8_t*>(st + P::OFF_MAT) + c * OWN_N, &m.mat[c], k0, j0, ip, bar);
+    }
+    return;
+  }
+  S::TA::template load_slow<LD>(st + P::OFF_A, p, c0, ip, j0, k0);
+  S::TB::template load_slow<LD>(st + P::OFF_B, p, c0 + 1, ip, j0, k0);
+  S::TC::template load_slow<LD>(st + P::OFF_C, p, c0 + 2, ip, j0, k0);
+  const int tz = threadIdx.x, w = threadIdx.y;
+#pragma unroll
+  for (int r = 0; r < RY; r++) {
+    const int y = w + TW * r, j = j0 + y, k = k0 + tz;
+    const bool ok = ip >= 0 && ip < p.g.n[0] && j < p.g.n[1] && k < p.g.n[2];
+    const long long off = (long long)ip * p.g.sx + (long long)j * p.g.sy + k;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      st[P::OFF_OWN + c * OWN_N + y * TZ + tz] = ok ? (LD ? __ldcg(p.f[cf + c] + off) : p.f[cf + c][off]) : 0.f;
+      if (!ISH)
+        reinterpret_cast<uint8_t*>(st + P::OFF_MAT)[c * OWN_N + y * TZ + tz] =
+            (ok && p.mat[c]) ? __ldg(p.mat[c] + off) : (uint8_t)0;
+    }
+  }
+  if (tid == 0) mbar_arrive(bar);
+}
+
+__device__ __forceinline__ bool tile_safe_yz(const Grid& g, int j0, int k0) {
+  return j0 - 2 >= g.safe_lo[1] && j0 + TYT + 1 <= g.safe_hi[1] && k0 - 4 >= g.safe_lo[2] && k0 + TZ + 3 <= g.safe_hi[2];
+}
+__device__ __forceinline__ bool plane_safe_x(const Grid& g, int i) { return i - 2 >= g.safe_lo[0] && i + 2 <= g.safe_hi[0]; }
+
+template <int ORDER, bool ISH>
+__device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, float* dsm) {
+  using P = Pipe<ORDER, ISH>;
+  using S = typename P::S;
+  constexpr int NST = P::NST, AHEAD = P::AHEAD, BEHIND = P::BEHIND, BASE = P::BASE, LEAD = P::LEAD;
+  MatShared& ms = *reinterpret_cast<MatShared*>(dsm + NST * P::STAGE);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(&ms) + sizeof(MatShared));
+  const int tz = threadIdx.x, w = threadIdx.y, tid = w * TZ + tz;
+  const int k0 = blockIdx.x * TZ, j0 = blockIdx.y * TYT;
+  const int xa = p.x0 + blockIdx.z * p.xchunk;
+  const int xb = min(xa + p.xchunk, p.x1);
+  if (tid == 0) {
+    for (int q = 0; q < NST; q++) mbar_init(&bars[q], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  if (!ISH) load_matshared(ms, p);
+  __syncthreads();
+  const bool yz_safe = tile_safe_yz(p.g, j0, k0);
+  // (fast path of the per-node update additionally needs every node and tap live)
+  const bool yz_in = j0 - 2 >= p.g.all_lo[1] && j0 + TYT + 1 <= p.g.all_hi[1] && k0 - 2 >= p.g.all_lo[2] &&
+                     k0 + TZ + 1 <= p.g.all_hi[2];
+  const int cb = ISH ? 1 : 4, cc = ISH ? 2 : 5;
+  float qb[RY][4], qc[RY][4];
+#pragma unroll
+  for (int r = 0; r < RY; r++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) { qb[r][q] = 0.f; qc[r][q] = 0.f; }
+  for (int q = 0; q < BEHIND; q++) {
+    float tb[RY], tcv[RY];
+    const int ip = xa - BEHIND + q;
+    const bool f = yz_in && ip >= p.g.all_lo[0] && ip <= p.g.all_hi[0];
+    load_xtaps<0>(p, cb, ip, j0, k0, f, tb);
+    load_xtaps<0>(p, cc, ip, j0, k0, f, tcv);
+#pragma unroll
+    for (int r = 0; r < RY; r++) { qb[r][BASE - BEHIND + q] = tb[r]; qc[r][BASE - BEHIND + q] = tcv[r]; }
+  }
+  const int last = xb - 1 + AHEAD;    // last plane that has to be staged
+  for (int ip = xa; ip < xa + AHEAD + LEAD && ip <= last; ip++)
+    stage_plane<ORDER, ISH, 0>(p, m, dsm + (ip % NST) * P::STAGE, &bars[ip % NST], ip, j0, k0,
+                               yz_safe && plane_safe_x(p.g, ip));
+  for (int i = xa; i < xb; i++) {
+    const int ipre = i + AHEAD + LEAD;
+    if (ipre <= last)
+      stage_plane<ORDER, ISH, 0>(p, m, dsm + (ipre % NST) * P::STAGE, &bars[ipre % NST], ipre, j0, k0,
+                                 yz_safe && plane_safe_x(p.g, ipre));
+    for (int q = 0; q <= AHEAD; q++) mbar_wait(&bars[(i + q) % NST], (unsigned)(((i + q - xa) / NST) & 1), p.err);
+    __syncthreads();
+    const bool fast = yz_in && i - 2 >= p.g.all_lo[0] && i + 2 <= p.g.all_hi[0];
+#pragma unroll
+    for (int r = 0; r < RY; r++) {
+      const int y = w + TW * r;
+#pragma unroll
+      for (int q = 0; q <= AHEAD; q++) {
+        const float* st = dsm + ((i + q) % NST) * P::STAGE;
+        qb[r][BASE + q] = S::TB::at(st + P::OFF_B, y, tz, 0, 0);
+        qc[r][BASE + q] = S::TC::at(st + P::OFF_C, y, tz, 0, 0);
+      }
+    }
+    const float* cur = dsm + (i % NST) * P::STAGE;
+    if (ISH) h_plane<ORDER, 0>(p, i, j0, k0, cur, qb, qc, fast, cur + P::OFF_OWN);
+    else e_plane<ORDER, 0>(p, i, j0, k0, cur, qb, qc, fast, cur + P::OFF_OWN,
+                           reinterpret_cast<const uint8_t*>(cur + P::OFF_MAT), ms);
+#pragma unroll
+    for (int r = 0; r < RY; r++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) { qb[r][q] = qb[r][q + 1]; qc[r][q] = qc[r][q + 1]; }
+    __syncthreads();
+  }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(NTHR) h_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
+  extern __shared__ __align__(128) float dsm[];
+  stream_body<ORDER, true>(p, m, dsm);
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(NTHR) e_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
+  extern __shared__ __align__(128) float dsm[];
+  stream_body<ORDER, false>(p, m, dsm);
+}
+
+}  // namespace dtmx
