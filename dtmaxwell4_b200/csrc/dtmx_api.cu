@@ -73,6 +73,7 @@ struct dtmx_ctx {
   int engine = 0, tblock = 0;
   TmaMaps maps{};
   int* d_err = nullptr;
+  signed char* d_umat = nullptr;
   std::string err;
 };
 
@@ -362,7 +363,11 @@ extern "C" int dtmx_create(const dtmx_config* cfg, dtmx_ctx** out) {
   if (!rc) rc = dalloc(ctx, &ctx->d_err, 1);
   for (int comp = 0; comp < 3 && !rc; comp++) rc = dalloc(ctx, &ctx->d_mat[comp], ctx->nstore + 64);
   if (!rc) rc = build_maps(ctx);
+  ctx->P.ntz = (c.nz + TZ - 1) / TZ;
+  ctx->P.nty = (c.ny + TYT - 1) / TYT;
+  if (!rc) rc = dalloc(ctx, &ctx->d_umat, (size_t)c.nx * ctx->P.nty * ctx->P.ntz);   // zeros: material 0 everywhere
   if (rc) { *out = ctx; return rc; }
+  ctx->P.umat = ctx->d_umat;
   ctx->P.err = ctx->d_err;
   for (int comp = 0; comp < 3; comp++) ctx->P.mat[comp] = ctx->d_mat[comp];
   ctx->P.cdt[0] = (float)(c.dt / c.dx); ctx->P.cdt[1] = (float)(c.dt / c.dy); ctx->P.cdt[2] = (float)(c.dt / c.dz);
@@ -465,6 +470,29 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
   }
   int rc = upload_mattable(ctx);
   if (rc) return rc;
+  {
+    // per (plane, y tile, z tile): the common non-dispersive material of all
+    // three E components, -1 if mixed or dispersive (selects the simple path)
+    const int nty = ctx->P.nty, ntz = ctx->P.ntz;
+    std::vector<signed char> um((size_t)c.nx * nty * ntz);
+    for (int i = 0; i < c.nx; i++)
+      for (int ty = 0; ty < nty; ty++)
+        for (int tz = 0; tz < ntz; tz++) {
+          int m0 = -2;
+          for (int j = ty * TYT; j < std::min(c.ny, ty * TYT + TYT) && m0 != -1; j++)
+            for (int comp = 0; comp < 3 && m0 != -1; comp++) {
+              const uint8_t* row = ctx->h_mat[comp].data() + store_index(ctx, i, j, 0);
+              for (int k = tz * TZ; k < std::min(c.nz, tz * TZ + TZ); k++) {
+                const int m = row[k];
+                if (m0 == -2) m0 = m;
+                if (m != m0 || table[m].npoles > 0) { m0 = -1; break; }
+              }
+            }
+          um[((size_t)i * nty + ty) * ntz + tz] = (signed char)(m0 < 0 ? -1 : m0);
+        }
+    CK(cudaMemcpyAsync(ctx->d_umat, um.data(), um.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
   Ade& A = ctx->P.ade;
   if (hi[0] >= 0) {
     size_t na = 1;

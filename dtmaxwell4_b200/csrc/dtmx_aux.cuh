@@ -106,14 +106,14 @@ __global__ void tfsf_kernel(Params p, TfsfDev t, const long long* d_step, int is
     const bool self_in = in_box(t, Xs[0], Xs[1], Xs[2]);
     int ax[2], gs[2];
     curl_terms(c, ax[0], gs[0], ax[1], gs[1]);
-    float total = 0.f;
+    double total = 0.0;
     bool any = false;
     for (int term = 0; term < 2; term++) {
       const int a = ax[term], g = gs[term];
-      float v[4];
+      double v[4];
       bool hit = false;
       for (int q = 0; q < 4; q++) {
-        v[q] = 0.f;
+        v[q] = 0.0;
         if (ORDER == 2 && (q == 0 || q == 3)) continue;
         int m[3] = {idx[0], idx[1], idx[2]};
         m[a] += t0 + q;
@@ -121,23 +121,24 @@ __global__ void tfsf_kernel(Params p, TfsfDev t, const long long* d_step, int is
         const bool tin = in_box(t, TX, TY_, TZ_);
         if (tin != self_in) {
           const double inc = incident(t, g, TX, TY_, TZ_, tt);
-          v[q] = (float)(self_in ? -inc : inc);
+          v[q] = self_in ? -inc : inc;
           hit = true;
         }
       }
       if (!hit) continue;
       any = true;
-      float sg = term == 0 ? 1.f : -1.f;
+      double sg = term == 0 ? 1.0 : -1.0;
       if (isH) sg = -sg;
-      total += sg * p.cdt[a] * dstencil<ORDER>(v[0], v[1], v[2], v[3]);
+      const double dv = ORDER == 2 ? v[2] - v[1] : (27.0 * (v[2] - v[1]) - (v[3] - v[0])) / 24.0;
+      total += sg * (double)p.cdt[a] * dv;
     }
     if (!any) continue;
     const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
     if (!isH) {
       const int mi = p.mat[c] ? (int)p.mat[c][id] : 0;
-      total *= p.mt->inv_eps[mi][c];
+      total *= (double)p.mt->inv_eps[mi][c];
     }
-    p.f[c][id] += total;
+    p.f[c][id] += (float)total;
   }
 }
 

@@ -77,6 +77,10 @@ struct Params {
   int x0, x1;                // planes [x0, x1) processed by a streaming launch
   int xchunk;                // planes per CTA along x
   int* err;                  // device error word (bounded waits that gave up)
+  // per (plane, y tile, z tile): the single non-dispersive material of all E
+  // nodes of that plane tile, or -1 when mixed/dispersive
+  const signed char* umat;
+  int ntz, nty;              // tiles along z and y
 };
 
 // TMA descriptors of one context: source tiles (40 z x rows y x 1 plane),
@@ -153,55 +157,6 @@ __device__ __forceinline__ long long slab_index(const Params& p, int a, int i, i
   return ((long long)i * p.g.n[1] + j) * th + cs;
 }
 
-// Absorber update of component c at cell (i,j,k), which lies in at least one
-// absorber slab: dif[a] are the signed, scaled derivative terms; returns the
-// new value given the old value F.
-__device__ __forceinline__ float absorb_update(const Params& p, int c, int i, int j, int k, const float* dif, float F) {
-  long long si[3];
-  const int idx[3] = {i, j, k};
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    si[a] = -1;
-    if (slot_of(c, a) < 0 || (p.ab.L[a][0] + p.ab.L[a][1]) == 0) continue;
-    si[a] = slab_index(p, a, i, j, k);
-  }
-  if (p.ab.kind == 1) {
-    float add = 0.f;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const int sl = slot_of(c, a);
-      if (sl < 0) continue;
-      if (si[a] < 0) { add += dif[a]; continue; }
-      const int h = 2 * idx[a] + comp_off(c, a);
-      float* psi = p.ab.aux[a][sl] + si[a];
-      const float nv = __ldg(p.ab.c0[a] + h) * *psi + __ldg(p.ab.c1[a] + h) * dif[a];
-      *psi = nv;
-      add += __ldg(p.ab.c2[a] + h) * dif[a] + nv;
-    }
-    return F + add;
-  }
-  // split field: F = rest + sum of stored directional parts
-  float rest = F, tot = 0.f;
-#pragma unroll
-  for (int a = 0; a < 3; a++)
-    if (si[a] >= 0) rest -= p.ab.aux[a][slot_of(c, a)][si[a]];
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    const int sl = slot_of(c, a);
-    if (sl < 0) continue;
-    if (si[a] >= 0) {
-      const int h = 2 * idx[a] + comp_off(c, a);
-      float* pp = p.ab.aux[a][sl] + si[a];
-      const float nv = __ldg(p.ab.c0[a] + h) * *pp + __ldg(p.ab.c1[a] + h) * dif[a];
-      *pp = nv;
-      tot += nv;
-    } else {
-      rest += dif[a];
-    }
-  }
-  return rest + tot;
-}
-
 // ---- asynchronous global -> shared copies (16-byte, L2 only: coherent with
 // writes made by other CTAs of the same launch)
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -211,6 +166,36 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// own-value tile: 3 components x TYT rows x TZ floats; material tile: 3 x TYT x TZ bytes
+constexpr int OWN_N = TYT * TZ;
+__device__ __forceinline__ float own_at(const float* so, int c, int y, int z) { return so[c * OWN_N + y * TZ + z]; }
+__device__ __forceinline__ int mat_at(const uint8_t* sm, int c, int y, int z) { return sm[c * OWN_N + y * TZ + z]; }
+
+// Absorber correction of component c at a slab node: the update is
+// F_new = F + dif[0] + dif[1] + dif[2] + correction, where for every slab axis a
+//   CPML:  correction_a = (1/kappa_a - 1) dif_a + psi_a,  psi_a <- b psi_a + a dif_a
+//   split: correction_a = (K1_a - 1) p_a + (K2_a - 1) dif_a,  p_a <- K1_a p_a + K2_a dif_a
+// (the split form follows from F = rest + sum p_a with rest += undamped terms).
+__device__ __forceinline__ float absorb_correction(const Params& p, int c, int i, int j, int k, const float* dif) {
+  const int idx[3] = {i, j, k};
+  float corr = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int sl = slot_of(c, a);
+    if (sl < 0 || !in_slab(p, a, idx[a])) continue;
+    const long long si = slab_index(p, a, i, j, k);
+    const int h = 2 * idx[a] + comp_off(c, a);
+    float* st = p.ab.aux[a][sl] + si;
+    const float old = *st;
+    const float k0 = __ldg(p.ab.c0[a] + h), k1 = __ldg(p.ab.c1[a] + h);
+    const float nv = k0 * old + k1 * dif[a];
+    *st = nv;
+    if (p.ab.kind == 1) corr += (__ldg(p.ab.c2[a] + h) - 1.f) * dif[a] + nv;
+    else corr += nv - old - dif[a];
+  }
+  return corr;
+}
 
 // Shared-memory copy of one component's plane tile: rows of TW_ROW floats
 // covering z in [k0-4, k0+36) (16-byte aligned), with YL/YH halo rows in y.
@@ -281,71 +266,20 @@ struct Stage {
   __device__ static float own_c(const float* sm, int y, int z) { return TC::at(sm + TA::N + TB::N, y, z, 0, 0); }
 };
 
+// CTA-uniform tests: does the tile at plane i touch an absorber slab / the ADE box?
+__device__ __forceinline__ bool tile_absorber(const Params& p, int i, int j0, int k0) {
+  if (p.ab.kind == 0) return false;
+  return in_slab(p, 0, i) || j0 < p.ab.L[1][0] || j0 + TYT > p.g.n[1] - p.ab.L[1][1] || k0 < p.ab.L[2][0] ||
+         k0 + TZ > p.g.n[2] - p.ab.L[2][1];
+}
+__device__ __forceinline__ bool tile_ade(const Params& p, int i, int j0, int k0) {
+  return i >= p.ade.lo[0] && i < p.ade.lo[0] + p.ade.n[0] && j0 + TYT > p.ade.lo[1] && j0 < p.ade.lo[1] + p.ade.n[1] &&
+         k0 + TZ > p.ade.lo[2] && k0 < p.ade.lo[2] + p.ade.n[2];
+}
+
 // Per-thread absorber context of one node: which slabs hold it.
 __device__ __forceinline__ bool node_in_absorber(const Params& p, bool inx, int j, int k) {
   return p.ab.kind != 0 && (inx || in_slab(p, 1, j) || in_slab(p, 2, k));
-}
-
-// ---------------------------------------------------------------- H half step
-// Hx -= dt (dy Ez - dz Ey),  Hy -= dt (dz Ex - dx Ez),  Hz -= dt (dx Ey - dy Ex)
-// qy[r][0..3], qz[r][0..3]: Ey, Ez of the thread's node r at planes i-2..i+1.
-// own-value tile: 3 components x TYT rows x TZ floats; material tile: 3 x TYT x TZ bytes
-constexpr int OWN_N = TYT * TZ;
-__device__ __forceinline__ float own_at(const float* so, int c, int y, int z) { return so[c * OWN_N + y * TZ + z]; }
-__device__ __forceinline__ int mat_at(const uint8_t* sm, int c, int y, int z) { return sm[c * OWN_N + y * TZ + z]; }
-
-template <int ORDER, int LD>
-__device__ __forceinline__ void h_plane(const Params& p, int i, int j0, int k0, const float* sm, const float (&qy)[RY][4],
-                                        const float (&qz)[RY][4], bool fast, const float* so) {
-  using S = Stage<ORDER, true>;
-  const float* sEx = sm;
-  const float* sEy = sEx + S::TA::N;
-  const float* sEz = sEy + S::TB::N;
-  const int tz = threadIdx.x, w = threadIdx.y;
-  const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
-  const bool inx = p.ab.kind != 0 && in_slab(p, 0, i);
-  const long long pbase = (long long)i * p.g.sx;
-#pragma unroll
-  for (int r = 0; r < RY; r++) {
-    const int y = w + TW * r;
-    const int j = j0 + y, k = k0 + tz;
-    if (!fast && (j >= p.g.n[1] || k >= p.g.n[2])) continue;
-    const long long off = pbase + (long long)j * p.g.sy + k;
-    const bool ab = node_in_absorber(p, inx, j, k);
-    float a0, a1, a2, a3;
-    // ---- Hx
-    if (fast || is_live(p.g, 3, i, j, k)) {
-      a0 = ORDER == 4 ? S::TC::at(sEz, y, tz, -2, 0) : 0.f; a1 = S::TC::at(sEz, y, tz, -1, 0);
-      a2 = S::TC::at(sEz, y, tz, 0, 0); a3 = ORDER == 4 ? S::TC::at(sEz, y, tz, 1, 0) : 0.f;
-      const float dyEz = dstencil<ORDER>(a0, a1, a2, a3);
-      a0 = ORDER == 4 ? S::TB::at(sEy, y, tz, 0, -2) : 0.f; a1 = S::TB::at(sEy, y, tz, 0, -1);
-      a2 = S::TB::at(sEy, y, tz, 0, 0); a3 = ORDER == 4 ? S::TB::at(sEy, y, tz, 0, 1) : 0.f;
-      const float dzEy = dstencil<ORDER>(a0, a1, a2, a3);
-      const float dif[3] = {0.f, -cy * dyEz, cz * dzEy};
-      const float F0 = own_at(so, 0, y, tz);
-      p.f[3][off] = ab ? absorb_update(p, 3, i, j, k, dif, F0) : F0 + dif[0] + dif[1] + dif[2];
-    }
-    // ---- Hy
-    if (fast || is_live(p.g, 4, i, j, k)) {
-      a0 = ORDER == 4 ? S::TA::at(sEx, y, tz, 0, -2) : 0.f; a1 = S::TA::at(sEx, y, tz, 0, -1);
-      a2 = S::TA::at(sEx, y, tz, 0, 0); a3 = ORDER == 4 ? S::TA::at(sEx, y, tz, 0, 1) : 0.f;
-      const float dzEx = dstencil<ORDER>(a0, a1, a2, a3);
-      const float dxEz = dstencil<ORDER>(qz[r][0], qz[r][1], qz[r][2], qz[r][3]);
-      const float dif[3] = {cx * dxEz, 0.f, -cz * dzEx};
-      const float F1 = own_at(so, 1, y, tz);
-      p.f[4][off] = ab ? absorb_update(p, 4, i, j, k, dif, F1) : F1 + dif[0] + dif[1] + dif[2];
-    }
-    // ---- Hz
-    if (fast || is_live(p.g, 5, i, j, k)) {
-      const float dxEy = dstencil<ORDER>(qy[r][0], qy[r][1], qy[r][2], qy[r][3]);
-      a0 = ORDER == 4 ? S::TA::at(sEx, y, tz, -2, 0) : 0.f; a1 = S::TA::at(sEx, y, tz, -1, 0);
-      a2 = S::TA::at(sEx, y, tz, 0, 0); a3 = ORDER == 4 ? S::TA::at(sEx, y, tz, 1, 0) : 0.f;
-      const float dyEx = dstencil<ORDER>(a0, a1, a2, a3);
-      const float dif[3] = {-cx * dxEy, cy * dyEx, 0.f};
-      const float F2 = own_at(so, 2, y, tz);
-      p.f[5][off] = ab ? absorb_update(p, 5, i, j, k, dif, F2) : F2 + dif[0] + dif[1] + dif[2];
-    }
-  }
 }
 
 // ---------------------------------------------------------------- E half step
@@ -383,71 +317,86 @@ __device__ __forceinline__ void load_matshared(MatShared& ms, const Params& p) {
   for (int q = tid; q < MAXMAT; q += NTHR) ms.npoles[q] = __ldg(&p.mt->npoles[q]);
 }
 
-__device__ __forceinline__ float e_node(const Params& p, const MatShared& ms, int c, int m, int i, int j, int k, bool ab,
-                                        float (&dif)[3], float F) {
-  const int np = ms.npoles[m];
-  if (np > 0) {
-    const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
-    if (bi >= 0 && bi < p.ade.n[0] && bj >= 0 && bj < p.ade.n[1] && bk >= 0 && bk < p.ade.n[2]) {
-      const long long ai = ((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk;
-      return ade_update(p, c, m, np, ai, dif[0] + dif[1] + dif[2], F);
-    }
-  }
-  const float ie = ms.inv_eps[m][c];
-  dif[0] *= ie; dif[1] *= ie; dif[2] *= ie;
-  return ab ? absorb_update(p, c, i, j, k, dif, F) : F + dif[0] + dif[1] + dif[2];
-}
-
-// Ex += dt/eps (dy Hz - dz Hy), Ey += dt/eps (dz Hx - dx Hz), Ez += dt/eps (dx Hy - dy Hx)
-// qy[r][0..3], qz[r][0..3]: Hy, Hz of the thread's node r at planes i-1..i+2.
-template <int ORDER, int LD>
-__device__ __forceinline__ void e_plane(const Params& p, int i, int j0, int k0, const float* sm, const float (&qy)[RY][4],
-                                        const float (&qz)[RY][4], bool fast, const float* so, const uint8_t* smat,
-                                        const MatShared& ms) {
-  using S = Stage<ORDER, false>;
-  const float* sHx = sm;
-  const float* sHy = sHx + S::TA::N;
-  const float* sHz = sHy + S::TB::N;
+// Update of one plane tile (all three components of the half step).  Common
+// path: F + sum of the signed derivative terms (times 1/eps for E); slab
+// nodes add the absorber correction, dispersive nodes (E step, tiles touching
+// the ADE box) are replaced by the ADE recursion, non-live nodes are skipped.
+//   um >= 0: every E node of the tile has non-dispersive material um
+// SIMPLE: every node live, no absorber, no ADE, uniform material um (>= 0).
+template <int ORDER, bool ISH, bool SIMPLE>
+__device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int k0, const float* sm,
+                                             const float (&qb)[RY][4], const float (&qc)[RY][4], const float* so,
+                                             const uint8_t* smat, const MatShared& ms, bool fast, int um) {
+  using S = Stage<ORDER, ISH>;
+  const float* sA = sm;
+  const float* sB = sA + S::TA::N;
+  const float* sC = sB + S::TB::N;
   const int tz = threadIdx.x, w = threadIdx.y;
   const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
-  const bool inx = p.ab.kind != 0 && in_slab(p, 0, i);
+  const int cf = ISH ? 3 : 0;
   const long long pbase = (long long)i * p.g.sx;
+  const bool tab = !SIMPLE && tile_absorber(p, i, j0, k0);
+  const bool inx = tab && in_slab(p, 0, i);
+  const bool tade = !SIMPLE && !ISH && tile_ade(p, i, j0, k0);
+  float iu[3] = {1.f, 1.f, 1.f};
+  if (SIMPLE && !ISH) { iu[0] = ms.inv_eps[um][0]; iu[1] = ms.inv_eps[um][1]; iu[2] = ms.inv_eps[um][2]; }
+  constexpr int o0 = ISH ? -2 : -1, o1 = o0 + 1, o2 = o0 + 2, o3 = o0 + 3;
 #pragma unroll
   for (int r = 0; r < RY; r++) {
     const int y = w + TW * r;
     const int j = j0 + y, k = k0 + tz;
-    if (!fast && (j >= p.g.n[1] || k >= p.g.n[2])) continue;
+    if (!SIMPLE && !fast && (j >= p.g.n[1] || k >= p.g.n[2])) continue;
     const long long off = pbase + (long long)j * p.g.sy + k;
-    const bool ab = node_in_absorber(p, inx, j, k);
-    float a0, a1, a2, a3;
-    // ---- Ex
-    if (fast || is_live(p.g, 0, i, j, k)) {
-      a0 = ORDER == 4 ? S::TC::at(sHz, y, tz, -1, 0) : 0.f; a1 = S::TC::at(sHz, y, tz, 0, 0);
-      a2 = S::TC::at(sHz, y, tz, 1, 0); a3 = ORDER == 4 ? S::TC::at(sHz, y, tz, 2, 0) : 0.f;
-      const float dyHz = dstencil<ORDER>(a0, a1, a2, a3);
-      a0 = ORDER == 4 ? S::TB::at(sHy, y, tz, 0, -1) : 0.f; a1 = S::TB::at(sHy, y, tz, 0, 0);
-      a2 = S::TB::at(sHy, y, tz, 0, 1); a3 = ORDER == 4 ? S::TB::at(sHy, y, tz, 0, 2) : 0.f;
-      const float dzHy = dstencil<ORDER>(a0, a1, a2, a3);
-      float dif[3] = {0.f, cy * dyHz, -cz * dzHy};
-      p.f[0][off] = e_node(p, ms, 0, mat_at(smat, 0, y, tz), i, j, k, ab, dif, own_at(so, 0, y, tz));
+    const float dyC = dstencil<ORDER>(ORDER == 4 ? S::TC::at(sC, y, tz, o0, 0) : 0.f, S::TC::at(sC, y, tz, o1, 0),
+                                      S::TC::at(sC, y, tz, o2, 0), ORDER == 4 ? S::TC::at(sC, y, tz, o3, 0) : 0.f);
+    const float dzB = dstencil<ORDER>(ORDER == 4 ? S::TB::at(sB, y, tz, 0, o0) : 0.f, S::TB::at(sB, y, tz, 0, o1),
+                                      S::TB::at(sB, y, tz, 0, o2), ORDER == 4 ? S::TB::at(sB, y, tz, 0, o3) : 0.f);
+    const float dzA = dstencil<ORDER>(ORDER == 4 ? S::TA::at(sA, y, tz, 0, o0) : 0.f, S::TA::at(sA, y, tz, 0, o1),
+                                      S::TA::at(sA, y, tz, 0, o2), ORDER == 4 ? S::TA::at(sA, y, tz, 0, o3) : 0.f);
+    const float dyA = dstencil<ORDER>(ORDER == 4 ? S::TA::at(sA, y, tz, o0, 0) : 0.f, S::TA::at(sA, y, tz, o1, 0),
+                                      S::TA::at(sA, y, tz, o2, 0), ORDER == 4 ? S::TA::at(sA, y, tz, o3, 0) : 0.f);
+    const float dxC = dstencil<ORDER>(qc[r][0], qc[r][1], qc[r][2], qc[r][3]);
+    const float dxB = dstencil<ORDER>(qb[r][0], qb[r][1], qb[r][2], qb[r][3]);
+    // signed, scaled derivative terms per component, [comp][axis]
+    float d[3][3];
+    if (ISH) {
+      // Hx -= dt(dy Ez - dz Ey); Hy -= dt(dz Ex - dx Ez); Hz -= dt(dx Ey - dy Ex)
+      d[0][0] = 0.f;       d[0][1] = -cy * dyC; d[0][2] = cz * dzB;
+      d[1][0] = cx * dxC;  d[1][1] = 0.f;       d[1][2] = -cz * dzA;
+      d[2][0] = -cx * dxB; d[2][1] = cy * dyA;  d[2][2] = 0.f;
+    } else {
+      // Ex += dt/eps(dy Hz - dz Hy); Ey += dt/eps(dz Hx - dx Hz); Ez += dt/eps(dx Hy - dy Hx)
+      d[0][0] = 0.f;       d[0][1] = cy * dyC;  d[0][2] = -cz * dzB;
+      d[1][0] = -cx * dxC; d[1][1] = 0.f;       d[1][2] = cz * dzA;
+      d[2][0] = cx * dxB;  d[2][1] = -cy * dyA; d[2][2] = 0.f;
     }
-    // ---- Ey
-    if (fast || is_live(p.g, 1, i, j, k)) {
-      a0 = ORDER == 4 ? S::TA::at(sHx, y, tz, 0, -1) : 0.f; a1 = S::TA::at(sHx, y, tz, 0, 0);
-      a2 = S::TA::at(sHx, y, tz, 0, 1); a3 = ORDER == 4 ? S::TA::at(sHx, y, tz, 0, 2) : 0.f;
-      const float dzHx = dstencil<ORDER>(a0, a1, a2, a3);
-      const float dxHz = dstencil<ORDER>(qz[r][0], qz[r][1], qz[r][2], qz[r][3]);
-      float dif[3] = {-cx * dxHz, 0.f, cz * dzHx};
-      p.f[1][off] = e_node(p, ms, 1, mat_at(smat, 1, y, tz), i, j, k, ab, dif, own_at(so, 1, y, tz));
-    }
-    // ---- Ez
-    if (fast || is_live(p.g, 2, i, j, k)) {
-      const float dxHy = dstencil<ORDER>(qy[r][0], qy[r][1], qy[r][2], qy[r][3]);
-      a0 = ORDER == 4 ? S::TA::at(sHx, y, tz, -1, 0) : 0.f; a1 = S::TA::at(sHx, y, tz, 0, 0);
-      a2 = S::TA::at(sHx, y, tz, 1, 0); a3 = ORDER == 4 ? S::TA::at(sHx, y, tz, 2, 0) : 0.f;
-      const float dyHx = dstencil<ORDER>(a0, a1, a2, a3);
-      float dif[3] = {cx * dxHy, -cy * dyHx, 0.f};
-      p.f[2][off] = e_node(p, ms, 2, mat_at(smat, 2, y, tz), i, j, k, ab, dif, own_at(so, 2, y, tz));
+    const bool ab = tab && (inx || in_slab(p, 1, j) || in_slab(p, 2, k));
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      if (!SIMPLE && !fast && !is_live(p.g, cf + c, i, j, k)) continue;
+      float F = own_at(so, c, y, tz);
+      if (SIMPLE) {
+        if (!ISH) { d[c][0] *= iu[c]; d[c][1] *= iu[c]; d[c][2] *= iu[c]; }
+        p.f[cf + c][off] = F + (d[c][0] + d[c][1] + d[c][2]);
+        continue;
+      }
+      if (!ISH) {
+        const int m = um >= 0 ? um : mat_at(smat, c, y, tz);
+        if (tade && ms.npoles[m] > 0) {
+          const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
+          if (bi >= 0 && bi < p.ade.n[0] && bj >= 0 && bj < p.ade.n[1] && bk >= 0 && bk < p.ade.n[2]) {
+            const long long ai = ((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk;
+            p.f[c][off] = ade_update(p, c, m, ms.npoles[m], ai, d[c][0] + d[c][1] + d[c][2], F);
+            continue;
+          }
+        }
+        const float ie = ms.inv_eps[m][c];
+        d[c][0] *= ie; d[c][1] *= ie; d[c][2] *= ie;
+      }
+      float inc = d[c][0] + d[c][1] + d[c][2];
+      if (ab) inc += absorb_correction(p, cf + c, i, j, k, d[c]);
+      const float nv = F + inc;
+      p.f[cf + c][off] = nv;
     }
   }
 }

@@ -164,7 +164,9 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
     if (ipre <= last)
       stage_plane<ORDER, ISH, 0>(p, m, dsm + (ipre % NST) * P::STAGE, &bars[ipre % NST], ipre, j0, k0,
                                  yz_safe && plane_safe_x(p.g, ipre));
-    for (int q = 0; q <= AHEAD; q++) mbar_wait(&bars[(i + q) % NST], (unsigned)(((i + q - xa) / NST) & 1), p.err);
+    // planes i..i+AHEAD-1 were waited for in earlier iterations (all of them at the start)
+    for (int q = (i == xa ? 0 : AHEAD); q <= AHEAD; q++)
+      mbar_wait(&bars[(i + q) % NST], (unsigned)(((i + q - xa) / NST) & 1), p.err);
     __syncthreads();
     const bool fast = yz_in && i - 2 >= p.g.all_lo[0] && i + 2 <= p.g.all_hi[0];
 #pragma unroll
@@ -178,9 +180,12 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
       }
     }
     const float* cur = dsm + (i % NST) * P::STAGE;
-    if (ISH) h_plane<ORDER, 0>(p, i, j0, k0, cur, qb, qc, fast, cur + P::OFF_OWN);
-    else e_plane<ORDER, 0>(p, i, j0, k0, cur, qb, qc, fast, cur + P::OFF_OWN,
-                           reinterpret_cast<const uint8_t*>(cur + P::OFF_MAT), ms);
+    const int um = ISH ? 0 : (int)__ldg(p.umat + ((long long)i * p.nty + blockIdx.y) * p.ntz + blockIdx.x);
+    const uint8_t* cmat = reinterpret_cast<const uint8_t*>(cur + P::OFF_MAT);
+    if (fast && um >= 0 && !tile_absorber(p, i, j0, k0))
+      plane_update<ORDER, ISH, true>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um);
+    else
+      plane_update<ORDER, ISH, false>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um);
 #pragma unroll
     for (int r = 0; r < RY; r++)
 #pragma unroll

@@ -96,6 +96,7 @@ class Simulation:
         self.shape = (cfg.nx, cfg.ny, cfg.nz)
         self._dft = []
         self._nprobes = 0
+        self.probe_list = []
 
     def _ck(self, rc):
         if rc != abi.OK:
@@ -138,6 +139,7 @@ class Simulation:
         pid = C.c_int(-1)
         self._ck(self._L.dtmx_add_probe(self._h, comp, i, j, k, mode, C.byref(pid)))
         self._nprobes += 1
+        self.probe_list.append((comp, i, j, k, mode))
         return pid.value
 
     def add_dft_plane(self, axis, index, comp_mask, omegas):

@@ -531,7 +531,7 @@ static void half_step(osim* s, int isH) {
             si[a] = slab_index(s, a, i, j, k);
             if (si[a] >= 0) { ins[a] = 1; any = 1; }
           }
-          if (!any || cf->absorber == DTMX_ABS_NONE) { *F += dif[0] + dif[1] + dif[2]; continue; }
+          if (!any || cf->absorber == DTMX_ABS_NONE) { *F += (dif[0] + dif[1] + dif[2]); continue; }
           if (cf->absorber == DTMX_ABS_CPML) {
             real add = 0;
             for (int a = 0; a < 3; a++) {
