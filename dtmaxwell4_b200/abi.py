@@ -1,13 +1,15 @@
 """ctypes mirror of include/dtmx.h (the C ABI of the CUDA engine).
 
-Struct layouts here must match the header field for field; tests/test_abi.py
+Struct layouts here must match the header field for field; tests/test_cpu.py
 checks the sizes against the compiled library.
 """
 import ctypes as C
 
 ABI_VERSION = 1
 
-OK, ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_NONFINITE, ERR_TIMEOUT, ERR_STATE, ERR_UNSUPPORTED, ERR_NODEVICE = range(9)
+(OK, ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_NONFINITE, ERR_TIMEOUT, ERR_STATE, ERR_UNSUPPORTED, ERR_NODEVICE,
+ ERR_TOO_LARGE) = range(10)
+NOALLOC_MAX_ELEMS = 1 << 24
 EX, EY, EZ, HX, HY, HZ = range(6)
 COMP_NAMES = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 GEOM_BOX, GEOM_REFERENCE = 0, 1

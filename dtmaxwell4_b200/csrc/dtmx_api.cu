@@ -78,7 +78,8 @@ struct dtmx_ctx {
 };
 
 static const char* kErrStr[] = {"ok", "invalid argument", "CUDA error", "out of device memory", "non-finite value",
-                                "device wait timed out", "invalid state", "unsupported", "no CUDA device"};
+                                "device wait timed out", "invalid state", "unsupported", "no CUDA device",
+                                "input exceeds the fixed scratch size of the no-allocation entry point"};
 
 #define CK(call)                                                                           \
   do {                                                                                     \
@@ -111,7 +112,7 @@ static int dalloc(dtmx_ctx* ctx, T** p, size_t count) {
 
 extern "C" int dtmx_version(void) { return DTMX_ABI_VERSION; }
 extern "C" const char* dtmx_error_string(int code) {
-  if (code < 0 || code > 8) return "unknown";
+  if (code < 0 || code > 9) return "unknown";
   return kErrStr[code];
 }
 extern "C" const char* dtmx_last_error(const dtmx_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }

@@ -21,7 +21,7 @@ EXPORTS = (
     "dtmx_read_probes", "dtmx_add_dft_plane", "dtmx_read_dft", "dtmx_step", "dtmx_sync",
     "dtmx_get_step", "dtmx_get_field", "dtmx_set_field", "dtmx_field_device_ptr",
     "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_get_stream",
-    "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes",
+    "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
 )
 
 
@@ -68,6 +68,7 @@ def load():
     L.dtmx_set_profiling.argtypes = [vp, ip]
     L.dtmx_read_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     L.dtmx_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
+    L.dtmx_count_nonfinite_noalloc.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int64, C.POINTER(C.c_int64)]
     _lib = L
     return L
 
@@ -212,6 +213,13 @@ class Simulation:
         self._ck(self._L.dtmx_get_stream(self._h, C.byref(v)))
         return v.value
 
+    def device_ptr(self, comp):
+        """(device address, element strides (x, y, z)) of a field component."""
+        p = C.c_void_p()
+        st = (C.c_int64 * 3)()
+        self._ck(self._L.dtmx_field_device_ptr(self._h, comp, C.byref(p), st))
+        return p.value, (st[0], st[1], st[2])
+
     def set_profiling(self, on=True):
         self._ck(self._L.dtmx_set_profiling(self._h, 1 if on else 0))
 
@@ -225,3 +233,13 @@ def abi_sizes():
     out = (C.c_int64 * 4)()
     load().dtmx_abi_sizes(out)
     return tuple(out)
+
+
+def count_nonfinite_noalloc(device_ptrs, nelem):
+    """NaN/Inf count over caller-owned device float arrays, allocating no
+    device memory (see dtmx_count_nonfinite_noalloc in include/dtmx.h).
+    Returns (status, count)."""
+    arr = (C.c_void_p * len(device_ptrs))(*device_ptrs)
+    out = C.c_int64(-1)
+    rc = load().dtmx_count_nonfinite_noalloc(arr, len(device_ptrs), int(nelem), C.byref(out))
+    return rc, out.value

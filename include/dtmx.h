@@ -44,7 +44,8 @@ enum {
   DTMX_ERR_TIMEOUT = 5,      /* a bounded device wait gave up (flag set by a kernel) */
   DTMX_ERR_STATE = 6,        /* call not valid in the current state */
   DTMX_ERR_UNSUPPORTED = 7,  /* combination not implemented */
-  DTMX_ERR_NODEVICE = 8      /* no CUDA device visible */
+  DTMX_ERR_NODEVICE = 8,     /* no CUDA device visible */
+  DTMX_ERR_TOO_LARGE = 9     /* input larger than a fixed-size scratch allows */
 };
 
 /* ---- field components -------------------------------------------------- */
@@ -227,6 +228,22 @@ int  dtmx_read_profile(dtmx_ctx* ctx, double* ms_h, double* ms_e, int64_t* count
 /* sizeof of the ABI structs, in the order config, material, point_source,
  * tfsf (for binding checks). */
 int  dtmx_abi_sizes(int64_t out[4]);
+
+/* Count NaN/Inf values in nfields caller-owned device arrays of nelem floats
+ * each, without allocating any device memory (no cudaMalloc/cudaFree and no
+ * allocating library routine).  For callers that cannot allocate: processes
+ * whose device memory is reserved by another allocator, or health-check
+ * threads that must stay out of the allocator.  No counterpart in the
+ * reference.  The reduction's scratch is a fixed file-scope device array, so:
+ *   - nfields*nelem must not exceed DTMX_NOALLOC_MAX_ELEMS, else
+ *     DTMX_ERR_TOO_LARGE (nothing is launched);
+ *   - the first call on a device looks up that array's device address with the
+ *     device current; make that first call before any stream capture;
+ *   - calls whose work overlaps on the GPU race on the shared array.
+ * Kernels run on the legacy default stream and the count is copied back
+ * synchronously into *count_out. */
+#define DTMX_NOALLOC_MAX_ELEMS (1LL << 24)
+int  dtmx_count_nonfinite_noalloc(const float* const* d_fields, int nfields, int64_t nelem, int64_t* count_out);
 
 /* Engine choice for dtmx_step: 0 = auto, 1 = one launch per half step,
  * 2 = L2-resident wavefront (several time steps per launch). */
