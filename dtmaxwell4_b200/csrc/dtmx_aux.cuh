@@ -103,13 +103,23 @@ __global__ void tfsf_kernel(Params p, TfsfDev t, const long long* d_step, int is
     if (!is_live(p.g, c, i, j, k)) continue;
     const int idx[3] = {i, j, k};
     const int Xs[3] = {2 * i + comp_off(c, 0), 2 * j + comp_off(c, 1), 2 * k + comp_off(c, 2)};
-    const bool self_in = in_box(t, Xs[0], Xs[1], Xs[2]);
     int ax[2], gs[2];
     curl_terms(c, ax[0], gs[0], ax[1], gs[1]);
     double total = 0.0;
     bool any = false;
+    bool self_known = false, self_in = false;
     for (int term = 0; term < 2; term++) {
       const int a = ax[term], g = gs[term];
+      // the plane wave has only Ez and Hy incident components
+      if (t.kind == 1 && g != 2 && g != 4) continue;
+      // a tap along a crosses the surface only if the node lies inside the box
+      // range on the other two axes and within 3 half cells of a face along a
+      const int b1 = (a + 1) % 3, b2 = (a + 2) % 3;
+      const int gb1 = 2 * idx[b1] + comp_off(g, b1), gb2 = 2 * idx[b2] + comp_off(g, b2);
+      if (gb1 < t.lo[b1] || gb1 > t.hi[b1] || gb2 < t.lo[b2] || gb2 > t.hi[b2]) continue;
+      const int Xa = Xs[a];
+      if (!((Xa >= t.lo[a] - 4 && Xa <= t.lo[a] + 3) || (Xa >= t.hi[a] - 3 && Xa <= t.hi[a] + 4))) continue;
+      if (!self_known) { self_in = in_box(t, Xs[0], Xs[1], Xs[2]); self_known = true; }
       double v[4];
       bool hit = false;
       for (int q = 0; q < 4; q++) {

@@ -64,7 +64,7 @@ struct Pipe {
   // planes beyond i needed by plane i (x taps): H step order 4: +1; E step: +2 (order 4) / +1 (order 2)
   static constexpr int AHEAD = ISH ? (ORDER == 4 ? 1 : 0) : (ORDER == 4 ? 2 : 1);
   static constexpr int BEHIND = ISH ? (ORDER == 4 ? 2 : 1) : (ORDER == 4 ? 1 : 0);
-  static constexpr int LEAD = 2;                       // planes in flight beyond the resident ones
+  static constexpr int LEAD = ISH ? 2 : 1;             // planes in flight beyond the resident ones
   static constexpr int NST = AHEAD + 1 + LEAD;
   static constexpr int BASE = ISH ? 2 : 1;             // queue slot of plane i (dstencil taps v0..v3)
   static constexpr size_t SMEM_BYTES = (size_t)NST * STAGE * 4 + sizeof(MatShared) + NST * 8 + 128;
