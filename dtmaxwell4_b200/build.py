@@ -11,8 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdtmx.so")
-SOURCES = ["dtmx_api.cu", "dtmx_noalloc.cu"]
-DEPS = ["dtmx_api.cu", "dtmx_noalloc.cu", "dtmx_device.cuh", "dtmx_aux.cuh", "dtmx_stream.cuh"]
+SOURCES = ["dtmx_api.cu", "dtmx_noalloc.cu", "dtmx_ref_driver.cpp"]
+DEPS = ["dtmx_api.cu", "dtmx_noalloc.cu", "dtmx_ref_driver.cpp", "dtmx_device.cuh", "dtmx_aux.cuh", "dtmx_stream.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -902,9 +902,10 @@ extern "C" int dtmx_read_profile(dtmx_ctx* ctx, double* ms_h, double* ms_e, int6
   return DTMX_OK;
 }
 
-extern "C" int dtmx_abi_sizes(int64_t out[4]) {
+extern "C" int dtmx_abi_sizes(int64_t out[6]) {
   if (!out) return DTMX_ERR_INVALID;
   out[0] = sizeof(dtmx_config); out[1] = sizeof(dtmx_material);
   out[2] = sizeof(dtmx_point_source); out[3] = sizeof(dtmx_tfsf);
+  out[4] = sizeof(dtmx_tfsfsrc); out[5] = sizeof(dtmx_ref_globals);
   return DTMX_OK;
 }

@@ -22,6 +22,7 @@ EXPORTS = (
     "dtmx_get_step", "dtmx_get_field", "dtmx_set_field", "dtmx_field_device_ptr",
     "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_get_stream",
     "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
+    "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
 )
 
 
@@ -230,7 +231,7 @@ class Simulation:
 
 
 def abi_sizes():
-    out = (C.c_int64 * 4)()
+    out = (C.c_int64 * 6)()
     load().dtmx_abi_sizes(out)
     return tuple(out)
 

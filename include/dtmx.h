@@ -226,8 +226,48 @@ int  dtmx_set_profiling(dtmx_ctx* ctx, int enable);
 int  dtmx_read_profile(dtmx_ctx* ctx, double* ms_h, double* ms_e, int64_t* count);
 
 /* sizeof of the ABI structs, in the order config, material, point_source,
- * tfsf (for binding checks). */
-int  dtmx_abi_sizes(int64_t out[4]);
+ * tfsf, tfsfsrc, ref_globals (for binding checks). */
+int  dtmx_abi_sizes(int64_t out[6]);
+
+/* ---- the reference's driver surface (SWIG module DTmxw, mxw.i:1-36) ------ */
+
+/* TFSFsrc (py_consts.h:73-91): the shotpoint the Python driver fills in. */
+typedef struct dtmx_tfsfsrc {
+  double tStop;
+  double srcXs, srcXa, srcXv, sphR;
+  double BoxMs, BoxPs, BoxMa, BoxPa, BoxMv, BoxPv;
+  double V_max;
+  int start;
+  double wavelength, w, k, Omega, kEnv, theta, phi;
+  double cSrc, Imp;
+  double t0, tw, T;
+} dtmx_tfsfsrc;
+
+/* Compile-time constants of the reference (py_consts.h, params.h:44-62) as
+ * run-time values: grid in rags (x = 3*Np, y = 3*Na cells, z = Nv cells),
+ * window Ns and big-step length Ntime, steps, and the run length Tsteps. */
+typedef struct dtmx_ref_globals {
+  int Np, Na, Nv, Ns, Ntime;
+  double ds, da, dv, dt;
+  int Tsteps;
+} dtmx_ref_globals;
+
+/* TFSFsrc::set (signal.hpp:99-115). */
+void dtmx_tfsfsrc_set(dtmx_tfsfsrc* s, double c, double impedance, double lmb);
+
+/* Material index arrays (nx*ny*nz each, z fastest) of the reference's analytic
+ * geometry, get_mat_indev (defs.h:128-148): Ag film with a hole lattice,
+ * organic, ITO and glass layers; indices into dtmx_ref_material_table. */
+int  dtmx_ref_materials(const dtmx_ref_globals* g, uint8_t* idx_x, uint8_t* idx_y, uint8_t* idx_z);
+/* Their material table (init_material, DTmxw.cu:604-635); returns the count. */
+int  dtmx_ref_material_table(dtmx_material* out, int n);
+
+/* The reference's _main with --test (DTmxw.cu:731-834): reference geometry
+ * (get_mat_indev, defs.h:128-148) and materials (init_material), split PML,
+ * TF/SF dipole from the shotpoint, the default sensor line of init_index
+ * written to <drop_dir>/<fld>-xXXXXXyYYYYYzZZZZZ.dat once per Ntime steps, and
+ * Tsteps/Ntime calls of dtmx_step(Ntime) (calcStep).  Returns 0 on success. */
+int  dtmx_ref_main(const dtmx_ref_globals* g, const dtmx_tfsfsrc* shotpoint, int argc, char** argv);
 
 /* Count NaN/Inf values in nfields caller-owned device arrays of nelem floats
  * each, without allocating any device memory (no cudaMalloc/cudaFree and no

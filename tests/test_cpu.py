@@ -28,10 +28,10 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_struct_sizes_match_bindings():
-    from dtmaxwell4_b200 import abi, engine
+    from dtmaxwell4_b200 import DTmxw, abi, engine
     sizes = engine.abi_sizes()
     assert sizes == (ctypes.sizeof(abi.Config), ctypes.sizeof(abi.Material), ctypes.sizeof(abi.PointSource),
-                     ctypes.sizeof(abi.TFSF))
+                     ctypes.sizeof(abi.TFSF), ctypes.sizeof(DTmxw.TFSFsrc), ctypes.sizeof(DTmxw.RefGlobals))
 
 
 def test_no_device_fails_loudly():
