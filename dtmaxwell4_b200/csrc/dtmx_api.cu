@@ -16,6 +16,7 @@
 #include "dtmx.h"
 #include "dtmx_device.cuh"
 #include "dtmx_aux.cuh"
+#include "dtmx_torre.cuh"
 
 using namespace dtmx;
 
@@ -24,6 +25,9 @@ struct DftHost {
   int ncomp;
   double* omega = nullptr;
   double2* acc = nullptr;
+  float* stage = nullptr;
+  long long* sstep = nullptr;
+  int nstaged = 0;          // samples staged since the last flush
 };
 
 struct dtmx_ctx {
@@ -73,6 +77,10 @@ struct dtmx_ctx {
   int engine = 0, tblock = 0;
   TmaMaps maps{};
   int* d_err = nullptr;
+  // wavefront engine
+  TorreMaps tmaps{};
+  bool tmaps_ok = false;
+  int* d_ctr = nullptr;
   signed char* d_umat = nullptr;
   std::string err;
 };
@@ -389,7 +397,7 @@ extern "C" void dtmx_destroy(dtmx_ctx* ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* p : ctx->allocs) cudaFree(p);
-  for (auto& d : ctx->dfts) { cudaFree(d.omega); cudaFree(d.acc); }
+  for (auto& d : ctx->dfts) { cudaFree(d.omega); cudaFree(d.acc); cudaFree(d.stage); cudaFree(d.sstep); }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -568,32 +576,37 @@ extern "C" int dtmx_set_tfsf(dtmx_ctx* ctx, const dtmx_tfsf* s) {
   for (int a = 0; a < 3; a++) { T.ctr[a] = (s->box_lo[a] + s->box_hi[a]) * 0.5; T.hd[a] = d[a] * 0.5; }
   T.dt = c.dt; T.c = s->c; T.w = s->w; T.kenv = s->kenv; T.tstop = s->tstop;
   T.ntime = s->ntime > 0 ? s->ntime : 1;
-  // shell regions: expanded box E minus inner box I, as 6 disjoint slabs
-  int e[3][2], in_[3][2];
-  bool has_inner = true;
-  for (int a = 0; a < 3; a++) {
-    e[a][0] = (int)std::floor((T.lo[a] - 4) / 2.0);
-    e[a][1] = (int)std::floor((T.hi[a] + 4) / 2.0);
-    in_[a][0] = e[a][0] + 5;
-    in_[a][1] = e[a][1] - 5;
-    if (in_[a][0] > in_[a][1]) has_inner = false;
-  }
-  T.nreg = 0;
-  auto add = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
-    if (x0 > x1 || y0 > y1 || z0 > z1) return;
-    int r = T.nreg++;
-    T.reg[r][0][0] = x0; T.reg[r][0][1] = x1; T.reg[r][1][0] = y0; T.reg[r][1][1] = y1; T.reg[r][2][0] = z0; T.reg[r][2][1] = z1;
-    T.reg_cells[r] = (long long)(x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1);
-  };
-  if (!has_inner) {
-    add(e[0][0], e[0][1], e[1][0], e[1][1], e[2][0], e[2][1]);
-  } else {
-    add(e[0][0], in_[0][0] - 1, e[1][0], e[1][1], e[2][0], e[2][1]);
-    add(in_[0][1] + 1, e[0][1], e[1][0], e[1][1], e[2][0], e[2][1]);
-    add(in_[0][0], in_[0][1], e[1][0], in_[1][0] - 1, e[2][0], e[2][1]);
-    add(in_[0][0], in_[0][1], in_[1][1] + 1, e[1][1], e[2][0], e[2][1]);
-    add(in_[0][0], in_[0][1], in_[1][0], in_[1][1], e[2][0], in_[2][0] - 1);
-    add(in_[0][0], in_[0][1], in_[1][0], in_[1][1], in_[2][1] + 1, e[2][1]);
+  // correction jobs: per half step, component and curl term (axis a, source
+  // component g), the nodes within 3 half cells of each face along a whose g
+  // taps lie inside the box range on the other two axes
+  for (int hs = 0; hs < 2; hs++) {
+    T.njob[hs] = 0;
+    for (int comp = hs * 3; comp < hs * 3 + 3; comp++) {
+      int ax[2], gs[2];
+      curl_terms(comp, ax[0], gs[0], ax[1], gs[1]);
+      for (int term = 0; term < 2; term++) {
+        const int a = ax[term], g = gs[term];
+        if (s->kind == DTMX_TFSF_PLANE_X && g != 2 && g != 4) continue;
+        for (int side = 0; side < 2; side++) {
+          TfsfJob jb{};
+          jb.c = comp;
+          bool empty = false;
+          for (int b = 0; b < 3; b++) {
+            int X0, X1, o;
+            if (b == a) { X0 = side ? T.hi[a] - 3 : T.lo[a] - 4; X1 = side ? T.hi[a] + 4 : T.lo[a] + 3; o = comp_off(comp, a); }
+            else { X0 = T.lo[b]; X1 = T.hi[b]; o = comp_off(g, b); }
+            // indices v with X0 <= 2v + o <= X1, clipped to the grid
+            int v0 = (int)std::ceil((X0 - o) / 2.0), v1 = (int)std::floor((X1 - o) / 2.0);
+            v0 = std::max(v0, 0); v1 = std::min(v1, n[b] - 1);
+            if (v0 > v1) empty = true;
+            jb.lo[b] = v0; jb.hi[b] = v1;
+          }
+          if (empty) continue;
+          jb.cells = (long long)(jb.hi[0] - jb.lo[0] + 1) * (jb.hi[1] - jb.lo[1] + 1) * (jb.hi[2] - jb.lo[2] + 1);
+          T.job[hs][T.njob[hs]++] = jb;
+        }
+      }
+    }
   }
   if (s->kind == DTMX_TFSF_PLANE_X) {
     T.line_M = 4096;
@@ -648,21 +661,36 @@ extern "C" int dtmx_add_dft_plane(dtmx_ctx* ctx, int axis, int index, int comp_m
   h.ncomp = __builtin_popcount(comp_mask);
   const size_t nacc = (size_t)h.ncomp * nfreq * h.d.n1 * h.d.n2;
   if (cudaMalloc(&h.omega, nfreq * sizeof(double)) != cudaSuccess) return fail(ctx, DTMX_ERR_OOM, "DFT allocation");
-  if (cudaMalloc(&h.acc, nacc * sizeof(double2)) != cudaSuccess) { cudaFree(h.omega); return fail(ctx, DTMX_ERR_OOM, "DFT allocation"); }
+  const size_t nstage = (size_t)DFT_STAGE * h.ncomp * h.d.n1 * h.d.n2;
+  if (cudaMalloc(&h.acc, nacc * sizeof(double2)) != cudaSuccess || cudaMalloc(&h.stage, nstage * sizeof(float)) != cudaSuccess ||
+      cudaMalloc(&h.sstep, DFT_STAGE * sizeof(long long)) != cudaSuccess) {
+    cudaFree(h.omega); cudaFree(h.acc); cudaFree(h.stage); cudaFree(h.sstep);
+    return fail(ctx, DTMX_ERR_OOM, "DFT allocation");
+  }
   CK(cudaMemsetAsync(h.acc, 0, nacc * sizeof(double2), ctx->stream));
   CK(cudaMemcpyAsync(h.omega, omegas, nfreq * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  h.d.omega = h.omega; h.d.acc = h.acc;
+  h.d.omega = h.omega; h.d.acc = h.acc; h.d.stage = h.stage; h.d.sstep = h.sstep;
   ctx->dfts.push_back(h);
   CK(cudaStreamSynchronize(ctx->stream));
   if (id_out) *id_out = (int)ctx->dfts.size() - 1;
   return DTMX_OK;
 }
 
+// fold the staged samples of one DFT plane into its accumulators
+static void dft_flush(dtmx_ctx* ctx, DftHost& h) {
+  if (h.nstaged == 0) return;
+  const long long npts = (long long)h.d.n1 * h.d.n2;
+  dft_flush_kernel<<<(unsigned)((npts + 255) / 256), 256, 0, ctx->stream>>>(h.d, h.nstaged, ctx->cfg.dt);
+  ctx->launches++;
+  h.nstaged = 0;
+}
+
 extern "C" int dtmx_read_dft(dtmx_ctx* ctx, int id, double* out, size_t out_len) {
   if (!ctx || id < 0 || id >= (int)ctx->dfts.size() || !out) return fail(ctx, DTMX_ERR_INVALID, "bad DFT id");
-  const DftHost& h = ctx->dfts[id];
+  DftHost& h = ctx->dfts[id];
   const size_t n = (size_t)h.ncomp * h.d.nfreq * h.d.n1 * h.d.n2 * 2;
   if (out_len < n) return fail(ctx, DTMX_ERR_INVALID, "output buffer too small");
+  dft_flush(ctx, h);
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaMemcpy(out, h.acc, n * sizeof(double), cudaMemcpyDeviceToHost));
   return DTMX_OK;
@@ -706,13 +734,15 @@ static int launch_step(dtmx_ctx* ctx) {
   else h_kernel<2><<<grd, blk, Pipe<2, true>::SMEM_BYTES, st>>>(P, ctx->maps);
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
   nl++;
-  dim3 tgrid;
+  dim3 tgrid[2];
+  for (int hs = 0; hs < 2 && ctx->has_tfsf; hs++) {
+    long long mx = 1;
+    for (int r = 0; r < ctx->T.njob[hs]; r++) mx = std::max(mx, ctx->T.job[hs][r].cells);
+    tgrid[hs] = dim3((unsigned)((mx + 255) / 256), std::max(1, ctx->T.njob[hs]));
+  }
   if (ctx->has_tfsf) {
-    long long mx = 0;
-    for (int r = 0; r < ctx->T.nreg; r++) mx = std::max(mx, ctx->T.reg_cells[r]);
-    tgrid = dim3((unsigned)((mx + 255) / 256), ctx->T.nreg);
-    if (o4) tfsf_kernel<4><<<tgrid, 256, 0, st>>>(P, ctx->T, ctx->d_step, 1);
-    else tfsf_kernel<2><<<tgrid, 256, 0, st>>>(P, ctx->T, ctx->d_step, 1);
+    if (o4) tfsf_kernel<4><<<tgrid[1], 256, 0, st>>>(P, ctx->T, ctx->d_step, 1);
+    else tfsf_kernel<2><<<tgrid[1], 256, 0, st>>>(P, ctx->T, ctx->d_step, 1);
     nl++;
   }
   const double r1 = c.dt / c.dx;
@@ -739,8 +769,8 @@ static int launch_step(dtmx_ctx* ctx) {
     nl++;
   }
   if (ctx->has_tfsf) {
-    if (o4) tfsf_kernel<4><<<tgrid, 256, 0, st>>>(P, ctx->T, ctx->d_step, 0);
-    else tfsf_kernel<2><<<tgrid, 256, 0, st>>>(P, ctx->T, ctx->d_step, 0);
+    if (o4) tfsf_kernel<4><<<tgrid[0], 256, 0, st>>>(P, ctx->T, ctx->d_step, 0);
+    else tfsf_kernel<2><<<tgrid[0], 256, 0, st>>>(P, ctx->T, ctx->d_step, 0);
     nl++;
   }
   if (pw) {
@@ -757,8 +787,9 @@ static int launch_step(dtmx_ctx* ctx) {
   }
   for (auto& d : ctx->dfts) {
     const long long npts = (long long)d.d.n1 * d.d.n2;
-    dft_kernel<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(P, d.d, ctx->d_step, c.dt);
+    dft_capture_kernel<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(P, d.d, ctx->d_step, d.nstaged);
     nl++;
+    if (++d.nstaged == DFT_STAGE) dft_flush(ctx, d);
   }
   advance_step_kernel<<<1, 1, 0, st>>>(ctx->d_step);
   nl++;
@@ -781,17 +812,129 @@ static int prepare(dtmx_ctx* ctx) {
     if ((rc = dalloc(ctx, &ctx->d_traces, ctx->probes.size() * (size_t)ctx->probe_cap))) return rc;
   }
   if (ctx->has_tfsf && ctx->h_mat[0].size()) {
+    // every E node that gets a correction, and the E nodes next to them, must be non-dispersive
     const TfsfDev& T = ctx->T;
-    for (int r = 0; r < T.nreg; r++)
-      for (int i = T.reg[r][0][0]; i <= T.reg[r][0][1]; i++)
-        for (int j = T.reg[r][1][0]; j <= T.reg[r][1][1]; j++)
-          for (int k = T.reg[r][2][0]; k <= T.reg[r][2][1]; k++)
+    for (int r = 0; r < T.njob[0]; r++) {
+      const TfsfJob& jb = T.job[0][r];
+      for (int i = std::max(0, jb.lo[0] - 1); i <= std::min(ctx->cfg.nx - 1, jb.hi[0] + 1); i++)
+        for (int j = std::max(0, jb.lo[1] - 1); j <= std::min(ctx->cfg.ny - 1, jb.hi[1] + 1); j++)
+          for (int k = std::max(0, jb.lo[2] - 1); k <= std::min(ctx->cfg.nz - 1, jb.hi[2] + 1); k++)
             for (int comp = 0; comp < 3; comp++)
               if (ctx->mats[ctx->h_mat[comp][store_index(ctx, i, j, k)]].npoles > 0)
                 return fail(ctx, DTMX_ERR_UNSUPPORTED, "dispersive material on the TF/SF surface");
+    }
   }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->prepared = true;
+  return DTMX_OK;
+}
+
+// ---------------------------------------------------------------- wavefront engine
+constexpr int TORRE_TY = 32;
+
+static int build_torre_maps(dtmx_ctx* ctx) {
+  if (ctx->tmaps_ok) return DTMX_OK;
+  const int R2 = ctx->cfg.order - 1, TY = TORRE_TY;
+  TorreMaps& m = ctx->tmaps;
+  int rc;
+  for (int h = 0; h < 2; h++) {
+    const int c0 = 3 * h;
+    if ((rc = make_map(ctx, &m.A[h], ctx->P.f[c0], false, 40, TY + R2))) return rc;
+    if ((rc = make_map(ctx, &m.B[h], ctx->P.f[c0 + 1], false, 40, TY))) return rc;
+    if ((rc = make_map(ctx, &m.C[h], ctx->P.f[c0 + 2], false, 32, TY + R2))) return rc;
+  }
+  for (int c = 0; c < 6; c++)
+    if ((rc = make_map(ctx, &m.core[c], ctx->P.f[c], false, 32, TY))) return rc;
+  for (int c = 0; c < 3; c++)
+    if ((rc = make_map(ctx, &m.mat[c], ctx->d_mat[c], true, 32, TY))) return rc;
+  ctx->tmaps_ok = true;
+  return DTMX_OK;
+}
+
+using TorreFn = void (*)(const Params, const TorreMaps, const TorreArgs);
+
+static TorreFn torre_fn(int order, int T, size_t* smem, int* nthr) {
+  constexpr int TY = TORRE_TY;
+#define DTMX_TORRE_CASE(O, TT)                                                         \
+  if (order == O && T == TT) {                                                          \
+    *smem = TorreLayout<O, TY>::SMEM; *nthr = TorreLayout<O, TY>::NTHR;                 \
+    return torre_kernel<O, 2 * TT, TY>;                                                 \
+  }
+  DTMX_TORRE_CASE(2, 1) DTMX_TORRE_CASE(2, 2) DTMX_TORRE_CASE(2, 3) DTMX_TORRE_CASE(2, 4)
+  DTMX_TORRE_CASE(4, 1) DTMX_TORRE_CASE(4, 2)
+#undef DTMX_TORRE_CASE
+  return nullptr;
+}
+
+// Can the wavefront engine run this context with T steps per launch?
+static bool torre_usable(dtmx_ctx* ctx, int T, std::string* why) {
+  const dtmx_config& c = ctx->cfg;
+  size_t smem = 0;
+  int nthr = 0;
+  TorreFn fn = torre_fn(c.order, T, &smem, &nthr);
+  if (!fn) { *why = "no kernel for order " + std::to_string(c.order) + " with " + std::to_string(T) + " steps per launch"; return false; }
+  if (c.geometry != DTMX_GEOM_BOX) { *why = "needs the box geometry"; return false; }
+  if (c.absorber == DTMX_ABS_SPLIT_PML) { *why = "split PML is not supported"; return false; }
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    *why = "shared memory attribute refused";
+    return false;
+  }
+  int per_sm = 0, nsm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, nthr, smem) != cudaSuccess ||
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->dev) != cudaSuccess) {
+    cudaGetLastError();
+    *why = "occupancy query failed";
+    return false;
+  }
+  const long long tiles = (long long)((c.nz + TT_Z - 1) / TT_Z) * ((c.ny + TORRE_TY - 1) / TORRE_TY);
+  if (tiles > (long long)per_sm * nsm) {
+    *why = std::to_string(tiles) + " tiles exceed the " + std::to_string(per_sm * nsm) + " co-resident CTAs";
+    return false;
+  }
+  return true;
+}
+
+// features the wavefront engine does not carry inside its launch
+static bool torre_features_ok(const dtmx_ctx* ctx, std::string* why) {
+  if (ctx->has_tfsf) { *why = "TF/SF source"; return false; }
+  if (!ctx->psrc.empty()) { *why = "point sources"; return false; }
+  if (!ctx->probes.empty()) { *why = "probes"; return false; }
+  if (!ctx->dfts.empty()) { *why = "DFT planes"; return false; }
+  return true;
+}
+
+__global__ void advance_step_by_kernel(long long* d_step, int n) { *d_step += n; }
+
+static int launch_torre(dtmx_ctx* ctx, int T) {
+  const dtmx_config& c = ctx->cfg;
+  int rc = build_torre_maps(ctx);
+  if (rc) return rc;
+  size_t smem = 0;
+  int nthr = 0;
+  TorreFn fn = torre_fn(c.order, T, &smem, &nthr);
+  const int ntz = (c.nz + TT_Z - 1) / TT_Z, nty = (c.ny + TORRE_TY - 1) / TORRE_TY;
+  if (!ctx->d_ctr && (rc = dalloc(ctx, &ctx->d_ctr, (size_t)ntz * nty))) return rc;
+  CK(cudaMemsetAsync(ctx->d_ctr, 0, sizeof(int) * ntz * nty, ctx->stream));
+  Params P = ctx->P;
+  P.x0 = 0; P.x1 = c.nx;
+  TorreArgs ta;
+  ta.ctr = ctx->d_ctr; ta.ntz = ntz; ta.nty = nty;
+  ta.nsteps = c.nx + (c.order == 4 ? TorreGeom<4>::off(2 * T - 1) : TorreGeom<2>::off(2 * T - 1));
+  void* args[] = {(void*)&P, (void*)&ctx->tmaps, (void*)&ta};
+  if (ctx->profiling) cudaEventRecord(ctx->ev[0], ctx->stream);
+  cudaError_t e = cudaLaunchCooperativeKernel((const void*)fn, dim3(ntz, nty), dim3(nthr), args, smem, ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, DTMX_ERR_CUDA, std::string("wavefront launch: ") + cudaGetErrorString(e));
+  if (ctx->profiling) {
+    cudaEventRecord(ctx->ev[1], ctx->stream);
+    cudaEventSynchronize(ctx->ev[1]);
+    float a = 0;
+    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+    ctx->prof_ms_h += a; ctx->prof_count += T;
+  }
+  advance_step_by_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_step, T);
+  ctx->launches += 2;
+  ctx->step += T;
   return DTMX_OK;
 }
 
@@ -799,7 +942,17 @@ extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
   if (!ctx || nsteps < 0) return fail(ctx, DTMX_ERR_INVALID, "bad step count");
   int rc0 = prepare(ctx);
   if (rc0) return rc0;
-  for (int s = 0; s < nsteps; s++) {
+  int left = nsteps;
+  if (ctx->engine == 2) {
+    std::string why;
+    if (!torre_features_ok(ctx, &why)) return fail(ctx, DTMX_ERR_UNSUPPORTED, "wavefront engine: " + why);
+    while (left >= ctx->tblock) {
+      int rc = launch_torre(ctx, ctx->tblock);
+      if (rc) return rc;
+      left -= ctx->tblock;
+    }
+  }
+  for (int s = 0; s < left; s++) {
     int rc = launch_step(ctx);
     if (rc) return rc;
     ctx->step++;
@@ -812,6 +965,13 @@ extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
 extern "C" int dtmx_sync(dtmx_ctx* ctx) {
   if (!ctx) return DTMX_ERR_INVALID;
   CK(cudaStreamSynchronize(ctx->stream));
+  int err = 0;
+  CK(cudaMemcpy(&err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) {
+    CK(cudaMemset(ctx->d_err, 0, sizeof(int)));
+    return fail(ctx, DTMX_ERR_TIMEOUT, err == 2 ? "a wavefront tile waited too long for its neighbours"
+                                                : "a staged load did not arrive in time");
+  }
   return DTMX_OK;
 }
 
@@ -870,8 +1030,15 @@ extern "C" int dtmx_kernel_launches(const dtmx_ctx* ctx, int64_t* n) {
 
 extern "C" int dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block) {
   if (!ctx || engine < 0 || engine > 2 || time_block < 0) return fail(ctx, DTMX_ERR_INVALID, "bad engine");
-  if (engine == 2) return fail(ctx, DTMX_ERR_UNSUPPORTED, "wavefront engine not built");
-  ctx->engine = engine; ctx->tblock = time_block;
+  if (engine == 2) {
+    const int T = time_block > 0 ? time_block : 2;
+    std::string why;
+    if (!torre_usable(ctx, T, &why)) return fail(ctx, DTMX_ERR_UNSUPPORTED, "wavefront engine: " + why);
+    ctx->tblock = T;
+  } else {
+    ctx->tblock = time_block;
+  }
+  ctx->engine = engine;
   return DTMX_OK;
 }
 

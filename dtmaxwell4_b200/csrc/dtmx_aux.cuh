@@ -6,6 +6,15 @@
 
 namespace dtmx {
 
+// One TF/SF correction job: component c over an index box that holds every
+// node of c whose taps along one curl axis cross one face of the box.
+struct TfsfJob {
+  int c;
+  int lo[3], hi[3];
+  long long cells;
+};
+constexpr int MAX_TFSF_JOBS = 12;    // 3 components x 2 curl terms x 2 faces
+
 struct TfsfDev {
   int active_cfg;            // a TF/SF source is configured
   int kind;                  // 0 dipole, 1 plane +x
@@ -15,9 +24,8 @@ struct TfsfDev {
   double dt, c, w, kenv, tstop;
   int ntime;
   const double* line_e; const double* line_h; int line_M, line_n;
-  int nreg;
-  int reg[6][3][2];          // disjoint cell regions covering the box surface shell
-  long long reg_cells[6];
+  int njob[2];               // [0] E half step, [1] H half step
+  TfsfJob job[2][MAX_TFSF_JOBS];
 };
 
 __device__ __forceinline__ bool tfsf_on(const TfsfDev& t, long long n) {
@@ -68,7 +76,7 @@ __device__ __forceinline__ double incident(const TfsfDev& t, int g, int X, int Y
 }
 
 // curl terms of component c: {axis, source component} for (+) and (-) terms
-__device__ __forceinline__ void curl_terms(int c, int& a0, int& g0, int& a1, int& g1) {
+__host__ __device__ __forceinline__ void curl_terms(int c, int& a0, int& g0, int& a1, int& g1) {
   switch (c) {
     case 0: a0 = 1; g0 = 5; a1 = 2; g1 = 4; break;
     case 1: a0 = 2; g0 = 3; a1 = 0; g1 = 5; break;
@@ -82,74 +90,90 @@ __device__ __forceinline__ void curl_terms(int c, int& a0, int& g0, int& a1, int
 // TF/SF correction of one half step (genAlg.py:209-234): a tap that crosses
 // the box surface gets +inc when the updated node is outside and the tap
 // inside, -inc in the opposite case.  The update is linear in the taps, so
-// the correction is added after the bulk update as dt/d * D(corrections).
+// the correction is added after the bulk update as dt/d * D(corrections),
+// summed over both curl terms of the node in double precision.
+template <int ORDER>
+__device__ __forceinline__ bool tfsf_node(const Params& p, const TfsfDev& t, int c, int i, int j, int k, bool isH,
+                                          double tt, double& total) {
+  const int t0 = isH ? -2 : -1;
+  const int idx[3] = {i, j, k};
+  const int Xs[3] = {2 * i + comp_off(c, 0), 2 * j + comp_off(c, 1), 2 * k + comp_off(c, 2)};
+  int ax[2], gs[2];
+  curl_terms(c, ax[0], gs[0], ax[1], gs[1]);
+  total = 0.0;
+  bool any = false;
+  bool self_known = false, self_in = false;
+  for (int term = 0; term < 2; term++) {
+    const int a = ax[term], g = gs[term];
+    // the plane wave has only Ez and Hy incident components
+    if (t.kind == 1 && g != 2 && g != 4) continue;
+    // a tap along a crosses the surface only if the node lies inside the box
+    // range on the other two axes and within 3 half cells of a face along a
+    const int b1 = (a + 1) % 3, b2 = (a + 2) % 3;
+    const int gb1 = 2 * idx[b1] + comp_off(g, b1), gb2 = 2 * idx[b2] + comp_off(g, b2);
+    if (gb1 < t.lo[b1] || gb1 > t.hi[b1] || gb2 < t.lo[b2] || gb2 > t.hi[b2]) continue;
+    const int Xa = Xs[a];
+    if (!((Xa >= t.lo[a] - 4 && Xa <= t.lo[a] + 3) || (Xa >= t.hi[a] - 3 && Xa <= t.hi[a] + 4))) continue;
+    if (!self_known) { self_in = in_box(t, Xs[0], Xs[1], Xs[2]); self_known = true; }
+    double v[4];
+    bool hit = false;
+    for (int q = 0; q < 4; q++) {
+      v[q] = 0.0;
+      if (ORDER == 2 && (q == 0 || q == 3)) continue;
+      int m[3] = {idx[0], idx[1], idx[2]};
+      m[a] += t0 + q;
+      const int TX = 2 * m[0] + comp_off(g, 0), TY_ = 2 * m[1] + comp_off(g, 1), TZ_ = 2 * m[2] + comp_off(g, 2);
+      const bool tin = in_box(t, TX, TY_, TZ_);
+      if (tin != self_in) {
+        const double inc = incident(t, g, TX, TY_, TZ_, tt);
+        v[q] = self_in ? -inc : inc;
+        hit = true;
+      }
+    }
+    if (!hit) continue;
+    any = true;
+    double sg = term == 0 ? 1.0 : -1.0;
+    if (isH) sg = -sg;
+    const double dv = ORDER == 2 ? v[2] - v[1] : (27.0 * (v[2] - v[1]) - (v[3] - v[0])) / 24.0;
+    total += sg * (double)p.cdt[a] * dv;
+  }
+  return any;
+}
+
+__device__ __forceinline__ bool in_job(const TfsfJob& jb, int i, int j, int k) {
+  return i >= jb.lo[0] && i <= jb.hi[0] && j >= jb.lo[1] && j <= jb.hi[1] && k >= jb.lo[2] && k <= jb.hi[2];
+}
+
+// One thread per node of a job (blockIdx.y); a node that also lies in an
+// earlier job of the same component is left to that job, so every node is
+// corrected exactly once with the sum of all its crossing taps.
 template <int ORDER>
 __global__ void tfsf_kernel(Params p, TfsfDev t, const long long* d_step, int isH) {
   const long long n = *d_step;
   if (!tfsf_on(t, n)) return;
+  const int hs = isH ? 1 : 0;
   const int r = blockIdx.y;
+  if (r >= t.njob[hs]) return;
+  const TfsfJob& jb = t.job[hs][r];
   const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (r >= t.nreg || cell >= t.reg_cells[r]) return;
-  const int ex = t.reg[r][0][1] - t.reg[r][0][0] + 1, ey = t.reg[r][1][1] - t.reg[r][1][0] + 1,
-            ez = t.reg[r][2][1] - t.reg[r][2][0] + 1;
-  (void)ex;
-  const int i = t.reg[r][0][0] + (int)(cell / ((long long)ey * ez));
-  const int j = t.reg[r][1][0] + (int)((cell / ez) % ey);
-  const int k = t.reg[r][2][0] + (int)(cell % ez);
+  if (cell >= jb.cells) return;
+  const int ey = jb.hi[1] - jb.lo[1] + 1, ez = jb.hi[2] - jb.lo[2] + 1;
+  const int i = jb.lo[0] + (int)(cell / ((long long)ey * ez));
+  const int j = jb.lo[1] + (int)((cell / ez) % ey);
+  const int k = jb.lo[2] + (int)(cell % ez);
+  const int c = jb.c;
+  if (!is_live(p.g, c, i, j, k)) return;
+  for (int q = 0; q < r; q++)
+    if (t.job[hs][q].c == c && in_job(t.job[hs][q], i, j, k)) return;
   const double tt = isH ? (double)n : (double)n + 0.5;
-  const int cbeg = isH ? 3 : 0;
-  const int t0 = isH ? -2 : -1;
-  for (int c = cbeg; c < cbeg + 3; c++) {
-    if (!is_live(p.g, c, i, j, k)) continue;
-    const int idx[3] = {i, j, k};
-    const int Xs[3] = {2 * i + comp_off(c, 0), 2 * j + comp_off(c, 1), 2 * k + comp_off(c, 2)};
-    int ax[2], gs[2];
-    curl_terms(c, ax[0], gs[0], ax[1], gs[1]);
-    double total = 0.0;
-    bool any = false;
-    bool self_known = false, self_in = false;
-    for (int term = 0; term < 2; term++) {
-      const int a = ax[term], g = gs[term];
-      // the plane wave has only Ez and Hy incident components
-      if (t.kind == 1 && g != 2 && g != 4) continue;
-      // a tap along a crosses the surface only if the node lies inside the box
-      // range on the other two axes and within 3 half cells of a face along a
-      const int b1 = (a + 1) % 3, b2 = (a + 2) % 3;
-      const int gb1 = 2 * idx[b1] + comp_off(g, b1), gb2 = 2 * idx[b2] + comp_off(g, b2);
-      if (gb1 < t.lo[b1] || gb1 > t.hi[b1] || gb2 < t.lo[b2] || gb2 > t.hi[b2]) continue;
-      const int Xa = Xs[a];
-      if (!((Xa >= t.lo[a] - 4 && Xa <= t.lo[a] + 3) || (Xa >= t.hi[a] - 3 && Xa <= t.hi[a] + 4))) continue;
-      if (!self_known) { self_in = in_box(t, Xs[0], Xs[1], Xs[2]); self_known = true; }
-      double v[4];
-      bool hit = false;
-      for (int q = 0; q < 4; q++) {
-        v[q] = 0.0;
-        if (ORDER == 2 && (q == 0 || q == 3)) continue;
-        int m[3] = {idx[0], idx[1], idx[2]};
-        m[a] += t0 + q;
-        const int TX = 2 * m[0] + comp_off(g, 0), TY_ = 2 * m[1] + comp_off(g, 1), TZ_ = 2 * m[2] + comp_off(g, 2);
-        const bool tin = in_box(t, TX, TY_, TZ_);
-        if (tin != self_in) {
-          const double inc = incident(t, g, TX, TY_, TZ_, tt);
-          v[q] = self_in ? -inc : inc;
-          hit = true;
-        }
-      }
-      if (!hit) continue;
-      any = true;
-      double sg = term == 0 ? 1.0 : -1.0;
-      if (isH) sg = -sg;
-      const double dv = ORDER == 2 ? v[2] - v[1] : (27.0 * (v[2] - v[1]) - (v[3] - v[0])) / 24.0;
-      total += sg * (double)p.cdt[a] * dv;
-    }
-    if (!any) continue;
-    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
-    if (!isH) {
-      const int mi = p.mat[c] ? (int)p.mat[c][id] : 0;
-      total *= (double)p.mt->inv_eps[mi][c];
-    }
-    p.f[c][id] += (float)total;
+  double total;
+  if (!tfsf_node<ORDER>(p, t, c, i, j, k, isH, tt, total)) return;
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+  if (!isH) {
+    const int mi = p.mat[c] ? (int)p.mat[c][id] : 0;
+    total *= (double)p.mt->inv_eps[mi][c];
   }
+  p.f[c][id] += (float)total;
 }
 
 // 1-D incident line (Ez at odd X, Hy at even X), same stencil and time step.
@@ -237,23 +261,21 @@ struct DftDev {
   int axis, index, comp_mask, nfreq, n1, n2;
   const double* omega;
   double2* acc;             // [ncomp][nfreq][n1*n2]
+  float* stage;             // [DFT_STAGE][ncomp][n1*n2] plane samples not yet accumulated
+  long long* sstep;         // [DFT_STAGE] step number s of each staged sample
 };
+constexpr int DFT_STAGE = 16;
 
 // Running DFT with FP64 accumulators: acc += f(t) exp(-i w t) dt, t = s*dt for E,
-// (s-1/2)*dt for H, s = steps completed.
-__global__ void dft_kernel(Params p, DftDev d, const long long* d_step, double dt) {
-  __shared__ double2 phE[64], phH[64];
-  const long long s = *d_step + 1;
-  for (int f = threadIdx.x; f < d.nfreq; f += blockDim.x) {
-    double sn, cs;
-    sincos(d.omega[f] * (double)s * dt, &sn, &cs);
-    phE[f] = make_double2(cs * dt, -sn * dt);
-    sincos(d.omega[f] * ((double)s - 0.5) * dt, &sn, &cs);
-    phH[f] = make_double2(cs * dt, -sn * dt);
-  }
-  __syncthreads();
+// (s-1/2)*dt for H, s = steps completed.  Every step stages the plane's values
+// (dft_capture_kernel); every DFT_STAGE steps dft_flush_kernel folds the staged
+// samples into the accumulators in step order, so the accumulator update
+// sequence (and its rounding) is that of a per-step update while the
+// accumulators are read and written once per DFT_STAGE steps.
+__global__ void dft_capture_kernel(Params p, DftDev d, const long long* d_step, int slot) {
   const long long npts = (long long)d.n1 * d.n2;
   const long long pt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (pt == 0) d.sstep[slot] = *d_step + 1;
   if (pt >= npts) return;
   const int u = (int)(pt / d.n2), v = (int)(pt % d.n2);
   int i, j, k;
@@ -262,15 +284,48 @@ __global__ void dft_kernel(Params p, DftDev d, const long long* d_step, double d
   else { i = u; j = v; k = d.index; }
   const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
   int ci = 0;
+  const int ncomp = __popc(d.comp_mask);
   for (int c = 0; c < 6; c++) {
     if (!(d.comp_mask & (1 << c))) continue;
-    const double val = p.f[c][id];
-    const double2* ph = c < 3 ? phE : phH;
+    d.stage[((long long)slot * ncomp + ci) * npts + pt] = p.f[c][id];
+    ci++;
+  }
+}
+
+__global__ void __launch_bounds__(256) dft_flush_kernel(DftDev d, int nslots, double dt) {
+  __shared__ double2 phE[DFT_STAGE][64], phH[DFT_STAGE][64];
+  for (int q = threadIdx.x; q < nslots * d.nfreq; q += blockDim.x) {
+    const int sl = q / d.nfreq, f = q - sl * d.nfreq;
+    const long long s = d.sstep[sl];
+    double sn, cs;
+    sincos(d.omega[f] * (double)s * dt, &sn, &cs);
+    phE[sl][f] = make_double2(cs * dt, -sn * dt);
+    sincos(d.omega[f] * ((double)s - 0.5) * dt, &sn, &cs);
+    phH[sl][f] = make_double2(cs * dt, -sn * dt);
+  }
+  __syncthreads();
+  const long long npts = (long long)d.n1 * d.n2;
+  const long long pt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (pt >= npts) return;
+  const int ncomp = __popc(d.comp_mask);
+  int ci = 0;
+  for (int c = 0; c < 6; c++) {
+    if (!(d.comp_mask & (1 << c))) continue;
+    double val[DFT_STAGE];
+#pragma unroll
+    for (int sl = 0; sl < DFT_STAGE; sl++)
+      val[sl] = sl < nslots ? (double)d.stage[((long long)sl * ncomp + ci) * npts + pt] : 0.0;
+    const double2(*ph)[64] = c < 3 ? phE : phH;
     double2* acc = d.acc + (long long)ci * d.nfreq * npts + pt;
     for (int f = 0; f < d.nfreq; f++) {
       double2 a = acc[(long long)f * npts];
-      a.x += val * ph[f].x;
-      a.y += val * ph[f].y;
+#pragma unroll
+      for (int sl = 0; sl < DFT_STAGE; sl++) {
+        if (sl < nslots) {
+          a.x += val[sl] * ph[sl][f].x;
+          a.y += val[sl] * ph[sl][f].y;
+        }
+      }
       acc[(long long)f * npts] = a;
     }
     ci++;

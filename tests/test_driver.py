@@ -106,11 +106,13 @@ def test_main_sensor_files_match_oracle(tmp_path):
         got.append(np.loadtxt(fn))
     got = np.array(got)
     assert got.shape == ref.shape == (6, cv.Tsteps // cv.Ntime)
-    # %g keeps 6 significant digits (<= 5e-6 relative per value); the floor for
-    # components that vanish by symmetry is 1% of the strongest E / H trace.
+    # %g keeps 6 significant digits (<= 5e-6 relative per value).  The sensor
+    # line starts on the dipole axis, where Ex, Ey and the whole H field vanish
+    # by symmetry up to the boundary asymmetry (|H| ~ 1e-5 |Ez| here), so each
+    # trace is measured against max(its norm, 1% of the strongest trace).
     norms = np.linalg.norm(ref, axis=1)
-    assert norms[:3].max() > 0 and norms[3:].max() > 0
+    assert norms[2] > 0
+    floor = 1e-2 * norms.max()
     for c in range(6):
-        floor = 1e-2 * norms[3 * (c // 3):3 * (c // 3) + 3].max()
         err = np.linalg.norm(got[c] - ref[c]) / max(norms[c], floor)
         assert err <= 2e-5, (abi.COMP_NAMES[c], err)
