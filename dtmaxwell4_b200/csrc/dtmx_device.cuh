@@ -128,11 +128,16 @@ __device__ __forceinline__ float fetch(const Params& p, int c, int i, int j, int
   return s * ldf<LD>(p.f[c] + ii * p.g.sx + jj * p.g.sy + kk);
 }
 
+// The node update is written with explicitly rounded operations (__fadd_rn,
+// __fmul_rn, __fmaf_rn: no compiler contraction), so every kernel that
+// evaluates it -- the per-half-step kernels and the wavefront engine -- gets
+// bit-identical results whatever code surrounds it.
 template <int ORDER>
 __device__ __forceinline__ float dstencil(float v0, float v1, float v2, float v3) {
-  if (ORDER == 2) return v2 - v1;
-  return (27.f * (v2 - v1) - (v3 - v0)) * (1.f / 24.f);
+  if (ORDER == 2) return __fsub_rn(v2, v1);
+  return __fmul_rn(__fmaf_rn(27.f, __fsub_rn(v2, v1), __fsub_rn(v0, v3)), 1.f / 24.f);
 }
+__device__ __forceinline__ float sum3(float a, float b, float c) { return __fadd_rn(__fadd_rn(a, b), c); }
 
 __device__ __forceinline__ bool is_live(const Grid& g, int c, int i, int j, int k) {
   return i >= g.live_lo[c][0] && i <= g.live_hi[c][0] && j >= g.live_lo[c][1] && j <= g.live_hi[c][1] &&
@@ -177,7 +182,21 @@ __device__ __forceinline__ int mat_at(const uint8_t* sm, int c, int y, int z) { 
 //   CPML:  correction_a = (1/kappa_a - 1) dif_a + psi_a,  psi_a <- b psi_a + a dif_a
 //   split: correction_a = (K1_a - 1) p_a + (K2_a - 1) dif_a,  p_a <- K1_a p_a + K2_a dif_a
 // (the split form follows from F = rest + sum p_a with rest += undamped terms).
-__device__ __forceinline__ float absorb_correction(const Params& p, int c, int i, int j, int k, const float* dif) {
+// Split form for callers that batch their slab loads: absorb_load reads the
+// auxiliary value of every slab axis of the node (0 elsewhere), absorb_apply
+// computes the correction from those values and stores the new ones.
+__device__ __forceinline__ void absorb_load(const Params& p, int c, int i, int j, int k, float (&old)[3]) {
+  const int idx[3] = {i, j, k};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    old[a] = 0.f;
+    const int sl = slot_of(c, a);
+    if (sl < 0 || !in_slab(p, a, idx[a])) continue;
+    old[a] = p.ab.aux[a][sl][slab_index(p, a, i, j, k)];
+  }
+}
+__device__ __forceinline__ float absorb_apply(const Params& p, int c, int i, int j, int k, const float* dif,
+                                              const float (&old)[3]) {
   const int idx[3] = {i, j, k};
   float corr = 0.f;
 #pragma unroll
@@ -186,15 +205,18 @@ __device__ __forceinline__ float absorb_correction(const Params& p, int c, int i
     if (sl < 0 || !in_slab(p, a, idx[a])) continue;
     const long long si = slab_index(p, a, i, j, k);
     const int h = 2 * idx[a] + comp_off(c, a);
-    float* st = p.ab.aux[a][sl] + si;
-    const float old = *st;
     const float k0 = __ldg(p.ab.c0[a] + h), k1 = __ldg(p.ab.c1[a] + h);
-    const float nv = k0 * old + k1 * dif[a];
-    *st = nv;
-    if (p.ab.kind == 1) corr += (__ldg(p.ab.c2[a] + h) - 1.f) * dif[a] + nv;
-    else corr += nv - old - dif[a];
+    const float nv = __fmaf_rn(k0, old[a], __fmul_rn(k1, dif[a]));
+    p.ab.aux[a][sl][si] = nv;
+    if (p.ab.kind == 1) corr = __fadd_rn(corr, __fmaf_rn(__fsub_rn(__ldg(p.ab.c2[a] + h), 1.f), dif[a], nv));
+    else corr = __fadd_rn(corr, __fsub_rn(__fsub_rn(nv, old[a]), dif[a]));
   }
   return corr;
+}
+__device__ __forceinline__ float absorb_correction(const Params& p, int c, int i, int j, int k, const float* dif) {
+  float old[3];
+  absorb_load(p, c, i, j, k, old);
+  return absorb_apply(p, c, i, j, k, dif, old);
 }
 
 // Shared-memory copy of one component's plane tile: rows of TW_ROW floats
@@ -292,13 +314,17 @@ __device__ __forceinline__ float ade_update(const Params& p, int c, int m, int n
   float jp[MAXPOLE], jm[MAXPOLE];
   for (int q = 0; q < np; q++) {
     jp[q] = p.ade.Jp[c][q][ai]; jm[q] = p.ade.Jm[c][q][ai];
-    sum += __ldg(&mt.kEJ[m][c][q][0]) * jp[q] + __ldg(&mt.kEJ[m][c][q][1]) * jm[q];
+    sum = __fadd_rn(sum, __fmaf_rn(__ldg(&mt.kEJ[m][c][q][0]), jp[q], __fmul_rn(__ldg(&mt.kEJ[m][c][q][1]), jm[q])));
   }
-  const float Ep = __ldg(&mt.kE[m][c][0]) * Em + __ldg(&mt.kE[m][c][1]) * F + __ldg(&mt.kE[m][c][2]) * rot - sum;
+  const float Ep = __fsub_rn(__fmaf_rn(__ldg(&mt.kE[m][c][0]), Em,
+                                       __fmaf_rn(__ldg(&mt.kE[m][c][1]), F, __fmul_rn(__ldg(&mt.kE[m][c][2]), rot))),
+                             sum);
   for (int q = 0; q < np; q++) {
-    p.ade.Jp[c][q][ai] = __ldg(&mt.kJ[m][c][q][0]) * jp[q] + __ldg(&mt.kJ[m][c][q][1]) * jm[q] +
-                         __ldg(&mt.kJ[m][c][q][2]) * Ep + __ldg(&mt.kJ[m][c][q][3]) * Em +
-                         __ldg(&mt.kJ[m][c][q][4]) * Etmp;
+    float a = __fmul_rn(__ldg(&mt.kJ[m][c][q][4]), Etmp);
+    a = __fmaf_rn(__ldg(&mt.kJ[m][c][q][3]), Em, a);
+    a = __fmaf_rn(__ldg(&mt.kJ[m][c][q][2]), Ep, a);
+    a = __fmaf_rn(__ldg(&mt.kJ[m][c][q][1]), jm[q], a);
+    p.ade.Jp[c][q][ai] = __fmaf_rn(__ldg(&mt.kJ[m][c][q][0]), jp[q], a);
     p.ade.Jm[c][q][ai] = jp[q];
   }
   p.ade.Em[c][ai] = Etmp;
@@ -361,14 +387,14 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
     float d[3][3];
     if (ISH) {
       // Hx -= dt(dy Ez - dz Ey); Hy -= dt(dz Ex - dx Ez); Hz -= dt(dx Ey - dy Ex)
-      d[0][0] = 0.f;       d[0][1] = -cy * dyC; d[0][2] = cz * dzB;
-      d[1][0] = cx * dxC;  d[1][1] = 0.f;       d[1][2] = -cz * dzA;
-      d[2][0] = -cx * dxB; d[2][1] = cy * dyA;  d[2][2] = 0.f;
+      d[0][0] = 0.f;                  d[0][1] = __fmul_rn(-cy, dyC); d[0][2] = __fmul_rn(cz, dzB);
+      d[1][0] = __fmul_rn(cx, dxC);   d[1][1] = 0.f;                 d[1][2] = __fmul_rn(-cz, dzA);
+      d[2][0] = __fmul_rn(-cx, dxB);  d[2][1] = __fmul_rn(cy, dyA);  d[2][2] = 0.f;
     } else {
       // Ex += dt/eps(dy Hz - dz Hy); Ey += dt/eps(dz Hx - dx Hz); Ez += dt/eps(dx Hy - dy Hx)
-      d[0][0] = 0.f;       d[0][1] = cy * dyC;  d[0][2] = -cz * dzB;
-      d[1][0] = -cx * dxC; d[1][1] = 0.f;       d[1][2] = cz * dzA;
-      d[2][0] = cx * dxB;  d[2][1] = -cy * dyA; d[2][2] = 0.f;
+      d[0][0] = 0.f;                  d[0][1] = __fmul_rn(cy, dyC);  d[0][2] = __fmul_rn(-cz, dzB);
+      d[1][0] = __fmul_rn(-cx, dxC);  d[1][1] = 0.f;                 d[1][2] = __fmul_rn(cz, dzA);
+      d[2][0] = __fmul_rn(cx, dxB);   d[2][1] = __fmul_rn(-cy, dyA); d[2][2] = 0.f;
     }
     const bool ab = tab && (inx || in_slab(p, 1, j) || in_slab(p, 2, k));
 #pragma unroll
@@ -376,8 +402,8 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
       if (!SIMPLE && !fast && !is_live(p.g, cf + c, i, j, k)) continue;
       float F = own_at(so, c, y, tz);
       if (SIMPLE) {
-        if (!ISH) { d[c][0] *= iu[c]; d[c][1] *= iu[c]; d[c][2] *= iu[c]; }
-        p.f[cf + c][off] = F + (d[c][0] + d[c][1] + d[c][2]);
+        if (!ISH) { d[c][0] = __fmul_rn(d[c][0], iu[c]); d[c][1] = __fmul_rn(d[c][1], iu[c]); d[c][2] = __fmul_rn(d[c][2], iu[c]); }
+        p.f[cf + c][off] = __fadd_rn(F, sum3(d[c][0], d[c][1], d[c][2]));
         continue;
       }
       if (!ISH) {
@@ -386,16 +412,16 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
           const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
           if (bi >= 0 && bi < p.ade.n[0] && bj >= 0 && bj < p.ade.n[1] && bk >= 0 && bk < p.ade.n[2]) {
             const long long ai = ((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk;
-            p.f[c][off] = ade_update(p, c, m, ms.npoles[m], ai, d[c][0] + d[c][1] + d[c][2], F);
+            p.f[c][off] = ade_update(p, c, m, ms.npoles[m], ai, sum3(d[c][0], d[c][1], d[c][2]), F);
             continue;
           }
         }
         const float ie = ms.inv_eps[m][c];
-        d[c][0] *= ie; d[c][1] *= ie; d[c][2] *= ie;
+        d[c][0] = __fmul_rn(d[c][0], ie); d[c][1] = __fmul_rn(d[c][1], ie); d[c][2] = __fmul_rn(d[c][2], ie);
       }
-      float inc = d[c][0] + d[c][1] + d[c][2];
-      if (ab) inc += absorb_correction(p, cf + c, i, j, k, d[c]);
-      const float nv = F + inc;
+      float inc = sum3(d[c][0], d[c][1], d[c][2]);
+      if (ab) inc = __fadd_rn(inc, absorb_correction(p, cf + c, i, j, k, d[c]));
+      const float nv = __fadd_rn(F, inc);
       p.f[cf + c][off] = nv;
     }
   }

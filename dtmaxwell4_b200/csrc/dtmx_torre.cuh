@@ -39,7 +39,9 @@
 namespace dtmx {
 
 constexpr int TT_Z = 32;           // tile extent along z
-constexpr int TT_NS = 4;           // stages in the ring
+constexpr int TT_NS = 5;           // stages in the ring
+constexpr int TT_K = 2;            // wave steps a producer may run ahead of its slowest neighbour
+constexpr int TT_NPUB = 4;         // step-completion barriers (> TT_K + 1)
 
 struct TorreMaps {
   CUtensorMap A[2];     // Ex / Hx: 40 z x (TY + 2R-1) y    (y and z halo)
@@ -62,10 +64,13 @@ struct TorreGeom {
   // E reads H at -(R-1)..R
   static constexpr int AH = R - 1, BH = R, AE = R, BE = R - 1;
   static constexpr int NQ = 2 * R;               // x taps per derivative
-  static constexpr int GAP_H = AH + 2, GAP_E = AE + 2;
+  // read-after-write with TT_K steps of prefetch: gap >= reach + TT_K + 1;
+  // write-after-read: gap(l+1) - back(l) >= TT_K holds then as well
+  static constexpr int GAP_H = AH + TT_K + 1, GAP_E = AE + TT_K + 1;
   __host__ __device__ static constexpr int off(int l) {
-    // l even: H level, odd: E level; off(0) = 0
-    return l == 0 ? 0 : off(l - 1) + ((l & 1) ? GAP_E : GAP_H);
+    // l even: H level, odd: E level; level 0 starts AH planes early so that
+    // its first items can fill the x-tap queue
+    return l == 0 ? AH : off(l - 1) + ((l & 1) ? GAP_E : GAP_H);
   }
 };
 
@@ -84,8 +89,8 @@ struct TorreLayout {
   static constexpr int O_OWN = O_CQ + SZ_Q, O_MAT = O_OWN + 3 * SZ_Q;
   static constexpr int STAGE = O_MAT + 3 * SZ_M;
   static constexpr int NCW = TY / 4;                       // consumer warps
-  static constexpr int NTHR = 32 * (NCW + 1);
-  static constexpr size_t SMEM = (size_t)TT_NS * STAGE + sizeof(MatShared) + 2 * TT_NS * 8 + TT_NS * 4 + 128;
+  static constexpr int NTHR = 32 * (NCW + 2);              // + producer warp + publisher warp
+  static constexpr size_t SMEM = (size_t)TT_NS * STAGE + sizeof(MatShared) + (2 * TT_NS + TT_NPUB) * 8 + TT_NS * 4 + 128;
   static constexpr unsigned BYTES_Q = 2u * TT_Z * TY * 4;
   static constexpr unsigned BYTES_SRC = (unsigned)(AW * (TY + R2) * 4 + AW * TY * 4 + CW * (TY + R2) * 4 + 3 * TT_Z * TY * 4);
   static constexpr unsigned BYTES_MAT = 3u * TT_Z * TY;
@@ -116,21 +121,29 @@ __device__ __forceinline__ bool item_live(int s, int l, int nx, int& x) {
   return x >= -a && x < nx;
 }
 
-// Producer: wait until every neighbour tile (and this one) has completed at
-// least `need` wave steps.  Bounded: gives up after ~2^24 polls per tile.
-__device__ __forceinline__ void wait_tiles(const Params& p, const TorreArgs& ta, int ty, int tz, int need) {
-  if (need <= 0) return;
-  const int nb[5][2] = {{ty, tz}, {ty - 1, tz}, {ty + 1, tz}, {ty, tz - 1}, {ty, tz + 1}};
-  for (int q = 0; q < 5; q++) {
-    const int y = nb[q][0], z = nb[q][1];
-    if (y < 0 || y >= ta.nty || z < 0 || z >= ta.ntz) continue;
-    const int* c = ta.ctr + y * ta.ntz + z;
-    long long it = 0;
-    while (ld_acquire(c) < need) {
-      if (++it > (1LL << 24)) { atomicExch(p.err, 2); break; }
-      __nanosleep(64);
-    }
+// Producer warp: wait until this tile and its four neighbours have completed
+// at least `need` wave steps.  Lane q watches tile q; the five counters are
+// read in parallel and a lane re-reads only while its cached value is short.
+// Bounded: gives up after ~2^22 rounds and records the timeout.
+__device__ __forceinline__ void wait_tiles(const Params& p, const TorreArgs& ta, int ty, int tz, int need, int& seen) {
+  const int lane = threadIdx.x & 31;
+  const int* c = nullptr;
+  if (lane < 5) {
+    const int dy = lane == 1 ? -1 : lane == 2 ? 1 : 0, dz = lane == 3 ? -1 : lane == 4 ? 1 : 0;
+    const int y = ty + dy, z = tz + dz;
+    if (y >= 0 && y < ta.nty && z >= 0 && z < ta.ntz) c = ta.ctr + y * ta.ntz + z;
   }
+  if (!c) seen = 1 << 30;
+  for (long long it = 0;; it++) {
+    if (seen < need) seen = ld_acquire(c);
+    if (__all_sync(0xffffffffu, seen >= need)) break;
+    if (it > (1LL << 22)) {
+      if (lane == 0) atomicExch(p.err, 2);
+      break;
+    }
+    __nanosleep(32);
+  }
+  __syncwarp();
 }
 
 template <int ORDER, int TY>
@@ -196,16 +209,25 @@ __device__ __forceinline__ void torre_store(const Params& p, const unsigned char
     for (int e = 0; e < 4; e++) {
       if (!ISH) {
         const float iu = ms.inv_eps[um][c];
-        d[0][e] *= iu; d[1][e] *= iu; d[2][e] *= iu;
+        d[0][e] = __fmul_rn(d[0][e], iu); d[1][e] = __fmul_rn(d[1][e], iu); d[2][e] = __fmul_rn(d[2][e], iu);
       }
-      out[e] = f4(o4, e) + (d[0][e] + d[1][e] + d[2][e]);
+      out[e] = __fadd_rn(f4(o4, e), sum3(d[0][e], d[1][e], d[2][e]));
     }
     *reinterpret_cast<float4*>(p.f[cf + c] + off0) = make_float4(out[0], out[1], out[2], out[3]);
     return;
   }
-  // general node: partial tile, absorber slab, dispersive or mixed materials
+  // general node: partial tile, absorber slab, dispersive or mixed materials.
+  // The slab auxiliaries of the four nodes are loaded together first.
   const bool inx = p.ab.kind != 0 && in_slab(p, 0, x);
   const uint8_t* smat = stg + L::O_MAT;
+  float old[4][3];
+  bool inab[4];
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int k = z0 + z + e;
+    inab[e] = j < p.g.n[1] && k < p.g.n[2] && node_in_absorber(p, inx, j, k);
+    if (inab[e]) absorb_load(p, cf + c, x, j, k, old[e]);
+  }
 #pragma unroll
   for (int e = 0; e < 4; e++) {
     const int k = z0 + z + e;
@@ -219,16 +241,16 @@ __device__ __forceinline__ void torre_store(const Params& p, const unsigned char
         const int bi = x - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
         if (bi >= 0 && bi < p.ade.n[0] && bj >= 0 && bj < p.ade.n[1] && bk >= 0 && bk < p.ade.n[2]) {
           const long long ai = ((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk;
-          out[e] = ade_update(p, c, m, ms.npoles[m], ai, dd[0] + dd[1] + dd[2], F);
+          out[e] = ade_update(p, c, m, ms.npoles[m], ai, sum3(dd[0], dd[1], dd[2]), F);
           continue;
         }
       }
       const float ie = ms.inv_eps[m][c];
-      dd[0] *= ie; dd[1] *= ie; dd[2] *= ie;
+      dd[0] = __fmul_rn(dd[0], ie); dd[1] = __fmul_rn(dd[1], ie); dd[2] = __fmul_rn(dd[2], ie);
     }
-    float inc = dd[0] + dd[1] + dd[2];
-    if (node_in_absorber(p, inx, j, k)) inc += absorb_correction(p, cf + c, x, j, k, dd);
-    out[e] = F + inc;
+    float inc = sum3(dd[0], dd[1], dd[2]);
+    if (inab[e]) inc = __fadd_rn(inc, absorb_apply(p, cf + c, x, j, k, dd, old[e]));
+    out[e] = __fadd_rn(F, inc);
   }
   if (j < p.g.n[1] && z0 + z + 3 < p.g.n[2]) {
     *reinterpret_cast<float4*>(p.f[cf + c] + off0) = make_float4(out[0], out[1], out[2], out[3]);
@@ -270,7 +292,8 @@ __device__ __forceinline__ void torre_item(const Params& p, const unsigned char*
   const float* sB = reinterpret_cast<const float*>(stg + L::O_B);
   const float* sC = reinterpret_cast<const float*>(stg + L::O_C);
   const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
-  const float sg = ISH ? -1.f : 1.f;     // H -= dt curl E, E += dt/eps curl H
+  // H -= dt curl E, E += dt/eps curl H: signed coefficients (negation is exact)
+  const float cyp = ISH ? -cy : cy, czp = ISH ? -cz : cz, cxp = ISH ? -cx : cx;
   const int j = y0 + y;
   const long long off0 = (long long)x * p.g.sx + (long long)j * p.g.sy + z0 + z;
   constexpr int zb = 4 + o0;              // index of tap 0 of node e = 0 in a z window
@@ -291,8 +314,8 @@ __device__ __forceinline__ void torre_item(const Params& p, const unsigned char*
       const float dyC = dtap<ORDER>(f4(rC[0], e), f4(rC[I1], e), f4(rC[I2], e), f4(rC[I3], e));
       const float dzB = dtap<ORDER>(wB[zb + e], wB[zb + e + 1], wB[zb + e + 2], wB[zb + e + 3 < 12 ? zb + e + 3 : 11]);
       d[0][e] = 0.f;
-      d[1][e] = (sg * cy) * dyC;
-      d[2][e] = (-sg * cz) * dzB;
+      d[1][e] = __fmul_rn(cyp, dyC);
+      d[2][e] = __fmul_rn(-czp, dzB);
     }
     torre_store<ORDER, ISH, TY>(p, stg, 0, d, x, j, y, z, z0, um, general, ms, off0);
   }
@@ -308,9 +331,9 @@ __device__ __forceinline__ void torre_item(const Params& p, const unsigned char*
     for (int e = 0; e < 4; e++) {
       const float dxC = dtap<ORDER>(qc[0][e], qc[I1][e], qc[I2][e], qc[I3][e]);
       const float dzA = dtap<ORDER>(wA[zb + e], wA[zb + e + 1], wA[zb + e + 2], wA[zb + e + 3 < 12 ? zb + e + 3 : 11]);
-      d[0][e] = (-sg * cx) * dxC;
+      d[0][e] = __fmul_rn(-cxp, dxC);
       d[1][e] = 0.f;
-      d[2][e] = (sg * cz) * dzA;
+      d[2][e] = __fmul_rn(czp, dzA);
     }
     torre_store<ORDER, ISH, TY>(p, stg, 1, d, x, j, y, z, z0, um, general, ms, off0);
   }
@@ -323,8 +346,8 @@ __device__ __forceinline__ void torre_item(const Params& p, const unsigned char*
     for (int e = 0; e < 4; e++) {
       const float dxB = dtap<ORDER>(qb[0][e], qb[I1][e], qb[I2][e], qb[I3][e]);
       const float dyA = dtap<ORDER>(f4(rA[0], e), f4(rA[I1], e), f4(rA[I2], e), f4(rA[I3], e));
-      d[0][e] = (sg * cx) * dxB;
-      d[1][e] = (-sg * cy) * dyA;
+      d[0][e] = __fmul_rn(cxp, dxB);
+      d[1][e] = __fmul_rn(-cyp, dyA);
       d[2][e] = 0.f;
     }
     torre_store<ORDER, ISH, TY>(p, stg, 2, d, x, j, y, z, z0, um, general, ms, off0);
@@ -350,29 +373,28 @@ __global__ void __launch_bounds__(TorreLayout<ORDER, TY>::NTHR, 1)
   MatShared& ms = *reinterpret_cast<MatShared*>(smem + TT_NS * L::STAGE);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + TT_NS * L::STAGE + sizeof(MatShared));
   uint64_t* empty = full + TT_NS;
-  int* stage_um = reinterpret_cast<int*>(empty + TT_NS);   // material of each staged E item
+  uint64_t* done = empty + TT_NS;                          // step completion, ring of TT_NPUB
+  int* stage_um = reinterpret_cast<int*>(done + TT_NPUB);  // material of each staged E item
   const int tz = blockIdx.x, ty = blockIdx.y;
   const int z0 = tz * TT_Z, y0 = ty * TY;
   const int nx = p.g.n[0];
-  const int warp = threadIdx.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
     for (int q = 0; q < TT_NS; q++) { mbar_init(&full[q], 1); mbar_init(&empty[q], L::NCW); }
+    for (int q = 0; q < TT_NPUB; q++) mbar_init(&done[q], L::NCW);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  {
-    const int tid = threadIdx.x;
-    for (int q = tid; q < MAXMAT * 3; q += L::NTHR) (&ms.inv_eps[0][0])[q] = __ldg(&p.mt->inv_eps[0][0] + q);
-    for (int q = tid; q < MAXMAT; q += L::NTHR) ms.npoles[q] = __ldg(&p.mt->npoles[q]);
-  }
+  for (int q = threadIdx.x; q < MAXMAT * 3; q += L::NTHR) (&ms.inv_eps[0][0])[q] = __ldg(&p.mt->inv_eps[0][0] + q);
+  for (int q = threadIdx.x; q < MAXMAT; q += L::NTHR) ms.npoles[q] = __ldg(&p.mt->npoles[q]);
   __syncthreads();
 
   if (warp == L::NCW) {
-    // ---------------- producer warp (lane 0 issues everything)
-    if ((threadIdx.x & 31) == 0) {
-      int it = 0;
-      for (int s = 0; s < ta.nsteps; s++) {
-        // step s reads values produced up to step s-2 (own and neighbours)
-        wait_tiles(p, ta, ty, tz, s - 1);
+    // ---------------- producer warp: neighbour waits (lanes 0-4), TMA issue (lane 0)
+    int it = 0, seen = 0;
+    for (int s = 0; s < ta.nsteps; s++) {
+      // step s reads values produced up to step s - TT_K - 1 (own and neighbours)
+      if (s - TT_K > 0) wait_tiles(p, ta, ty, tz, s - TT_K, seen);
+      if (lane == 0) {
         fence_proxy_async_global();
 #pragma unroll 1
         for (int l = 0; l < NL; l++) {
@@ -386,6 +408,19 @@ __global__ void __launch_bounds__(TorreLayout<ORDER, TY>::NTHR, 1)
           issue_item<ORDER, TY>(p, m, stages + st * L::STAGE, &full[st], l, x, y0, z0, want_mat);
           it++;
         }
+      }
+      __syncwarp();
+    }
+    return;
+  }
+  if (warp == L::NCW + 1) {
+    // ---------------- publisher warp: release each completed wave step
+    if (lane == 0) {
+      int* mine = ta.ctr + ty * ta.ntz + tz;
+      for (int s = 0; s < ta.nsteps; s++) {
+        mbar_wait(&done[s % TT_NPUB], (unsigned)((s / TT_NPUB) & 1), p.err);
+        __threadfence();
+        st_release(mine, s + 1);
       }
     }
     return;
@@ -414,15 +449,12 @@ __global__ void __launch_bounds__(TorreLayout<ORDER, TY>::NTHR, 1)
       if (isE) torre_item<ORDER, false, TY>(p, stg, qb[l], qc[l], x, y0, z0, um, gen, ms);
       else torre_item<ORDER, true, TY>(p, stg, qb[l], qc[l], x, y0, z0, um, gen, ms);
       __syncwarp();
-      if ((threadIdx.x & 31) == 0) mbar_arrive(&empty[st]);
+      if (lane == 0) mbar_arrive(&empty[st]);
       it++;
     }
-    // publish step s: all consumer stores of the step precede the release
-    named_bar(1, 32 * L::NCW);
-    if (threadIdx.x == 0) {
-      __threadfence();
-      st_release(ta.ctr + ty * ta.ntz + tz, s + 1);
-    }
+    // this warp's stores of step s precede its arrival (release) on the step barrier
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&done[s % TT_NPUB]);
   }
 }
 
