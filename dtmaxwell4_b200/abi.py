@@ -101,8 +101,10 @@ def make_config(nx, ny, nz, dx=1.0, dy=None, dz=None, dt=None, courant=0.5, orde
     return cfg
 
 
-def make_material(eps=1.0, poles=(), eps_inf=1.0, sigma=0.0):
-    """eps: scalar or 3-tuple; poles: iterable of (kind, Deps, wp, gp, gp_)."""
+def make_material(eps=1.0, poles=(), eps_inf=1.0, sigma=0.0, gyro=None):
+    """eps: scalar or 3-tuple; poles: iterable of (kind, Deps, wp, gp, gp_);
+    gyro: (wp, gamma, wc) of a magnetised-Drude current (bias along +z), with
+    eps_inf the background permittivity."""
     m = Material()
     if isinstance(eps, (int, float)):
         eps = (eps, eps, eps)
@@ -117,4 +119,17 @@ def make_material(eps=1.0, poles=(), eps_inf=1.0, sigma=0.0):
         m.pole[p][0], m.pole[p][1], m.pole[p][2], m.pole[p][3] = Deps, wp, gp, gp_
     m.eps_inf = eps_inf
     m.sigma = sigma
+    if gyro is not None:
+        m.gyro_wp, m.gyro_gamma, m.gyro_wc = (float(v) for v in gyro)
     return m
+
+
+def gyro_for(eps_diag, g, omega0, wc_ratio=0.5):
+    """Magnetised-Drude parameters (eps_inf, (wp, 0, wc)) whose lossless tensor
+    at omega0 has diagonal eps_diag and off-diagonal magnitude g:
+    eps_xx = eps_inf - wp^2/(w0^2 - wc^2), |eps_xy| = wp^2 wc / (w0 (w0^2 - wc^2)),
+    with wc = wc_ratio * omega0."""
+    wc = wc_ratio * omega0
+    den = omega0 ** 2 - wc ** 2
+    wp2 = g * omega0 * den / wc
+    return eps_diag + wp2 / den, (wp2 ** 0.5, 0.0, wc)

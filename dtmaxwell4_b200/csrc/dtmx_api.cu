@@ -77,6 +77,8 @@ struct dtmx_ctx {
   int engine = 0, tblock = 0;
   TmaMaps maps{};
   int* d_err = nullptr;
+  bool has_gyro = false;
+  int gcur = 0;              // gyrotropic current buffer holding J^{n-1/2}
   // wavefront engine
   TorreMaps tmaps{};
   bool tmaps_ok = false;
@@ -445,7 +447,9 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
     if (M.npoles < 0 || M.npoles > DTMX_MAX_POLES) return fail(ctx, DTMX_ERR_INVALID, "npoles out of range");
     if (M.npoles > 0 && !(M.eps_inf > 0)) return fail(ctx, DTMX_ERR_INVALID, "dispersive material needs eps_inf > 0");
     if (M.npoles == 0 && !(M.eps[0] > 0 && M.eps[1] > 0 && M.eps[2] > 0)) return fail(ctx, DTMX_ERR_INVALID, "eps must be > 0");
-    if (M.gyro_wp != 0) return fail(ctx, DTMX_ERR_UNSUPPORTED, "gyrotropic materials are not supported by this build");
+    if (M.gyro_wp < 0) return fail(ctx, DTMX_ERR_INVALID, "gyro_wp must be >= 0");
+    if (M.gyro_wp > 0 && (M.npoles > 0 || !(M.eps_inf > 0)))
+      return fail(ctx, DTMX_ERR_INVALID, "a gyrotropic material needs npoles = 0 and eps_inf > 0");
   }
   MatTable& t = ctx->h_mt;
   memset(&t, 0, sizeof(t));
@@ -454,6 +458,15 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
     t.npoles[m] = table[m].npoles;
     for (int c = 0; c < 3; c++) t.inv_eps[m][c] = table[m].npoles > 0 ? 0.f : (float)(1.0 / table[m].eps[c]);
     if (table[m].npoles > 0) disp_coeffs(table[m], ctx->cfg.dt, t, m);
+    if (table[m].gyro_wp > 0) {
+      const double dt = ctx->cfg.dt;
+      for (int c = 0; c < 3; c++) t.inv_eps[m][c] = (float)(1.0 / table[m].eps_inf);
+      t.gA[m] = (float)std::exp(-table[m].gyro_gamma * dt);
+      t.gC[m] = (float)std::cos(table[m].gyro_wc * dt);
+      t.gS[m] = (float)std::sin(table[m].gyro_wc * dt);
+      t.gB[m] = (float)(table[m].gyro_wp * table[m].gyro_wp * dt);
+      t.gjc[m] = (float)(dt / table[m].eps_inf);
+    }
   }
   ctx->nmat = nmat;
   const dtmx_config& c = ctx->cfg;
@@ -468,7 +481,7 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
           const uint8_t m = row[k];
           if (m >= nmat) return fail(ctx, DTMX_ERR_INVALID, "material index out of range");
           dst[k] = m;
-          if (table[m].npoles > 0) {
+          if (table[m].npoles > 0 || table[m].gyro_wp > 0) {
             const int v[3] = {i, j, k};
             for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], v[a]); hi[a] = std::max(hi[a], v[a]); }
           }
@@ -494,7 +507,7 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
               for (int k = tz * TZ; k < std::min(c.nz, tz * TZ + TZ); k++) {
                 const int m = row[k];
                 if (m0 == -2) m0 = m;
-                if (m != m0 || table[m].npoles > 0) { m0 = -1; break; }
+                if (m != m0 || table[m].npoles > 0 || table[m].gyro_wp > 0) { m0 = -1; break; }
               }
             }
           um[((size_t)i * nty + ty) * ntz + tz] = (signed char)(m0 < 0 ? -1 : m0);
@@ -507,7 +520,13 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
     size_t na = 1;
     for (int a = 0; a < 3; a++) { A.lo[a] = lo[a]; A.n[a] = hi[a] - lo[a] + 1; na *= A.n[a]; }
     int maxp = 0;
-    for (int m = 0; m < nmat; m++) maxp = std::max(maxp, table[m].npoles);
+    bool gyro = false;
+    for (int m = 0; m < nmat; m++) { maxp = std::max(maxp, table[m].npoles); gyro = gyro || table[m].gyro_wp > 0; }
+    ctx->has_gyro = gyro;
+    ctx->gcur = 0;
+    for (int comp = 0; comp < 3 && gyro; comp++)
+      for (int b = 0; b < 2; b++)
+        if ((rc = dalloc(ctx, &A.Jg[b][comp], na))) return rc;
     for (int comp = 0; comp < 3; comp++) {
       if ((rc = dalloc(ctx, &A.Em[comp], na))) return rc;
       for (int q = 0; q < maxp; q++) {
@@ -751,6 +770,13 @@ static int launch_step(dtmx_ctx* ctx) {
     else line_h_kernel<2><<<8, 256, 0, st>>>(ctx->line_e, ctx->line_h, ctx->T.line_n, r1);
     nl++;
   }
+  if (ctx->has_gyro) {
+    const long long na = (long long)P.ade.n[0] * P.ade.n[1] * P.ade.n[2];
+    gyro_current_kernel<<<(unsigned)std::min<long long>((na + 255) / 256, 148LL * 16), 256, 0, st>>>(P, ctx->gcur);
+    P.ade.gnew = 1 - ctx->gcur;
+    ctx->gcur = 1 - ctx->gcur;
+    nl++;
+  }
   if (ctx->profiling) cudaEventRecord(ctx->ev[2], st);
   if (o4) e_kernel<4><<<grd, blk, Pipe<4, false>::SMEM_BYTES, st>>>(P, ctx->maps);
   else e_kernel<2><<<grd, blk, Pipe<2, false>::SMEM_BYTES, st>>>(P, ctx->maps);
@@ -820,8 +846,9 @@ static int prepare(dtmx_ctx* ctx) {
         for (int j = std::max(0, jb.lo[1] - 1); j <= std::min(ctx->cfg.ny - 1, jb.hi[1] + 1); j++)
           for (int k = std::max(0, jb.lo[2] - 1); k <= std::min(ctx->cfg.nz - 1, jb.hi[2] + 1); k++)
             for (int comp = 0; comp < 3; comp++)
-              if (ctx->mats[ctx->h_mat[comp][store_index(ctx, i, j, k)]].npoles > 0)
-                return fail(ctx, DTMX_ERR_UNSUPPORTED, "dispersive material on the TF/SF surface");
+              if (ctx->mats[ctx->h_mat[comp][store_index(ctx, i, j, k)]].npoles > 0 ||
+                  ctx->mats[ctx->h_mat[comp][store_index(ctx, i, j, k)]].gyro_wp > 0)
+                return fail(ctx, DTMX_ERR_UNSUPPORTED, "dispersive or gyrotropic material on the TF/SF surface");
     }
   }
   CK(cudaStreamSynchronize(ctx->stream));
@@ -875,6 +902,7 @@ static bool torre_usable(dtmx_ctx* ctx, int T, std::string* why) {
   if (!fn) { *why = "no kernel for order " + std::to_string(c.order) + " with " + std::to_string(T) + " steps per launch"; return false; }
   if (c.geometry != DTMX_GEOM_BOX) { *why = "needs the box geometry"; return false; }
   if (c.absorber == DTMX_ABS_SPLIT_PML) { *why = "split PML is not supported"; return false; }
+  if (ctx->has_gyro) { *why = "gyrotropic materials need a current pass between half steps"; return false; }
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
     cudaGetLastError();
     *why = "shared memory attribute refused";
@@ -897,6 +925,7 @@ static bool torre_usable(dtmx_ctx* ctx, int T, std::string* why) {
 
 // features the wavefront engine does not carry inside its launch
 static bool torre_features_ok(const dtmx_ctx* ctx, std::string* why) {
+  if (ctx->has_gyro) { *why = "gyrotropic materials"; return false; }
   if (ctx->has_tfsf) { *why = "TF/SF source"; return false; }
   if (!ctx->psrc.empty()) { *why = "point sources"; return false; }
   if (!ctx->probes.empty()) { *why = "probes"; return false; }

@@ -332,6 +332,47 @@ __global__ void __launch_bounds__(256) dft_flush_kernel(DftDev d, int nslots, do
   }
 }
 
+// Magnetised-Drude current over the ADE box (dtmx.h, dtmx_material):
+// J^{n+1/2} into buffer 1-cur from J^{n-1/2} (buffer cur) and E^n.
+__device__ __forceinline__ float gyro_old(const Params& p, int cur, int c, int i, int j, int k) {
+  const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
+  if (bi < 0 || bi >= p.ade.n[0] || bj < 0 || bj >= p.ade.n[1] || bk < 0 || bk >= p.ade.n[2]) return 0.f;
+  return p.ade.Jg[cur][c][((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk];
+}
+
+__global__ void gyro_current_kernel(Params p, int cur) {
+  const long long na = (long long)p.ade.n[0] * p.ade.n[1] * p.ade.n[2];
+  const MatTable& mt = *p.mt;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < na; q += (long long)gridDim.x * blockDim.x) {
+    const int bk = (int)(q % p.ade.n[2]);
+    const long long r = q / p.ade.n[2];
+    const int bj = (int)(r % p.ade.n[1]), bi = (int)(r / p.ade.n[1]);
+    const int i = p.ade.lo[0] + bi, j = p.ade.lo[1] + bj, k = p.ade.lo[2] + bk;
+    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int m = p.mat[c] ? (int)p.mat[c][id] : 0;
+      if (mt.gjc[m] == 0.f) continue;
+      const float E = p.f[c][id], Jo = p.ade.Jg[cur][c][q];
+      float t;
+      if (c == 0) {
+        const float avg = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(__fadd_rn(gyro_old(p, cur, 1, i - 1, j, k), gyro_old(p, cur, 1, i, j, k)),
+                                                               gyro_old(p, cur, 1, i - 1, j + 1, k)),
+                                                     gyro_old(p, cur, 1, i, j + 1, k)));
+        t = __fmaf_rn(mt.gC[m], Jo, __fmul_rn(mt.gS[m], avg));
+      } else if (c == 1) {
+        const float avg = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(__fadd_rn(gyro_old(p, cur, 0, i, j - 1, k), gyro_old(p, cur, 0, i + 1, j - 1, k)),
+                                                               gyro_old(p, cur, 0, i, j, k)),
+                                                     gyro_old(p, cur, 0, i + 1, j, k)));
+        t = __fmaf_rn(mt.gC[m], Jo, -__fmul_rn(mt.gS[m], avg));
+      } else {
+        t = Jo;
+      }
+      p.ade.Jg[1 - cur][c][q] = __fmaf_rn(mt.gA[m], t, __fmul_rn(mt.gB[m], E));
+    }
+  }
+}
+
 __global__ void mask_nonlive_kernel(Params p, int comp, long long ncell) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(q % p.g.n[2]);

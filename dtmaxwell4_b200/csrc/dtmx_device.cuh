@@ -57,6 +57,8 @@ struct MatTable {
   float kEJ[MAXMAT][3][MAXPOLE][2];
   float kE[MAXMAT][3][3];
   float kJ[MAXMAT][3][MAXPOLE][5];
+  // magnetised-Drude (gyrotropic) current: decay, rotation cos/sin, E drive, dt/eps_inf (0: not gyrotropic)
+  float gA[MAXMAT], gC[MAXMAT], gS[MAXMAT], gB[MAXMAT], gjc[MAXMAT];
 };
 
 struct Ade {
@@ -64,6 +66,8 @@ struct Ade {
   float* Em[3];
   float* Jp[3][MAXPOLE];
   float* Jm[3][MAXPOLE];
+  float* Jg[2][3];           // gyrotropic current, double-buffered
+  int gnew;                  // buffer holding J^{n+1/2} during the E half step
 };
 
 struct Params {
@@ -335,12 +339,21 @@ __device__ __forceinline__ float ade_update(const Params& p, int c, int m, int n
 struct MatShared {
   float inv_eps[MAXMAT][3];
   int npoles[MAXMAT];
+  float gjc[MAXMAT];
 };
 
 __device__ __forceinline__ void load_matshared(MatShared& ms, const Params& p) {
   const int tid = threadIdx.y * TZ + threadIdx.x;
   for (int q = tid; q < MAXMAT * 3; q += NTHR) (&ms.inv_eps[0][0])[q] = __ldg(&p.mt->inv_eps[0][0] + q);
-  for (int q = tid; q < MAXMAT; q += NTHR) ms.npoles[q] = __ldg(&p.mt->npoles[q]);
+  for (int q = tid; q < MAXMAT; q += NTHR) { ms.npoles[q] = __ldg(&p.mt->npoles[q]); ms.gjc[q] = __ldg(&p.mt->gjc[q]); }
+}
+
+// E -= dt/eps_inf J^{n+1/2} on a gyrotropic node (J computed by gyro_current_kernel)
+__device__ __forceinline__ float gyro_subtract(const Params& p, int c, int i, int j, int k, float gjc, float nv) {
+  const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
+  if (bi < 0 || bi >= p.ade.n[0] || bj < 0 || bj >= p.ade.n[1] || bk < 0 || bk >= p.ade.n[2]) return nv;
+  const long long ai = ((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk;
+  return __fsub_rn(nv, __fmul_rn(gjc, p.ade.Jg[p.ade.gnew][c][ai]));
 }
 
 // Update of one plane tile (all three components of the half step).  Common
@@ -421,7 +434,11 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
       }
       float inc = sum3(d[c][0], d[c][1], d[c][2]);
       if (ab) inc = __fadd_rn(inc, absorb_correction(p, cf + c, i, j, k, d[c]));
-      const float nv = __fadd_rn(F, inc);
+      float nv = __fadd_rn(F, inc);
+      if (!ISH) {
+        const int m = um >= 0 ? um : mat_at(smat, c, y, tz);
+        if (ms.gjc[m] != 0.f) nv = gyro_subtract(p, c, i, j, k, ms.gjc[m], nv);
+      }
       p.f[cf + c][off] = nv;
     }
   }

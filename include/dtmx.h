@@ -111,9 +111,15 @@ typedef struct dtmx_material {
   double eps_inf;
   double sigma;
   /* Gyrotropic magnetised-Drude current (no reference counterpart: the
-   * reference's Gyration() is disabled, genAlg.py:303-304): plasma frequency,
-   * collision rate and cyclotron frequency (bias along +z).  Active when
-   * gyro_wp != 0; mutually exclusive with npoles > 0. */
+   * reference's Gyration() is disabled, genAlg.py:303-304): plasma frequency
+   * wp, collision rate gamma and cyclotron frequency wc (bias along +z).
+   * Active when gyro_wp > 0; then eps_inf is the background permittivity,
+   * eps[] is ignored and npoles must be 0.  With J on the E nodes:
+   *   eps_inf dE/dt = curl H - J,   dJ/dt = -gamma J + wp^2 E + wc J x z,
+   * stepped as J_x <- a (cos th J_x + sin th <J_y>) + b E_x,
+   *            J_y <- a (cos th J_y - sin th <J_x>) + b E_y,  J_z <- a J_z + b E_z,
+   * a = exp(-gamma dt), th = wc dt, b = wp^2 dt, <.> the 4-node average of
+   * the other component around the node; then E += dt/eps_inf (curl H - J). */
   double gyro_wp, gyro_gamma, gyro_wc;
   double reserved[4];
 } dtmx_material;

@@ -87,6 +87,12 @@ typedef struct {
   int ade_box[3][2];   /* cell box holding ADE state, [lo, hi) */
   size_t ade_n;
   real* Em[3]; real* Jp[3][DTMX_MAX_POLES]; real* Jm[3][DTMX_MAX_POLES];
+  /* gyrotropic current: coefficients per material, double-buffered J over the ADE box */
+  int gyro[DTMX_MAX_MATERIALS];
+  real gA[DTMX_MAX_MATERIALS], gC[DTMX_MAX_MATERIALS], gS[DTMX_MAX_MATERIALS], gB[DTMX_MAX_MATERIALS];
+  real gjc[DTMX_MAX_MATERIALS];
+  int has_gyro, gcur;
+  real* Jg[2][3];
   /* sources */
   dtmx_point_source psrc[64]; int npsrc;
   int has_tfsf; dtmx_tfsf tfsf;
@@ -464,6 +470,70 @@ static int near_box(const osim* s, int X, int Y, int Z) {
   return close;
 }
 
+/* ADE-box index of cell (i,j,k), -1 outside the box */
+static long ade_index(const osim* s, int i, int j, int k) {
+  if (i < s->ade_box[0][0] || i >= s->ade_box[0][1] || j < s->ade_box[1][0] || j >= s->ade_box[1][1] ||
+      k < s->ade_box[2][0] || k >= s->ade_box[2][1])
+    return -1;
+  return ((long)(i - s->ade_box[0][0]) * (s->ade_box[1][1] - s->ade_box[1][0]) + (j - s->ade_box[1][0])) *
+             (s->ade_box[2][1] - s->ade_box[2][0]) + (k - s->ade_box[2][0]);
+}
+
+static real gyro_old(const osim* s, int c, int i, int j, int k) {
+  long ai = ade_index(s, i, j, k);
+  return ai < 0 ? 0 : s->Jg[s->gcur][c][ai];
+}
+
+/* Magnetised-Drude current J^{n+1/2} from J^{n-1/2} and E^n (dtmx.h,
+ * dtmx_material), written to the other buffer; the E half step then
+ * subtracts dt/eps_inf J^{n+1/2}. */
+static void gyro_pass(osim* s) {
+  if (!s->has_gyro || s->ade_n == 0) return;
+  const int cur = s->gcur, nxt = 1 - cur;
+  #pragma omp parallel for schedule(static)
+  for (int i = s->ade_box[0][0]; i < s->ade_box[0][1]; i++)
+    for (int j = s->ade_box[1][0]; j < s->ade_box[1][1]; j++)
+      for (int k = s->ade_box[2][0]; k < s->ade_box[2][1]; k++) {
+        size_t id = IDX(s, i, j, k);
+        long ai = ade_index(s, i, j, k);
+        for (int c = 0; c < 3; c++) {
+          int mi = s->midx[c] ? s->midx[c][id] : 0;
+          if (!s->gyro[mi]) continue;
+          real E = s->f[c][id], Jo = s->Jg[cur][c][ai], t;
+          if (c == 0) {
+            real avg = (real)0.25 * (((gyro_old(s, 1, i - 1, j, k) + gyro_old(s, 1, i, j, k)) + gyro_old(s, 1, i - 1, j + 1, k)) +
+                                     gyro_old(s, 1, i, j + 1, k));
+            t = s->gC[mi] * Jo + s->gS[mi] * avg;
+          } else if (c == 1) {
+            real avg = (real)0.25 * (((gyro_old(s, 0, i, j - 1, k) + gyro_old(s, 0, i + 1, j - 1, k)) + gyro_old(s, 0, i, j, k)) +
+                                     gyro_old(s, 0, i + 1, j, k));
+            t = s->gC[mi] * Jo - s->gS[mi] * avg;
+          } else {
+            t = Jo;
+          }
+          s->Jg[nxt][c][ai] = s->gA[mi] * t + s->gB[mi] * E;
+        }
+      }
+}
+
+/* E -= dt/eps_inf J^{n+1/2} on gyrotropic nodes; J^{n+1/2} becomes current */
+static void gyro_finish(osim* s) {
+  if (!s->has_gyro || s->ade_n == 0) return;
+  const int nxt = 1 - s->gcur;
+  #pragma omp parallel for schedule(static)
+  for (int i = s->ade_box[0][0]; i < s->ade_box[0][1]; i++)
+    for (int j = s->ade_box[1][0]; j < s->ade_box[1][1]; j++)
+      for (int k = s->ade_box[2][0]; k < s->ade_box[2][1]; k++) {
+        size_t id = IDX(s, i, j, k);
+        long ai = ade_index(s, i, j, k);
+        for (int c = 0; c < 3; c++) {
+          int mi = s->midx[c] ? s->midx[c][id] : 0;
+          if (s->gyro[mi]) s->f[c][id] -= s->gjc[mi] * s->Jg[nxt][c][ai];
+        }
+      }
+  s->gcur = nxt;
+}
+
 static void half_step(osim* s, int isH) {
   const dtmx_config* cf = &s->cfg;
   double dd[3] = {cf->dx, cf->dy, cf->dz};
@@ -601,6 +671,7 @@ void PFX(destroy)(void* h) {
   for (int c = 0; c < 3; c++) {
     free(s->Em[c]);
     for (int p = 0; p < DTMX_MAX_POLES; p++) { free(s->Jp[c][p]); free(s->Jm[c][p]); }
+    free(s->Jg[0][c]); free(s->Jg[1][c]);
   }
   free(s->line_e); free(s->line_h); free(s->traces);
   for (int d = 0; d < s->ndft; d++) { free(s->dft[d].omega); free(s->dft[d].acc); }
@@ -647,7 +718,22 @@ int PFX(set_materials)(void* h, const dtmx_material* table, int nmat, const uint
   if (nmat < 1 || nmat > DTMX_MAX_MATERIALS || !ix) return DTMX_ERR_INVALID;
   s->nmat = nmat;
   memcpy(s->mat, table, nmat * sizeof(dtmx_material));
+  s->has_gyro = 0;
   for (int m = 0; m < nmat; m++) {
+    s->gyro[m] = table[m].gyro_wp > 0;
+    if (s->gyro[m]) {
+      /* magnetised-Drude current (dtmx.h, dtmx_material) */
+      if (table[m].npoles > 0 || !(table[m].eps_inf > 0)) return DTMX_ERR_INVALID;
+      double dt = s->cfg.dt;
+      for (int c = 0; c < 3; c++) s->inv_eps[m][c] = (real)(1.0 / table[m].eps_inf);
+      s->gA[m] = (real)exp(-table[m].gyro_gamma * dt);
+      s->gC[m] = (real)cos(table[m].gyro_wc * dt);
+      s->gS[m] = (real)sin(table[m].gyro_wc * dt);
+      s->gB[m] = (real)(table[m].gyro_wp * table[m].gyro_wp * dt);
+      s->gjc[m] = (real)(dt / table[m].eps_inf);
+      s->has_gyro = 1;
+      continue;
+    }
     for (int c = 0; c < 3; c++) s->inv_eps[m][c] = (real)(1.0 / table[m].eps[c]);
     if (table[m].npoles > 0) disp_coeffs(s, m);
   }
@@ -665,7 +751,7 @@ int PFX(set_materials)(void* h, const dtmx_material* table, int nmat, const uint
       for (int k = 0; k < s->nz; k++) {
         size_t id = IDX(s, i, j, k);
         int dis = 0;
-        for (int c = 0; c < 3; c++) { const dtmx_material* M = &s->mat[s->midx[c][id]]; if (M->npoles > 0) dis = 1; }
+        for (int c = 0; c < 3; c++) { const dtmx_material* M = &s->mat[s->midx[c][id]]; if (M->npoles > 0 || M->gyro_wp > 0) dis = 1; }
         if (!dis) continue;
         int v[3] = {i, j, k};
         for (int a = 0; a < 3; a++) { if (v[a] < lo[a]) lo[a] = v[a]; if (v[a] > hi[a]) hi[a] = v[a]; }
@@ -673,13 +759,16 @@ int PFX(set_materials)(void* h, const dtmx_material* table, int nmat, const uint
   for (int c = 0; c < 3; c++) {
     free(s->Em[c]); s->Em[c] = NULL;
     for (int p = 0; p < DTMX_MAX_POLES; p++) { free(s->Jp[c][p]); free(s->Jm[c][p]); s->Jp[c][p] = s->Jm[c][p] = NULL; }
+    for (int b = 0; b < 2; b++) { free(s->Jg[b][c]); s->Jg[b][c] = NULL; }
   }
+  s->gcur = 0;
   if (hi[0] < 0) { for (int a = 0; a < 3; a++) { s->ade_box[a][0] = 0; s->ade_box[a][1] = 0; } s->ade_n = 0; return DTMX_OK; }
   s->ade_n = 1;
   for (int a = 0; a < 3; a++) { s->ade_box[a][0] = lo[a]; s->ade_box[a][1] = hi[a] + 1; s->ade_n *= (size_t)(hi[a] + 1 - lo[a]); }
   for (int c = 0; c < 3; c++) {
     s->Em[c] = calloc(s->ade_n, sizeof(real));
     for (int p = 0; p < DTMX_MAX_POLES; p++) { s->Jp[c][p] = calloc(s->ade_n, sizeof(real)); s->Jm[c][p] = calloc(s->ade_n, sizeof(real)); }
+    if (s->has_gyro) for (int b = 0; b < 2; b++) s->Jg[b][c] = calloc(s->ade_n, sizeof(real));
   }
   return DTMX_OK;
 }
@@ -793,7 +882,9 @@ int PFX(step)(void* h, int nsteps) {
     int pw = s->has_tfsf && s->tfsf.kind == DTMX_TFSF_PLANE_X;
     half_step(s, 1);
     if (pw) line_update_h(s);
+    gyro_pass(s);
     half_step(s, 0);
+    gyro_finish(s);
     if (pw) {
       line_update_e(s);
       s->line_e[s->line_src] += line_wave(&s->tfsf, ((double)s->step + 0.5) * s->cfg.dt);

@@ -159,3 +159,50 @@ def test_oracle_cpml_absorbs():
     o.step(380)
     e2 = sum(float((o.get_field(c) ** 2).sum()) for c in range(6))
     assert e2 < 1e-4 * e1, (e1, e2)
+
+
+def _gyro_uniform_recursion(einf, wp, wc, gamma, dt, steps):
+    """The magnetised-Drude scheme on a spatially uniform state (curl H = 0):
+    the (Ex, Ey, Jx, Jy) map of one step, started from Ex = 1."""
+    a, C, S, b, jc = math.exp(-gamma * dt), math.cos(wc * dt), math.sin(wc * dt), wp * wp * dt, dt / einf
+    ex, ey, jx, jy = 1.0, 0.0, 0.0, 0.0
+    out = []
+    for _ in range(steps):
+        jx, jy = a * (C * jx + S * jy) + b * ex, a * (C * jy - S * jx) + b * ey
+        ex, ey = ex - jc * jx, ey - jc * jy
+        out.append((ex, ey))
+    return np.array(out)
+
+
+def test_oracle_gyrotropic_uniform_mode():
+    """Magnetised-Drude current: a uniform Ex in a gyrotropic block follows the
+    single-node recursion (until the block edges, where the 4-node averages see
+    zero current, reach the probe), and that recursion rotates the polarisation
+    at the two magnetoplasma frequencies w = (+-wc + sqrt(wc^2 + 4 wp^2/eps_inf))/2."""
+    import pyoracle
+    from dtmaxwell4_b200 import abi
+    n, steps = 84, 30
+    einf, wp, wc, gamma = 1.5, 0.8, 0.6, 0.02
+    cfg = abi.make_config(n, n, 6, courant=0.5, order=2, geometry=abi.GEOM_REFERENCE, absorber=abi.ABS_NONE, pml=0)
+    o = pyoracle.OracleSim(cfg)
+    o.set_materials([abi.make_material(1.0), abi.make_material(eps_inf=einf, gyro=(wp, gamma, wc))],
+                    np.ones((n, n, 6), np.uint8))
+    o.set_field(abi.EX, np.ones((n, n, 6)))
+    o.add_probe(abi.EX, n // 2, n // 2, 3)
+    o.add_probe(abi.EY, n // 2, n // 2, 3)
+    o.step(steps)
+    tr = o.read_probes(steps + 5)
+    ref = _gyro_uniform_recursion(einf, wp, wc, gamma, cfg.dt, steps)
+    assert np.abs(tr[0] - ref[:, 0]).max() < 1e-12 and np.abs(tr[1] - ref[:, 1]).max() < 1e-12
+    assert np.abs(ref[:, 1]).max() > 0.05            # the bias field rotates the polarisation
+    # eigenfrequencies of the one-step map (lossless, small dt) vs the continuous modes
+    dt = 0.01
+    C, S, b, jc = math.cos(wc * dt), math.sin(wc * dt), wp * wp * dt, dt / einf
+    T = np.zeros((4, 4))
+    # state (Jx, Jy, Ex, Ey): J' = R J + b E ; E' = E - jc J'
+    T[:2, :2] = [[C, S], [-S, C]]; T[:2, 2:] = b * np.eye(2)
+    T[2:, :] = np.hstack([-jc * T[:2, :2], np.eye(2) - jc * b * np.eye(2)])
+    w = sorted(abs(np.angle(np.linalg.eigvals(T))) / dt)
+    expect = sorted([(s * wc + math.sqrt(wc * wc + 4 * wp * wp / einf)) / 2 for s in (1, -1)])
+    got = sorted(set(round(v, 6) for v in w))
+    assert len(got) == 2 and all(abs(g / e - 1) < 2e-3 for g, e in zip(got, expect)), (got, expect)

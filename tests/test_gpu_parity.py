@@ -197,3 +197,22 @@ def test_invalid_configs_fail_loudly():
         Simulation(abi.make_config(32, 32, 32, dt=0.5, order=4))           # > 6/7 limit
     with pytest.raises(DtmxError):
         Simulation(abi.make_config(32, 32, 32, geometry=abi.GEOM_REFERENCE, absorber=abi.ABS_CPML))
+
+
+def test_gyrotropic_layer_point_dipole():
+    """Magnetised-Drude layer (eps_diag 4, off-diagonal 0.3 at the source
+    frequency) under a CPML box with an Ez dipole above it."""
+    from dtmaxwell4_b200 import abi, scenarios
+    n = 40
+    lam = 12.0
+    w0 = 2 * math.pi / lam
+    einf, gyro = abi.gyro_for(4.0, 0.3, w0)
+    sc = scenarios.point_dipole_sphere(n=n, steps=300, pml=6, radius=0.1, eps=1.0, order=2, courant=0.5, lambda0=lam)
+    idx = np.zeros((n, n, n), np.uint8)
+    idx[:, :, 8:18] = 1
+    sc["materials"] = ([abi.make_material(1.0), abi.make_material(eps_inf=einf, gyro=gyro)], [idx, idx, idx])
+    g, o, _, _ = _pair(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    _compare_probes(g, o)
+    _compare_fields(g, o)
