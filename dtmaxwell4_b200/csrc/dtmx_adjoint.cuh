@@ -1,0 +1,169 @@
+// dtmx_adjoint.cuh -- discrete adjoint of the field update for gradients with
+// respect to per-node permittivity (no reference counterpart: the reference
+// has no differentiation path).
+//
+// Forward step (box geometry, CPML or no absorber, non-dispersive nodes):
+//   H' = H + sum_a g_a d_a + sum_slab b_a psi_a,   psi_a' = b_a psi_a + al_a d_a,
+//   d_a = s_a D_a(E) for H, d_a = ie s_a D_a(H') for E,
+// with g_a = 1 outside the axis-a slab and 1/kappa_a + al_a inside.  The
+// adjoint step applies the transposes in reverse order: the E update (lam_H
+// += D^T w_E, then lam_psiE <- b (lam_E + lam_psiE)), then the H update
+// (lam_E += D^T w_H, lam_psiH <- b (lam_H + lam_psiH)), where w = s ie (g lam
+// + al lam_psi) is the adjoint of d.  D^T is gathered tap by tap with the
+// forward stencil weights; outside the grid every value is zero, as in the
+// forward box geometry.  Each kernel is a plain per-node gather: the adjoint
+// is run on the recomputed segments of a checkpointed forward run.
+#pragma once
+#include "dtmx_device.cuh"
+
+namespace dtmx {
+
+struct AdjDev {
+  float* lam[6];            // adjoint of E (0-2) and H (3-5), field layout
+  float* lpsi[3][4];        // adjoint of the CPML auxiliaries, slab layout
+  double* grad;             // [3][nd] dJ/d(1/eps) accumulated in double precision
+  const float* hist;        // [K+1][3][nd] design-region E of the recomputed segment
+  int nd;
+};
+
+// curl table: updated component -> {axis, source component} of its + and - terms
+__device__ __forceinline__ void curl_pair(int c, int t, int& a, int& g) {
+  const int T[6][2][2] = {{{1, 5}, {2, 4}}, {{2, 3}, {0, 5}}, {{0, 4}, {1, 3}},
+                          {{1, 2}, {2, 1}}, {{2, 0}, {0, 2}}, {{0, 1}, {1, 0}}};
+  a = T[c][t][0];
+  g = T[c][t][1];
+}
+
+// w of updated component cu, curl term t, at node (i,j,k); zero outside the grid
+template <int ORDER>
+__device__ __forceinline__ float adj_w(const Params& p, const AdjDev& A, int cu, int t, int i, int j, int k) {
+  if (i < 0 || i >= p.g.n[0] || j < 0 || j >= p.g.n[1] || k < 0 || k >= p.g.n[2]) return 0.f;
+  int a, g;
+  curl_pair(cu, t, a, g);
+  const bool isH = cu >= 3;
+  float sg = t == 0 ? 1.f : -1.f;
+  if (isH) sg = -sg;
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+  float ie = 1.f;
+  if (!isH) {
+    const long long di = design_index(p, i, j, k);
+    const int m = p.mat[cu] ? (int)p.mat[cu][id] : 0;
+    ie = di >= 0 ? p.des_ie[cu][di] : p.mt->inv_eps[m][cu];
+  }
+  float ld = A.lam[cu][id];
+  const int idx[3] = {i, j, k};
+  if (p.ab.kind == 1 && in_slab(p, a, idx[a])) {
+    const int h = 2 * idx[a] + comp_off(cu, a);
+    const float al = __ldg(p.ab.c1[a] + h), gk = __fadd_rn(__ldg(p.ab.c2[a] + h), al);
+    ld = __fmaf_rn(gk, ld, __fmul_rn(al, A.lpsi[a][slot_of(cu, a)][slab_index(p, a, i, j, k)]));
+  }
+  return __fmul_rn(__fmul_rn(sg * p.cdt[a], ie), ld);
+}
+
+// lam of the source field += D^T w of the updated field (updH: the H update)
+template <int ORDER>
+__global__ void adj_gather_kernel(Params p, AdjDev A, int updH) {
+  const long long n = (long long)p.g.n[0] * p.g.n[1] * p.g.n[2];
+  const int t0 = updH ? -2 : -1;
+  const float W4[4] = {1.f / 24.f, -27.f / 24.f, 27.f / 24.f, -1.f / 24.f}, W2[4] = {0.f, -1.f, 1.f, 0.f};
+  const int cu0 = updH ? 3 : 0, cs0 = updH ? 0 : 3;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(q % p.g.n[2]);
+    const long long r = q / p.g.n[2];
+    const int j = (int)(r % p.g.n[1]), i = (int)(r / p.g.n[1]);
+    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+#pragma unroll
+    for (int gs = 0; gs < 3; gs++) {
+      float acc = 0.f;
+      for (int cu = cu0; cu < cu0 + 3; cu++)
+        for (int t = 0; t < 2; t++) {
+          int a, g;
+          curl_pair(cu, t, a, g);
+          if (g != cs0 + gs) continue;
+#pragma unroll
+          for (int o = 0; o < 4; o++) {
+            const float wgt = ORDER == 4 ? W4[o] : W2[o];
+            if (wgt == 0.f) continue;
+            int m[3] = {i, j, k};
+            m[a] -= t0 + o;
+            acc = __fmaf_rn(wgt, adj_w<ORDER>(p, A, cu, t, m[0], m[1], m[2]), acc);
+          }
+        }
+      A.lam[cs0 + gs][id] = __fadd_rn(A.lam[cs0 + gs][id], acc);
+    }
+  }
+}
+
+// lam_psi <- b (lam + lam_psi) over the slab cells of the updated field
+__global__ void adj_psi_kernel(Params p, AdjDev A, int updH, int a) {
+  const int n[3] = {p.g.n[0], p.g.n[1], p.g.n[2]};
+  const int th = p.ab.L[a][0] + p.ab.L[a][1];
+  const long long cnt = (long long)th * ((long long)n[0] * n[1] * n[2] / n[a]);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < cnt; q += (long long)gridDim.x * blockDim.x) {
+    // slab layout of slab_index: a=0 [cs][ny][nz], a=1 [nx][cs][nz], a=2 [nx][ny][cs]
+    int i, j, k, cs;
+    if (a == 0) { k = (int)(q % n[2]); j = (int)((q / n[2]) % n[1]); cs = (int)(q / ((long long)n[1] * n[2])); i = 0; }
+    else if (a == 1) { k = (int)(q % n[2]); cs = (int)((q / n[2]) % th); i = (int)(q / ((long long)th * n[2])); j = 0; }
+    else { cs = (int)(q % th); j = (int)((q / th) % n[1]); i = (int)(q / ((long long)th * n[1])); k = 0; }
+    const int v = cs < p.ab.L[a][0] ? cs : n[a] - p.ab.L[a][1] + (cs - p.ab.L[a][0]);
+    if (a == 0) i = v; else if (a == 1) j = v; else k = v;
+    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+    for (int cu = updH ? 3 : 0; cu < (updH ? 6 : 3); cu++) {
+      const int sl = slot_of(cu, a);
+      if (sl < 0) continue;
+      const int idx[3] = {i, j, k};
+      const float b = __ldg(p.ab.c0[a] + 2 * idx[a] + comp_off(cu, a));
+      A.lpsi[a][sl][q] = __fmul_rn(b, __fadd_rn(A.lam[cu][id], A.lpsi[a][sl][q]));
+    }
+  }
+}
+
+// Objective sources of step s on the plane x = X: F holds the final DFTs
+// (Ey, Ez, Hy, Hz; re, im) of J = sum Re(Ey conj(Hz) - Ez conj(Hy)).
+__global__ void adj_source_kernel(Params p, AdjDev A, const double* F, long long s, int X, double omega, double dt) {
+  const int npl = p.g.n[1] * p.g.n[2];
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= npl) return;
+  const double sE = (double)s, sH = sE - 0.5;
+  double se, ce, sh, ch;
+  sincos(omega * sE * dt, &se, &ce);
+  sincos(omega * sH * dt, &sh, &ch);
+  const double per = ce * dt, pei = -se * dt, phr = ch * dt, phi = -sh * dt;
+  const double* ey = F + (0 * (long long)npl + u) * 2;
+  const double* ez = F + (1 * (long long)npl + u) * 2;
+  const double* hy = F + (2 * (long long)npl + u) * 2;
+  const double* hz = F + (3 * (long long)npl + u) * 2;
+  const int j = u / p.g.n[2], k = u % p.g.n[2];
+  const long long id = (long long)X * p.g.sx + (long long)j * p.g.sy + k;
+  A.lam[1][id] += (float)(per * hz[0] + pei * hz[1]);
+  A.lam[2][id] -= (float)(per * hy[0] + pei * hy[1]);
+  A.lam[5][id] += (float)(ey[0] * phr + ey[1] * phi);
+  A.lam[4][id] -= (float)(ez[0] * phr + ez[1] * phi);
+}
+
+// grad += lam_E (E^s - E^{s-1}) / ie over the design region (hist slots st, st-1)
+__global__ void adj_grad_kernel(Params p, AdjDev A, int st) {
+  const int nd = A.nd;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 3 * nd) return;
+  const int c = q / nd, di = q - c * nd;
+  const int i = p.des_lo[0] + di / (p.des_n[1] * p.des_n[2]);
+  const int j = p.des_lo[1] + (di / p.des_n[2]) % p.des_n[1];
+  const int k = p.des_lo[2] + di % p.des_n[2];
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+  const double dE = (double)A.hist[((long long)st * 3 + c) * nd + di] - (double)A.hist[((long long)(st - 1) * 3 + c) * nd + di];
+  A.grad[q] += (double)A.lam[c][id] * dE / (double)p.des_ie[c][di];
+}
+
+// design-region E into history slot st
+__global__ void design_capture_kernel(Params p, float* hist, int st, int nd) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= 3 * nd) return;
+  const int c = q / nd, di = q - c * nd;
+  const int i = p.des_lo[0] + di / (p.des_n[1] * p.des_n[2]);
+  const int j = p.des_lo[1] + (di / p.des_n[2]) % p.des_n[1];
+  const int k = p.des_lo[2] + di % p.des_n[2];
+  hist[((long long)st * 3 + c) * nd + di] = p.f[c][(long long)i * p.g.sx + (long long)j * p.g.sy + k];
+}
+
+}  // namespace dtmx

@@ -17,6 +17,7 @@
 #include "dtmx_device.cuh"
 #include "dtmx_aux.cuh"
 #include "dtmx_torre.cuh"
+#include "dtmx_adjoint.cuh"
 
 using namespace dtmx;
 
@@ -78,6 +79,12 @@ struct dtmx_ctx {
   TmaMaps maps{};
   int* d_err = nullptr;
   bool has_gyro = false;
+  // design region and the objective of dtmx_forward_adjoint
+  float* d_des_ie[3] = {};
+  std::vector<float> h_des_ie[3];
+  bool monitors_off = false;  // probes and DFT planes paused (recomputed segments)
+  bool obj_on = false;        // capture the objective's flux DFT each step
+  DftHost obj{};
   int gcur = 0;              // gyrotropic current buffer holding J^{n-1/2}
   // wavefront engine
   TorreMaps tmaps{};
@@ -174,6 +181,14 @@ static void setup_grid(dtmx_ctx* ctx) {
     g.safe_lo[a] = g.btype[a][0] == 0 ? -(1 << 28) : g.all_lo[a];
     g.safe_hi[a] = g.btype[a][1] == 0 ? (1 << 28) : g.all_hi[a];
   }
+}
+
+// Does the (plane i, y tile ty, z tile tz) streaming tile intersect the design region?
+static bool design_touches(const dtmx_ctx* ctx, int i, int ty, int tz) {
+  const Params& P = ctx->P;
+  if (!P.des_on) return false;
+  return i >= P.des_lo[0] && i < P.des_lo[0] + P.des_n[0] && ty * TYT < P.des_lo[1] + P.des_n[1] &&
+         ty * TYT + TYT > P.des_lo[1] && tz * TZ < P.des_lo[2] + P.des_n[2] && tz * TZ + TZ > P.des_lo[2];
 }
 
 // ---------------------------------------------------------------- TMA descriptors
@@ -400,6 +415,7 @@ extern "C" void dtmx_destroy(dtmx_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (void* p : ctx->allocs) cudaFree(p);
   for (auto& d : ctx->dfts) { cudaFree(d.omega); cudaFree(d.acc); cudaFree(d.stage); cudaFree(d.sstep); }
+  cudaFree(ctx->obj.omega); cudaFree(ctx->obj.acc); cudaFree(ctx->obj.stage); cudaFree(ctx->obj.sstep);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -435,6 +451,34 @@ static void disp_coeffs(const dtmx_material& M, double dt, MatTable& t, int mi) 
 
 static inline size_t store_index(const dtmx_ctx* ctx, int i, int j, int k) {
   return ((size_t)i * ctx->cfg.ny + j) * ctx->nzp + k;
+}
+
+// Per (plane, y tile, z tile): the common non-dispersive material of all
+// three E components, -1 if mixed, dispersive, gyrotropic or in the design
+// region (selects the simple path of the field kernels).
+static int upload_umat(dtmx_ctx* ctx) {
+  const dtmx_config& c = ctx->cfg;
+  const int nty = ctx->P.nty, ntz = ctx->P.ntz;
+  const bool have = !ctx->h_mat[0].empty();
+  std::vector<signed char> um((size_t)c.nx * nty * ntz);
+  for (int i = 0; i < c.nx; i++)
+    for (int ty = 0; ty < nty; ty++)
+      for (int tz = 0; tz < ntz; tz++) {
+        int m0 = have ? -2 : 0;
+        for (int j = ty * TYT; have && j < std::min(c.ny, ty * TYT + TYT) && m0 != -1; j++)
+          for (int comp = 0; comp < 3 && m0 != -1; comp++) {
+            const uint8_t* row = ctx->h_mat[comp].data() + store_index(ctx, i, j, 0);
+            for (int k = tz * TZ; k < std::min(c.nz, tz * TZ + TZ); k++) {
+              const int m = row[k];
+              if (m0 == -2) m0 = m;
+              if (m != m0 || ctx->mats[m].npoles > 0 || ctx->mats[m].gyro_wp > 0) { m0 = -1; break; }
+            }
+          }
+        um[((size_t)i * nty + ty) * ntz + tz] = (signed char)(m0 < 0 || design_touches(ctx, i, ty, tz) ? -1 : m0);
+      }
+  CK(cudaMemcpyAsync(ctx->d_umat, um.data(), um.size(), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DTMX_OK;
 }
 
 extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int nmat, const uint8_t* idx_x,
@@ -492,29 +536,7 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
   }
   int rc = upload_mattable(ctx);
   if (rc) return rc;
-  {
-    // per (plane, y tile, z tile): the common non-dispersive material of all
-    // three E components, -1 if mixed or dispersive (selects the simple path)
-    const int nty = ctx->P.nty, ntz = ctx->P.ntz;
-    std::vector<signed char> um((size_t)c.nx * nty * ntz);
-    for (int i = 0; i < c.nx; i++)
-      for (int ty = 0; ty < nty; ty++)
-        for (int tz = 0; tz < ntz; tz++) {
-          int m0 = -2;
-          for (int j = ty * TYT; j < std::min(c.ny, ty * TYT + TYT) && m0 != -1; j++)
-            for (int comp = 0; comp < 3 && m0 != -1; comp++) {
-              const uint8_t* row = ctx->h_mat[comp].data() + store_index(ctx, i, j, 0);
-              for (int k = tz * TZ; k < std::min(c.nz, tz * TZ + TZ); k++) {
-                const int m = row[k];
-                if (m0 == -2) m0 = m;
-                if (m != m0 || table[m].npoles > 0 || table[m].gyro_wp > 0) { m0 = -1; break; }
-              }
-            }
-          um[((size_t)i * nty + ty) * ntz + tz] = (signed char)(m0 < 0 ? -1 : m0);
-        }
-    CK(cudaMemcpyAsync(ctx->d_umat, um.data(), um.size(), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-  }
+  if ((rc = upload_umat(ctx))) return rc;
   Ade& A = ctx->P.ade;
   if (hi[0] >= 0) {
     size_t na = 1;
@@ -805,13 +827,21 @@ static int launch_step(dtmx_ctx* ctx) {
     else line_e_kernel<2><<<8, 256, 0, st>>>(ctx->line_e, ctx->line_h, ctx->T.line_n, r1, ctx->line_src, ctx->d_step, c.dt, s.amp, s.f0, s.tau, s.t0);
     nl++;
   }
-  if (!ctx->probes.empty()) {
+  if (!ctx->probes.empty() && !ctx->monitors_off) {
     const int every = c.probe_every > 0 ? c.probe_every : 1;
     probe_kernel<<<((int)ctx->probes.size() + 127) / 128, 128, 0, st>>>(P, ctx->d_probes, (int)ctx->probes.size(), ctx->d_traces,
                                                                        ctx->probe_cap, ctx->d_step, every);
     nl++;
   }
   for (auto& d : ctx->dfts) {
+    if (ctx->monitors_off) break;
+    const long long npts = (long long)d.d.n1 * d.d.n2;
+    dft_capture_kernel<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(P, d.d, ctx->d_step, d.nstaged);
+    nl++;
+    if (++d.nstaged == DFT_STAGE) dft_flush(ctx, d);
+  }
+  if (ctx->obj_on) {
+    DftHost& d = ctx->obj;
     const long long npts = (long long)d.d.n1 * d.d.n2;
     dft_capture_kernel<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(P, d.d, ctx->d_step, d.nstaged);
     nl++;
@@ -988,6 +1018,210 @@ extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ctx, DTMX_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return DTMX_OK;
+}
+
+// ---------------------------------------------------------------- design region and adjoint
+extern "C" int dtmx_set_design(dtmx_ctx* ctx, const int* lo, const int* n, const float* eps) {
+  if (!ctx || !lo || !n || !eps) return fail(ctx, DTMX_ERR_INVALID, "bad design region");
+  const dtmx_config& c = ctx->cfg;
+  const int dim[3] = {c.nx, c.ny, c.nz};
+  for (int a = 0; a < 3; a++)
+    if (n[a] < 1 || lo[a] < 0 || lo[a] + n[a] > dim[a]) return fail(ctx, DTMX_ERR_INVALID, "design region outside the grid");
+  if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "the design region must be set before the first step");
+  const size_t nd = (size_t)n[0] * n[1] * n[2];
+  for (int comp = 0; comp < 3; comp++) {
+    ctx->h_des_ie[comp].resize(nd);
+    for (size_t q = 0; q < nd; q++) {
+      const float e = eps[comp * nd + q];
+      if (!(e > 0)) return fail(ctx, DTMX_ERR_INVALID, "design permittivity must be > 0");
+      ctx->h_des_ie[comp][q] = (float)(1.0 / (double)e);
+    }
+  }
+  for (int comp = 0; comp < 3; comp++) {
+    if (ctx->d_des_ie[comp] && (size_t)ctx->P.des_n[0] * ctx->P.des_n[1] * ctx->P.des_n[2] != nd) ctx->d_des_ie[comp] = nullptr;
+    int rc;
+    if (!ctx->d_des_ie[comp] && (rc = dalloc(ctx, &ctx->d_des_ie[comp], nd))) return rc;
+    CK(cudaMemcpyAsync(ctx->d_des_ie[comp], ctx->h_des_ie[comp].data(), nd * 4, cudaMemcpyHostToDevice, ctx->stream));
+    ctx->P.des_ie[comp] = ctx->d_des_ie[comp];
+  }
+  for (int a = 0; a < 3; a++) { ctx->P.des_lo[a] = lo[a]; ctx->P.des_n[a] = n[a]; }
+  ctx->P.des_on = 1;
+  return upload_umat(ctx);
+}
+
+// device buffers that make up the restartable state of a context
+static void state_parts(dtmx_ctx* ctx, std::vector<std::pair<void*, size_t>>& parts) {
+  parts.clear();
+  for (int comp = 0; comp < 6; comp++) parts.push_back({ctx->P.f[comp], ctx->nstore * 4});
+  for (int a = 0; a < 3; a++) {
+    const size_t cnt = (size_t)(ctx->P.ab.L[a][0] + ctx->P.ab.L[a][1]) * (ctx->ncell / (size_t)ctx->P.g.n[a]);
+    for (int q = 0; q < 4; q++)
+      if (ctx->P.ab.aux[a][q]) parts.push_back({ctx->P.ab.aux[a][q], cnt * 4});
+  }
+  parts.push_back({ctx->d_step, sizeof(long long)});
+  if (ctx->line_e) {
+    parts.push_back({ctx->line_e, (size_t)ctx->T.line_n * 8});
+    parts.push_back({ctx->line_h, (size_t)ctx->T.line_n * 8});
+  }
+}
+
+static int state_copy(dtmx_ctx* ctx, char* ck, bool save) {
+  std::vector<std::pair<void*, size_t>> parts;
+  state_parts(ctx, parts);
+  size_t off = 0;
+  for (auto& pr : parts) {
+    if (save) CK(cudaMemcpyAsync(ck + off, pr.first, pr.second, cudaMemcpyDeviceToDevice, ctx->stream));
+    else CK(cudaMemcpyAsync(pr.first, ck + off, pr.second, cudaMemcpyDeviceToDevice, ctx->stream));
+    off += (pr.second + 255) / 256 * 256;
+  }
+  return DTMX_OK;
+}
+
+static size_t state_bytes(dtmx_ctx* ctx) {
+  std::vector<std::pair<void*, size_t>> parts;
+  state_parts(ctx, parts);
+  size_t off = 0;
+  for (auto& pr : parts) off += (pr.second + 255) / 256 * 256;
+  return off;
+}
+
+extern "C" int dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_every, int plane_x, double omega,
+                                    double* objective, float* grad_eps) {
+  if (!ctx || nsteps < 1 || checkpoint_every < 1 || !objective || !grad_eps) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
+  const dtmx_config& c = ctx->cfg;
+  Params& P = ctx->P;
+  if (!P.des_on) return fail(ctx, DTMX_ERR_STATE, "no design region");
+  if (plane_x < 0 || plane_x >= c.nx) return fail(ctx, DTMX_ERR_INVALID, "objective plane outside the grid");
+  if (c.geometry != DTMX_GEOM_BOX || c.absorber == DTMX_ABS_SPLIT_PML)
+    return fail(ctx, DTMX_ERR_UNSUPPORTED, "the adjoint needs the box geometry with CPML or no absorber");
+  if (P.ade.Em[0] || ctx->has_gyro) return fail(ctx, DTMX_ERR_UNSUPPORTED, "the adjoint supports non-dispersive materials only");
+  for (const auto& q : ctx->psrc) {
+    const long long sz = ctx->nzp, sy = (long long)c.ny * sz;
+    const int i = (int)(q.id / sy), j = (int)((q.id % sy) / sz), k = (int)(q.id % sz);
+    if (design_index(P, i, j, k) >= 0) return fail(ctx, DTMX_ERR_INVALID, "a point source lies in the design region");
+  }
+  int rc = prepare(ctx);
+  if (rc) return rc;
+  const int N = nsteps, K = std::min(checkpoint_every, nsteps);
+  const int nseg = (N + K - 1) / K;
+  const int nd = P.des_n[0] * P.des_n[1] * P.des_n[2];
+  const int npl = c.ny * c.nz;
+  // objective flux DFT on the plane x = plane_x: Ey, Ez, Hy, Hz at omega
+  DftHost& O = ctx->obj;
+  if (!O.acc || O.d.index != plane_x) {
+    cudaFree(O.omega); cudaFree(O.acc); cudaFree(O.stage); cudaFree(O.sstep);
+    O = DftHost{};
+    O.d.axis = 0; O.d.index = plane_x; O.d.comp_mask = (1 << 1) | (1 << 2) | (1 << 4) | (1 << 5); O.d.nfreq = 1;
+    O.d.n1 = c.ny; O.d.n2 = c.nz; O.ncomp = 4;
+    if (cudaMalloc(&O.omega, 8) != cudaSuccess || cudaMalloc(&O.acc, (size_t)4 * npl * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&O.stage, (size_t)DFT_STAGE * 4 * npl * 4) != cudaSuccess || cudaMalloc(&O.sstep, DFT_STAGE * 8) != cudaSuccess)
+      return fail(ctx, DTMX_ERR_OOM, "objective DFT allocation");
+    O.d.omega = O.omega; O.d.acc = O.acc; O.d.stage = O.stage; O.d.sstep = O.sstep;
+  }
+  CK(cudaMemcpyAsync(O.omega, &omega, 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(O.acc, 0, (size_t)4 * npl * sizeof(double2), ctx->stream));
+  O.nstaged = 0;
+  // checkpoints of the state every K steps plus the final state
+  const size_t sb = state_bytes(ctx);
+  std::vector<char*> ck(nseg + 1, nullptr);
+  auto release = [&]() {
+    for (char* q : ck) cudaFree(q);
+  };
+  for (auto& q : ck)
+    if (cudaMalloc(&q, sb) != cudaSuccess) { release(); return fail(ctx, DTMX_ERR_OOM, "checkpoint allocation"); }
+  const long long s0 = ctx->step;
+  ctx->obj_on = true;
+  for (int st = 0; st < N; st++) {
+    if (st % K == 0) state_copy(ctx, ck[st / K], true);
+    if ((rc = launch_step(ctx))) { ctx->obj_on = false; release(); return rc; }
+    ctx->step++;
+  }
+  ctx->obj_on = false;
+  state_copy(ctx, ck[nseg], true);
+  dft_flush(ctx, O);
+  std::vector<double> F((size_t)8 * npl);
+  CK(cudaMemcpyAsync(F.data(), O.acc, F.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  double J = 0;
+  for (int u = 0; u < npl; u++) {
+    const double *ey = &F[(0 * (size_t)npl + u) * 2], *ez = &F[(1 * (size_t)npl + u) * 2];
+    const double *hy = &F[(2 * (size_t)npl + u) * 2], *hz = &F[(3 * (size_t)npl + u) * 2];
+    J += ey[0] * hz[0] + ey[1] * hz[1] - (ez[0] * hy[0] + ez[1] * hy[1]);
+  }
+  *objective = J;
+  // adjoint state
+  AdjDev A{};
+  A.nd = nd;
+  std::vector<void*> tmp;
+  auto tfree = [&]() {
+    for (void* q : tmp) cudaFree(q);
+  };
+  auto talloc = [&](void** q, size_t bytes) {
+    if (cudaMalloc(q, bytes) != cudaSuccess) return false;
+    tmp.push_back(*q);
+    return cudaMemsetAsync(*q, 0, bytes, ctx->stream) == cudaSuccess;
+  };
+  bool ok = true;
+  for (int comp = 0; comp < 6; comp++) ok = ok && talloc((void**)&A.lam[comp], (ctx->nstore + 64) * 4);
+  for (int a = 0; a < 3; a++) {
+    const size_t cnt = (size_t)(P.ab.L[a][0] + P.ab.L[a][1]) * (ctx->ncell / (size_t)P.g.n[a]);
+    for (int q = 0; q < 4; q++) A.lpsi[a][q] = nullptr;
+    if (!P.ab.aux[a][0]) continue;
+    for (int q = 0; q < 4; q++) ok = ok && talloc((void**)&A.lpsi[a][q], cnt * 4);
+  }
+  float* hist = nullptr;
+  double* dF = nullptr;
+  ok = ok && talloc((void**)&A.grad, (size_t)3 * nd * 8) && talloc((void**)&hist, (size_t)(K + 1) * 3 * nd * 4) &&
+       talloc((void**)&dF, F.size() * 8);
+  if (!ok) { tfree(); release(); return fail(ctx, DTMX_ERR_OOM, "adjoint allocation"); }
+  A.hist = hist;
+  CK(cudaMemcpyAsync(dF, F.data(), F.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  const bool o4 = c.order == 4;
+  const long long ncell = (long long)ctx->ncell;
+  const unsigned gb = (unsigned)std::min<long long>((ncell + 255) / 256, 148LL * 32);
+  const unsigned gd = (unsigned)((3 * nd + 255) / 256);
+  ctx->monitors_off = true;
+  for (int seg = nseg - 1; seg >= 0; seg--) {
+    const int start = seg * K, len = std::min(N, start + K) - start;
+    state_copy(ctx, ck[seg], false);
+    ctx->step = s0 + start;
+    design_capture_kernel<<<gd, 256, 0, ctx->stream>>>(ctx->P, hist, 0, nd);
+    for (int q = 1; q <= len; q++) {
+      if ((rc = launch_step(ctx))) break;
+      ctx->step++;
+      design_capture_kernel<<<gd, 256, 0, ctx->stream>>>(ctx->P, hist, q, nd);
+    }
+    if (rc) break;
+    for (int q = len; q >= 1; q--) {
+      adj_source_kernel<<<(npl + 255) / 256, 256, 0, ctx->stream>>>(P, A, dF, s0 + start + q, plane_x, omega, c.dt);
+      adj_grad_kernel<<<gd, 256, 0, ctx->stream>>>(P, A, q);
+      for (int updH = 0; updH < 2; updH++) {
+        if (o4) adj_gather_kernel<4><<<gb, 256, 0, ctx->stream>>>(P, A, updH);
+        else adj_gather_kernel<2><<<gb, 256, 0, ctx->stream>>>(P, A, updH);
+        for (int a = 0; a < 3; a++) {
+          if (!A.lpsi[a][0]) continue;
+          const long long cnt = (long long)(P.ab.L[a][0] + P.ab.L[a][1]) * (ncell / P.g.n[a]);
+          adj_psi_kernel<<<(unsigned)std::min<long long>((cnt + 255) / 256, 148LL * 32), 256, 0, ctx->stream>>>(P, A, updH, a);
+        }
+      }
+    }
+  }
+  ctx->monitors_off = false;
+  state_copy(ctx, ck[nseg], false);
+  ctx->step = s0 + N;
+  std::vector<double> g((size_t)3 * nd);
+  CK(cudaMemcpyAsync(g.data(), A.grad, g.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  tfree();
+  release();
+  if (rc) return rc;
+  if (e != cudaSuccess) return fail(ctx, DTMX_ERR_CUDA, std::string("adjoint: ") + cudaGetErrorString(e));
+  for (int comp = 0; comp < 3; comp++)
+    for (int q = 0; q < nd; q++) {
+      const double ie = ctx->h_des_ie[comp][q];
+      grad_eps[(size_t)comp * nd + q] = (float)(-ie * ie * g[(size_t)comp * nd + q]);
+    }
   return DTMX_OK;
 }
 

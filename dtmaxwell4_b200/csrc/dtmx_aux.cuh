@@ -171,7 +171,8 @@ __global__ void tfsf_kernel(Params p, TfsfDev t, const long long* d_step, int is
   const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
   if (!isH) {
     const int mi = p.mat[c] ? (int)p.mat[c][id] : 0;
-    total *= (double)p.mt->inv_eps[mi][c];
+    const long long di = design_index(p, i, j, k);
+    total *= (double)(di >= 0 ? p.des_ie[c][di] : p.mt->inv_eps[mi][c]);
   }
   p.f[c][id] += (float)total;
 }

@@ -85,7 +85,18 @@ struct Params {
   // nodes of that plane tile, or -1 when mixed/dispersive
   const signed char* umat;
   int ntz, nty;              // tiles along z and y
+  // design region: per-node 1/eps of the E components over a cell box
+  const float* des_ie[3];
+  int des_lo[3], des_n[3];
+  int des_on;
 };
+
+__host__ __device__ __forceinline__ long long design_index(const Params& p, int i, int j, int k) {
+  if (!p.des_on) return -1;
+  const int a = i - p.des_lo[0], b = j - p.des_lo[1], c = k - p.des_lo[2];
+  if (a < 0 || a >= p.des_n[0] || b < 0 || b >= p.des_n[1] || c < 0 || c >= p.des_n[2]) return -1;
+  return ((long long)a * p.des_n[1] + b) * p.des_n[2] + c;
+}
 
 // TMA descriptors of one context: source tiles (40 z x rows y x 1 plane),
 // own-value tiles (32 x 16 x 1) of every component and material tiles.
@@ -429,7 +440,8 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
             continue;
           }
         }
-        const float ie = ms.inv_eps[m][c];
+        const long long di = design_index(p, i, j, k);
+        const float ie = di >= 0 ? p.des_ie[c][di] : ms.inv_eps[m][c];
         d[c][0] = __fmul_rn(d[c][0], ie); d[c][1] = __fmul_rn(d[c][1], ie); d[c][2] = __fmul_rn(d[c][2], ie);
       }
       float inc = sum3(d[c][0], d[c][1], d[c][2]);

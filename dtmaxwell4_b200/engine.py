@@ -23,6 +23,7 @@ EXPORTS = (
     "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_get_stream",
     "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
     "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
+    "dtmx_set_design", "dtmx_forward_adjoint",
 )
 
 
@@ -69,6 +70,8 @@ def load():
     L.dtmx_set_profiling.argtypes = [vp, ip]
     L.dtmx_read_profile.argtypes = [vp, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int64)]
     L.dtmx_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
+    L.dtmx_set_design.argtypes = [vp, C.POINTER(ip), C.POINTER(ip), vp]
+    L.dtmx_forward_adjoint.argtypes = [vp, ip, ip, ip, C.c_double, C.POINTER(C.c_double), vp]
     L.dtmx_count_nonfinite_noalloc.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int64, C.POINTER(C.c_int64)]
     _lib = L
     return L
@@ -155,6 +158,24 @@ class Simulation:
 
     def set_engine(self, engine, time_block=0):
         self._ck(self._L.dtmx_set_engine(self._h, engine, time_block))
+
+    # ---- differentiation
+    def set_design(self, lo, eps):
+        """Per-node permittivity (shape (3, n0, n1, n2)) of the E components
+        over the cell box starting at lo."""
+        eps = np.ascontiguousarray(eps, dtype=np.float32)
+        assert eps.ndim == 4 and eps.shape[0] == 3
+        self._design = (tuple(int(v) for v in lo), eps.shape[1:])
+        self._ck(self._L.dtmx_set_design(self._h, (C.c_int * 3)(*self._design[0]), (C.c_int * 3)(*eps.shape[1:]),
+                                         eps.ctypes.data))
+
+    def forward_adjoint(self, nsteps, plane_x, omega, checkpoint_every=100):
+        """Advance nsteps; return (J, dJ/d eps) of the Poynting-flux objective."""
+        grad = np.zeros((3,) + tuple(self._design[1]), np.float32)
+        J = C.c_double()
+        self._ck(self._L.dtmx_forward_adjoint(self._h, int(nsteps), int(checkpoint_every), int(plane_x), float(omega),
+                                              C.byref(J), grad.ctypes.data))
+        return J.value, grad
 
     # ---- run
     def step(self, n):

@@ -275,6 +275,29 @@ int  dtmx_ref_material_table(dtmx_material* out, int n);
  * Tsteps/Ntime calls of dtmx_step(Ntime) (calcStep).  Returns 0 on success. */
 int  dtmx_ref_main(const dtmx_ref_globals* g, const dtmx_tfsfsrc* shotpoint, int argc, char** argv);
 
+/* ---- differentiation (no reference counterpart: the reference has no
+ * gradient path) -------------------------------------------------------------- */
+
+/* Per-node permittivity of the three E components over the cell box
+ * [lo, lo+n): eps holds 3*n0*n1*n2 values (component-major, z fastest).  Inside
+ * the box it replaces the material permittivity (the materials there must be
+ * non-dispersive).  Set before the first step. */
+int  dtmx_set_design(dtmx_ctx* ctx, const int lo[3], const int n[3], const float* eps);
+
+/* Advance nsteps from the current state and return the objective
+ *   J = sum over the plane x = plane_x of Re(Ey^ conj(Hz^) - Ez^ conj(Hy^)),
+ * the Poynting flux of the running DFTs at omega (E^ = sum_s E^s e^{-i w s dt} dt,
+ * H^ with t = (s - 1/2) dt), and dJ/d eps at every design node (3*nd floats,
+ * the layout of dtmx_set_design).  The gradient is the discrete adjoint of the
+ * update (transposed stencils and CPML recursions), run backward over
+ * segments of checkpoint_every steps that are recomputed from state
+ * checkpoints kept in device memory; the accumulation is in double precision.
+ * Box geometry, CPML or no absorber, non-dispersive materials, no point source
+ * inside the design region.  On return the context holds the state after
+ * nsteps, as after dtmx_step(nsteps). */
+int  dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_every, int plane_x, double omega,
+                          double* objective, float* grad_eps);
+
 /* Count NaN/Inf values in nfields caller-owned device arrays of nelem floats
  * each, without allocating any device memory (no cudaMalloc/cudaFree and no
  * allocating library routine).  For callers that cannot allocate: processes

@@ -93,6 +93,9 @@ typedef struct {
   real gjc[DTMX_MAX_MATERIALS];
   int has_gyro, gcur;
   real* Jg[2][3];
+  /* design region: per-node 1/eps of each E component over a cell box */
+  int des_on, des_lo[3], des_n[3];
+  real* des_ie[3];
   /* sources */
   dtmx_point_source psrc[64]; int npsrc;
   int has_tfsf; dtmx_tfsf tfsf;
@@ -470,6 +473,21 @@ static int near_box(const osim* s, int X, int Y, int Z) {
   return close;
 }
 
+/* design-region index of cell (i,j,k), -1 outside */
+static long des_index(const osim* s, int i, int j, int k) {
+  if (!s->des_on) return -1;
+  int v[3] = {i - s->des_lo[0], j - s->des_lo[1], k - s->des_lo[2]};
+  for (int a = 0; a < 3; a++) if (v[a] < 0 || v[a] >= s->des_n[a]) return -1;
+  return ((long)v[0] * s->des_n[1] + v[1]) * s->des_n[2] + v[2];
+}
+
+/* 1/eps of E component c at a non-dispersive node: the design value inside the
+ * design region, else the material's */
+static real node_ie(const osim* s, int c, int mi, int i, int j, int k) {
+  long di = des_index(s, i, j, k);
+  return di >= 0 ? s->des_ie[c][di] : s->inv_eps[mi][c];
+}
+
 /* ADE-box index of cell (i,j,k), -1 outside the box */
 static long ade_index(const osim* s, int i, int j, int k) {
   if (i < s->ade_box[0][0] || i >= s->ade_box[0][1] || j < s->ade_box[1][0] || j >= s->ade_box[1][1] ||
@@ -587,7 +605,7 @@ static void half_step(osim* s, int isH) {
               *F = Ep;
               continue;
             }
-            real ie = s->inv_eps[mi][c];
+            real ie = node_ie(s, c, mi, i, j, k);
             dif[0] *= ie; dif[1] *= ie; dif[2] *= ie;
           }
           /* absorber */
@@ -671,7 +689,7 @@ void PFX(destroy)(void* h) {
   for (int c = 0; c < 3; c++) {
     free(s->Em[c]);
     for (int p = 0; p < DTMX_MAX_POLES; p++) { free(s->Jp[c][p]); free(s->Jm[c][p]); }
-    free(s->Jg[0][c]); free(s->Jg[1][c]);
+    free(s->Jg[0][c]); free(s->Jg[1][c]); free(s->des_ie[c]);
   }
   free(s->line_e); free(s->line_h); free(s->traces);
   for (int d = 0; d < s->ndft; d++) { free(s->dft[d].omega); free(s->dft[d].acc); }
@@ -931,4 +949,209 @@ int PFX(threads)(void) {
 #else
   return 1;
 #endif
+}
+
+
+/* ------------------------------------------------------------------ adjoint
+ * Discrete adjoint of the forward step for the gradient of a Poynting-flux
+ * objective with respect to per-node permittivity in a design region.
+ *
+ * Forward step (box geometry, CPML or none, non-dispersive):
+ *   H' = H + sum_a g_a d_a + sum_slab b_a psi_a,  psi_a' = b_a psi_a + al_a d_a,
+ *   d_a = s_a D_a(E)  (H half step),  then the same for E with d_a = ie s_a D_a(H'),
+ * where g_a = 1 outside the axis-a slab and 1/kappa_a + al_a inside, and the
+ * staggered difference operators satisfy D_E^T = -D_H (zero outside the box).
+ * The adjoint step applies the transposes in reverse order.
+ *
+ * Objective: J = sum over the plane x = X of Re(Ey^ conj(Hz^) - Ez^ conj(Hy^)),
+ * with E^ = sum_s E^s exp(-i w s dt) dt and H^ = sum_s H^{s-1/2} exp(-i w (s-1/2) dt) dt
+ * (the engine's DFT convention).  Gradient: dJ/d ie_c(p) =
+ * sum_s lamE_c^s(p) (E_c^s(p) - E_c^{s-1}(p)) / ie_c(p), dJ/d eps = -ie^2 dJ/d ie.
+ */
+int PFX(set_design)(void* h, const int* lo, const int* n, const double* eps) {
+  osim* s = h;
+  size_t nd = (size_t)n[0] * n[1] * n[2];
+  for (int a = 0; a < 3; a++)
+    if (n[a] < 1 || lo[a] < 0 || lo[a] + n[a] > (a == 0 ? s->nx : a == 1 ? s->ny : s->nz)) return DTMX_ERR_INVALID;
+  for (int c = 0; c < 3; c++) {
+    free(s->des_ie[c]);
+    s->des_ie[c] = malloc(nd * sizeof(real));
+    for (size_t q = 0; q < nd; q++) s->des_ie[c][q] = (real)(1.0 / eps[c * nd + q]);
+  }
+  for (int a = 0; a < 3; a++) { s->des_lo[a] = lo[a]; s->des_n[a] = n[a]; }
+  s->des_on = 1;
+  return DTMX_OK;
+}
+
+/* slab coefficients of axis a at half-coordinate hc: g (update gain), b, al */
+static void slab_coefs(const osim* s, int a, int hc, int inslab, double* g, double* b, double* al) {
+  if (!inslab) { *g = 1; *b = 0; *al = 0; return; }
+  *b = s->cb[a][hc]; *al = s->ca[a][hc]; *g = s->cik[a][hc] + s->ca[a][hc];
+}
+
+static real lget(const osim* s, real* const* arr, int c, int i, int j, int k) {
+  if (i < 0 || i >= s->nx || j < 0 || j >= s->ny || k < 0 || k >= s->nz) return 0;
+  return arr[c][IDX(s, i, j, k)];
+}
+
+/* w_{c,a}(p) = s_a ie(p) (g lam(p) + al lampsi(p)) for updated component c at
+ * node p (the adjoint of d_a), zero outside the grid */
+static double adj_w(const osim* s, real* const* lam, real* const lpsi[3][4], int c, int t, int i, int j, int k) {
+  if (i < 0 || i >= s->nx || j < 0 || j >= s->ny || k < 0 || k >= s->nz) return 0;
+  const dtmx_config* cf = &s->cfg;
+  const double dd[3] = {cf->dx, cf->dy, cf->dz};
+  int a = CURL[c][t][0];
+  int isH = c >= 3;
+  double sg = t == 0 ? 1 : -1;
+  if (isH) sg = -sg;
+  double sa = sg * cf->dt / dd[a];
+  size_t id = IDX(s, i, j, k);
+  double ie = 1;
+  if (!isH) ie = node_ie(s, c, s->midx[c] ? s->midx[c][id] : 0, i, j, k);
+  int sl = slot_of(c, a);
+  long si = (cf->absorber == DTMX_ABS_CPML && s->L[a][0] + s->L[a][1] > 0) ? slab_index(s, a, i, j, k) : -1;
+  int nn[3] = {i, j, k};
+  double g, b, al;
+  slab_coefs(s, a, 2 * nn[a] + OFF[c][a], si >= 0, &g, &b, &al);
+  double ld = g * lam[c][id] + (si >= 0 ? al * lpsi[a][sl][si] : 0);
+  return sa * ie * ld;
+}
+
+/* lam of the source field += D^T of the w of the updated field (one half step) */
+static void adj_half(osim* s, real** lam, real* lpsi[3][4], int updH) {
+  /* updated components cu (H if updH), sources cs */
+  int cu0 = updH ? 3 : 0, cs0 = updH ? 0 : 3;
+  int order = s->cfg.order;
+  /* taps of the forward derivative of the updated component: offsets t0..t0+3 */
+  int t0 = updH ? -2 : -1;
+  const double W4[4] = {1.0 / 24, -27.0 / 24, 27.0 / 24, -1.0 / 24}, W2[4] = {0, -1, 1, 0};
+  const double* W = order == 4 ? W4 : W2;
+  real* add[3];
+  for (int c = 0; c < 3; c++) add[c] = calloc(s->ncell, sizeof(real));
+  for (int cu = cu0; cu < cu0 + 3; cu++)
+    for (int t = 0; t < 2; t++) {
+      int a = CURL[cu][t][0], g = CURL[cu][t][1];
+      #pragma omp parallel for schedule(static)
+      for (int i = 0; i < s->nx; i++)
+        for (int j = 0; j < s->ny; j++)
+          for (int k = 0; k < s->nz; k++) {
+            /* source node q = (i,j,k) of component g receives from updated nodes p = q - (t0+o) e_a */
+            double acc = 0;
+            for (int o = 0; o < 4; o++) {
+              if (W[o] == 0) continue;
+              int m[3] = {i, j, k};
+              m[a] -= t0 + o;
+              acc += W[o] * adj_w(s, lam, lpsi, cu, t, m[0], m[1], m[2]);
+            }
+            add[g - cs0][IDX(s, i, j, k)] += (real)acc;
+          }
+    }
+  /* slab adjoint recursion of the updated field: lampsi <- b (lam + lampsi) */
+  if (s->cfg.absorber == DTMX_ABS_CPML)
+    for (int cu = cu0; cu < cu0 + 3; cu++)
+      for (int a = 0; a < 3; a++) {
+        int sl = slot_of(cu, a);
+        if (sl < 0 || s->L[a][0] + s->L[a][1] == 0) continue;
+        for (int i = 0; i < s->nx; i++)
+          for (int j = 0; j < s->ny; j++)
+            for (int k = 0; k < s->nz; k++) {
+              long si = slab_index(s, a, i, j, k);
+              if (si < 0) continue;
+              int nn[3] = {i, j, k};
+              double g, b, al;
+              slab_coefs(s, a, 2 * nn[a] + OFF[cu][a], 1, &g, &b, &al);
+              lpsi[a][sl][si] = (real)(b * (lam[cu][IDX(s, i, j, k)] + lpsi[a][sl][si]));
+            }
+      }
+  for (int c = 0; c < 3; c++) {
+    for (size_t q = 0; q < s->ncell; q++) lam[cs0 + c][q] += add[c][q];
+    free(add[c]);
+  }
+}
+
+int PFX(forward_adjoint)(void* h, int nsteps, int X, double omega, double* J_out, double* grad_out) {
+  osim* s = h;
+  if (!s->des_on || X < 0 || X >= s->nx || nsteps < 1) return DTMX_ERR_INVALID;
+  if (s->cfg.geometry != DTMX_GEOM_BOX || s->cfg.absorber == DTMX_ABS_SPLIT_PML || s->ade_n) return DTMX_ERR_UNSUPPORTED;
+  const double dt = s->cfg.dt;
+  const size_t nd = (size_t)s->des_n[0] * s->des_n[1] * s->des_n[2];
+  const size_t npl = (size_t)s->ny * s->nz;
+  /* forward: design-region E history and the flux DFT */
+  real* hist = malloc((size_t)(nsteps + 1) * 3 * nd * sizeof(real));
+  double* F = calloc(4 * npl * 2, sizeof(double));   /* Ey, Ez, Hy, Hz (re, im) */
+  int64_t s0 = s->step;
+  for (int st = 0; st <= nsteps; st++) {
+    if (st > 0) PFX(step)(h, 1);
+    for (int c = 0; c < 3; c++)
+      for (int i = 0; i < s->des_n[0]; i++)
+        for (int j = 0; j < s->des_n[1]; j++)
+          for (int k = 0; k < s->des_n[2]; k++)
+            hist[((size_t)st * 3 + c) * nd + ((size_t)i * s->des_n[1] + j) * s->des_n[2] + k] =
+                s->f[c][IDX(s, s->des_lo[0] + i, s->des_lo[1] + j, s->des_lo[2] + k)];
+    if (st == 0) continue;
+    double sE = (double)(s->step), sH = sE - 0.5;
+    double pe[2] = {cos(omega * sE * dt) * dt, -sin(omega * sE * dt) * dt};
+    double ph[2] = {cos(omega * sH * dt) * dt, -sin(omega * sH * dt) * dt};
+    const int comp[4] = {DTMX_EY, DTMX_EZ, DTMX_HY, DTMX_HZ};
+    for (int q = 0; q < 4; q++)
+      for (size_t u = 0; u < npl; u++) {
+        double v = s->f[comp[q]][(size_t)X * npl + u];
+        const double* pp = q < 2 ? pe : ph;
+        F[(q * npl + u) * 2] += v * pp[0];
+        F[(q * npl + u) * 2 + 1] += v * pp[1];
+      }
+  }
+  /* J = sum Re(Ey conj(Hz)) - Re(Ez conj(Hy)) */
+  double J = 0;
+  for (size_t u = 0; u < npl; u++) {
+    const double *ey = F + (0 * npl + u) * 2, *ez = F + (1 * npl + u) * 2, *hy = F + (2 * npl + u) * 2, *hz = F + (3 * npl + u) * 2;
+    J += ey[0] * hz[0] + ey[1] * hz[1] - (ez[0] * hy[0] + ez[1] * hy[1]);
+  }
+  *J_out = J;
+  /* backward */
+  real* lam[6];
+  for (int c = 0; c < 6; c++) lam[c] = calloc(s->ncell, sizeof(real));
+  real* lpsi[3][4];
+  for (int a = 0; a < 3; a++) {
+    size_t th = (size_t)(s->L[a][0] + s->L[a][1]);
+    size_t ns = th * (a == 0 ? npl : a == 1 ? (size_t)s->nx * s->nz : (size_t)s->nx * s->ny);
+    for (int q = 0; q < 4; q++) lpsi[a][q] = calloc(ns ? ns : 1, sizeof(real));
+  }
+  double* grad = calloc(3 * nd, sizeof(double));
+  for (int st = nsteps; st >= 1; st--) {
+    double sE = (double)(s0 + st), sH = sE - 0.5;
+    double pe[2] = {cos(omega * sE * dt) * dt, -sin(omega * sE * dt) * dt};
+    double ph[2] = {cos(omega * sH * dt) * dt, -sin(omega * sH * dt) * dt};
+    /* objective sources at x^st = (E^st, H^{st-1/2}) */
+    for (size_t u = 0; u < npl; u++) {
+      const double *ey = F + (0 * npl + u) * 2, *ez = F + (1 * npl + u) * 2, *hy = F + (2 * npl + u) * 2, *hz = F + (3 * npl + u) * 2;
+      size_t id = (size_t)X * npl + u;
+      lam[DTMX_EY][id] += (real)(pe[0] * hz[0] + pe[1] * hz[1]);
+      lam[DTMX_EZ][id] -= (real)(pe[0] * hy[0] + pe[1] * hy[1]);
+      lam[DTMX_HZ][id] += (real)(ey[0] * ph[0] + ey[1] * ph[1]);
+      lam[DTMX_HY][id] -= (real)(ez[0] * ph[0] + ez[1] * ph[1]);
+    }
+    /* gradient with respect to ie of the E update of step st */
+    for (int c = 0; c < 3; c++)
+      for (int i = 0; i < s->des_n[0]; i++)
+        for (int j = 0; j < s->des_n[1]; j++)
+          for (int k = 0; k < s->des_n[2]; k++) {
+            size_t di = ((size_t)i * s->des_n[1] + j) * s->des_n[2] + k;
+            size_t id = IDX(s, s->des_lo[0] + i, s->des_lo[1] + j, s->des_lo[2] + k);
+            double dE = (double)hist[((size_t)st * 3 + c) * nd + di] - (double)hist[((size_t)(st - 1) * 3 + c) * nd + di];
+            grad[c * nd + di] += (double)lam[c][id] * dE / (double)s->des_ie[c][di];
+          }
+    /* lam^{st-1} = A^T lam^{st}: E update transposed, then H update transposed */
+    adj_half(s, lam, lpsi, 0);
+    adj_half(s, lam, lpsi, 1);
+  }
+  for (int c = 0; c < 3; c++)
+    for (size_t q = 0; q < nd; q++) {
+      double ie = s->des_ie[c][q];
+      grad_out[c * nd + q] = -ie * ie * grad[c * nd + q];
+    }
+  for (int c = 0; c < 6; c++) free(lam[c]);
+  for (int a = 0; a < 3; a++) for (int q = 0; q < 4; q++) free(lpsi[a][q]);
+  free(grad); free(hist); free(F);
+  return DTMX_OK;
 }

@@ -41,6 +41,9 @@ def lib():
             g("set_field").argtypes = [C.c_void_p, C.c_int, C.c_void_p]
             g("read_probes").argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
             g("read_dft").argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+            g("set_design").argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p]
+            g("forward_adjoint").argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double),
+                                             C.c_void_p]
         _lib = L
     return _lib
 
@@ -101,6 +104,27 @@ class OracleSim:
 
     def step(self, n):
         self._f("step")(self._h, int(n))
+
+    def set_design(self, lo, eps):
+        """Per-node permittivity of the three E components over the cell box
+        starting at lo; eps has shape (3, n0, n1, n2)."""
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        self._design = (tuple(lo), eps.shape[1:])
+        lo_c = (C.c_int * 3)(*lo)
+        n_c = (C.c_int * 3)(*eps.shape[1:])
+        if self._f("set_design")(self._h, lo_c, n_c, eps.ctypes.data) != 0:
+            raise ValueError("bad design region")
+
+    def forward_adjoint(self, nsteps, plane_x, omega):
+        """Run nsteps forward, return (J, dJ/d eps) for the Poynting flux
+        through the plane x = plane_x at omega (discrete adjoint, FP64)."""
+        shape = self._design[1]
+        grad = np.zeros((3,) + tuple(shape), np.float64)
+        J = C.c_double()
+        rc = self._f("forward_adjoint")(self._h, int(nsteps), int(plane_x), float(omega), C.byref(J), grad.ctypes.data)
+        if rc != 0:
+            raise ValueError("forward_adjoint failed: %d" % rc)
+        return J.value, grad
 
     def get_field(self, comp):
         out = np.empty(self.shape, dtype=np.float64)

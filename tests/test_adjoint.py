@@ -1,0 +1,131 @@
+"""Gradient of a Poynting-flux objective with respect to per-node
+permittivity by the discrete adjoint.
+
+Oracle (CPU): the FP64 adjoint equals central finite differences of the FP64
+forward.  GPU: the FP32 engine's adjoint (checkpointed recompute) against the
+FP64 adjoint and against its own central differences, checkpoint-interval
+invariance, the final state, and the torch.autograd binding.
+"""
+import math
+
+import numpy as np
+import pytest
+
+N_STEPS, PLANE_X, OMEGA = 60, 15, 2 * math.pi / 8.0
+LO = (9, 7, 7)
+
+
+def _eps():
+    return np.random.default_rng(1).uniform(1, 4, size=(3, 3, 3, 3))
+
+
+def _setup(sim, order):
+    from dtmaxwell4_b200 import abi, scenarios
+    f0, tau, t0 = scenarios.gauss_sine_params(8.0)
+    sim.add_point_source(abi.PointSource(comp=abi.EZ, i=6, j=9, k=9, waveform=abi.WAVE_GAUSS_SINE, amp=1.0, f0=f0,
+                                         tau=tau, t0=t0))
+    return sim
+
+
+def _cfg(order):
+    from dtmaxwell4_b200 import abi
+    return abi.make_config(22, 18, 18, dx=1.0, courant=0.5 if order == 2 else 0.4, order=order,
+                           absorber=abi.ABS_CPML, pml=4)
+
+
+def _oracle(order, eps):
+    import pyoracle
+    o = _setup(pyoracle.OracleSim(_cfg(order)), order)
+    o.set_design(LO, eps)
+    return o.forward_adjoint(N_STEPS, PLANE_X, OMEGA)
+
+
+@pytest.mark.parametrize("order", [2, 4])
+def test_oracle_adjoint_matches_finite_differences(order):
+    eps = _eps()
+    J, g = _oracle(order, eps)
+    assert J != 0
+    for cell in [(2, 1, 1, 1), (0, 0, 2, 1), (2, 0, 0, 2)]:
+        h = 1e-4
+        ep, em = eps.copy(), eps.copy()
+        ep[cell] += h
+        em[cell] -= h
+        fd = (_oracle(order, ep)[0] - _oracle(order, em)[0]) / (2 * h)
+        assert abs(g[cell] - fd) <= 1e-6 * abs(fd), (cell, g[cell], fd)
+
+
+def _gpu(order, eps, K=100):
+    from dtmaxwell4_b200 import Simulation
+    s = _setup(Simulation(_cfg(order)), order)
+    s.set_design(LO, eps)
+    J, g = s.forward_adjoint(N_STEPS, PLANE_X, OMEGA, K)
+    return J, g, s
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("order", [2, 4])
+def test_gpu_adjoint_against_fp64_adjoint(order):
+    eps = _eps()
+    J, g, s = _gpu(order, eps)
+    s.close()
+    Jo, go = _oracle(order, eps.astype(np.float32).astype(np.float64))
+    assert abs(J - Jo) <= 1e-5 * abs(Jo), (J, Jo)
+    cos = float((g * go).sum() / (np.linalg.norm(g) * np.linalg.norm(go)))
+    rel = float(np.linalg.norm(g - go) / np.linalg.norm(go))
+    assert cos >= 0.9999 and rel <= 1e-3, (cos, rel)
+
+
+@pytest.mark.gpu
+def test_gpu_adjoint_against_central_differences():
+    """16 seeded cells, h = 1e-3 (the FP32 forward differenced)."""
+    eps = _eps().astype(np.float32)
+    J, g, s = _gpu(2, eps)
+    s.close()
+    rng = np.random.default_rng(5)
+    cells = [tuple(int(v) for v in (rng.integers(3), *rng.integers(0, 3, size=3))) for _ in range(16)]
+    fd, ad = [], []
+    for cell in cells:
+        h = 1e-3
+        ep, em = eps.copy(), eps.copy()
+        ep[cell] += h
+        em[cell] -= h
+        Jp, _, sp = _gpu(2, ep)
+        sp.close()
+        Jm, _, sm = _gpu(2, em)
+        sm.close()
+        fd.append((Jp - Jm) / (2 * h))
+        ad.append(float(g[cell]))
+    fd, ad = np.array(fd), np.array(ad)
+    cos = float(fd @ ad / (np.linalg.norm(fd) * np.linalg.norm(ad)))
+    assert cos >= 0.999, (cos, fd, ad)
+
+
+@pytest.mark.gpu
+def test_gpu_adjoint_checkpoint_interval_and_final_state():
+    from dtmaxwell4_b200 import Simulation
+    eps = _eps()
+    J1, g1, s1 = _gpu(4, eps, K=100)
+    J2, g2, s2 = _gpu(4, eps, K=7)
+    assert J1 == J2 and np.array_equal(g1, g2)
+    ref = _setup(Simulation(_cfg(4)), 4)
+    ref.set_design(LO, eps)
+    ref.step(N_STEPS)
+    for c in range(6):
+        assert np.array_equal(s2.get_field(c), ref.get_field(c)), c
+    for q in (s1, s2, ref):
+        q.close()
+
+
+@pytest.mark.gpu
+def test_torch_autograd_binding():
+    import torch
+    from dtmaxwell4_b200 import Simulation
+    from dtmaxwell4_b200.autograd import flux_objective
+    eps0 = _eps()
+    eps = torch.tensor(eps0, dtype=torch.float32, requires_grad=True)
+    J = flux_objective(eps, lambda: _setup(Simulation(_cfg(2)), 2), LO, N_STEPS, PLANE_X, OMEGA)
+    (2.0 * J).backward()
+    Jd, gd, s = _gpu(2, eps0)
+    s.close()
+    assert float(J.detach()) == pytest.approx(Jd, rel=1e-6)
+    np.testing.assert_allclose(eps.grad.numpy(), 2.0 * gd, rtol=1e-6, atol=0)
