@@ -24,14 +24,21 @@ struct AdjDev {
   double* grad;             // [3][nd] dJ/d(1/eps) accumulated in double precision
   const float* hist;        // [K+1][3][nd] design-region E of the recomputed segment
   int nd;
+  float* w[3][2];           // adjoint of the scaled derivative terms d of the updated field, field layout
 };
 
 // curl table: updated component -> {axis, source component} of its + and - terms
+__host__ __device__ __forceinline__ constexpr int curl_axis(int c, int t) {
+  // Ex: y,z  Ey: z,x  Ez: x,y  (same pattern for H)
+  return ((c % 3) + 1 + t) % 3;
+}
+__host__ __device__ __forceinline__ constexpr int curl_src(int c, int t) {
+  // Ex: Hz,Hy  Ey: Hx,Hz  Ez: Hy,Hx ; Hx: Ez,Ey  Hy: Ex,Ez  Hz: Ey,Ex
+  return (c < 3 ? 3 : 0) + ((c % 3) + 2 - t) % 3;
+}
 __device__ __forceinline__ void curl_pair(int c, int t, int& a, int& g) {
-  const int T[6][2][2] = {{{1, 5}, {2, 4}}, {{2, 3}, {0, 5}}, {{0, 4}, {1, 3}},
-                          {{1, 2}, {2, 1}}, {{2, 0}, {0, 2}}, {{0, 1}, {1, 0}}};
-  a = T[c][t][0];
-  g = T[c][t][1];
+  a = curl_axis(c, t);
+  g = curl_src(c, t);
 }
 
 // w of updated component cu, curl term t, at node (i,j,k); zero outside the grid
@@ -60,61 +67,71 @@ __device__ __forceinline__ float adj_w(const Params& p, const AdjDev& A, int cu,
   return __fmul_rn(__fmul_rn(sg * p.cdt[a], ie), ld);
 }
 
-// lam of the source field += D^T w of the updated field (updH: the H update)
-template <int ORDER>
-__global__ void adj_gather_kernel(Params p, AdjDev A, int updH) {
-  const long long n = (long long)p.g.n[0] * p.g.n[1] * p.g.n[2];
-  const int t0 = updH ? -2 : -1;
-  const float W4[4] = {1.f / 24.f, -27.f / 24.f, 27.f / 24.f, -1.f / 24.f}, W2[4] = {0.f, -1.f, 1.f, 0.f};
-  const int cu0 = updH ? 3 : 0, cs0 = updH ? 0 : 3;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(q % p.g.n[2]);
-    const long long r = q / p.g.n[2];
-    const int j = (int)(r % p.g.n[1]), i = (int)(r / p.g.n[1]);
-    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+// w of the updated field at every node (3 components x 2 curl terms), then
+// the slab recursion lam_psi <- b (lam + lam_psi) (w uses the old lam_psi).
+// One thread per node: blockIdx.z = x plane, (threadIdx.x, blockIdx.x) = z,
+// (threadIdx.y, blockIdx.y) = y.
+template <int ORDER, int UPDH>
+__global__ void adj_w_kernel(Params p, AdjDev A) {
+  constexpr int updH = UPDH;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, i = blockIdx.z;
+  if (j >= p.g.n[1] || k >= p.g.n[2]) return;
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+  constexpr int cu0 = updH ? 3 : 0;
 #pragma unroll
-    for (int gs = 0; gs < 3; gs++) {
-      float acc = 0.f;
-      for (int cu = cu0; cu < cu0 + 3; cu++)
-        for (int t = 0; t < 2; t++) {
-          int a, g;
-          curl_pair(cu, t, a, g);
-          if (g != cs0 + gs) continue;
+  for (int c = 0; c < 3; c++)
 #pragma unroll
-          for (int o = 0; o < 4; o++) {
-            const float wgt = ORDER == 4 ? W4[o] : W2[o];
-            if (wgt == 0.f) continue;
-            int m[3] = {i, j, k};
-            m[a] -= t0 + o;
-            acc = __fmaf_rn(wgt, adj_w<ORDER>(p, A, cu, t, m[0], m[1], m[2]), acc);
-          }
-        }
-      A.lam[cs0 + gs][id] = __fadd_rn(A.lam[cs0 + gs][id], acc);
+    for (int t = 0; t < 2; t++) A.w[c][t][id] = adj_w<ORDER>(p, A, cu0 + c, t, i, j, k);
+  if (p.ab.kind != 1) return;
+  const int idx[3] = {i, j, k};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    if (!in_slab(p, a, idx[a])) continue;
+    const long long si = slab_index(p, a, i, j, k);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int cu = cu0 + c, sl = slot_of(cu, a);
+      if (sl < 0) continue;
+      const float b = __ldg(p.ab.c0[a] + 2 * idx[a] + comp_off(cu, a));
+      A.lpsi[a][sl][si] = __fmul_rn(b, __fadd_rn(A.lam[cu][id], A.lpsi[a][sl][si]));
     }
   }
 }
 
-// lam_psi <- b (lam + lam_psi) over the slab cells of the updated field
-__global__ void adj_psi_kernel(Params p, AdjDev A, int updH, int a) {
-  const int n[3] = {p.g.n[0], p.g.n[1], p.g.n[2]};
-  const int th = p.ab.L[a][0] + p.ab.L[a][1];
-  const long long cnt = (long long)th * ((long long)n[0] * n[1] * n[2] / n[a]);
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < cnt; q += (long long)gridDim.x * blockDim.x) {
-    // slab layout of slab_index: a=0 [cs][ny][nz], a=1 [nx][cs][nz], a=2 [nx][ny][cs]
-    int i, j, k, cs;
-    if (a == 0) { k = (int)(q % n[2]); j = (int)((q / n[2]) % n[1]); cs = (int)(q / ((long long)n[1] * n[2])); i = 0; }
-    else if (a == 1) { k = (int)(q % n[2]); cs = (int)((q / n[2]) % th); i = (int)(q / ((long long)th * n[2])); j = 0; }
-    else { cs = (int)(q % th); j = (int)((q / th) % n[1]); i = (int)(q / ((long long)th * n[1])); k = 0; }
-    const int v = cs < p.ab.L[a][0] ? cs : n[a] - p.ab.L[a][1] + (cs - p.ab.L[a][0]);
-    if (a == 0) i = v; else if (a == 1) j = v; else k = v;
-    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
-    for (int cu = updH ? 3 : 0; cu < (updH ? 6 : 3); cu++) {
-      const int sl = slot_of(cu, a);
-      if (sl < 0) continue;
-      const int idx[3] = {i, j, k};
-      const float b = __ldg(p.ab.c0[a] + 2 * idx[a] + comp_off(cu, a));
-      A.lpsi[a][sl][q] = __fmul_rn(b, __fadd_rn(A.lam[cu][id], A.lpsi[a][sl][q]));
-    }
+// lam of the source field += D^T w, gathered tap by tap with the forward
+// stencil weights (zero outside the grid); same thread layout as adj_w_kernel.
+template <int ORDER, int UPDH>
+__global__ void adj_curl_kernel(Params p, AdjDev A) {
+  constexpr int updH = UPDH;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, i = blockIdx.z;
+  if (j >= p.g.n[1] || k >= p.g.n[2]) return;
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+  constexpr int t0 = updH ? -2 : -1;
+  constexpr int cu0 = updH ? 3 : 0, cs0 = updH ? 0 : 3;
+  const int idx[3] = {i, j, k};
+  const long long st[3] = {p.g.sx, p.g.sy, 1};
+#pragma unroll
+  for (int gs = 0; gs < 3; gs++) {
+    float acc = 0.f;
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+#pragma unroll
+      for (int t = 0; t < 2; t++) {
+        int a, g;
+        curl_pair(cu0 + c, t, a, g);
+        if (g != cs0 + gs) continue;
+        const float* w = A.w[c][t];
+#pragma unroll
+        for (int o = 0; o < 4; o++) {
+          const float wgt = ORDER == 4 ? (o == 0 ? 1.f / 24.f : o == 1 ? -27.f / 24.f : o == 2 ? 27.f / 24.f : -1.f / 24.f)
+                                       : (o == 1 ? -1.f : o == 2 ? 1.f : 0.f);
+          if (ORDER == 2 && (o == 0 || o == 3)) continue;
+          const int v = idx[a] - (t0 + o);
+          if (v < 0 || v >= p.g.n[a]) continue;
+          acc = __fmaf_rn(wgt, w[id - (long long)(t0 + o) * st[a]], acc);
+        }
+      }
+    A.lam[cs0 + gs][id] = __fadd_rn(A.lam[cs0 + gs][id], acc);
   }
 }
 

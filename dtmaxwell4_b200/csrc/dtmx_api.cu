@@ -1086,11 +1086,30 @@ static size_t state_bytes(dtmx_ctx* ctx) {
   return off;
 }
 
-extern "C" int dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_every, int plane_x, double omega,
-                                    double* objective, float* grad_eps) {
-  if (!ctx || nsteps < 1 || checkpoint_every < 1 || !objective || !grad_eps) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
+// Forward + adjoint run of one context, split into phases so that a batch of
+// contexts can interleave them step by step (each context on its own stream).
+struct FaRun {
+  int N = 0, K = 0, nseg = 0, nd = 0, npl = 0, plane_x = 0;
+  double omega = 0, J = 0;
+  long long s0 = 0;
+  std::vector<char*> ck;
+  std::vector<void*> tmp;
+  AdjDev A{};
+  float* hist = nullptr;
+  double* dF = nullptr;
+  int seg = -1, len = 0;
+  void release() {
+    for (char* q : ck) cudaFree(q);
+    for (void* q : tmp) cudaFree(q);
+    ck.clear();
+    tmp.clear();
+  }
+};
+
+static int fa_begin(dtmx_ctx* ctx, FaRun& R, int nsteps, int checkpoint_every, int plane_x, double omega) {
   const dtmx_config& c = ctx->cfg;
   Params& P = ctx->P;
+  if (nsteps < 1 || checkpoint_every < 1) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
   if (!P.des_on) return fail(ctx, DTMX_ERR_STATE, "no design region");
   if (plane_x < 0 || plane_x >= c.nx) return fail(ctx, DTMX_ERR_INVALID, "objective plane outside the grid");
   if (c.geometry != DTMX_GEOM_BOX || c.absorber == DTMX_ABS_SPLIT_PML)
@@ -1103,10 +1122,11 @@ extern "C" int dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_ev
   }
   int rc = prepare(ctx);
   if (rc) return rc;
-  const int N = nsteps, K = std::min(checkpoint_every, nsteps);
-  const int nseg = (N + K - 1) / K;
-  const int nd = P.des_n[0] * P.des_n[1] * P.des_n[2];
-  const int npl = c.ny * c.nz;
+  R.N = nsteps; R.K = std::min(checkpoint_every, nsteps);
+  R.nseg = (R.N + R.K - 1) / R.K;
+  R.nd = P.des_n[0] * P.des_n[1] * P.des_n[2];
+  R.npl = c.ny * c.nz;
+  R.plane_x = plane_x; R.omega = omega;
   // objective flux DFT on the plane x = plane_x: Ey, Ez, Hy, Hz at omega
   DftHost& O = ctx->obj;
   if (!O.acc || O.d.index != plane_x) {
@@ -1114,115 +1134,199 @@ extern "C" int dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_ev
     O = DftHost{};
     O.d.axis = 0; O.d.index = plane_x; O.d.comp_mask = (1 << 1) | (1 << 2) | (1 << 4) | (1 << 5); O.d.nfreq = 1;
     O.d.n1 = c.ny; O.d.n2 = c.nz; O.ncomp = 4;
-    if (cudaMalloc(&O.omega, 8) != cudaSuccess || cudaMalloc(&O.acc, (size_t)4 * npl * sizeof(double2)) != cudaSuccess ||
-        cudaMalloc(&O.stage, (size_t)DFT_STAGE * 4 * npl * 4) != cudaSuccess || cudaMalloc(&O.sstep, DFT_STAGE * 8) != cudaSuccess)
+    if (cudaMalloc(&O.omega, 8) != cudaSuccess || cudaMalloc(&O.acc, (size_t)4 * R.npl * sizeof(double2)) != cudaSuccess ||
+        cudaMalloc(&O.stage, (size_t)DFT_STAGE * 4 * R.npl * 4) != cudaSuccess || cudaMalloc(&O.sstep, DFT_STAGE * 8) != cudaSuccess)
       return fail(ctx, DTMX_ERR_OOM, "objective DFT allocation");
     O.d.omega = O.omega; O.d.acc = O.acc; O.d.stage = O.stage; O.d.sstep = O.sstep;
   }
   CK(cudaMemcpyAsync(O.omega, &omega, 8, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemsetAsync(O.acc, 0, (size_t)4 * npl * sizeof(double2), ctx->stream));
+  CK(cudaMemsetAsync(O.acc, 0, (size_t)4 * R.npl * sizeof(double2), ctx->stream));
   O.nstaged = 0;
   // checkpoints of the state every K steps plus the final state
   const size_t sb = state_bytes(ctx);
-  std::vector<char*> ck(nseg + 1, nullptr);
-  auto release = [&]() {
-    for (char* q : ck) cudaFree(q);
-  };
-  for (auto& q : ck)
-    if (cudaMalloc(&q, sb) != cudaSuccess) { release(); return fail(ctx, DTMX_ERR_OOM, "checkpoint allocation"); }
-  const long long s0 = ctx->step;
+  R.ck.assign(R.nseg + 1, nullptr);
+  for (auto& q : R.ck)
+    if (cudaMalloc(&q, sb) != cudaSuccess) { R.release(); return fail(ctx, DTMX_ERR_OOM, "checkpoint allocation"); }
+  R.s0 = ctx->step;
   ctx->obj_on = true;
-  for (int st = 0; st < N; st++) {
-    if (st % K == 0) state_copy(ctx, ck[st / K], true);
-    if ((rc = launch_step(ctx))) { ctx->obj_on = false; release(); return rc; }
-    ctx->step++;
-  }
+  return DTMX_OK;
+}
+
+// forward step st (0-based) of the run
+static int fa_forward(dtmx_ctx* ctx, FaRun& R, int st) {
+  if (st % R.K == 0) state_copy(ctx, R.ck[st / R.K], true);
+  int rc = launch_step(ctx);
+  if (rc) return rc;
+  ctx->step++;
+  return DTMX_OK;
+}
+
+// end of the forward pass: objective, adjoint buffers (waits for the stream)
+static int fa_forward_done(dtmx_ctx* ctx, FaRun& R) {
+  Params& P = ctx->P;
   ctx->obj_on = false;
-  state_copy(ctx, ck[nseg], true);
+  state_copy(ctx, R.ck[R.nseg], true);
+  DftHost& O = ctx->obj;
   dft_flush(ctx, O);
-  std::vector<double> F((size_t)8 * npl);
+  std::vector<double> F((size_t)8 * R.npl);
   CK(cudaMemcpyAsync(F.data(), O.acc, F.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   double J = 0;
-  for (int u = 0; u < npl; u++) {
-    const double *ey = &F[(0 * (size_t)npl + u) * 2], *ez = &F[(1 * (size_t)npl + u) * 2];
-    const double *hy = &F[(2 * (size_t)npl + u) * 2], *hz = &F[(3 * (size_t)npl + u) * 2];
+  for (int u = 0; u < R.npl; u++) {
+    const double *ey = &F[(0 * (size_t)R.npl + u) * 2], *ez = &F[(1 * (size_t)R.npl + u) * 2];
+    const double *hy = &F[(2 * (size_t)R.npl + u) * 2], *hz = &F[(3 * (size_t)R.npl + u) * 2];
     J += ey[0] * hz[0] + ey[1] * hz[1] - (ez[0] * hy[0] + ez[1] * hy[1]);
   }
-  *objective = J;
-  // adjoint state
-  AdjDev A{};
-  A.nd = nd;
-  std::vector<void*> tmp;
-  auto tfree = [&]() {
-    for (void* q : tmp) cudaFree(q);
-  };
+  R.J = J;
+  AdjDev& A = R.A;
+  A = AdjDev{};
+  A.nd = R.nd;
   auto talloc = [&](void** q, size_t bytes) {
     if (cudaMalloc(q, bytes) != cudaSuccess) return false;
-    tmp.push_back(*q);
+    R.tmp.push_back(*q);
     return cudaMemsetAsync(*q, 0, bytes, ctx->stream) == cudaSuccess;
   };
   bool ok = true;
   for (int comp = 0; comp < 6; comp++) ok = ok && talloc((void**)&A.lam[comp], (ctx->nstore + 64) * 4);
   for (int a = 0; a < 3; a++) {
     const size_t cnt = (size_t)(P.ab.L[a][0] + P.ab.L[a][1]) * (ctx->ncell / (size_t)P.g.n[a]);
-    for (int q = 0; q < 4; q++) A.lpsi[a][q] = nullptr;
     if (!P.ab.aux[a][0]) continue;
     for (int q = 0; q < 4; q++) ok = ok && talloc((void**)&A.lpsi[a][q], cnt * 4);
   }
-  float* hist = nullptr;
-  double* dF = nullptr;
-  ok = ok && talloc((void**)&A.grad, (size_t)3 * nd * 8) && talloc((void**)&hist, (size_t)(K + 1) * 3 * nd * 4) &&
-       talloc((void**)&dF, F.size() * 8);
-  if (!ok) { tfree(); release(); return fail(ctx, DTMX_ERR_OOM, "adjoint allocation"); }
-  A.hist = hist;
-  CK(cudaMemcpyAsync(dF, F.data(), F.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-  const bool o4 = c.order == 4;
-  const long long ncell = (long long)ctx->ncell;
-  const unsigned gb = (unsigned)std::min<long long>((ncell + 255) / 256, 148LL * 32);
-  const unsigned gd = (unsigned)((3 * nd + 255) / 256);
+  for (int c3 = 0; c3 < 3; c3++)
+    for (int t = 0; t < 2; t++) ok = ok && talloc((void**)&A.w[c3][t], (ctx->nstore + 64) * 4);
+  ok = ok && talloc((void**)&A.grad, (size_t)3 * R.nd * 8) && talloc((void**)&R.hist, (size_t)(R.K + 1) * 3 * R.nd * 4) &&
+       talloc((void**)&R.dF, F.size() * 8);
+  if (!ok) { R.release(); return fail(ctx, DTMX_ERR_OOM, "adjoint allocation"); }
+  A.hist = R.hist;
+  CK(cudaMemcpyAsync(R.dF, F.data(), F.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
   ctx->monitors_off = true;
-  for (int seg = nseg - 1; seg >= 0; seg--) {
-    const int start = seg * K, len = std::min(N, start + K) - start;
-    state_copy(ctx, ck[seg], false);
-    ctx->step = s0 + start;
-    design_capture_kernel<<<gd, 256, 0, ctx->stream>>>(ctx->P, hist, 0, nd);
-    for (int q = 1; q <= len; q++) {
-      if ((rc = launch_step(ctx))) break;
-      ctx->step++;
-      design_capture_kernel<<<gd, 256, 0, ctx->stream>>>(ctx->P, hist, q, nd);
-    }
-    if (rc) break;
-    for (int q = len; q >= 1; q--) {
-      adj_source_kernel<<<(npl + 255) / 256, 256, 0, ctx->stream>>>(P, A, dF, s0 + start + q, plane_x, omega, c.dt);
-      adj_grad_kernel<<<gd, 256, 0, ctx->stream>>>(P, A, q);
-      for (int updH = 0; updH < 2; updH++) {
-        if (o4) adj_gather_kernel<4><<<gb, 256, 0, ctx->stream>>>(P, A, updH);
-        else adj_gather_kernel<2><<<gb, 256, 0, ctx->stream>>>(P, A, updH);
-        for (int a = 0; a < 3; a++) {
-          if (!A.lpsi[a][0]) continue;
-          const long long cnt = (long long)(P.ab.L[a][0] + P.ab.L[a][1]) * (ncell / P.g.n[a]);
-          adj_psi_kernel<<<(unsigned)std::min<long long>((cnt + 255) / 256, 148LL * 32), 256, 0, ctx->stream>>>(P, A, updH, a);
-        }
-      }
-    }
-  }
-  ctx->monitors_off = false;
-  state_copy(ctx, ck[nseg], false);
-  ctx->step = s0 + N;
-  std::vector<double> g((size_t)3 * nd);
-  CK(cudaMemcpyAsync(g.data(), A.grad, g.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
-  tfree();
-  release();
+  return DTMX_OK;
+}
+
+static unsigned design_blocks(const FaRun& R) { return (unsigned)((3 * R.nd + 255) / 256); }
+
+// restore checkpoint seg and record the design region of its first state
+static int fa_segment_begin(dtmx_ctx* ctx, FaRun& R, int seg) {
+  R.seg = seg;
+  const int start = seg * R.K;
+  R.len = std::min(R.N, start + R.K) - start;
+  state_copy(ctx, R.ck[seg], false);
+  ctx->step = R.s0 + start;
+  design_capture_kernel<<<design_blocks(R), 256, 0, ctx->stream>>>(ctx->P, R.hist, 0, R.nd);
+  return DTMX_OK;
+}
+
+// recompute step q (1..len) of the current segment
+static int fa_recompute(dtmx_ctx* ctx, FaRun& R, int q) {
+  int rc = launch_step(ctx);
   if (rc) return rc;
+  ctx->step++;
+  design_capture_kernel<<<design_blocks(R), 256, 0, ctx->stream>>>(ctx->P, R.hist, q, R.nd);
+  return DTMX_OK;
+}
+
+// adjoint of step q (len..1) of the current segment
+static int fa_adjoint(dtmx_ctx* ctx, FaRun& R, int q) {
+  const Params& P = ctx->P;
+  const dtmx_config& c = ctx->cfg;
+  AdjDev& A = R.A;
+  cudaStream_t st = ctx->stream;
+  adj_source_kernel<<<(R.npl + 255) / 256, 256, 0, st>>>(P, A, R.dF, R.s0 + (long long)R.seg * R.K + q, R.plane_x, R.omega, c.dt);
+  adj_grad_kernel<<<design_blocks(R), 256, 0, st>>>(P, A, q);
+  const dim3 blk(32, 8), grd((c.nz + 31) / 32, (c.ny + 7) / 8, c.nx);
+  if (c.order == 4) {
+    adj_w_kernel<4, 0><<<grd, blk, 0, st>>>(P, A);
+    adj_curl_kernel<4, 0><<<grd, blk, 0, st>>>(P, A);
+    adj_w_kernel<4, 1><<<grd, blk, 0, st>>>(P, A);
+    adj_curl_kernel<4, 1><<<grd, blk, 0, st>>>(P, A);
+  } else {
+    adj_w_kernel<2, 0><<<grd, blk, 0, st>>>(P, A);
+    adj_curl_kernel<2, 0><<<grd, blk, 0, st>>>(P, A);
+    adj_w_kernel<2, 1><<<grd, blk, 0, st>>>(P, A);
+    adj_curl_kernel<2, 1><<<grd, blk, 0, st>>>(P, A);
+  }
+  ctx->launches += 6;
+  return DTMX_OK;
+}
+
+// final state back in place, gradient to the caller (waits for the stream)
+static int fa_finish(dtmx_ctx* ctx, FaRun& R, double* objective, float* grad_eps) {
+  ctx->monitors_off = false;
+  state_copy(ctx, R.ck[R.nseg], false);
+  ctx->step = R.s0 + R.N;
+  std::vector<double> g((size_t)3 * R.nd);
+  CK(cudaMemcpyAsync(g.data(), R.A.grad, g.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  R.release();
   if (e != cudaSuccess) return fail(ctx, DTMX_ERR_CUDA, std::string("adjoint: ") + cudaGetErrorString(e));
   for (int comp = 0; comp < 3; comp++)
-    for (int q = 0; q < nd; q++) {
+    for (int q = 0; q < R.nd; q++) {
       const double ie = ctx->h_des_ie[comp][q];
-      grad_eps[(size_t)comp * nd + q] = (float)(-ie * ie * g[(size_t)comp * nd + q]);
+      grad_eps[(size_t)comp * R.nd + q] = (float)(-ie * ie * g[(size_t)comp * R.nd + q]);
     }
+  *objective = R.J;
   return DTMX_OK;
+}
+
+static void fa_abort(dtmx_ctx* ctx, FaRun& R) {
+  cudaStreamSynchronize(ctx->stream);
+  ctx->obj_on = false;
+  ctx->monitors_off = false;
+  R.release();
+}
+
+extern "C" int dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_every, int plane_x, double omega,
+                                    double* objective, float* grad_eps) {
+  if (!ctx || !objective || !grad_eps) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
+  FaRun R;
+  int rc = fa_begin(ctx, R, nsteps, checkpoint_every, plane_x, omega);
+  if (rc) return rc;
+  for (int st = 0; st < R.N && !rc; st++) rc = fa_forward(ctx, R, st);
+  if (!rc) rc = fa_forward_done(ctx, R);
+  for (int seg = R.nseg - 1; seg >= 0 && !rc; seg--) {
+    fa_segment_begin(ctx, R, seg);
+    for (int q = 1; q <= R.len && !rc; q++) rc = fa_recompute(ctx, R, q);
+    for (int q = R.len; q >= 1 && !rc; q--) rc = fa_adjoint(ctx, R, q);
+  }
+  if (rc) { fa_abort(ctx, R); return rc; }
+  return fa_finish(ctx, R, objective, grad_eps);
+}
+
+// Batch of independent forward + adjoint runs: every phase is issued for all
+// contexts step by step, each context on its own stream, so that the GPU runs
+// the instances' kernels concurrently (instances of uneven sizes fill each
+// other's gaps) and no instance waits on the host between its steps.
+extern "C" int dtmx_batch_forward_adjoint(dtmx_ctx* const* ctxs, int n, int nsteps, int checkpoint_every,
+                                          const int* plane_x, const double* omega, double* objectives,
+                                          float* const* grads) {
+  if (!ctxs || n < 1 || !plane_x || !omega || !objectives || !grads) return DTMX_ERR_INVALID;
+  std::vector<FaRun> R(n);
+  int rc = DTMX_OK, bad = -1;
+  auto abort_all = [&](int upto) {
+    for (int b = 0; b < upto; b++) fa_abort(ctxs[b], R[b]);
+  };
+  for (int b = 0; b < n; b++)
+    if ((rc = fa_begin(ctxs[b], R[b], nsteps, checkpoint_every, plane_x[b], omega[b]))) { abort_all(b); return rc; }
+  for (int st = 0; st < nsteps && !rc; st++)
+    for (int b = 0; b < n && !rc; b++) { rc = fa_forward(ctxs[b], R[b], st); bad = b; }
+  for (int b = 0; b < n && !rc; b++) { rc = fa_forward_done(ctxs[b], R[b]); bad = b; }
+  const int nseg = R[0].nseg;
+  for (int seg = nseg - 1; seg >= 0 && !rc; seg--) {
+    for (int b = 0; b < n; b++) fa_segment_begin(ctxs[b], R[b], seg);
+    const int len = R[0].len;
+    for (int q = 1; q <= len && !rc; q++)
+      for (int b = 0; b < n && !rc; b++) { rc = fa_recompute(ctxs[b], R[b], q); bad = b; }
+    for (int q = len; q >= 1 && !rc; q--)
+      for (int b = 0; b < n && !rc; b++) { rc = fa_adjoint(ctxs[b], R[b], q); bad = b; }
+  }
+  if (rc) { abort_all(n); (void)bad; return rc; }
+  for (int b = 0; b < n; b++) {
+    int r = fa_finish(ctxs[b], R[b], &objectives[b], grads[b]);
+    if (r && !rc) rc = r;
+  }
+  return rc;
 }
 
 extern "C" int dtmx_sync(dtmx_ctx* ctx) {

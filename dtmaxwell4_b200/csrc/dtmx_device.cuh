@@ -430,8 +430,9 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
         p.f[cf + c][off] = __fadd_rn(F, sum3(d[c][0], d[c][1], d[c][2]));
         continue;
       }
+      int m = 0;
       if (!ISH) {
-        const int m = um >= 0 ? um : mat_at(smat, c, y, tz);
+        m = um >= 0 ? um : mat_at(smat, c, y, tz);
         if (tade && ms.npoles[m] > 0) {
           const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
           if (bi >= 0 && bi < p.ade.n[0] && bj >= 0 && bj < p.ade.n[1] && bk >= 0 && bk < p.ade.n[2]) {
@@ -440,17 +441,17 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
             continue;
           }
         }
-        const long long di = design_index(p, i, j, k);
-        const float ie = di >= 0 ? p.des_ie[c][di] : ms.inv_eps[m][c];
+        float ie = ms.inv_eps[m][c];
+        if (p.des_on) {
+          const long long di = design_index(p, i, j, k);
+          if (di >= 0) ie = p.des_ie[c][di];
+        }
         d[c][0] = __fmul_rn(d[c][0], ie); d[c][1] = __fmul_rn(d[c][1], ie); d[c][2] = __fmul_rn(d[c][2], ie);
       }
       float inc = sum3(d[c][0], d[c][1], d[c][2]);
       if (ab) inc = __fadd_rn(inc, absorb_correction(p, cf + c, i, j, k, d[c]));
       float nv = __fadd_rn(F, inc);
-      if (!ISH) {
-        const int m = um >= 0 ? um : mat_at(smat, c, y, tz);
-        if (ms.gjc[m] != 0.f) nv = gyro_subtract(p, c, i, j, k, ms.gjc[m], nv);
-      }
+      if (!ISH && tade && ms.gjc[m] != 0.f) nv = gyro_subtract(p, c, i, j, k, ms.gjc[m], nv);
       p.f[cf + c][off] = nv;
     }
   }

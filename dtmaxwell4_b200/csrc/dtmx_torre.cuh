@@ -245,8 +245,11 @@ __device__ __forceinline__ void torre_store(const Params& p, const unsigned char
           continue;
         }
       }
-      const long long di = design_index(p, x, j, k);
-      const float ie = di >= 0 ? p.des_ie[c][di] : ms.inv_eps[m][c];
+      float ie = ms.inv_eps[m][c];
+      if (p.des_on) {
+        const long long di = design_index(p, x, j, k);
+        if (di >= 0) ie = p.des_ie[c][di];
+      }
       dd[0] = __fmul_rn(dd[0], ie); dd[1] = __fmul_rn(dd[1], ie); dd[2] = __fmul_rn(dd[2], ie);
     }
     float inc = sum3(dd[0], dd[1], dd[2]);

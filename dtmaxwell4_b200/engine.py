@@ -23,7 +23,7 @@ EXPORTS = (
     "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_get_stream",
     "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
     "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
-    "dtmx_set_design", "dtmx_forward_adjoint",
+    "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint",
 )
 
 
@@ -72,6 +72,8 @@ def load():
     L.dtmx_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
     L.dtmx_set_design.argtypes = [vp, C.POINTER(ip), C.POINTER(ip), vp]
     L.dtmx_forward_adjoint.argtypes = [vp, ip, ip, ip, C.c_double, C.POINTER(C.c_double), vp]
+    L.dtmx_batch_forward_adjoint.argtypes = [C.POINTER(vp), ip, ip, ip, C.POINTER(ip), C.POINTER(C.c_double),
+                                             C.POINTER(C.c_double), C.POINTER(vp)]
     L.dtmx_count_nonfinite_noalloc.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int64, C.POINTER(C.c_int64)]
     _lib = L
     return L
@@ -249,6 +251,24 @@ class Simulation:
         a, b, n = C.c_double(), C.c_double(), C.c_int64()
         self._ck(self._L.dtmx_read_profile(self._h, C.byref(a), C.byref(b), C.byref(n)))
         return a.value, b.value, n.value
+
+
+def batch_forward_adjoint(sims, nsteps, plane_x, omega, checkpoint_every=100):
+    """dtmx_batch_forward_adjoint over Simulations that have design regions:
+    returns ([J], [dJ/d eps])."""
+    L = load()
+    n = len(sims)
+    grads = [np.zeros((3,) + tuple(s._design[1]), np.float32) for s in sims]
+    hs = (C.c_void_p * n)(*[s._h for s in sims])
+    px = (C.c_int * n)(*[int(v) for v in plane_x])
+    om = (C.c_double * n)(*[float(v) for v in omega])
+    J = (C.c_double * n)()
+    gp = (C.c_void_p * n)(*[g.ctypes.data for g in grads])
+    rc = L.dtmx_batch_forward_adjoint(hs, n, int(nsteps), int(checkpoint_every), px, om, J, gp)
+    if rc != 0:
+        msgs = [L.dtmx_last_error(s._h).decode() for s in sims]
+        raise DtmxError(rc, "; ".join(m for m in msgs if m))
+    return list(J), grads
 
 
 def abi_sizes():

@@ -120,3 +120,38 @@ def apply(sim, sc):
     for (axis, index, mask, om) in sc["dft"]:
         ids.append(sim.add_dft_plane(axis, index, mask, om))
     return ids
+
+
+def design_block_instance(seed, edges=(64, 96, 128, 160, 192, 224, 256), pml=10, steps=1500, nblocks=8,
+                          design=16, lambda0=24.0, order=2, courant=0.5):
+    """One instance of the batched workload: each axis edge drawn from
+    `edges`, `nblocks` random dielectric blocks with eps ~ U[1, 12], one Ez
+    dipole at a random interior position, a CPML of `pml` cells and a
+    `design`^3 per-node permittivity region at the centre (initialised to
+    U[1, 12]); the objective is the flux through the plane x = nx - pml - 4
+    at lambda0.  The gradient is taken with respect to the design region."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = (int(v) for v in rng.choice(edges, size=3))
+    cfg = abi.make_config(nx, ny, nz, dx=1.0, courant=courant, order=order, pml=pml)
+    idx = np.zeros((nx, ny, nz), np.uint8)
+    mats = [abi.make_material(1.0)]
+    lo_d = [n // 2 - design // 2 for n in (nx, ny, nz)]
+    for b in range(nblocks):
+        size = rng.integers(4, 17, size=3)
+        lo = [int(rng.integers(pml + 1, n - pml - s - 1)) for n, s in zip((nx, ny, nz), size)]
+        mats.append(abi.make_material(float(rng.uniform(1.0, 12.0))))
+        idx[lo[0]:lo[0] + size[0], lo[1]:lo[1] + size[1], lo[2]:lo[2] + size[2]] = len(mats) - 1
+    # the source stays outside the design region and away from the absorber
+    while True:
+        p = [int(rng.integers(pml + 4, n - pml - 4)) for n in (nx, ny, nz)]
+        if not all(lo_d[a] - 2 <= p[a] < lo_d[a] + design + 2 for a in range(3)):
+            break
+    f0, tau, t0 = gauss_sine_params(lambda0)
+    src = abi.PointSource(comp=abi.EZ, i=p[0], j=p[1], k=p[2], waveform=abi.WAVE_GAUSS_SINE, amp=1.0, f0=f0, tau=tau,
+                          t0=t0)
+    eps = rng.uniform(1.0, 12.0, size=(3, design, design, design)).astype(np.float32)
+    return dict(name="design_block_instance", cfg=cfg, materials=(mats, [idx, idx, idx]), point_sources=[src],
+                tfsf=None, probes=[], dft=[], steps=steps, design=(tuple(lo_d), eps), plane_x=nx - pml - 4,
+                omega=2 * math.pi / lambda0,
+                desc="%dx%dx%d, %d blocks eps~U[1,12], Ez dipole, %d-cell CPML, %d^3 design region" %
+                     (nx, ny, nz, nblocks, pml, design))

@@ -298,6 +298,14 @@ int  dtmx_set_design(dtmx_ctx* ctx, const int lo[3], const int n[3], const float
 int  dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_every, int plane_x, double omega,
                           double* objective, float* grad_eps);
 
+/* A batch of independent dtmx_forward_adjoint runs (contexts of any sizes,
+ * same nsteps and checkpoint_every): every phase is issued step by step for
+ * all contexts, each on its own stream, so their kernels run concurrently.
+ * plane_x, omega and objectives have n entries, grads n pointers of 3*nd_b
+ * floats.  Results equal those of n separate dtmx_forward_adjoint calls. */
+int  dtmx_batch_forward_adjoint(dtmx_ctx* const* ctxs, int n, int nsteps, int checkpoint_every, const int* plane_x,
+                                const double* omega, double* objectives, float* const* grads);
+
 /* Count NaN/Inf values in nfields caller-owned device arrays of nelem floats
  * each, without allocating any device memory (no cudaMalloc/cudaFree and no
  * allocating library routine).  For callers that cannot allocate: processes
