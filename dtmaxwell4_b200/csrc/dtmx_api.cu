@@ -10,6 +10,8 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <map>
+#include <tuple>
 
 #include <cudaTypedefs.h>
 
@@ -76,6 +78,9 @@ struct dtmx_ctx {
   long long prof_count = 0;
   bool prof_pending = false;
   int engine = 0, tblock = 0;
+  int xchunk = 0;               // planes per CTA of the per-step kernels (0: automatic)
+  cudaGraphExec_t graph16 = nullptr;   // 16 captured per-step launch sequences
+  long long graph_launches = 0;
   TmaMaps maps{};
   int* d_err = nullptr;
   bool has_gyro = false;
@@ -413,6 +418,7 @@ extern "C" int dtmx_create(const dtmx_config* cfg, dtmx_ctx** out) {
 extern "C" void dtmx_destroy(dtmx_ctx* ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->graph16) cudaGraphExecDestroy(ctx->graph16);
   for (void* p : ctx->allocs) cudaFree(p);
   for (auto& d : ctx->dfts) { cudaFree(d.omega); cudaFree(d.acc); cudaFree(d.stage); cudaFree(d.sstep); }
   cudaFree(ctx->obj.omega); cudaFree(ctx->obj.acc); cudaFree(ctx->obj.stage); cudaFree(ctx->obj.sstep);
@@ -739,6 +745,7 @@ extern "C" int dtmx_read_dft(dtmx_ctx* ctx, int id, double* out, size_t out_len)
 
 // ---------------------------------------------------------------- stepping
 static int xchunk_for(const dtmx_ctx* ctx) {
+  if (ctx->xchunk > 0) return ctx->xchunk;
   const dtmx_config& c = ctx->cfg;
   const long long tiles = (long long)((c.nz + TZ - 1) / TZ) * ((c.ny + TYT - 1) / TYT);
   const long long target = 148LL * 8 * 3;   // about three waves of 8 CTAs per SM
@@ -997,6 +1004,44 @@ static int launch_torre(dtmx_ctx* ctx, int T) {
   return DTMX_OK;
 }
 
+// Capture (once) and launch 16 per-step launch sequences as one graph.  The
+// host-side bookkeeping of the 16 steps (staging slots, flushes, buffer
+// parity) is done during the capture; the captured kernels read the step
+// number from the device counter, so the graph is valid at every 16-step
+// boundary of an aligned run.
+static int graph_steps16(dtmx_ctx* ctx) {
+  if (!ctx->graph16) {
+    set_kernel_attributes();
+    const long long step0 = ctx->step;
+    const long long launches0 = ctx->launches;
+    const int gcur0 = ctx->gcur;
+    std::vector<int> staged0;
+    for (auto& d : ctx->dfts) staged0.push_back(d.nstaged);
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return fail(ctx, DTMX_ERR_CUDA, "graph capture could not start");
+    int rc = DTMX_OK;
+    for (int q = 0; q < 16 && !rc; q++) rc = launch_step(ctx);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc || e != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return rc ? rc : fail(ctx, DTMX_ERR_CUDA, "graph capture failed"); }
+    e = cudaGraphInstantiate(&ctx->graph16, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { ctx->graph16 = nullptr; cudaGetLastError(); return fail(ctx, DTMX_ERR_CUDA, "graph instantiation failed"); }
+    // the capture ran the bookkeeping of 16 steps; the graph below executes them
+    if (ctx->gcur != gcur0) return fail(ctx, DTMX_ERR_STATE, "graph capture: unexpected buffer parity");
+    for (size_t q = 0; q < ctx->dfts.size(); q++)
+      if (ctx->dfts[q].nstaged != staged0[q]) return fail(ctx, DTMX_ERR_STATE, "graph capture: staging not aligned");
+    ctx->launches = launches0 + (ctx->launches - launches0);
+    ctx->graph_launches = ctx->launches - launches0;
+    (void)step0;
+  } else {
+    ctx->launches += ctx->graph_launches;
+  }
+  CK(cudaGraphLaunch(ctx->graph16, ctx->stream));
+  ctx->step += 16;
+  return DTMX_OK;
+}
+
 extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
   if (!ctx || nsteps < 0) return fail(ctx, DTMX_ERR_INVALID, "bad step count");
   int rc0 = prepare(ctx);
@@ -1011,10 +1056,23 @@ extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
       left -= ctx->tblock;
     }
   }
-  for (int s = 0; s < left; s++) {
+  while (left > 0) {
+    // 16 steps as one CUDA graph when every DFT staging cycle is at its start
+    // (the captured sequence then repeats exactly: staging slots, the flush
+    // every 16 steps and the gyrotropic buffer parity)
+    bool aligned = left >= 16 && !ctx->profiling && !ctx->monitors_off && ctx->engine != 2;
+    for (auto& d : ctx->dfts) aligned = aligned && d.nstaged == 0;
+    if (ctx->obj_on) aligned = aligned && ctx->obj.nstaged == 0;
+    if (aligned && !ctx->obj_on) {
+      int rc = graph_steps16(ctx);
+      if (rc) return rc;
+      left -= 16;
+      continue;
+    }
     int rc = launch_step(ctx);
     if (rc) return rc;
     ctx->step++;
+    left--;
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ctx, DTMX_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
@@ -1058,6 +1116,17 @@ static void state_parts(dtmx_ctx* ctx, std::vector<std::pair<void*, size_t>>& pa
     const size_t cnt = (size_t)(ctx->P.ab.L[a][0] + ctx->P.ab.L[a][1]) * (ctx->ncell / (size_t)ctx->P.g.n[a]);
     for (int q = 0; q < 4; q++)
       if (ctx->P.ab.aux[a][q]) parts.push_back({ctx->P.ab.aux[a][q], cnt * 4});
+  }
+  const Ade& A = ctx->P.ade;
+  const size_t na = (size_t)A.n[0] * A.n[1] * A.n[2];
+  for (int comp = 0; comp < 3 && na; comp++) {
+    if (A.Em[comp]) parts.push_back({A.Em[comp], na * 4});
+    for (int q = 0; q < MAXPOLE; q++) {
+      if (A.Jp[comp][q]) parts.push_back({A.Jp[comp][q], na * 4});
+      if (A.Jm[comp][q]) parts.push_back({A.Jm[comp][q], na * 4});
+    }
+    for (int b = 0; b < 2; b++)
+      if (A.Jg[b][comp]) parts.push_back({A.Jg[b][comp], na * 4});
   }
   parts.push_back({ctx->d_step, sizeof(long long)});
   if (ctx->line_e) {
@@ -1329,6 +1398,95 @@ extern "C" int dtmx_batch_forward_adjoint(dtmx_ctx* const* ctxs, int n, int nste
   return rc;
 }
 
+// ---------------------------------------------------------------- autotuner
+// Times every applicable engine configuration for trial_steps steps from the
+// current state (monitors paused, state restored after each trial) and keeps
+// the fastest: the per-step engine with x chunks of {auto, 4, 8, 16, 32, 64}
+// planes per CTA, and the wavefront engine with 1, 2 and 4 steps per launch.
+// Results are cached per grid shape and feature set for the process.
+struct TuneKey {
+  int nx, ny, nz, order, absorber, geometry, feats;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(nx, ny, nz, order, absorber, geometry, feats) < std::tie(o.nx, o.ny, o.nz, o.order, o.absorber, o.geometry, o.feats);
+  }
+};
+struct TuneVal { int engine, tblock, xchunk; double ms; };
+static std::map<TuneKey, TuneVal>& tune_cache() {
+  static std::map<TuneKey, TuneVal> m;
+  return m;
+}
+
+extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, int* tblock_out, int* xchunk_out,
+                             double* ms_per_step_out) {
+  if (!ctx || trial_steps < 1) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
+  int rc = prepare(ctx);
+  if (rc) return rc;
+  const dtmx_config& c = ctx->cfg;
+  const int feats = (ctx->has_tfsf ? 1 : 0) | (ctx->psrc.empty() ? 0 : 2) | (ctx->probes.empty() ? 0 : 4) |
+                    (ctx->dfts.empty() ? 0 : 8) | (ctx->P.ade.Em[0] ? 16 : 0) | (ctx->has_gyro ? 32 : 0) |
+                    (ctx->P.des_on ? 64 : 0);
+  const TuneKey key{c.nx, c.ny, c.nz, c.order, c.absorber, c.geometry, feats};
+  TuneVal best{1, 0, 0, 1e30};
+  auto it = tune_cache().find(key);
+  if (it != tune_cache().end()) {
+    best = it->second;
+  } else {
+    char* ck = nullptr;
+    if (cudaMalloc(&ck, state_bytes(ctx)) != cudaSuccess) return fail(ctx, DTMX_ERR_OOM, "autotune state copy");
+    state_copy(ctx, ck, true);
+    const long long step0 = ctx->step;
+    const int gcur0 = ctx->gcur, eng0 = ctx->engine, tb0 = ctx->tblock, xc0 = ctx->xchunk;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    std::vector<TuneVal> cand;
+    for (int xc : {0, 4, 8, 16, 32, 64})
+      if (xc <= c.nx) cand.push_back({1, 0, xc, 0});
+    std::string why;
+    if (torre_features_ok(ctx, &why))
+      for (int T : {1, 2, 4})
+        if (trial_steps >= T && torre_usable(ctx, T, &why)) cand.push_back({2, T, 0, 0});
+    ctx->monitors_off = true;
+    for (auto& cd : cand) {
+      ctx->xchunk = cd.xchunk;
+      int r = DTMX_OK;
+      const int n = cd.engine == 2 ? (trial_steps / cd.tblock) * cd.tblock : trial_steps;
+      cudaEventRecord(e0, ctx->stream);
+      if (cd.engine == 2) {
+        for (int q = 0; q < n && !r; q += cd.tblock) r = launch_torre(ctx, cd.tblock);
+      } else {
+        for (int q = 0; q < n && !r; q++) { r = launch_step(ctx); ctx->step++; }
+      }
+      cudaEventRecord(e1, ctx->stream);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      cd.ms = r ? 1e30 : ms / n;
+      if (r) cudaGetLastError();
+      state_copy(ctx, ck, false);
+      ctx->step = step0;
+      ctx->gcur = gcur0;
+      if (cd.ms < best.ms) best = cd;
+    }
+    ctx->monitors_off = false;
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ck);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->engine = eng0; ctx->tblock = tb0; ctx->xchunk = xc0;
+    tune_cache()[key] = best;
+  }
+  ctx->engine = best.engine;
+  ctx->tblock = best.tblock;
+  ctx->xchunk = best.xchunk;
+  if (ctx->graph16) { cudaGraphExecDestroy(ctx->graph16); ctx->graph16 = nullptr; }
+  if (engine_out) *engine_out = best.engine;
+  if (tblock_out) *tblock_out = best.tblock;
+  if (xchunk_out) *xchunk_out = best.xchunk;
+  if (ms_per_step_out) *ms_per_step_out = best.ms;
+  return DTMX_OK;
+}
+
 extern "C" int dtmx_sync(dtmx_ctx* ctx) {
   if (!ctx) return DTMX_ERR_INVALID;
   CK(cudaStreamSynchronize(ctx->stream));
@@ -1406,6 +1564,7 @@ extern "C" int dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block) {
     ctx->tblock = time_block;
   }
   ctx->engine = engine;
+  if (ctx->graph16) { cudaGraphExecDestroy(ctx->graph16); ctx->graph16 = nullptr; }
   return DTMX_OK;
 }
 

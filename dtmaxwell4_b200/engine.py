@@ -23,7 +23,7 @@ EXPORTS = (
     "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_get_stream",
     "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
     "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
-    "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint",
+    "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
 )
 
 
@@ -72,6 +72,7 @@ def load():
     L.dtmx_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
     L.dtmx_set_design.argtypes = [vp, C.POINTER(ip), C.POINTER(ip), vp]
     L.dtmx_forward_adjoint.argtypes = [vp, ip, ip, ip, C.c_double, C.POINTER(C.c_double), vp]
+    L.dtmx_autotune.argtypes = [vp, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), C.POINTER(C.c_double)]
     L.dtmx_batch_forward_adjoint.argtypes = [C.POINTER(vp), ip, ip, ip, C.POINTER(ip), C.POINTER(C.c_double),
                                              C.POINTER(C.c_double), C.POINTER(vp)]
     L.dtmx_count_nonfinite_noalloc.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int64, C.POINTER(C.c_int64)]
@@ -178,6 +179,12 @@ class Simulation:
         self._ck(self._L.dtmx_forward_adjoint(self._h, int(nsteps), int(checkpoint_every), int(plane_x), float(omega),
                                               C.byref(J), grad.ctypes.data))
         return J.value, grad
+
+    def autotune(self, trial_steps=20):
+        """Pick the fastest engine configuration; returns (engine, time_block, xchunk, ms_per_step)."""
+        e, t, x, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        self._ck(self._L.dtmx_autotune(self._h, int(trial_steps), C.byref(e), C.byref(t), C.byref(x), C.byref(ms)))
+        return e.value, t.value, x.value, ms.value
 
     # ---- run
     def step(self, n):

@@ -326,6 +326,15 @@ int  dtmx_count_nonfinite_noalloc(const float* const* d_fields, int nfields, int
  * 2 = L2-resident wavefront (several time steps per launch). */
 int  dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block);
 
+/* Time every applicable engine configuration for trial_steps steps from the
+ * current state (probes and DFT planes paused; the state is restored after
+ * each trial) and keep the fastest: the per-step engine with several x-chunk
+ * sizes and the wavefront engine with 1, 2 and 4 steps per launch (the
+ * reference's torre height, chosen at run time instead of compiled in,
+ * params.h:50-52).  Results are cached per grid shape and feature set. */
+int  dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, int* time_block_out, int* xchunk_out,
+                   double* ms_per_step_out);
+
 #ifdef __cplusplus
 }
 #endif
