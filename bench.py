@@ -34,8 +34,17 @@ def parse():
     ap.add_argument("--n", type=int, default=384)
     ap.add_argument("--tsteps", type=int, default=100)
     ap.add_argument("--engine", type=int, default=0)
+    ap.add_argument("--tblock", type=int, default=0, help="time steps per wavefront launch (--engine 2)")
+    ap.add_argument("--workload", default="drude", choices=["drude", "plain"],
+                    help="drude: the headline workload; plain: seeded fields in vacuum with the CPML only "
+                         "(no sources or monitors), to time the field kernels of both engines")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
+    ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched measurements")
+    ap.add_argument("--extras-only", action="store_true", help="print only the adjoint and batched measurements")
+    ap.add_argument("--adj-steps", type=int, default=2000)
+    ap.add_argument("--batch-instances", type=int, default=16)
+    ap.add_argument("--batch-steps", type=int, default=300)
     return ap.parse_args()
 
 
@@ -137,11 +146,20 @@ def run_ours(args, rank, world):
 
     dev = rank % max(1, torch.cuda.device_count())
     torch.cuda.set_device(dev)
-    sc = scenarios.drude_sphere_tfsf(n=args.n, steps=args.tsteps * (args.steps + args.warmup + 8))
+    if args.workload == "plain":
+        sc = scenarios.drude_sphere_tfsf(n=args.n, steps=args.tsteps * (args.steps + args.warmup + 8))
+        sc = dict(sc, materials=(None, None), tfsf=None, probes=[], dft=[], point_sources=[],
+                  desc="%d^3 vacuum, seeded fields (normal, sigma 1e-3), 12-cell CPML, no sources or monitors" % args.n)
+    else:
+        sc = scenarios.drude_sphere_tfsf(n=args.n, steps=args.tsteps * (args.steps + args.warmup + 8))
     sim = Simulation(sc["cfg"])
     scenarios.apply(sim, sc)
+    if args.workload == "plain":
+        rng = np.random.default_rng(0)
+        for c in range(6):
+            sim.set_field(c, (rng.standard_normal(sim.shape, dtype=np.float32) * 1e-3))
     if args.engine:
-        sim.set_engine(args.engine)
+        sim.set_engine(args.engine, args.tblock)
     ncell = sc["cfg"].nx * sc["cfg"].ny * sc["cfg"].nz
     stream = torch.cuda.ExternalStream(sim.stream_handle())
     for _ in range(args.warmup):
@@ -178,16 +196,27 @@ def run_ours(args, rank, world):
     sim.set_profiling(False)
     hb, eb = algorithmic_bytes(sc)
     peak, peak_kind = measured_peaks()
-    if e_ms >= h_ms:
-        kname, kms, kbytes = "e_kernel", e_ms / cnt, eb
+    if args.engine == 2:
+        # one wavefront launch reads and writes the state once for tblock steps
+        T = max(1, args.tblock)
+        kb = (hb + eb) - 36 * ncell - 3 * ncell          # the H and E reads/writes of one step ...
+        kb += 48 * ncell + 3 * ncell                        # ... become one read + one write of all fields
+        kms = h_ms / cnt * T
+        achieved = kb / (kms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "torre_kernel", "achieved": round(achieved, 1), "peak": peak,
+                "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": kb, "ms_per_launch": round(kms, 4), "steps_per_launch": T}
     else:
-        kname, kms, kbytes = "h_kernel", h_ms / cnt, hb
-    achieved = kbytes / (kms * 1e-3) / 1e9
-    roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
-            "algorithmic_bytes_per_launch": kbytes, "ms_per_launch": round(kms, 4),
-            "h_ms_per_launch": round(h_ms / cnt, 4), "e_ms_per_launch": round(e_ms / cnt, 4),
-            "step_bytes_per_cell_update": round((hb + eb) / ncell, 2)}
+        if e_ms >= h_ms:
+            kname, kms, kbytes = "e_kernel", e_ms / cnt, eb
+        else:
+            kname, kms, kbytes = "h_kernel", h_ms / cnt, hb
+        achieved = kbytes / (kms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_launch": kbytes, "ms_per_launch": round(kms, 4),
+                "h_ms_per_launch": round(h_ms / cnt, 4), "e_ms_per_launch": round(e_ms / cnt, 4),
+                "step_bytes_per_cell_update": round((hb + eb) / ncell, 2)}
 
     # end to end through the public API with host buffers: the state lives in
     # pinned host memory (as the reference's windowed calcStep keeps it in host
@@ -219,6 +248,86 @@ def run_ours(args, rank, world):
            "steps": e_steps}
     sim.close()
     return value, ms_max, launches, roof, e2e, clk, sc
+
+
+def run_adjoint(args):
+    """Forward + adjoint of the differentiation workload (256x256x192, 64x64x32
+    design region, 2000 steps, checkpoint every 100): gradients/s and the
+    forward-only rate of the same run for comparison."""
+    import torch
+    from dtmaxwell4_b200 import Simulation, scenarios
+    sc = scenarios.design_region(steps=args.adj_steps)
+
+    def make():
+        s = Simulation(sc["cfg"])
+        scenarios.apply(s, sc)
+        s.set_design(*sc["design"])
+        return s
+    w = make()
+    w.forward_adjoint(40, sc["plane_x"], sc["omega"], 20)
+    w.close()
+    s = make()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.step(sc["steps"])
+    s.sync()
+    t_fwd = time.perf_counter() - t0
+    s.close()
+    s = make()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, g = s.forward_adjoint(sc["steps"], sc["plane_x"], sc["omega"], 100)
+    t_fa = time.perf_counter() - t0
+    s.close()
+    c = sc["cfg"]
+    cells = c.nx * c.ny * c.nz
+    return {"workload": sc["desc"] + ", %d steps, checkpoint every 100" % sc["steps"],
+            "grads_per_s": round(1.0 / t_fa, 4), "seconds": round(t_fa, 3),
+            "forward_gcell_per_s": round(cells * sc["steps"] / t_fwd / 1e9, 3),
+            "forward_adjoint_gcell_per_s": round(cells * sc["steps"] / t_fa / 1e9, 3),
+            "cost_over_forward": round(t_fa / t_fwd, 2), "objective": J,
+            "note": "wall clock around the public-API calls, host-synchronised"}
+
+
+def run_batched(args):
+    """Independent design-block instances (edges from {64..256}, 8 blocks,
+    one dipole, 10-cell CPML): one-at-a-time forward+adjoint loop against the
+    interleaved batch, gradients/s of each and whether results are identical."""
+    import numpy as np
+    import torch
+    from dtmaxwell4_b200 import Simulation, engine, scenarios
+    n, steps = args.batch_instances, args.batch_steps
+    scs = [scenarios.design_block_instance(seed, steps=steps) for seed in range(n)]
+
+    def make(sc):
+        s = Simulation(sc["cfg"])
+        scenarios.apply(s, sc)
+        s.set_design(*sc["design"])
+        return s
+    w = make(scs[0])
+    w.forward_adjoint(20, scs[0]["plane_x"], scs[0]["omega"], 10)
+    w.close()
+    sims = [make(sc) for sc in scs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loop = [s.forward_adjoint(steps, sc["plane_x"], sc["omega"], 100) for s, sc in zip(sims, scs)]
+    t_loop = time.perf_counter() - t0
+    for s in sims:
+        s.close()
+    sims = [make(sc) for sc in scs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    J, G = engine.batch_forward_adjoint(sims, steps, [sc["plane_x"] for sc in scs], [sc["omega"] for sc in scs], 100)
+    t_batch = time.perf_counter() - t0
+    for s in sims:
+        s.close()
+    same = all(J[b] == loop[b][0] and np.array_equal(G[b], loop[b][1]) for b in range(n))
+    cells = sum(sc["cfg"].nx * sc["cfg"].ny * sc["cfg"].nz for sc in scs)
+    return {"workload": "%d design-block instances (edges 64..256, 8 blocks, dipole, 10-cell CPML, 16^3 design), "
+                        "%d steps each, checkpoint every 100" % (n, steps),
+            "cells": cells, "loop_grads_per_s": round(n / t_loop, 3), "batch_grads_per_s": round(n / t_batch, 3),
+            "batch_over_loop": round(t_loop / t_batch, 3), "identical_to_loop": bool(same),
+            "note": "wall clock around the public-API calls, host-synchronised"}
 
 
 def cpu_sample(args, n, tsteps):
@@ -265,6 +374,10 @@ def main():
         return 0
 
     import torch
+    if args.extras_only:
+        if rank == 0:
+            print(json.dumps({"adjoint": run_adjoint(args), "batched": run_batched(args)}))
+        return 0
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     value, ms, launches, roof, e2e, clk, sc = run_ours(args, rank, world)
@@ -273,6 +386,10 @@ def main():
         v, cores, dt = cpu_sample(args, args.n, args.cpu_steps)
         cpu = {"value": round(v, 5), "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "%d time steps of the %d^3 workload (oracle FP32, %.1f s)" % (args.cpu_steps, args.n, dt)}
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras["adjoint"] = run_adjoint(args)
+        extras["batched"] = run_batched(args)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
@@ -280,11 +397,14 @@ def main():
         line = {"metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "drude_sphere_tfsf %d^3, %d time steps per step" % (args.n, args.tsteps),
+                "config": {"workload": "%s %d^3, %d time steps per step" % (
+                               "drude_sphere_tfsf" if args.workload == "drude" else "plain_cpml", args.n, args.tsteps),
+                           "engine": "per-step" if args.engine != 2 else "wavefront T=%d" % max(1, args.tblock),
                            "desc": sc["desc"], "time_steps_per_step": args.tsteps,
                            "l2": "inputs larger than L2 (%.2f GB of fields)" % (6 * args.n ** 3 * 4 / 1e9),
                            "parallelism": "replicas%d" % world},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+        line.update(extras)
         print(json.dumps(line))
     return 0
 

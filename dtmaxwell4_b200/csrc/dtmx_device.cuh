@@ -391,6 +391,17 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
   float iu[3] = {1.f, 1.f, 1.f};
   if (SIMPLE && !ISH) { iu[0] = ms.inv_eps[um][0]; iu[1] = ms.inv_eps[um][1]; iu[2] = ms.inv_eps[um][2]; }
   constexpr int o0 = ISH ? -2 : -1, o1 = o0 + 1, o2 = o0 + 2, o3 = o0 + 3;
+  // absorber auxiliaries of the thread's nodes, loaded together up front
+  float old[RY][3][3];
+  if (!SIMPLE && tab) {
+#pragma unroll
+    for (int r = 0; r < RY; r++) {
+      const int j = j0 + w + TW * r, k = k0 + tz;
+      if (j >= p.g.n[1] || k >= p.g.n[2] || !(inx || in_slab(p, 1, j) || in_slab(p, 2, k))) continue;
+#pragma unroll
+      for (int c = 0; c < 3; c++) absorb_load(p, cf + c, i, j, k, old[r][c]);
+    }
+  }
 #pragma unroll
   for (int r = 0; r < RY; r++) {
     const int y = w + TW * r;
@@ -449,7 +460,7 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
         d[c][0] = __fmul_rn(d[c][0], ie); d[c][1] = __fmul_rn(d[c][1], ie); d[c][2] = __fmul_rn(d[c][2], ie);
       }
       float inc = sum3(d[c][0], d[c][1], d[c][2]);
-      if (ab) inc = __fadd_rn(inc, absorb_correction(p, cf + c, i, j, k, d[c]));
+      if (ab) inc = __fadd_rn(inc, absorb_apply(p, cf + c, i, j, k, d[c], old[r][c]));
       float nv = __fadd_rn(F, inc);
       if (!ISH && tade && ms.gjc[m] != 0.f) nv = gyro_subtract(p, c, i, j, k, ms.gjc[m], nv);
       p.f[cf + c][off] = nv;

@@ -155,3 +155,23 @@ def design_block_instance(seed, edges=(64, 96, 128, 160, 192, 224, 256), pml=10,
                 omega=2 * math.pi / lambda0,
                 desc="%dx%dx%d, %d blocks eps~U[1,12], Ez dipole, %d-cell CPML, %d^3 design region" %
                      (nx, ny, nz, nblocks, pml, design))
+
+
+def design_region(n=(256, 256, 192), design=(64, 64, 32), pml=10, lambda0=24.0, steps=2000, seed=0, order=2,
+                  courant=0.5):
+    """Differentiation workload: a centred design region of per-node
+    permittivity eps ~ U[1, 12] (seed), an Ez dipole between the design
+    region and the low-x absorber, and the Poynting flux at lambda0 through
+    the plane x = nx - pml - 4 as the objective."""
+    nx, ny, nz = n
+    cfg = abi.make_config(nx, ny, nz, dx=1.0, courant=courant, order=order, pml=pml)
+    lo = tuple((m - d) // 2 for m, d in zip(n, design))
+    eps = np.random.default_rng(seed).uniform(1.0, 12.0, size=(3,) + tuple(design)).astype(np.float32)
+    f0, tau, t0 = gauss_sine_params(lambda0)
+    src = abi.PointSource(comp=abi.EZ, i=(pml + lo[0]) // 2, j=ny // 2, k=nz // 2, waveform=abi.WAVE_GAUSS_SINE,
+                          amp=1.0, f0=f0, tau=tau, t0=t0)
+    return dict(name="design_region", cfg=cfg, materials=(None, None), point_sources=[src], tfsf=None, probes=[],
+                dft=[], steps=steps, design=(lo, eps), plane_x=nx - pml - 4, omega=2 * math.pi / lambda0,
+                desc="%dx%dx%d, %dx%dx%d design region eps~U[1,12] (seed %d), Ez dipole, %d-cell CPML, "
+                     "flux at lambda0=%g through x=%d" % (nx, ny, nz, design[0], design[1], design[2], seed, pml,
+                                                            lambda0, nx - pml - 4))
