@@ -809,6 +809,15 @@ static int launch_step(dtmx_ctx* ctx) {
   if (ctx->profiling) cudaEventRecord(ctx->ev[2], st);
   if (o4) e_kernel<4><<<grd, blk, Pipe<4, false>::SMEM_BYTES, st>>>(P, ctx->maps);
   else e_kernel<2><<<grd, blk, Pipe<2, false>::SMEM_BYTES, st>>>(P, ctx->maps);
+  if (P.ade.Em[0] || ctx->has_gyro) {
+    // dispersive and gyrotropic nodes of the E half step (e_kernel skipped them)
+    const long long na = (long long)P.ade.n[0] * P.ade.n[1] * P.ade.n[2];
+    const unsigned ag = (unsigned)std::min<long long>((na + 255) / 256, 148LL * 16);
+    const bool box = c.geometry == DTMX_GEOM_BOX;
+    if (o4) { if (box) ade_node_kernel<4, true><<<ag, 256, 0, st>>>(P); else ade_node_kernel<4, false><<<ag, 256, 0, st>>>(P); }
+    else { if (box) ade_node_kernel<2, true><<<ag, 256, 0, st>>>(P); else ade_node_kernel<2, false><<<ag, 256, 0, st>>>(P); }
+    nl++;
+  }
   if (ctx->profiling) {
     cudaEventRecord(ctx->ev[3], st);
     // read back this step's two kernel durations (keeps the events reusable)

@@ -374,6 +374,58 @@ __global__ void gyro_current_kernel(Params p, int cur) {
   }
 }
 
+// Dispersive and gyrotropic E nodes, after e_kernel (which leaves dispersive
+// nodes untouched): the ADE recursion (countDisp, dispersion.cpp:85-99) with
+// rot = dt curl H recomputed from H exactly as the field kernels compute it,
+// and E -= dt/eps_inf J^{n+1/2} on gyrotropic nodes.  One thread per cell of
+// the ADE box; BOX: zero-outside geometry (bounds-checked taps).
+template <int ORDER, bool BOX>
+__global__ void ade_node_kernel(Params p) {
+  const long long na = (long long)p.ade.n[0] * p.ade.n[1] * p.ade.n[2];
+  const MatTable& mt = *p.mt;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < na; q += (long long)gridDim.x * blockDim.x) {
+    const int bk = (int)(q % p.ade.n[2]);
+    const long long rr = q / p.ade.n[2];
+    const int bj = (int)(rr % p.ade.n[1]), bi = (int)(rr / p.ade.n[1]);
+    const int i = p.ade.lo[0] + bi, j = p.ade.lo[1] + bj, k = p.ade.lo[2] + bk;
+    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+    const int idx[3] = {i, j, k};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      if (!is_live(p.g, c, i, j, k)) continue;
+      const int m = p.mat[c] ? (int)p.mat[c][id] : 0;
+      const int np = mt.npoles[m];
+      if (np > 0) {
+        float d[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int t = 0; t < 2; t++) {
+          const int a = (c + 1 + t) % 3;             // curl axis of term t
+          const int g = 3 + (c + 2 - t) % 3;         // source H component of term t
+          float v[4];
+#pragma unroll
+          for (int o = 0; o < 4; o++) {
+            v[o] = 0.f;
+            if (ORDER == 2 && (o == 0 || o == 3)) continue;
+            int m3[3] = {i, j, k};
+            m3[a] += o - 1;                          // E taps at -1..+2
+            if (BOX) {
+              const long long sa = a == 0 ? p.g.sx : a == 1 ? p.g.sy : 1;
+              v[o] = (m3[a] >= 0 && m3[a] < p.g.n[a]) ? p.f[g][id + (long long)(o - 1) * sa] : 0.f;
+            } else {
+              v[o] = fetch<1>(p, g, m3[0], m3[1], m3[2]);
+            }
+          }
+          d[a] = __fmul_rn(t == 0 ? p.cdt[a] : -p.cdt[a], dstencil<ORDER>(v[0], v[1], v[2], v[3]));
+        }
+        (void)idx;
+        p.f[c][id] = ade_update(p, c, m, np, q, sum3(d[0], d[1], d[2]), p.f[c][id]);
+      } else if (mt.gjc[m] != 0.f) {
+        p.f[c][id] = __fsub_rn(p.f[c][id], __fmul_rn(mt.gjc[m], p.ade.Jg[p.ade.gnew][c][q]));
+      }
+    }
+  }
+}
+
 __global__ void mask_nonlive_kernel(Params p, int comp, long long ncell) {
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
     const int k = (int)(q % p.g.n[2]);

@@ -445,12 +445,9 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
       if (!ISH) {
         m = um >= 0 ? um : mat_at(smat, c, y, tz);
         if (tade && ms.npoles[m] > 0) {
+          // dispersive node: left to ade_node_kernel, which runs after this kernel
           const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
-          if (bi >= 0 && bi < p.ade.n[0] && bj >= 0 && bj < p.ade.n[1] && bk >= 0 && bk < p.ade.n[2]) {
-            const long long ai = ((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk;
-            p.f[c][off] = ade_update(p, c, m, ms.npoles[m], ai, sum3(d[c][0], d[c][1], d[c][2]), F);
-            continue;
-          }
+          if (bi >= 0 && bi < p.ade.n[0] && bj >= 0 && bj < p.ade.n[1] && bk >= 0 && bk < p.ade.n[2]) continue;
         }
         float ie = ms.inv_eps[m][c];
         if (p.des_on) {
@@ -462,7 +459,6 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
       float inc = sum3(d[c][0], d[c][1], d[c][2]);
       if (ab) inc = __fadd_rn(inc, absorb_apply(p, cf + c, i, j, k, d[c], old[r][c]));
       float nv = __fadd_rn(F, inc);
-      if (!ISH && tade && ms.gjc[m] != 0.f) nv = gyro_subtract(p, c, i, j, k, ms.gjc[m], nv);
       p.f[cf + c][off] = nv;
     }
   }

@@ -81,13 +81,16 @@ __device__ __forceinline__ void stage_plane(const Params& p, const TmaMaps& m, f
   const int tid = threadIdx.y * TZ + threadIdx.x;
   if (fast) {
     if (tid == 0) {
-      mbar_arrive_expect_tx(bar, P::BYTES);
+      // the material tile is needed only when this plane is updated with mixed materials
+      const bool want_mat = !ISH && ip >= 0 && ip < p.g.n[0] &&
+                            __ldg(p.umat + ((long long)ip * p.nty + blockIdx.y) * p.ntz + blockIdx.x) < 0;
+      mbar_arrive_expect_tx(bar, P::BYTES - (ISH || want_mat ? 0u : 3u * OWN_N));
       tma_load_3d(st + P::OFF_A, &m.src[c0], k0 - ZO, j0 - S::YL, ip, bar);
       tma_load_3d(st + P::OFF_B, &m.src[c0 + 1], k0 - ZO, j0, ip, bar);
       tma_load_3d(st + P::OFF_C, &m.src[c0 + 2], k0 - ZO, j0 - S::YL, ip, bar);
 #pragma unroll
       for (int c = 0; c < 3; c++) tma_load_3d(st + P::OFF_OWN + c * OWN_N, &m.own[cf + c], k0, j0, ip, bar);
-      if (!ISH)
+      if (want_mat)
 #pragma unroll
         for (int c = 0; c < 3; c++)
           tma_load_3d(reinterpret_cast<uint8_t*>(st + P::OFF_MAT) + c * OWN_N, &m.mat[c], k0, j0, ip, bar);
