@@ -645,6 +645,22 @@ extern "C" int dtmx_set_tfsf(dtmx_ctx* ctx, const dtmx_tfsf* s) {
             // indices v with X0 <= 2v + o <= X1, clipped to the grid
             int v0 = (int)std::ceil((X0 - o) / 2.0), v1 = (int)std::floor((X1 - o) / 2.0);
             v0 = std::max(v0, 0); v1 = std::min(v1, n[b] - 1);
+            if (b == a) {
+              // along the curl axis keep only the indices where a tap of g actually
+              // crosses the box surface (the other two axes agree for c and g)
+              const int t0 = hs ? -2 : -1, qa = c.order == 4 ? 0 : 1, qb = c.order == 4 ? 3 : 2;
+              auto crosses = [&](int v) {
+                const int S = 2 * v + comp_off(comp, a);
+                const bool sin_ = S >= T.lo[a] && S <= T.hi[a];
+                for (int q = qa; q <= qb; q++) {
+                  const int G = 2 * (v + t0 + q) + comp_off(g, a);
+                  if ((G >= T.lo[a] && G <= T.hi[a]) != sin_) return true;
+                }
+                return false;
+              };
+              while (v0 <= v1 && !crosses(v0)) v0++;
+              while (v1 >= v0 && !crosses(v1)) v1--;
+            }
             if (v0 > v1) empty = true;
             jb.lo[b] = v0; jb.hi[b] = v1;
           }
