@@ -367,6 +367,22 @@ __device__ __forceinline__ float gyro_subtract(const Params& p, int c, int i, in
   return __fsub_rn(nv, __fmul_rn(gjc, p.ade.Jg[p.ade.gnew][c][ai]));
 }
 
+// Absorber auxiliaries of the thread's nodes in plane i (absorber tiles only).
+// They do not depend on the staged tiles, so the streaming loop issues these
+// loads before it waits for the plane's stage, hiding their latency.
+template <bool ISH>
+__device__ __forceinline__ void absorb_prefetch(const Params& p, int i, int j0, int k0, float (&old)[RY][3][3]) {
+  const int cf = ISH ? 3 : 0;
+  const bool inx = in_slab(p, 0, i);
+#pragma unroll
+  for (int r = 0; r < RY; r++) {
+    const int j = j0 + threadIdx.y + TW * r, k = k0 + threadIdx.x;
+    if (j >= p.g.n[1] || k >= p.g.n[2] || !(inx || in_slab(p, 1, j) || in_slab(p, 2, k))) continue;
+#pragma unroll
+    for (int c = 0; c < 3; c++) absorb_load(p, cf + c, i, j, k, old[r][c]);
+  }
+}
+
 // Update of one plane tile (all three components of the half step).  Common
 // path: F + sum of the signed derivative terms (times 1/eps for E); slab
 // nodes add the absorber correction, dispersive nodes (E step, tiles touching
@@ -376,7 +392,8 @@ __device__ __forceinline__ float gyro_subtract(const Params& p, int c, int i, in
 template <int ORDER, bool ISH, bool SIMPLE>
 __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int k0, const float* sm,
                                              const float (&qb)[RY][4], const float (&qc)[RY][4], const float* so,
-                                             const uint8_t* smat, const MatShared& ms, bool fast, int um) {
+                                             const uint8_t* smat, const MatShared& ms, bool fast, int um,
+                                             const float (&old)[RY][3][3]) {
   using S = Stage<ORDER, ISH>;
   const float* sA = sm;
   const float* sB = sA + S::TA::N;
@@ -391,17 +408,6 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
   float iu[3] = {1.f, 1.f, 1.f};
   if (SIMPLE && !ISH) { iu[0] = ms.inv_eps[um][0]; iu[1] = ms.inv_eps[um][1]; iu[2] = ms.inv_eps[um][2]; }
   constexpr int o0 = ISH ? -2 : -1, o1 = o0 + 1, o2 = o0 + 2, o3 = o0 + 3;
-  // absorber auxiliaries of the thread's nodes, loaded together up front
-  float old[RY][3][3];
-  if (!SIMPLE && tab) {
-#pragma unroll
-    for (int r = 0; r < RY; r++) {
-      const int j = j0 + w + TW * r, k = k0 + tz;
-      if (j >= p.g.n[1] || k >= p.g.n[2] || !(inx || in_slab(p, 1, j) || in_slab(p, 2, k))) continue;
-#pragma unroll
-      for (int c = 0; c < 3; c++) absorb_load(p, cf + c, i, j, k, old[r][c]);
-    }
-  }
 #pragma unroll
   for (int r = 0; r < RY; r++) {
     const int y = w + TW * r;

@@ -167,9 +167,19 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
     if (ipre <= last)
       stage_plane<ORDER, ISH, 0>(p, m, dsm + (ipre % NST) * P::STAGE, &bars[ipre % NST], ipre, j0, k0,
                                  yz_safe && plane_safe_x(p.g, ipre));
-    // planes i..i+AHEAD-1 were waited for in earlier iterations (all of them at the start)
-    for (int q = (i == xa ? 0 : AHEAD); q <= AHEAD; q++)
-      mbar_wait(&bars[(i + q) % NST], (unsigned)(((i + q - xa) / NST) & 1), p.err);
+    // values that do not depend on the staged tiles are loaded before the stage
+    // wait, so their latency overlaps it: the plane's uniform material and the
+    // absorber auxiliaries of the thread's nodes
+    const int um = ISH ? 0 : (int)__ldg(p.umat + ((long long)i * p.nty + blockIdx.y) * p.ntz + blockIdx.x);
+    float old[RY][3][3];
+    const bool tab = tile_absorber(p, i, j0, k0);
+    if (tab) absorb_prefetch<ISH>(p, i, j0, k0, old);
+    // planes i..i+AHEAD-1 were waited for in earlier iterations (all of them at the
+    // start); one thread polls the stage barriers and the CTA barrier then releases
+    // everybody (and orders the staged data for them) without spinning issue slots
+    if (tid == 0)
+      for (int q = (i == xa ? 0 : AHEAD); q <= AHEAD; q++)
+        mbar_wait(&bars[(i + q) % NST], (unsigned)(((i + q - xa) / NST) & 1), p.err);
     __syncthreads();
     const bool fast = yz_in && i - 2 >= p.g.all_lo[0] && i + 2 <= p.g.all_hi[0];
 #pragma unroll
@@ -183,12 +193,11 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
       }
     }
     const float* cur = dsm + (i % NST) * P::STAGE;
-    const int um = ISH ? 0 : (int)__ldg(p.umat + ((long long)i * p.nty + blockIdx.y) * p.ntz + blockIdx.x);
     const uint8_t* cmat = reinterpret_cast<const uint8_t*>(cur + P::OFF_MAT);
-    if (fast && um >= 0 && !tile_absorber(p, i, j0, k0))
-      plane_update<ORDER, ISH, true>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um);
+    if (fast && um >= 0 && !tab)
+      plane_update<ORDER, ISH, true>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
     else
-      plane_update<ORDER, ISH, false>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um);
+      plane_update<ORDER, ISH, false>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
 #pragma unroll
     for (int r = 0; r < RY; r++)
 #pragma unroll
