@@ -1512,6 +1512,96 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
   return DTMX_OK;
 }
 
+// ---------------------------------------------------------------- field and state files
+// Field snapshot in the reference's .arr layout (drop.cu:84-107): int32 header
+// {12, 0, 0, 0, 3, sizeof(float), nz, ny, nx} (a 12-byte comment of zeros, the
+// rank, the element size and the extents, fastest first), then the values
+// with z fastest and x slowest; dense cells instead of the reference's one
+// value per rag.
+extern "C" int dtmx_write_arr(dtmx_ctx* ctx, int comp, const char* path) {
+  if (!ctx || comp < 0 || comp > 5 || !path) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
+  const dtmx_config& c = ctx->cfg;
+  std::vector<float> buf((size_t)c.nx * c.ny * c.nz);
+  int rc = dtmx_get_field(ctx, comp, buf.data());
+  if (rc) return rc;
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(ctx, DTMX_ERR_INVALID, std::string("cannot open ") + path);
+  const int32_t hdr[9] = {12, 0, 0, 0, 3, (int32_t)sizeof(float), c.nz, c.ny, c.nx};
+  const bool ok = fwrite(hdr, sizeof(hdr), 1, f) == 1 && fwrite(buf.data(), 4, buf.size(), f) == buf.size();
+  if (fclose(f) != 0 || !ok) return fail(ctx, DTMX_ERR_INVALID, std::string("write failed: ") + path);
+  return DTMX_OK;
+}
+
+// Restartable state file: a header (magic, version, grid, order, geometry,
+// absorber, step, byte count) and the device state of the context (fields,
+// absorber and ADE state, step counter, plane-wave line), so that loading it
+// into a context set up the same way and stepping on reproduces the saved run
+// bit for bit.  Probe traces and DFT accumulators are not part of it.
+struct StateHeader {
+  char magic[8];
+  int32_t version, nx, ny, nz, order, geometry, absorber, pad;
+  int64_t step, bytes;
+};
+
+extern "C" int dtmx_save_state(dtmx_ctx* ctx, const char* path) {
+  if (!ctx || !path) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
+  int rc = prepare(ctx);
+  if (rc) return rc;
+  const size_t sb = state_bytes(ctx);
+  char* dev = nullptr;
+  if (cudaMalloc(&dev, sb) != cudaSuccess) return fail(ctx, DTMX_ERR_OOM, "state buffer");
+  state_copy(ctx, dev, true);
+  std::vector<char> host(sb);
+  cudaError_t e = cudaMemcpyAsync(host.data(), dev, sb, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(ctx, DTMX_ERR_CUDA, std::string("state copy: ") + cudaGetErrorString(e));
+  const dtmx_config& c = ctx->cfg;
+  StateHeader h{};
+  memcpy(h.magic, "DTMXSTAT", 8);
+  h.version = 1; h.nx = c.nx; h.ny = c.ny; h.nz = c.nz; h.order = c.order; h.geometry = c.geometry;
+  h.absorber = c.absorber; h.step = ctx->step; h.bytes = (int64_t)sb;
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(ctx, DTMX_ERR_INVALID, std::string("cannot open ") + path);
+  const bool ok = fwrite(&h, sizeof(h), 1, f) == 1 && fwrite(host.data(), 1, sb, f) == sb;
+  if (fclose(f) != 0 || !ok) return fail(ctx, DTMX_ERR_INVALID, std::string("write failed: ") + path);
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_load_state(dtmx_ctx* ctx, const char* path) {
+  if (!ctx || !path) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
+  int rc = prepare(ctx);
+  if (rc) return rc;
+  FILE* f = fopen(path, "rb");
+  if (!f) return fail(ctx, DTMX_ERR_INVALID, std::string("cannot open ") + path);
+  StateHeader h{};
+  const size_t sb = state_bytes(ctx);
+  const dtmx_config& c = ctx->cfg;
+  if (fread(&h, sizeof(h), 1, f) != 1 || memcmp(h.magic, "DTMXSTAT", 8) != 0 || h.version != 1) {
+    fclose(f);
+    return fail(ctx, DTMX_ERR_INVALID, "not a state file");
+  }
+  if (h.nx != c.nx || h.ny != c.ny || h.nz != c.nz || h.order != c.order || h.geometry != c.geometry ||
+      h.absorber != c.absorber || h.bytes != (int64_t)sb) {
+    fclose(f);
+    return fail(ctx, DTMX_ERR_INVALID, "state file does not match this context (grid, scheme or state layout)");
+  }
+  std::vector<char> host(sb);
+  const bool ok = fread(host.data(), 1, sb, f) == sb;
+  fclose(f);
+  if (!ok) return fail(ctx, DTMX_ERR_INVALID, "truncated state file");
+  char* dev = nullptr;
+  if (cudaMalloc(&dev, sb) != cudaSuccess) return fail(ctx, DTMX_ERR_OOM, "state buffer");
+  cudaError_t e = cudaMemcpyAsync(dev, host.data(), sb, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) { state_copy(ctx, dev, false); e = cudaStreamSynchronize(ctx->stream); }
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(ctx, DTMX_ERR_CUDA, std::string("state copy: ") + cudaGetErrorString(e));
+  ctx->step = h.step;
+  // the host-side parity of the gyrotropic current buffers follows the step count
+  if (ctx->has_gyro) ctx->gcur = (int)(h.step & 1);
+  return DTMX_OK;
+}
+
 extern "C" int dtmx_sync(dtmx_ctx* ctx) {
   if (!ctx) return DTMX_ERR_INVALID;
   CK(cudaStreamSynchronize(ctx->stream));

@@ -24,6 +24,7 @@ EXPORTS = (
     "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
     "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
     "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
+    "dtmx_write_arr", "dtmx_save_state", "dtmx_load_state",
 )
 
 
@@ -72,6 +73,9 @@ def load():
     L.dtmx_abi_sizes.argtypes = [C.POINTER(C.c_int64)]
     L.dtmx_set_design.argtypes = [vp, C.POINTER(ip), C.POINTER(ip), vp]
     L.dtmx_forward_adjoint.argtypes = [vp, ip, ip, ip, C.c_double, C.POINTER(C.c_double), vp]
+    L.dtmx_write_arr.argtypes = [vp, ip, C.c_char_p]
+    L.dtmx_save_state.argtypes = [vp, C.c_char_p]
+    L.dtmx_load_state.argtypes = [vp, C.c_char_p]
     L.dtmx_autotune.argtypes = [vp, ip, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), C.POINTER(C.c_double)]
     L.dtmx_batch_forward_adjoint.argtypes = [C.POINTER(vp), ip, ip, ip, C.POINTER(ip), C.POINTER(C.c_double),
                                              C.POINTER(C.c_double), C.POINTER(vp)]
@@ -180,6 +184,16 @@ class Simulation:
                                               C.byref(J), grad.ctypes.data))
         return J.value, grad
 
+    def write_arr(self, comp, path):
+        """Field snapshot in the reference's .arr layout (see read_arr)."""
+        self._ck(self._L.dtmx_write_arr(self._h, comp, os.fsencode(path)))
+
+    def save_state(self, path):
+        self._ck(self._L.dtmx_save_state(self._h, os.fsencode(path)))
+
+    def load_state(self, path):
+        self._ck(self._L.dtmx_load_state(self._h, os.fsencode(path)))
+
     def autotune(self, trial_steps=20):
         """Pick the fastest engine configuration; returns (engine, time_block, xchunk, ms_per_step)."""
         e, t, x, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
@@ -276,6 +290,19 @@ def batch_forward_adjoint(sims, nsteps, plane_x, omega, checkpoint_every=100):
         msgs = [L.dtmx_last_error(s._h).decode() for s in sims]
         raise DtmxError(rc, "; ".join(m for m in msgs if m))
     return list(J), grads
+
+
+def read_arr(path):
+    """Read an .arr file (int32 header {12, 0, 0, 0, dim, elsize, n_fastest, ..})
+    into an array indexed [x, y, z]."""
+    with open(path, "rb") as f:
+        hdr = np.frombuffer(f.read(4), np.int32)
+        comment = f.read(int(hdr[0]))
+        dim, es = np.frombuffer(f.read(8), np.int32)
+        ext = np.frombuffer(f.read(4 * int(dim)), np.int32)
+        data = np.frombuffer(f.read(), np.float32 if es == 4 else np.float64)
+    del comment
+    return data.reshape(tuple(int(v) for v in ext[::-1]))
 
 
 def abi_sizes():

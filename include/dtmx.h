@@ -306,6 +306,19 @@ int  dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_every, int p
 int  dtmx_batch_forward_adjoint(dtmx_ctx* const* ctxs, int n, int nsteps, int checkpoint_every, const int* plane_x,
                                 const double* omega, double* objectives, float* const* grads);
 
+/* ---- files (reference field drops, drop.cu:45-107; restart) ------------------ */
+
+/* Write component comp as an .arr file: int32 header {12, 0, 0, 0, 3, 4, nz,
+ * ny, nx} followed by nx*ny*nz floats, z fastest (the reference's drop layout
+ * with dense cells instead of one value per rag). */
+int  dtmx_write_arr(dtmx_ctx* ctx, int comp, const char* path);
+/* Save / restore the complete time-stepping state (fields, absorber and
+ * dispersive state, step counter, plane-wave line) of a context; a context set
+ * up the same way that loads the file continues the saved run bit for bit.
+ * Probe traces and DFT accumulators are not included. */
+int  dtmx_save_state(dtmx_ctx* ctx, const char* path);
+int  dtmx_load_state(dtmx_ctx* ctx, const char* path);
+
 /* Count NaN/Inf values in nfields caller-owned device arrays of nelem floats
  * each, without allocating any device memory (no cudaMalloc/cudaFree and no
  * allocating library routine).  For callers that cannot allocate: processes

@@ -206,3 +206,14 @@ def test_oracle_gyrotropic_uniform_mode():
     expect = sorted([(s * wc + math.sqrt(wc * wc + 4 * wp * wp / einf)) / 2 for s in (1, -1)])
     got = sorted(set(round(v, 6) for v in w))
     assert len(got) == 2 and all(abs(g / e - 1) < 2e-3 for g, e in zip(got, expect)), (got, expect)
+
+
+def test_read_arr_layout(tmp_path):
+    """The .arr reader: int32 {12, 0, 0, 0, 3, 4, nz, ny, nx}, z fastest."""
+    from dtmaxwell4_b200 import engine
+    a = np.arange(2 * 3 * 5, dtype=np.float32).reshape(2, 3, 5)
+    p = tmp_path / "f.arr"
+    with open(p, "wb") as f:
+        np.array([12, 0, 0, 0, 3, 4, 5, 3, 2], np.int32).tofile(f)
+        a.tofile(f)
+    assert np.array_equal(engine.read_arr(str(p)), a)
