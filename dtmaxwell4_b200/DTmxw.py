@@ -40,7 +40,8 @@ class TFSFsrc(C.Structure):
         L.dtmx_tfsfsrc_set(C.byref(self), c, imp, lmb)
 
     def check(self):
-        """TFSFsrc::check (signal.hpp:116-133)."""
+        """TFSFsrc::check (signal.hpp:116-133); the shotpoint line prints srcXv
+        twice, as the reference does."""
         print("TF/SF source: Box(s,v,a) |%g-%g|x|%g-%g|x|%g-%g|" % (self.BoxMs, self.BoxPs, self.BoxMv, self.BoxPv,
                                                                    self.BoxMa, self.BoxPa))
         print("TF/SF source: Shotpoint(s,v,a) = %g,%g,%g" % (self.srcXs, self.srcXv, self.srcXv))

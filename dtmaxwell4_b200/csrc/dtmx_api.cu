@@ -1397,25 +1397,25 @@ extern "C" int dtmx_batch_forward_adjoint(dtmx_ctx* const* ctxs, int n, int nste
                                           float* const* grads) {
   if (!ctxs || n < 1 || !plane_x || !omega || !objectives || !grads) return DTMX_ERR_INVALID;
   std::vector<FaRun> R(n);
-  int rc = DTMX_OK, bad = -1;
+  int rc = DTMX_OK;
   auto abort_all = [&](int upto) {
     for (int b = 0; b < upto; b++) fa_abort(ctxs[b], R[b]);
   };
   for (int b = 0; b < n; b++)
     if ((rc = fa_begin(ctxs[b], R[b], nsteps, checkpoint_every, plane_x[b], omega[b]))) { abort_all(b); return rc; }
   for (int st = 0; st < nsteps && !rc; st++)
-    for (int b = 0; b < n && !rc; b++) { rc = fa_forward(ctxs[b], R[b], st); bad = b; }
-  for (int b = 0; b < n && !rc; b++) { rc = fa_forward_done(ctxs[b], R[b]); bad = b; }
+    for (int b = 0; b < n && !rc; b++) rc = fa_forward(ctxs[b], R[b], st);
+  for (int b = 0; b < n && !rc; b++) rc = fa_forward_done(ctxs[b], R[b]);
   const int nseg = R[0].nseg;
   for (int seg = nseg - 1; seg >= 0 && !rc; seg--) {
     for (int b = 0; b < n; b++) fa_segment_begin(ctxs[b], R[b], seg);
     const int len = R[0].len;
     for (int q = 1; q <= len && !rc; q++)
-      for (int b = 0; b < n && !rc; b++) { rc = fa_recompute(ctxs[b], R[b], q); bad = b; }
+      for (int b = 0; b < n && !rc; b++) rc = fa_recompute(ctxs[b], R[b], q);
     for (int q = len; q >= 1 && !rc; q--)
-      for (int b = 0; b < n && !rc; b++) { rc = fa_adjoint(ctxs[b], R[b], q); bad = b; }
+      for (int b = 0; b < n && !rc; b++) rc = fa_adjoint(ctxs[b], R[b], q);
   }
-  if (rc) { abort_all(n); (void)bad; return rc; }
+  if (rc) { abort_all(n); return rc; }
   for (int b = 0; b < n; b++) {
     int r = fa_finish(ctxs[b], R[b], &objectives[b], grads[b]);
     if (r && !rc) rc = r;

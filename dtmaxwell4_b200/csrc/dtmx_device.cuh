@@ -197,9 +197,10 @@ __device__ __forceinline__ int mat_at(const uint8_t* sm, int c, int y, int z) { 
 //   CPML:  correction_a = (1/kappa_a - 1) dif_a + psi_a,  psi_a <- b psi_a + a dif_a
 //   split: correction_a = (K1_a - 1) p_a + (K2_a - 1) dif_a,  p_a <- K1_a p_a + K2_a dif_a
 // (the split form follows from F = rest + sum p_a with rest += undamped terms).
-// Split form for callers that batch their slab loads: absorb_load reads the
-// auxiliary value of every slab axis of the node (0 elsewhere), absorb_apply
-// computes the correction from those values and stores the new ones.
+// Split into a load and an apply step so that callers can issue the slab
+// loads early: absorb_load reads the auxiliary value of every slab axis of the
+// node (0 elsewhere), absorb_apply computes the correction from those values
+// and stores the new ones.
 __device__ __forceinline__ void absorb_load(const Params& p, int c, int i, int j, int k, float (&old)[3]) {
   const int idx[3] = {i, j, k};
 #pragma unroll
@@ -227,11 +228,6 @@ __device__ __forceinline__ float absorb_apply(const Params& p, int c, int i, int
     else corr = __fadd_rn(corr, __fsub_rn(__fsub_rn(nv, old[a]), dif[a]));
   }
   return corr;
-}
-__device__ __forceinline__ float absorb_correction(const Params& p, int c, int i, int j, int k, const float* dif) {
-  float old[3];
-  absorb_load(p, c, i, j, k, old);
-  return absorb_apply(p, c, i, j, k, dif, old);
 }
 
 // Shared-memory copy of one component's plane tile: rows of TW_ROW floats
