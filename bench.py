@@ -158,8 +158,13 @@ def run_ours(args, rank, world):
         rng = np.random.default_rng(0)
         for c in range(6):
             sim.set_field(c, (rng.standard_normal(sim.shape, dtype=np.float32) * 1e-3))
+    run_ours.tuned = (max(1, args.engine), args.tblock, 0, 0.0)
     if args.engine:
         sim.set_engine(args.engine, args.tblock)
+    else:
+        # engine configuration chosen by the library's autotuner (state is restored after the trials)
+        tuned = sim.autotune(12)
+        run_ours.tuned = tuned
     ncell = sc["cfg"].nx * sc["cfg"].ny * sc["cfg"].nz
     stream = torch.cuda.ExternalStream(sim.stream_handle())
     for _ in range(args.warmup):
@@ -405,7 +410,9 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": "%s %d^3, %d time steps per step" % (
                                "drude_sphere_tfsf" if args.workload == "drude" else "plain_cpml", args.n, args.tsteps),
-                           "engine": "per-step" if args.engine != 2 else "wavefront T=%d" % max(1, args.tblock),
+                           "engine": ("wavefront T=%d" % max(1, args.tblock)) if args.engine == 2 else
+                                     "engine %d, T %d, x chunk %d (0: automatic)%s" % (tuple(run_ours.tuned[:3]) + (
+                                         ", chosen by dtmx_autotune" if not args.engine else "",)),
                            "desc": sc["desc"], "time_steps_per_step": args.tsteps,
                            "l2": "inputs larger than L2 (%.2f GB of fields)" % (6 * args.n ** 3 * 4 / 1e9),
                            "parallelism": "replicas%d" % world},

@@ -1465,7 +1465,7 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     std::vector<TuneVal> cand;
-    for (int xc : {0, 4, 8, 16, 32, 64})
+    for (int xc : {0, 4, 6, 8, 10, 12, 16, 24, 32, 64})
       if (xc <= c.nx) cand.push_back({1, 0, xc, 0});
     std::string why;
     if (torre_features_ok(ctx, &why))

@@ -341,8 +341,8 @@ int  dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block);
 
 /* Time every applicable engine configuration for trial_steps steps from the
  * current state (probes and DFT planes paused; the state is restored after
- * each trial) and keep the fastest: the per-step engine with several x-chunk
- * sizes and the wavefront engine with 1, 2 and 4 steps per launch (the
+ * each trial) and keep the fastest: the per-step engine with x chunks of 4 to 64
+ * planes per CTA and the wavefront engine with 1, 2 and 4 steps per launch (the
  * reference's torre height, chosen at run time instead of compiled in,
  * params.h:50-52).  Results are cached per grid shape and feature set. */
 int  dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, int* time_block_out, int* xchunk_out,
