@@ -139,6 +139,21 @@ def algorithmic_bytes(sc):
     return hb, eb
 
 
+def max_over_ranks(ms, world, device):
+    """The timed region's duration on this rank -> the maximum over all ranks
+    (every rank takes part; the slowest replica sets the job's time)."""
+    import torch
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(cell_updates_per_rank, world, ms_max):
+    """Whole-job Gcell-updates/s: the work of all replicas over the slowest rank's time."""
+    return cell_updates_per_rank * world / (ms_max * 1e-3) / 1e9
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -186,12 +201,8 @@ def run_ours(args, rank, world):
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     torch.cuda.synchronize()
-    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
-    cell_updates = ncell * args.tsteps * args.steps * world
-    value = cell_updates / (ms_max * 1e-3) / 1e9
+    ms_max = max_over_ranks(ms, world, "cuda")
+    value = aggregate_rate(ncell * args.tsteps * args.steps, world, ms_max)
     assert sim.check_finite(), "non-finite fields"
 
     # roofline of the dominant field kernel: per-launch device time with events
@@ -250,10 +261,7 @@ def run_ours(args, rank, world):
             sim.get_field(c, out=arrs[c])
     e1.record(stream)
     e1.synchronize()
-    te = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MAX)
-    e2e_val = ncell * args.tsteps * e_steps * world / (float(te.item()) * 1e-3) / 1e9
+    e2e_val = aggregate_rate(ncell * args.tsteps * e_steps, world, max_over_ranks(e0.elapsed_time(e1), world, "cuda"))
     nb = 6 * ncell * 4
     e2e = {"value": round(e2e_val, 3), "unit": UNIT, "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
            "steps": e_steps}
