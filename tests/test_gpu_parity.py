@@ -216,3 +216,37 @@ def test_gyrotropic_layer_point_dipole():
     o.step(sc["steps"])
     _compare_probes(g, o)
     _compare_fields(g, o)
+
+
+def test_two_pole_sphere_uneven_grid_order4():
+    """Lorentz + Drude two-pole ADE sphere, order 4, CPML, uneven grid with
+    partial y and z tiles, soft Ez source."""
+    from dtmaxwell4_b200 import abi, scenarios
+    sc = scenarios.point_dipole_sphere(n=(36, 44, 52), steps=200, pml=6, radius=6, eps=1.0, order=4, courant=0.4,
+                                       lambda0=10.0)
+    two = abi.make_material(1.0, poles=[(abi.POLE_LORENTZ, 1.5, 0.5, 0.05, 0.0), (abi.POLE_DRUDE, 1.0, 0.8, 0.02, 0.0)],
+                            eps_inf=2.0)
+    mats, idx = sc["materials"]
+    sc["materials"] = ([mats[0], two], idx)
+    sc["point_sources"][0].i -= 8                 # the source sits outside the sphere
+    g, o, _, _ = _pair(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    _compare_probes(g, o)
+    _compare_fields(g, o)
+
+
+def test_gyrotropic_layer_order4():
+    from dtmaxwell4_b200 import abi, scenarios
+    n = 40
+    w0 = 2 * math.pi / 12.0
+    einf, gyro = abi.gyro_for(4.0, 0.3, w0)
+    sc = scenarios.point_dipole_sphere(n=n, steps=240, pml=6, radius=0.1, eps=1.0, order=4, courant=0.4, lambda0=12.0)
+    idx = np.zeros((n, n, n), np.uint8)
+    idx[:, :, 8:18] = 1
+    sc["materials"] = ([abi.make_material(1.0), abi.make_material(eps_inf=einf, gyro=gyro)], [idx, idx, idx])
+    g, o, _, _ = _pair(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    _compare_probes(g, o)
+    _compare_fields(g, o)
