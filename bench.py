@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--adj-steps", type=int, default=2000)
     ap.add_argument("--batch-instances", type=int, default=16)
     ap.add_argument("--batch-steps", type=int, default=300)
+    ap.add_argument("--gyro-steps", type=int, default=100, help="timed steps of the 1024x1024x1536 gyrotropic run")
+    ap.add_argument("--gyro-n", type=int, nargs=3, default=[1024, 1024, 1536])
+    ap.add_argument("--no-gyro", action="store_true", help="skip the gyrotropic / Purcell measurement")
     return ap.parse_args()
 
 
@@ -349,6 +352,62 @@ def run_batched(args):
             "note": "wall clock around the public-API calls, host-synchronised"}
 
 
+def run_gyro_purcell(args):
+    """Gyrotropic photonic-crystal workload with its FP64 flux box: the
+    forward rate at the full 1024 x 1024 x 1536 size over a bounded number of
+    steps, and the Purcell spectrum W/W0 of the same lattice, slab, layer and
+    dipole on a 256 x 256 x 512 cut of it run for the full 8000 steps against
+    a vacuum run with the same source and box."""
+    import numpy as np
+    from dtmaxwell4_b200 import Simulation, purcell, scenarios
+    out = {}
+    # full size: forward rate
+    n = tuple(args.gyro_n)
+    sc = scenarios.gyro_crystal_purcell(n=n, steps=args.gyro_steps)
+    s = Simulation(sc["cfg"])
+    scenarios.apply(s, sc)
+    scenarios.apply_flux(s, sc)
+    s.step(3)
+    s.sync()
+    t0 = time.perf_counter()
+    s.step(args.gyro_steps)
+    s.sync()
+    dt = time.perf_counter() - t0
+    s.close()
+    hb, eb = algorithmic_bytes(sc)
+    gyro = sum(int((sc["materials"][1][c] == 2).sum()) for c in range(3))
+    ncell = n[0] * n[1] * n[2]
+    b_cell = (hb + eb + 8 * gyro) / ncell
+    rate = ncell * args.gyro_steps / dt / 1e9
+    hbm, kind = measured_peaks()
+    out.update({"workload": sc["desc"] + ", %d timed steps (of 8000) after 3 warm-up steps" % args.gyro_steps,
+                "gcell_per_s": round(rate, 3), "ms_per_step": round(1e3 * dt / args.gyro_steps, 3),
+                "bytes_per_cell_update": round(b_cell, 2),
+                "hbm_frac": round(rate * 1e9 * b_cell / (hbm * 1e9), 4), "hbm_peak_gbs": hbm, "peak_kind": kind})
+    del sc
+    # Purcell spectrum on a cut of the structure, full step count
+    cut = scenarios.gyro_crystal_purcell(n=(256, 256, 512), steps=8000)
+    vac = scenarios.gyro_crystal_purcell(n=(128, 128, 128), steps=8000, structure=False)
+    power = []
+    t0 = time.perf_counter()
+    for sc in (cut, vac):
+        s = Simulation(sc["cfg"])
+        scenarios.apply(s, sc)
+        fid, = scenarios.apply_flux(s, sc)
+        s.step(sc["steps"])
+        power.append(s.read_flux(fid)[1])
+        s.close()
+    t_p = time.perf_counter() - t0
+    om = cut["flux"][0][2]
+    w = purcell.purcell_flux(power[0], power[1], cut["eps_src"], vac["eps_src"])
+    lam = 2 * np.pi / om
+    out["purcell"] = {"workload": cut["desc"] + "; W0: " + vac["desc"] + "; 8000 steps each",
+                      "wavelength_cells": [round(float(v), 3) for v in lam],
+                      "w_over_w0": [round(float(v), 5) for v in w], "seconds": round(t_p, 2),
+                      "note": "flux-box powers normalised to equal source currents (eps_src^2)"}
+    return out
+
+
 def cpu_sample(args, n, tsteps):
     """Time the oracle (FP32 port, all host threads) on a bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -395,7 +454,10 @@ def main():
     import torch
     if args.extras_only:
         if rank == 0:
-            print(json.dumps({"adjoint": run_adjoint(args), "batched": run_batched(args)}))
+            ex = {"adjoint": run_adjoint(args), "batched": run_batched(args)}
+            if not args.no_gyro:
+                ex["gyro_purcell"] = run_gyro_purcell(args)
+            print(json.dumps(ex))
         return 0
     if world > 1:
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
@@ -409,6 +471,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         extras["adjoint"] = run_adjoint(args)
         extras["batched"] = run_batched(args)
+        if not args.no_gyro:
+            extras["gyro_purcell"] = run_gyro_purcell(args)
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()

@@ -33,6 +33,15 @@ struct DftHost {
   int nstaged = 0;          // samples staged since the last flush
 };
 
+// Six DFT patches of the tangential E and H components on the faces of a box
+// and the device buffer their flux reduction writes to.
+struct FluxHost {
+  int face[6];              // DFT ids: x lo, x hi, y lo, y hi, z lo, z hi
+  double sgn_area[6];       // outward sign times the cell face area
+  int nfreq;
+  double* d_out = nullptr;  // [6][nfreq]
+};
+
 struct dtmx_ctx {
   dtmx_config cfg{};
   int dev = 0;
@@ -66,6 +75,7 @@ struct dtmx_ctx {
   float* d_traces = nullptr;
   int probe_cap = 0;
   std::vector<DftHost> dfts;
+  std::vector<FluxHost> fluxes;
   // state
   long long* d_step = nullptr;
   int* d_flag = nullptr;
@@ -421,6 +431,7 @@ extern "C" void dtmx_destroy(dtmx_ctx* ctx) {
   if (ctx->graph16) cudaGraphExecDestroy(ctx->graph16);
   for (void* p : ctx->allocs) cudaFree(p);
   for (auto& d : ctx->dfts) { cudaFree(d.omega); cudaFree(d.acc); cudaFree(d.stage); cudaFree(d.sstep); }
+  for (auto& fx : ctx->fluxes) cudaFree(fx.d_out);
   cudaFree(ctx->obj.omega); cudaFree(ctx->obj.acc); cudaFree(ctx->obj.stage); cudaFree(ctx->obj.sstep);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -711,16 +722,20 @@ extern "C" int dtmx_read_probes(dtmx_ctx* ctx, float* out, int max_samples, int*
   return DTMX_OK;
 }
 
-extern "C" int dtmx_add_dft_plane(dtmx_ctx* ctx, int axis, int index, int comp_mask, int nfreq, const double* omegas, int* id_out) {
+extern "C" int dtmx_add_dft_patch(dtmx_ctx* ctx, int axis, int index, int lo1, int n1, int lo2, int n2, int comp_mask,
+                                  int nfreq, const double* omegas, int* id_out) {
   if (!ctx || axis < 0 || axis > 2 || nfreq < 1 || nfreq > 64 || !omegas || (comp_mask & ~63) || !comp_mask)
     return fail(ctx, DTMX_ERR_INVALID, "bad DFT plane");
   const int n[3] = {ctx->cfg.nx, ctx->cfg.ny, ctx->cfg.nz};
+  const int e1 = n[axis == 0 ? 1 : 0], e2 = n[axis == 2 ? 1 : 2];
   if (index < 0 || index >= n[axis]) return fail(ctx, DTMX_ERR_INVALID, "DFT plane index out of range");
+  if (lo1 < 0 || n1 < 1 || lo1 + n1 > e1 || lo2 < 0 || n2 < 1 || lo2 + n2 > e2)
+    return fail(ctx, DTMX_ERR_INVALID, "DFT patch outside the plane");
   if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "DFT planes must be added before the first step");
-  DftHost h;
+  DftHost h{};
   h.d.axis = axis; h.d.index = index; h.d.comp_mask = comp_mask; h.d.nfreq = nfreq;
-  h.d.n1 = n[axis == 0 ? 1 : 0];
-  h.d.n2 = n[axis == 2 ? 1 : 2];
+  h.d.lo1 = lo1; h.d.n1 = n1;
+  h.d.lo2 = lo2; h.d.n2 = n2;
   h.ncomp = __builtin_popcount(comp_mask);
   const size_t nacc = (size_t)h.ncomp * nfreq * h.d.n1 * h.d.n2;
   if (cudaMalloc(&h.omega, nfreq * sizeof(double)) != cudaSuccess) return fail(ctx, DTMX_ERR_OOM, "DFT allocation");
@@ -736,6 +751,49 @@ extern "C" int dtmx_add_dft_plane(dtmx_ctx* ctx, int axis, int index, int comp_m
   ctx->dfts.push_back(h);
   CK(cudaStreamSynchronize(ctx->stream));
   if (id_out) *id_out = (int)ctx->dfts.size() - 1;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_add_dft_plane(dtmx_ctx* ctx, int axis, int index, int comp_mask, int nfreq, const double* omegas, int* id_out) {
+  if (!ctx || axis < 0 || axis > 2) return fail(ctx, DTMX_ERR_INVALID, "bad DFT plane");
+  const int n[3] = {ctx->cfg.nx, ctx->cfg.ny, ctx->cfg.nz};
+  return dtmx_add_dft_patch(ctx, axis, index, 0, n[axis == 0 ? 1 : 0], 0, n[axis == 2 ? 1 : 2], comp_mask, nfreq, omegas,
+                            id_out);
+}
+
+extern "C" int dtmx_add_flux_box(dtmx_ctx* ctx, const int lo[3], const int hi[3], int nfreq, const double* omegas,
+                                 int* id_out) {
+  if (!ctx || !lo || !hi) return fail(ctx, DTMX_ERR_INVALID, "bad flux box");
+  const int n[3] = {ctx->cfg.nx, ctx->cfg.ny, ctx->cfg.nz};
+  const double ds[3] = {ctx->cfg.dx, ctx->cfg.dy, ctx->cfg.dz};
+  for (int a = 0; a < 3; a++)
+    if (lo[a] < 0 || hi[a] <= lo[a] || hi[a] >= n[a]) return fail(ctx, DTMX_ERR_INVALID, "flux box outside the grid");
+  FluxHost fx{};
+  fx.nfreq = nfreq;
+  for (int a = 0; a < 3; a++) {
+    // in-plane axes in (slow, fast) order and the tangential components
+    const int s1 = a == 0 ? 1 : 0, s2 = a == 2 ? 1 : 2;
+    const int b = (a + 1) % 3, c = (a + 2) % 3;
+    const int mask = (1 << b) | (1 << c) | (1 << (3 + b)) | (1 << (3 + c));
+    for (int side = 0; side < 2; side++) {
+      int id = -1;
+      const int rc = dtmx_add_dft_patch(ctx, a, side ? hi[a] : lo[a], lo[s1], hi[s1] - lo[s1], lo[s2], hi[s2] - lo[s2],
+                                        mask, nfreq, omegas, &id);
+      if (rc) return rc;
+      fx.face[2 * a + side] = id;
+      fx.sgn_area[2 * a + side] = (side ? 1.0 : -1.0) * ds[s1] * ds[s2];
+    }
+  }
+  if (cudaMalloc(&fx.d_out, (size_t)6 * nfreq * sizeof(double)) != cudaSuccess)
+    return fail(ctx, DTMX_ERR_OOM, "flux box allocation");
+  ctx->fluxes.push_back(fx);
+  if (id_out) *id_out = (int)ctx->fluxes.size() - 1;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_flux_faces(dtmx_ctx* ctx, int id, int faces[6]) {
+  if (!ctx || id < 0 || id >= (int)ctx->fluxes.size() || !faces) return fail(ctx, DTMX_ERR_INVALID, "bad flux box id");
+  for (int q = 0; q < 6; q++) faces[q] = ctx->fluxes[id].face[q];
   return DTMX_OK;
 }
 
@@ -756,6 +814,28 @@ extern "C" int dtmx_read_dft(dtmx_ctx* ctx, int id, double* out, size_t out_len)
   dft_flush(ctx, h);
   CK(cudaStreamSynchronize(ctx->stream));
   CK(cudaMemcpy(out, h.acc, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_read_flux(dtmx_ctx* ctx, int id, double* out, size_t out_len) {
+  if (!ctx || id < 0 || id >= (int)ctx->fluxes.size() || !out) return fail(ctx, DTMX_ERR_INVALID, "bad flux box id");
+  FluxHost& fx = ctx->fluxes[id];
+  const int nf = fx.nfreq;
+  if (out_len < (size_t)7 * nf) return fail(ctx, DTMX_ERR_INVALID, "output buffer too small");
+  for (int q = 0; q < 6; q++) {
+    DftHost& h = ctx->dfts[fx.face[q]];
+    dft_flush(ctx, h);
+    flux_face_kernel<<<nf, FLUX_THREADS, 0, ctx->stream>>>(h.d, fx.sgn_area[q], fx.d_out + (size_t)q * nf);
+    ctx->launches++;
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpy(out, fx.d_out, (size_t)6 * nf * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int f = 0; f < nf; f++) {
+    double t = 0.0;
+    for (int q = 0; q < 6; q++) t += out[(size_t)q * nf + f];
+    out[(size_t)6 * nf + f] = t;
+  }
   return DTMX_OK;
 }
 

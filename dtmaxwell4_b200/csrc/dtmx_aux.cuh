@@ -260,6 +260,7 @@ __global__ void probe_kernel(Params p, const ProbeDev* pr, int np, float* traces
 
 struct DftDev {
   int axis, index, comp_mask, nfreq, n1, n2;
+  int lo1, lo2;             // window origin along the two in-plane axes (slow, fast)
   const double* omega;
   double2* acc;             // [ncomp][nfreq][n1*n2]
   float* stage;             // [DFT_STAGE][ncomp][n1*n2] plane samples not yet accumulated
@@ -278,7 +279,7 @@ __global__ void dft_capture_kernel(Params p, DftDev d, const long long* d_step, 
   const long long pt = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (pt == 0) d.sstep[slot] = *d_step + 1;
   if (pt >= npts) return;
-  const int u = (int)(pt / d.n2), v = (int)(pt % d.n2);
+  const int u = d.lo1 + (int)(pt / d.n2), v = d.lo2 + (int)(pt % d.n2);
   int i, j, k;
   if (d.axis == 0) { i = d.index; j = u; k = v; }
   else if (d.axis == 1) { i = u; j = d.index; k = v; }
@@ -331,6 +332,36 @@ __global__ void __launch_bounds__(256) dft_flush_kernel(DftDev d, int nslots, do
     }
     ci++;
   }
+}
+
+// Outward Poynting flux of one face of a flux box at every frequency of its
+// DFT patch: out[f] = sgn_area * sum_pts Re(E_b conj(H_c) - E_c conj(H_b)) with
+// (a, b, c) = (normal, (a+1)%3, (a+2)%3), so that (b, c, a) is right-handed.
+// One block per frequency; every thread sums a fixed stride of points and a
+// fixed tree combines the threads, so the value does not depend on timing.
+constexpr int FLUX_THREADS = 256;
+__device__ __forceinline__ int dft_slot(int mask, int comp) { return __popc(mask & ((1 << comp) - 1)); }
+__global__ void __launch_bounds__(FLUX_THREADS) flux_face_kernel(DftDev d, double sgn_area, double* out) {
+  __shared__ double red[FLUX_THREADS];
+  const int f = blockIdx.x;
+  const int a = d.axis, b = (a + 1) % 3, c = (a + 2) % 3;
+  const long long npts = (long long)d.n1 * d.n2;
+  const double2* Eb = d.acc + ((long long)dft_slot(d.comp_mask, b) * d.nfreq + f) * npts;
+  const double2* Ec = d.acc + ((long long)dft_slot(d.comp_mask, c) * d.nfreq + f) * npts;
+  const double2* Hb = d.acc + ((long long)dft_slot(d.comp_mask, 3 + b) * d.nfreq + f) * npts;
+  const double2* Hc = d.acc + ((long long)dft_slot(d.comp_mask, 3 + c) * d.nfreq + f) * npts;
+  double s = 0.0;
+  for (long long pt = threadIdx.x; pt < npts; pt += FLUX_THREADS) {
+    const double2 eb = Eb[pt], ec = Ec[pt], hb = Hb[pt], hc = Hc[pt];
+    s += (eb.x * hc.x + eb.y * hc.y) - (ec.x * hb.x + ec.y * hb.y);
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = FLUX_THREADS / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[f] = sgn_area * red[0];
 }
 
 // Magnetised-Drude current over the ADE box (dtmx.h, dtmx_material):

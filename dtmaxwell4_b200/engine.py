@@ -25,6 +25,7 @@ EXPORTS = (
     "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
     "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
     "dtmx_write_arr", "dtmx_save_state", "dtmx_load_state",
+    "dtmx_add_dft_patch", "dtmx_add_flux_box", "dtmx_read_flux", "dtmx_flux_faces",
 )
 
 
@@ -58,6 +59,10 @@ def load():
     L.dtmx_read_probes.argtypes = [vp, vp, ip, C.POINTER(ip)]
     L.dtmx_add_dft_plane.argtypes = [vp, ip, ip, ip, ip, vp, C.POINTER(ip)]
     L.dtmx_read_dft.argtypes = [vp, ip, vp, C.c_size_t]
+    L.dtmx_add_dft_patch.argtypes = [vp, ip, ip, ip, ip, ip, ip, ip, ip, vp, C.POINTER(ip)]
+    L.dtmx_add_flux_box.argtypes = [vp, C.POINTER(ip), C.POINTER(ip), ip, vp, C.POINTER(ip)]
+    L.dtmx_read_flux.argtypes = [vp, ip, vp, C.c_size_t]
+    L.dtmx_flux_faces.argtypes = [vp, ip, C.POINTER(ip)]
     L.dtmx_step.argtypes = [vp, ip]
     L.dtmx_sync.argtypes = [vp]
     L.dtmx_get_step.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -107,6 +112,7 @@ class Simulation:
         self._h = h
         self.shape = (cfg.nx, cfg.ny, cfg.nz)
         self._dft = []
+        self._flux = []
         self._nprobes = 0
         self.probe_list = []
 
@@ -162,6 +168,41 @@ class Simulation:
         del n[axis]
         self._dft.append((bin(comp_mask).count("1"), len(om), n[0], n[1]))
         return did.value
+
+    def add_dft_patch(self, axis, index, lo1, n1, lo2, n2, comp_mask, omegas):
+        """Running DFT on an n1 x n2 window of the plane {axis = index}."""
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        did = C.c_int(-1)
+        self._ck(self._L.dtmx_add_dft_patch(self._h, axis, index, lo1, n1, lo2, n2, comp_mask, len(om),
+                                            om.ctypes.data, C.byref(did)))
+        self._dft.append((bin(comp_mask).count("1"), len(om), n1, n2))
+        return did.value
+
+    def add_flux_box(self, lo, hi, omegas):
+        """Six face DFT windows of a power flux box (dtmx_add_flux_box); returns its id."""
+        om = np.ascontiguousarray(omegas, dtype=np.float64)
+        lo3 = (C.c_int * 3)(*[int(v) for v in lo])
+        hi3 = (C.c_int * 3)(*[int(v) for v in hi])
+        fid = C.c_int(-1)
+        self._ck(self._L.dtmx_add_flux_box(self._h, lo3, hi3, len(om), om.ctypes.data, C.byref(fid)))
+        faces = (C.c_int * 6)()
+        self._ck(self._L.dtmx_flux_faces(self._h, fid.value, faces))
+        for a in range(3):
+            n = [hi[q] - lo[q] for q in range(3) if q != a]
+            for _ in range(2):
+                self._dft.append((4, len(om), n[0], n[1]))
+        self._flux.append((len(om), list(faces)))
+        return fid.value
+
+    def flux_faces(self, fid):
+        return list(self._flux[fid][1])
+
+    def read_flux(self, fid):
+        """(faces[6, nfreq], total[nfreq]): outward FP64 flux of each face and their sum."""
+        nf = self._flux[fid][0]
+        out = np.zeros(7 * nf, dtype=np.float64)
+        self._ck(self._L.dtmx_read_flux(self._h, fid, out.ctypes.data, out.size))
+        return out[: 6 * nf].reshape(6, nf), out[6 * nf:]
 
     def set_engine(self, engine, time_block=0):
         self._ck(self._L.dtmx_set_engine(self._h, engine, time_block))

@@ -7,6 +7,12 @@ Workloads (all in c = 1 units with dx = 1 cell unless stated):
   source with a Gaussian-modulated sine, CPML on all faces, Ez/Hx traces at
   seeded random probe points (128^3, lambda0 = 20 cells, Courant 0.5, 10-cell
   CPML, sphere r = 20 cells eps = 4, 1000 steps at full size).
+* gyro_crystal_purcell -- photonic-crystal slab (eps 12, triangular lattice of
+  air holes) on a magnetised-Drude gyrotropic layer (eps_diag 4, off-diagonal
+  0.3 at the source frequency), soft Ez dipole in a missing-hole defect at the
+  slab's mid-plane, running FP64 DFTs on the six faces of a flux box around
+  the dipole (1024 x 1024 x 1536, slab 40 cells, layer 200 cells, period 32,
+  hole radius 10, box half-width 20, 32 frequencies, 8000 steps at full size).
 * drude_sphere_tfsf -- Drude sphere (eps_inf = 1, wp = 2 pi c/(8 dx),
   gamma = wp/50) lit by a +x, Ez-polarised Gaussian-pulse plane wave through a
   TF/SF box inset 20 cells from a 12-cell CPML; running DFT at 16 frequencies
@@ -103,6 +109,90 @@ def drude_sphere_tfsf(n=384, steps=4000, pml=12, inset=20, radius=None, order=2,
                 desc="%dx%dx%d Drude sphere r=%g (wp=2pi/8, gamma=wp/50), TF/SF +x Ez plane wave lambda0=%g, "
                      "%d-cell CPML, box inset %d, %d-freq DFT plane x=%d" % (nx, ny, nz, radius, lambda0, pml,
                                                                              inset, nfreq, xplane))
+
+
+def triangular_holes(nx, ny, center, period, radius, comp):
+    """2-D mask (nx, ny) of the E component comp's nodes inside the air holes of
+    a triangular lattice (a1 = (period, 0), a2 = (period/2, period sqrt(3)/2))
+    through `center`, leaving the hole at `center` out (the defect).  Needs
+    radius < period/2: a node then lies within `radius` of at most one site,
+    and the nearest site of each of the two lattice rows around it is tested."""
+    if not radius < 0.5 * period:
+        raise ValueError("hole radius must be below half the period")
+    off = [(0, 1), (1, 0), (1, 1)][comp]
+    x = (np.arange(nx) + 0.5 * off[0])[:, None] - center[0]
+    y = (np.arange(ny) + 0.5 * off[1])[None, :] - center[1]
+    h = period * math.sqrt(3.0) / 2.0
+    mask = np.zeros((nx, ny), bool)
+    l0 = np.floor(y / h)
+    for dl in (0.0, 1.0):
+        l = l0 + dl
+        m = np.round((x - 0.5 * l * period) / period)
+        cx, cy = m * period + 0.5 * l * period, l * h
+        hit = (x - cx) ** 2 + (y - cy) ** 2 <= radius ** 2
+        mask |= hit & ~((m == 0) & (l == 0))
+    return mask
+
+
+def gyro_crystal_purcell(n=(1024, 1024, 1536), slab=40, layer=200, period=32, radius=10, eps_slab=12.0,
+                         eps_diag=4.0, g=0.3, pml=10, a_over_lambda=0.3, box_half=20, nfreq=32, steps=8000, order=2,
+                         courant=0.5, structure=True):
+    """Gyrotropic + Purcell workload (z is the slab normal).  The slab fills
+    z in [zs, zs + slab) with zs = nz/2 - slab/2, the gyrotropic layer the
+    `layer` cells below it; the lattice of air holes (period, radius) runs
+    through the slab with the centre hole left out; the soft Ez dipole sits
+    at the centre of that defect.  Source centre wavelength lambda0 =
+    period / a_over_lambda; the gyrotropic tensor is fitted at its angular
+    frequency; the flux box is the dipole +- box_half cells on every axis with
+    nfreq frequencies over the pulse's -20 dB band.  structure=False gives the
+    same grid, source and box in vacuum (the W0 run of a Purcell ratio)."""
+    nx, ny, nz = n
+    lambda0 = period / a_over_lambda
+    w0 = 2.0 * math.pi / lambda0
+    cfg = abi.make_config(nx, ny, nz, dx=1.0, courant=courant, order=order, pml=pml)
+    d = (nx // 2, ny // 2, nz // 2)
+    zs = nz // 2 - slab // 2
+    einf, gyro = abi.gyro_for(eps_diag, g, w0)
+    mats = [abi.make_material(1.0), abi.make_material(eps_slab), abi.make_material(eps_inf=einf, gyro=gyro)]
+    idx = None
+    if structure:
+        idx = []
+        for c in range(3):
+            a = np.zeros((nx, ny, nz), np.uint8)
+            zo = 0.5 if c < 2 else 0.0                       # Ex, Ey sit at k + 1/2, Ez at k
+            z = np.arange(nz) + zo
+            in_slab = (z >= zs) & (z < zs + slab)
+            in_layer = (z >= zs - layer) & (z < zs)
+            holes = triangular_holes(nx, ny, (d[0] + 0.5, d[1] + 0.5), period, radius, c)
+            k0, k1 = int(np.argmax(in_slab)), int(nz - np.argmax(in_slab[::-1]))
+            a[:, :, k0:k1] = np.where(holes, 0, 1).astype(np.uint8)[:, :, None]
+            if in_layer.any():
+                l0, l1 = int(np.argmax(in_layer)), int(nz - np.argmax(in_layer[::-1]))
+                a[:, :, l0:l1] = 2
+            idx.append(a)
+    f0, tau, t0 = gauss_sine_params(lambda0)
+    src = abi.PointSource(comp=abi.EZ, i=d[0], j=d[1], k=d[2], waveform=abi.WAVE_GAUSS_SINE, amp=1.0, f0=f0,
+                          tau=tau, t0=t0)
+    df = math.sqrt(math.log(10.0)) / (math.pi * tau)
+    omegas = 2.0 * math.pi * np.linspace(f0 - df, f0 + df, nfreq)
+    lo = [v - box_half for v in d]
+    hi = [v + box_half for v in d]
+    if structure:
+        desc = ("%dx%dx%d: slab %d cells eps=%g, triangular air holes period %d r=%d, %d-cell gyrotropic layer "
+                "(eps_diag=%g, g=%g, magnetised Drude), Ez dipole in a missing-hole defect, %d-cell CPML, "
+                "%d-freq FP64 flux box +-%d" % (nx, ny, nz, slab, eps_slab, period, radius, layer, eps_diag, g, pml,
+                                               nfreq, box_half))
+    else:
+        desc = ("%dx%dx%d vacuum, the same Ez dipole (lambda0=%g), %d-cell CPML, %d-freq FP64 flux box +-%d"
+                % (nx, ny, nz, lambda0, pml, nfreq, box_half))
+    return dict(name="gyro_crystal_purcell", cfg=cfg, materials=(mats if structure else None, idx),
+                point_sources=[src], tfsf=None, probes=[(abi.EZ, d[0], d[1], d[2], abi.PROBE_NODE)], dft=[],
+                flux=[(lo, hi, omegas)], steps=steps, eps_src=eps_slab if structure else 1.0, desc=desc)
+
+
+def apply_flux(sim, sc):
+    """Add the scenario's flux boxes to a Simulation; returns their ids."""
+    return [sim.add_flux_box(lo, hi, om) for (lo, hi, om) in sc.get("flux", [])]
 
 
 def apply(sim, sc):

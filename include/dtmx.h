@@ -201,6 +201,30 @@ int  dtmx_add_dft_plane(dtmx_ctx* ctx, int axis, int index, int comp_mask,
 /* out: [ncomp_selected][nfreq][plane points][2] doubles, plane points in
  * (slow, fast) order of the two remaining axes. */
 int  dtmx_read_dft(dtmx_ctx* ctx, int id, double* out, size_t out_len);
+/* Running DFT on the n1 x n2 window starting at (lo1, lo2) of the plane
+ * {axis = index}, the two in-plane axes in (slow, fast) order; read back with
+ * dtmx_read_dft like a plane (window points in place of plane points).
+ * dtmx_add_dft_plane is the full-plane window. */
+int  dtmx_add_dft_patch(dtmx_ctx* ctx, int axis, int index, int lo1, int n1, int lo2, int n2,
+                        int comp_mask, int nfreq, const double* omegas, int* id_out);
+
+/* Power flux box (no reference counterpart: the reference estimates the
+ * Purcell factor from the field at the dipole, purcell.gp:3, after an offline
+ * Fourier transform, calc_purcell.sh).  Six DFT windows of the tangential E
+ * and H components on the faces {axis a = lo[a]} and {axis a = hi[a]}, each
+ * covering [lo_b, hi_b) x [lo_c, hi_c) of the other two axes (nodes of those
+ * cell indices).  The outward flux of a face normal to axis a is
+ *   sign * d_b * d_c * sum Re(E_b conj(H_c) - E_c conj(H_b)),
+ * (a, b, c) cyclic, sign -1 on the lo face and +1 on the hi face, accumulated
+ * in FP64 on the device from the running DFTs (dtmx_add_dft_plane's
+ * convention).  Requires 0 <= lo[a] < hi[a] < n[a]. */
+int  dtmx_add_flux_box(dtmx_ctx* ctx, const int lo[3], const int hi[3], int nfreq,
+                       const double* omegas, int* id_out);
+/* out[7*nfreq]: the outward flux of the faces (x lo, x hi, y lo, y hi, z lo,
+ * z hi), nfreq values each, then their sum. */
+int  dtmx_read_flux(dtmx_ctx* ctx, int id, double* out, size_t out_len);
+/* DFT ids of the six face windows (same order), for dtmx_read_dft. */
+int  dtmx_flux_faces(dtmx_ctx* ctx, int id, int faces[6]);
 
 /* Advance nsteps leapfrog steps (H half step then E half step each,
  * genAlg.py:420-501).  Asynchronous on the context stream.  Replaces

@@ -152,3 +152,39 @@ class OracleSim:
 
 def threads():
     return lib().orc64_threads()
+
+
+FLUX_MASK = {0: (1 << abi.EY) | (1 << abi.EZ) | (1 << abi.HY) | (1 << abi.HZ),
+             1: (1 << abi.EX) | (1 << abi.EZ) | (1 << abi.HX) | (1 << abi.HZ),
+             2: (1 << abi.EX) | (1 << abi.EY) | (1 << abi.HX) | (1 << abi.HY)}
+
+
+def add_flux_planes(sim, lo, hi, omegas):
+    """Full-plane DFTs of the tangential components on the six faces of a flux
+    box (the oracle has no windows: flux_box_from_planes cuts them).  Returns
+    {(axis, side): dft id} with side 0 = lo face, 1 = hi face."""
+    ids = {}
+    for a in range(3):
+        for side, v in enumerate((lo[a], hi[a])):
+            ids[(a, side)] = sim.add_dft_plane(a, v, FLUX_MASK[a], omegas)
+    return ids
+
+
+def flux_box_from_planes(sim, ids, lo, hi, ds=(1.0, 1.0, 1.0)):
+    """Outward FP64 flux of each face (x lo, x hi, y lo, y hi, z lo, z hi) and
+    their sum, from full-plane oracle DFTs: face normal a, (a, b, c) cyclic,
+    sign * d_b d_c * sum over [lo_b, hi_b) x [lo_c, hi_c) of
+    Re(E_b conj(H_c) - E_c conj(H_b)).  Returns (faces[6, nfreq], total[nfreq])."""
+    faces = []
+    for a in range(3):
+        b, c = (a + 1) % 3, (a + 2) % 3
+        s1, s2 = (1, 2) if a == 0 else ((0, 2) if a == 1 else (0, 1))
+        comps = [q for q in range(6) if FLUX_MASK[a] & (1 << q)]
+        for side in (0, 1):
+            F = sim.read_dft(ids[(a, side)])[:, :, lo[s1]:hi[s1], lo[s2]:hi[s2]]
+            Eb, Ec = F[comps.index(b)], F[comps.index(c)]
+            Hb, Hc = F[comps.index(3 + b)], F[comps.index(3 + c)]
+            s = (Eb * np.conj(Hc) - Ec * np.conj(Hb)).real.sum(axis=(1, 2))
+            faces.append((1.0 if side else -1.0) * ds[s1] * ds[s2] * s)
+    faces = np.array(faces)
+    return faces, faces.sum(axis=0)
