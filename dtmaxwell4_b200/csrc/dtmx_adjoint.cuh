@@ -41,49 +41,48 @@ __device__ __forceinline__ void curl_pair(int c, int t, int& a, int& g) {
   g = curl_src(c, t);
 }
 
-// w of updated component cu, curl term t, at node (i,j,k); zero outside the grid
-template <int ORDER>
-__device__ __forceinline__ float adj_w(const Params& p, const AdjDev& A, int cu, int t, int i, int j, int k) {
-  if (i < 0 || i >= p.g.n[0] || j < 0 || j >= p.g.n[1] || k < 0 || k >= p.g.n[2]) return 0.f;
-  int a, g;
-  curl_pair(cu, t, a, g);
-  const bool isH = cu >= 3;
-  float sg = t == 0 ? 1.f : -1.f;
-  if (isH) sg = -sg;
-  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
-  float ie = 1.f;
-  if (!isH) {
-    const long long di = design_index(p, i, j, k);
-    const int m = p.mat[cu] ? (int)p.mat[cu][id] : 0;
-    ie = di >= 0 ? p.des_ie[cu][di] : p.mt->inv_eps[m][cu];
-  }
-  float ld = A.lam[cu][id];
-  const int idx[3] = {i, j, k};
-  if (p.ab.kind == 1 && in_slab(p, a, idx[a])) {
-    const int h = 2 * idx[a] + comp_off(cu, a);
-    const float al = __ldg(p.ab.c1[a] + h), gk = __fadd_rn(__ldg(p.ab.c2[a] + h), al);
-    ld = __fmaf_rn(gk, ld, __fmul_rn(al, A.lpsi[a][slot_of(cu, a)][slab_index(p, a, i, j, k)]));
-  }
-  return __fmul_rn(__fmul_rn(sg * p.cdt[a], ie), ld);
-}
-
-// w of the updated field at every node (3 components x 2 curl terms), then
-// the slab recursion lam_psi <- b (lam + lam_psi) (w uses the old lam_psi).
+// w of the updated field at every node (3 components x 2 curl terms):
+//   w_{c,t} = sg_t cdt_a ie_c (g_a lam_c + al_a lam_psi)   (a = curl axis of term t;
+//   g_a lam + al lam_psi only inside the axis-a slab, lam elsewhere),
+// then the slab recursion lam_psi <- b (lam + lam_psi) (w uses the old lam_psi).
+// The node's 1/eps, design index and lam are loaded once per component.
 // One thread per node: blockIdx.z = x plane, (threadIdx.x, blockIdx.x) = z,
 // (threadIdx.y, blockIdx.y) = y.
 template <int ORDER, int UPDH>
 __global__ void adj_w_kernel(Params p, AdjDev A) {
-  constexpr int updH = UPDH;
+  constexpr bool updH = UPDH != 0;
   const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, i = blockIdx.z;
   if (j >= p.g.n[1] || k >= p.g.n[2]) return;
   const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
   constexpr int cu0 = updH ? 3 : 0;
-#pragma unroll
-  for (int c = 0; c < 3; c++)
-#pragma unroll
-    for (int t = 0; t < 2; t++) A.w[c][t][id] = adj_w<ORDER>(p, A, cu0 + c, t, i, j, k);
-  if (p.ab.kind != 1) return;
   const int idx[3] = {i, j, k};
+  const bool cpml = p.ab.kind == 1;
+  const long long di = updH ? -1 : design_index(p, i, j, k);
+  float lam[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int cu = cu0 + c;
+    float ie = 1.f;
+    if (!updH) {
+      const int m = p.mat[cu] ? (int)p.mat[cu][id] : 0;
+      ie = di >= 0 ? p.des_ie[cu][di] : p.mt->inv_eps[m][cu];
+    }
+    lam[c] = A.lam[cu][id];
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int a = curl_axis(cu, t);
+      float sg = t == 0 ? 1.f : -1.f;
+      if (updH) sg = -sg;
+      float ld = lam[c];
+      if (cpml && in_slab(p, a, idx[a])) {
+        const int h = 2 * idx[a] + comp_off(cu, a);
+        const float al = __ldg(p.ab.c1[a] + h), gk = __fadd_rn(__ldg(p.ab.c2[a] + h), al);
+        ld = __fmaf_rn(gk, ld, __fmul_rn(al, A.lpsi[a][slot_of(cu, a)][slab_index(p, a, i, j, k)]));
+      }
+      A.w[c][t][id] = __fmul_rn(__fmul_rn(sg * p.cdt[a], ie), ld);
+    }
+  }
+  if (!cpml) return;
 #pragma unroll
   for (int a = 0; a < 3; a++) {
     if (!in_slab(p, a, idx[a])) continue;
@@ -93,7 +92,7 @@ __global__ void adj_w_kernel(Params p, AdjDev A) {
       const int cu = cu0 + c, sl = slot_of(cu, a);
       if (sl < 0) continue;
       const float b = __ldg(p.ab.c0[a] + 2 * idx[a] + comp_off(cu, a));
-      A.lpsi[a][sl][si] = __fmul_rn(b, __fadd_rn(A.lam[cu][id], A.lpsi[a][sl][si]));
+      A.lpsi[a][sl][si] = __fmul_rn(b, __fadd_rn(lam[c], A.lpsi[a][sl][si]));
     }
   }
 }

@@ -99,6 +99,7 @@ struct dtmx_ctx {
   std::vector<float> h_des_ie[3];
   bool monitors_off = false;  // probes and DFT planes paused (recomputed segments)
   bool obj_on = false;        // capture the objective's flux DFT each step
+  long long adj_budget = -1;  // bytes of design-region history the adjoint may keep (-1: a quarter of free memory)
   DftHost obj{};
   int gcur = 0;              // gyrotropic current buffer holding J^{n-1/2}
   // wavefront engine
@@ -1272,6 +1273,7 @@ struct FaRun {
   float* hist = nullptr;
   double* dF = nullptr;
   int seg = -1, len = 0;
+  bool full = false;          // the forward pass records the whole design history: no checkpoints, no recompute
   void release() {
     for (char* q : ck) cudaFree(q);
     for (void* q : tmp) cudaFree(q);
@@ -1280,7 +1282,23 @@ struct FaRun {
   }
 };
 
-static int fa_begin(dtmx_ctx* ctx, FaRun& R, int nsteps, int checkpoint_every, int plane_x, double omega) {
+// Does the design-region E history of a whole run fit the context's budget?
+// Then the forward pass records it and the adjoint needs no recomputation.
+static double fa_history_bytes(const dtmx_ctx* ctx, int nsteps) {
+  const Params& P = ctx->P;
+  return (double)(nsteps + 1) * 3.0 * P.des_n[0] * P.des_n[1] * P.des_n[2] * 4.0;
+}
+static double free_device_bytes() {
+  size_t fr = 0, tot = 0;
+  return cudaMemGetInfo(&fr, &tot) == cudaSuccess ? (double)fr : 0.0;
+}
+static bool fa_history_fits(dtmx_ctx* ctx, int nsteps) {
+  const double bytes = fa_history_bytes(ctx, nsteps);
+  if (ctx->adj_budget >= 0) return bytes <= (double)ctx->adj_budget;
+  return bytes <= 0.25 * free_device_bytes();
+}
+
+static int fa_begin(dtmx_ctx* ctx, FaRun& R, int nsteps, int checkpoint_every, int plane_x, double omega, bool full) {
   const dtmx_config& c = ctx->cfg;
   Params& P = ctx->P;
   if (nsteps < 1 || checkpoint_every < 1) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
@@ -1296,7 +1314,8 @@ static int fa_begin(dtmx_ctx* ctx, FaRun& R, int nsteps, int checkpoint_every, i
   }
   int rc = prepare(ctx);
   if (rc) return rc;
-  R.N = nsteps; R.K = std::min(checkpoint_every, nsteps);
+  R.full = full;
+  R.N = nsteps; R.K = full ? nsteps : std::min(checkpoint_every, nsteps);
   R.nseg = (R.N + R.K - 1) / R.K;
   R.nd = P.des_n[0] * P.des_n[1] * P.des_n[2];
   R.npl = c.ny * c.nz;
@@ -1316,22 +1335,44 @@ static int fa_begin(dtmx_ctx* ctx, FaRun& R, int nsteps, int checkpoint_every, i
   CK(cudaMemcpyAsync(O.omega, &omega, 8, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(O.acc, 0, (size_t)4 * R.npl * sizeof(double2), ctx->stream));
   O.nstaged = 0;
-  // checkpoints of the state every K steps plus the final state
-  const size_t sb = state_bytes(ctx);
-  R.ck.assign(R.nseg + 1, nullptr);
-  for (auto& q : R.ck)
-    if (cudaMalloc(&q, sb) != cudaSuccess) { R.release(); return fail(ctx, DTMX_ERR_OOM, "checkpoint allocation"); }
+  if (full) {
+    // design-region history of every step: slot s holds E after s steps of the run
+    void* h = nullptr;
+    if (cudaMalloc(&h, (size_t)(R.N + 1) * 3 * R.nd * 4) != cudaSuccess)
+      return fail(ctx, DTMX_ERR_OOM, "design history allocation");
+    R.tmp.push_back(h);
+    R.hist = (float*)h;
+  } else {
+    // checkpoints of the state every K steps plus the final state
+    const size_t sb = state_bytes(ctx);
+    R.ck.assign(R.nseg + 1, nullptr);
+    for (auto& q : R.ck)
+      if (cudaMalloc(&q, sb) != cudaSuccess) { R.release(); return fail(ctx, DTMX_ERR_OOM, "checkpoint allocation"); }
+  }
   R.s0 = ctx->step;
   ctx->obj_on = true;
   return DTMX_OK;
 }
 
+static unsigned design_blocks(const FaRun& R) { return (unsigned)((3 * R.nd + 255) / 256); }
+
 // forward step st (0-based) of the run
 static int fa_forward(dtmx_ctx* ctx, FaRun& R, int st) {
-  if (st % R.K == 0) state_copy(ctx, R.ck[st / R.K], true);
+  if (R.full) {
+    if (st == 0) {
+      design_capture_kernel<<<design_blocks(R), 256, 0, ctx->stream>>>(ctx->P, R.hist, 0, R.nd);
+      ctx->launches++;
+    }
+  } else if (st % R.K == 0) {
+    state_copy(ctx, R.ck[st / R.K], true);
+  }
   int rc = launch_step(ctx);
   if (rc) return rc;
   ctx->step++;
+  if (R.full) {
+    design_capture_kernel<<<design_blocks(R), 256, 0, ctx->stream>>>(ctx->P, R.hist, st + 1, R.nd);
+    ctx->launches++;
+  }
   return DTMX_OK;
 }
 
@@ -1339,7 +1380,7 @@ static int fa_forward(dtmx_ctx* ctx, FaRun& R, int st) {
 static int fa_forward_done(dtmx_ctx* ctx, FaRun& R) {
   Params& P = ctx->P;
   ctx->obj_on = false;
-  state_copy(ctx, R.ck[R.nseg], true);
+  if (!R.full) state_copy(ctx, R.ck[R.nseg], true);
   DftHost& O = ctx->obj;
   dft_flush(ctx, O);
   std::vector<double> F((size_t)8 * R.npl);
@@ -1369,8 +1410,8 @@ static int fa_forward_done(dtmx_ctx* ctx, FaRun& R) {
   }
   for (int c3 = 0; c3 < 3; c3++)
     for (int t = 0; t < 2; t++) ok = ok && talloc((void**)&A.w[c3][t], (ctx->nstore + 64) * 4);
-  ok = ok && talloc((void**)&A.grad, (size_t)3 * R.nd * 8) && talloc((void**)&R.hist, (size_t)(R.K + 1) * 3 * R.nd * 4) &&
-       talloc((void**)&R.dF, F.size() * 8);
+  ok = ok && talloc((void**)&A.grad, (size_t)3 * R.nd * 8) && talloc((void**)&R.dF, F.size() * 8);
+  if (!R.full) ok = ok && talloc((void**)&R.hist, (size_t)(R.K + 1) * 3 * R.nd * 4);
   if (!ok) { R.release(); return fail(ctx, DTMX_ERR_OOM, "adjoint allocation"); }
   A.hist = R.hist;
   CK(cudaMemcpyAsync(R.dF, F.data(), F.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
@@ -1379,13 +1420,13 @@ static int fa_forward_done(dtmx_ctx* ctx, FaRun& R) {
   return DTMX_OK;
 }
 
-static unsigned design_blocks(const FaRun& R) { return (unsigned)((3 * R.nd + 255) / 256); }
-
 // restore checkpoint seg and record the design region of its first state
+// (with the whole history recorded: the one segment is the run, nothing to restore)
 static int fa_segment_begin(dtmx_ctx* ctx, FaRun& R, int seg) {
   R.seg = seg;
   const int start = seg * R.K;
   R.len = std::min(R.N, start + R.K) - start;
+  if (R.full) return DTMX_OK;
   state_copy(ctx, R.ck[seg], false);
   ctx->step = R.s0 + start;
   design_capture_kernel<<<design_blocks(R), 256, 0, ctx->stream>>>(ctx->P, R.hist, 0, R.nd);
@@ -1394,6 +1435,7 @@ static int fa_segment_begin(dtmx_ctx* ctx, FaRun& R, int seg) {
 
 // recompute step q (1..len) of the current segment
 static int fa_recompute(dtmx_ctx* ctx, FaRun& R, int q) {
+  if (R.full) return DTMX_OK;
   int rc = launch_step(ctx);
   if (rc) return rc;
   ctx->step++;
@@ -1428,7 +1470,7 @@ static int fa_adjoint(dtmx_ctx* ctx, FaRun& R, int q) {
 // final state back in place, gradient to the caller (waits for the stream)
 static int fa_finish(dtmx_ctx* ctx, FaRun& R, double* objective, float* grad_eps) {
   ctx->monitors_off = false;
-  state_copy(ctx, R.ck[R.nseg], false);
+  if (!R.full) state_copy(ctx, R.ck[R.nseg], false);
   ctx->step = R.s0 + R.N;
   std::vector<double> g((size_t)3 * R.nd);
   CK(cudaMemcpyAsync(g.data(), R.A.grad, g.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1455,7 +1497,8 @@ extern "C" int dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_ev
                                     double* objective, float* grad_eps) {
   if (!ctx || !objective || !grad_eps) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
   FaRun R;
-  int rc = fa_begin(ctx, R, nsteps, checkpoint_every, plane_x, omega);
+  if (nsteps < 1 || checkpoint_every < 1) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
+  int rc = fa_begin(ctx, R, nsteps, checkpoint_every, plane_x, omega, fa_history_fits(ctx, nsteps));
   if (rc) return rc;
   for (int st = 0; st < R.N && !rc; st++) rc = fa_forward(ctx, R, st);
   if (!rc) rc = fa_forward_done(ctx, R);
@@ -1466,6 +1509,12 @@ extern "C" int dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_ev
   }
   if (rc) { fa_abort(ctx, R); return rc; }
   return fa_finish(ctx, R, objective, grad_eps);
+}
+
+extern "C" int dtmx_set_adjoint_memory(dtmx_ctx* ctx, int64_t bytes) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  ctx->adj_budget = bytes < 0 ? -1 : (long long)bytes;
+  return DTMX_OK;
 }
 
 // Batch of independent forward + adjoint runs: every phase is issued for all
@@ -1481,8 +1530,19 @@ extern "C" int dtmx_batch_forward_adjoint(dtmx_ctx* const* ctxs, int n, int nste
   auto abort_all = [&](int upto) {
     for (int b = 0; b < upto; b++) fa_abort(ctxs[b], R[b]);
   };
+  // one mode for the whole batch (the segments advance in lock step)
+  bool full = nsteps >= 1;
+  double total = 0.0;
+  bool automatic = true;
+  for (int b = 0; b < n; b++) {
+    full = full && ctxs[b] && fa_history_fits(ctxs[b], nsteps);
+    if (!full) break;
+    total += fa_history_bytes(ctxs[b], nsteps);
+    automatic = automatic && ctxs[b]->adj_budget < 0;
+  }
+  if (full && automatic) full = total <= 0.25 * free_device_bytes();
   for (int b = 0; b < n; b++)
-    if ((rc = fa_begin(ctxs[b], R[b], nsteps, checkpoint_every, plane_x[b], omega[b]))) { abort_all(b); return rc; }
+    if ((rc = fa_begin(ctxs[b], R[b], nsteps, checkpoint_every, plane_x[b], omega[b], full))) { abort_all(b); return rc; }
   for (int st = 0; st < nsteps && !rc; st++)
     for (int b = 0; b < n && !rc; b++) rc = fa_forward(ctxs[b], R[b], st);
   for (int b = 0; b < n && !rc; b++) rc = fa_forward_done(ctxs[b], R[b]);

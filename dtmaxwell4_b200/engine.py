@@ -26,6 +26,7 @@ EXPORTS = (
     "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
     "dtmx_write_arr", "dtmx_save_state", "dtmx_load_state",
     "dtmx_add_dft_patch", "dtmx_add_flux_box", "dtmx_read_flux", "dtmx_flux_faces",
+    "dtmx_set_adjoint_memory",
 )
 
 
@@ -63,6 +64,7 @@ def load():
     L.dtmx_add_flux_box.argtypes = [vp, C.POINTER(ip), C.POINTER(ip), ip, vp, C.POINTER(ip)]
     L.dtmx_read_flux.argtypes = [vp, ip, vp, C.c_size_t]
     L.dtmx_flux_faces.argtypes = [vp, ip, C.POINTER(ip)]
+    L.dtmx_set_adjoint_memory.argtypes = [vp, C.c_int64]
     L.dtmx_step.argtypes = [vp, ip]
     L.dtmx_sync.argtypes = [vp]
     L.dtmx_get_step.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -224,6 +226,11 @@ class Simulation:
         self._ck(self._L.dtmx_forward_adjoint(self._h, int(nsteps), int(checkpoint_every), int(plane_x), float(omega),
                                               C.byref(J), grad.ctypes.data))
         return J.value, grad
+
+    def set_adjoint_memory(self, nbytes):
+        """Budget for the recorded design-region history of forward_adjoint
+        (0: always checkpoint and recompute; negative: a quarter of free memory)."""
+        self._ck(self._L.dtmx_set_adjoint_memory(self._h, int(nbytes)))
 
     def write_arr(self, comp, path):
         """Field snapshot in the reference's .arr layout (see read_arr)."""

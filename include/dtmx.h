@@ -313,14 +313,23 @@ int  dtmx_set_design(dtmx_ctx* ctx, const int lo[3], const int n[3], const float
  * the Poynting flux of the running DFTs at omega (E^ = sum_s E^s e^{-i w s dt} dt,
  * H^ with t = (s - 1/2) dt), and dJ/d eps at every design node (3*nd floats,
  * the layout of dtmx_set_design).  The gradient is the discrete adjoint of the
- * update (transposed stencils and CPML recursions), run backward over
- * segments of checkpoint_every steps that are recomputed from state
- * checkpoints kept in device memory; the accumulation is in double precision.
+ * update (transposed stencils and CPML recursions), run backward over the
+ * steps; the accumulation is in double precision.  The adjoint needs, of the
+ * forward run, only E in the design region at every step: when that history
+ * ((nsteps+1) * 3 * nd floats) fits the budget of dtmx_set_adjoint_memory the
+ * forward pass records it and nothing is recomputed; otherwise the state is
+ * checkpointed every checkpoint_every steps in device memory and each segment
+ * is recomputed before its adjoint.  Both modes give bit-identical results.
  * Box geometry, CPML or no absorber, non-dispersive materials, no point source
  * inside the design region.  On return the context holds the state after
  * nsteps, as after dtmx_step(nsteps). */
 int  dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_every, int plane_x, double omega,
                           double* objective, float* grad_eps);
+
+/* Device memory the adjoint may use for the recorded design-region history:
+ * bytes >= 0 sets the budget (0 always checkpoints and recomputes), a negative
+ * value restores the default, a quarter of the free device memory. */
+int  dtmx_set_adjoint_memory(dtmx_ctx* ctx, int64_t bytes);
 
 /* A batch of independent dtmx_forward_adjoint runs (contexts of any sizes,
  * same nsteps and checkpoint_every): every phase is issued step by step for

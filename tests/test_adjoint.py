@@ -2,9 +2,10 @@
 permittivity by the discrete adjoint.
 
 Oracle (CPU): the FP64 adjoint equals central finite differences of the FP64
-forward.  GPU: the FP32 engine's adjoint (checkpointed recompute) against the
-FP64 adjoint and against its own central differences, checkpoint-interval
-invariance, the final state, and the torch.autograd binding.
+forward.  GPU: the FP32 engine's adjoint against the FP64 adjoint and against
+its own central differences, identical results from the recorded design
+history and from checkpointed recompute at two intervals, the final state, and
+the torch.autograd binding.
 """
 import math
 
@@ -54,10 +55,11 @@ def test_oracle_adjoint_matches_finite_differences(order):
         assert abs(g[cell] - fd) <= 1e-6 * abs(fd), (cell, g[cell], fd)
 
 
-def _gpu(order, eps, K=100):
+def _gpu(order, eps, K=100, budget=-1):
     from dtmaxwell4_b200 import Simulation
     s = _setup(Simulation(_cfg(order)), order)
     s.set_design(LO, eps)
+    s.set_adjoint_memory(budget)
     J, g = s.forward_adjoint(N_STEPS, PLANE_X, OMEGA, K)
     return J, g, s
 
@@ -102,17 +104,22 @@ def test_gpu_adjoint_against_central_differences():
 
 @pytest.mark.gpu
 def test_gpu_adjoint_checkpoint_interval_and_final_state():
+    """Recorded design history (default budget) and checkpointed recompute
+    (budget 0, two intervals) give bit-identical objectives and gradients and
+    leave the state of a plain forward run."""
     from dtmaxwell4_b200 import Simulation
     eps = _eps()
-    J1, g1, s1 = _gpu(4, eps, K=100)
-    J2, g2, s2 = _gpu(4, eps, K=7)
-    assert J1 == J2 and np.array_equal(g1, g2)
+    J0, g0, s0 = _gpu(4, eps)
+    J1, g1, s1 = _gpu(4, eps, K=100, budget=0)
+    J2, g2, s2 = _gpu(4, eps, K=7, budget=0)
+    assert J0 == J1 == J2 and np.array_equal(g0, g1) and np.array_equal(g1, g2)
     ref = _setup(Simulation(_cfg(4)), 4)
     ref.set_design(LO, eps)
     ref.step(N_STEPS)
     for c in range(6):
         assert np.array_equal(s2.get_field(c), ref.get_field(c)), c
-    for q in (s1, s2, ref):
+        assert np.array_equal(s0.get_field(c), ref.get_field(c)), c
+    for q in (s0, s1, s2, ref):
         q.close()
 
 
