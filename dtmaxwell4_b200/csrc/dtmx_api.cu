@@ -489,7 +489,9 @@ static int upload_umat(dtmx_ctx* ctx) {
             for (int k = tz * TZ; k < std::min(c.nz, tz * TZ + TZ); k++) {
               const int m = row[k];
               if (m0 == -2) m0 = m;
-              if (m != m0 || ctx->mats[m].npoles > 0 || ctx->mats[m].gyro_wp > 0) { m0 = -1; break; }
+              // (a gyrotropic node takes the plain update with 1/eps_inf; its current is
+              // subtracted by the post-pass, so a uniform gyrotropic tile stays uniform)
+              if (m != m0 || ctx->mats[m].npoles > 0) { m0 = -1; break; }
             }
           }
         um[((size_t)i * nty + ty) * ntz + tz] = (signed char)(m0 < 0 || design_touches(ctx, i, ty, tz) ? -1 : m0);
@@ -1268,17 +1270,36 @@ struct FaRun {
   double omega = 0, J = 0;
   long long s0 = 0;
   std::vector<char*> ck;
-  std::vector<void*> tmp;
   AdjDev A{};
   float* hist = nullptr;
   double* dF = nullptr;
   int seg = -1, len = 0;
   bool full = false;          // the forward pass records the whole design history: no checkpoints, no recompute
+  cudaStream_t st = nullptr;
+  std::vector<void*> bufs;
+  // Device buffers of the run come from the device's stream-ordered pool:
+  // released blocks stay in the pool (release threshold raised once per
+  // process), so later runs -- on this context or a fresh one -- reuse them
+  // without a device-wide synchronisation.
+  void* take(dtmx_ctx* ctx, size_t bytes) {
+    static const bool pool_kept = [] {
+      int dev = 0;
+      cudaMemPool_t pool;
+      if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return false;
+      uint64_t keep = ~0ull;
+      return cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess;
+    }();
+    (void)pool_kept;
+    st = ctx->stream;
+    void* q = nullptr;
+    if (cudaMallocAsync(&q, bytes, ctx->stream) != cudaSuccess) return nullptr;
+    bufs.push_back(q);
+    return q;
+  }
   void release() {
-    for (char* q : ck) cudaFree(q);
-    for (void* q : tmp) cudaFree(q);
+    for (void* q : bufs) cudaFreeAsync(q, st);
+    bufs.clear();
     ck.clear();
-    tmp.clear();
   }
 };
 
@@ -1337,17 +1358,15 @@ static int fa_begin(dtmx_ctx* ctx, FaRun& R, int nsteps, int checkpoint_every, i
   O.nstaged = 0;
   if (full) {
     // design-region history of every step: slot s holds E after s steps of the run
-    void* h = nullptr;
-    if (cudaMalloc(&h, (size_t)(R.N + 1) * 3 * R.nd * 4) != cudaSuccess)
-      return fail(ctx, DTMX_ERR_OOM, "design history allocation");
-    R.tmp.push_back(h);
+    void* h = R.take(ctx, (size_t)(R.N + 1) * 3 * R.nd * 4);
+    if (!h) return fail(ctx, DTMX_ERR_OOM, "design history allocation");
     R.hist = (float*)h;
   } else {
     // checkpoints of the state every K steps plus the final state
     const size_t sb = state_bytes(ctx);
     R.ck.assign(R.nseg + 1, nullptr);
     for (auto& q : R.ck)
-      if (cudaMalloc(&q, sb) != cudaSuccess) { R.release(); return fail(ctx, DTMX_ERR_OOM, "checkpoint allocation"); }
+      if (!(q = (char*)R.take(ctx, sb))) { R.release(); return fail(ctx, DTMX_ERR_OOM, "checkpoint allocation"); }
   }
   R.s0 = ctx->step;
   ctx->obj_on = true;
@@ -1397,8 +1416,7 @@ static int fa_forward_done(dtmx_ctx* ctx, FaRun& R) {
   A = AdjDev{};
   A.nd = R.nd;
   auto talloc = [&](void** q, size_t bytes) {
-    if (cudaMalloc(q, bytes) != cudaSuccess) return false;
-    R.tmp.push_back(*q);
+    if (!(*q = R.take(ctx, bytes))) return false;
     return cudaMemsetAsync(*q, 0, bytes, ctx->stream) == cudaSuccess;
   };
   bool ok = true;

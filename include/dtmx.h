@@ -322,7 +322,9 @@ int  dtmx_set_design(dtmx_ctx* ctx, const int lo[3], const int n[3], const float
  * is recomputed before its adjoint.  Both modes give bit-identical results.
  * Box geometry, CPML or no absorber, non-dispersive materials, no point source
  * inside the design region.  On return the context holds the state after
- * nsteps, as after dtmx_step(nsteps). */
+ * nsteps, as after dtmx_step(nsteps).  The run's device buffers (adjoint
+ * fields, history or checkpoints) come from the device's stream-ordered memory
+ * pool and return to it afterwards; the pool keeps them for later runs. */
 int  dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_every, int plane_x, double omega,
                           double* objective, float* grad_eps);
 
