@@ -136,3 +136,35 @@ def test_torch_autograd_binding():
     s.close()
     assert float(J.detach()) == pytest.approx(Jd, rel=1e-6)
     np.testing.assert_allclose(eps.grad.numpy(), 2.0 * gd, rtol=1e-6, atol=0)
+
+
+@pytest.mark.gpu
+def test_full_size_gradient_directional_difference():
+    """The differentiation configuration at full size (256x256x192, 64x64x32
+    design region, 2000 steps): the directional central difference of J along
+    d = sign(dJ/deps) with h = 1e-3 on every design node equals sum |dJ/deps|.
+    (Per-node differences at this size change J by less than its FP32 rounding;
+    they are checked at the small size above.)"""
+    from dtmaxwell4_b200 import Simulation, scenarios
+    sc = scenarios.design_region()
+    lo, eps = sc["design"]
+
+    def run(e):
+        s = Simulation(sc["cfg"])
+        scenarios.apply(s, sc)
+        s.set_design(lo, e)
+        J, g = s.forward_adjoint(sc["steps"], sc["plane_x"], sc["omega"], 100)
+        s.close()
+        return J, g
+    J, g = run(eps)
+    d = np.sign(g).astype(np.float32)
+    h = 1e-3
+    Jp, _ = run((eps + h * d).astype(np.float32))
+    Jm, _ = run((eps - h * d).astype(np.float32))
+    # the perturbation actually applied, in FP32
+    hp = ((eps + h * d).astype(np.float64) - eps) * d
+    hm = (eps.astype(np.float64) - (eps - h * d).astype(np.float32)) * d
+    fd = (Jp - Jm) / (2 * h)
+    ad = float((np.abs(g).astype(np.float64) * (hp + hm) / (2 * h)).sum())
+    print("J %.9g  directional FD %.9g  adjoint %.9g  rel %.2e" % (J, fd, ad, abs(fd - ad) / abs(ad)))
+    assert abs(fd - ad) <= 1e-2 * abs(ad)

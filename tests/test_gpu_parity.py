@@ -72,6 +72,22 @@ def test_point_dipole_sphere(order, courant):
     assert g.check_finite()
 
 
+def test_point_dipole_sphere_full_size():
+    """The 128^3 point-dipole configuration at full size and length: 1000
+    steps, 10-cell CPML, sphere r = 20 eps = 4, Ez and Hx traces at 8 seeded
+    probes against the FP64 oracle (<= 1e-5; the FP32 oracle itself stays
+    within 2e-6 of FP64 on this run)."""
+    from dtmaxwell4_b200 import scenarios
+    sc = scenarios.point_dipole_sphere()
+    assert (sc["cfg"].nx, sc["steps"], len(sc["probes"])) == (128, 1000, 16)
+    g, o, _, _ = _pair(sc)
+    g.step(sc["steps"])
+    o.step(sc["steps"])
+    assert g.read_probes().shape == (16, 1000)
+    _compare_probes(g, o)
+    assert g.check_finite()
+
+
 def test_drude_sphere_plane_tfsf_dft():
     from dtmaxwell4_b200 import scenarios
     sc = scenarios.drude_sphere_tfsf(n=48, steps=260, pml=8, inset=6, radius=7, lambda0=10.0, nfreq=4)
