@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--gyro-steps", type=int, default=100, help="timed steps of the 1024x1024x1536 gyrotropic run")
     ap.add_argument("--gyro-n", type=int, nargs=3, default=[1024, 1024, 1536])
     ap.add_argument("--no-gyro", action="store_true", help="skip the gyrotropic / Purcell measurement")
+    ap.add_argument("--gyro-only", action="store_true", help="with --extras-only: only the gyrotropic measurement")
+    ap.add_argument("--no-purcell", action="store_true", help="gyrotropic measurement without the Purcell spectrum")
     return ap.parse_args()
 
 
@@ -396,6 +398,8 @@ def run_gyro_purcell(args):
                 "bytes_per_cell_update": round(b_cell, 2),
                 "hbm_frac": round(rate * 1e9 * b_cell / (hbm * 1e9), 4), "hbm_peak_gbs": hbm, "peak_kind": kind})
     del sc
+    if args.no_purcell:
+        return out
     # Purcell spectrum on a cut of the structure, full step count
     cut = scenarios.gyro_crystal_purcell(n=(256, 256, 512), steps=8000)
     vac = scenarios.gyro_crystal_purcell(n=(128, 128, 128), steps=8000, structure=False)
@@ -465,7 +469,7 @@ def main():
     import torch
     if args.extras_only:
         if rank == 0:
-            ex = {"adjoint": run_adjoint(args), "batched": run_batched(args)}
+            ex = {} if args.gyro_only else {"adjoint": run_adjoint(args), "batched": run_batched(args)}
             if not args.no_gyro:
                 ex["gyro_purcell"] = run_gyro_purcell(args)
             print(json.dumps(ex))

@@ -898,9 +898,9 @@ static int launch_step(dtmx_ctx* ctx) {
     else line_h_kernel<2><<<8, 256, 0, st>>>(ctx->line_e, ctx->line_h, ctx->T.line_n, r1);
     nl++;
   }
+  const dim3 ablk(32, 8), agrd((P.ade.n[2] + 31) / 32, (P.ade.n[1] + 7) / 8, std::max(1, P.ade.n[0]));
   if (ctx->has_gyro) {
-    const long long na = (long long)P.ade.n[0] * P.ade.n[1] * P.ade.n[2];
-    gyro_current_kernel<<<(unsigned)std::min<long long>((na + 255) / 256, 148LL * 16), 256, 0, st>>>(P, ctx->gcur);
+    gyro_current_kernel<<<agrd, ablk, 0, st>>>(P, ctx->gcur);
     P.ade.gnew = 1 - ctx->gcur;
     ctx->gcur = 1 - ctx->gcur;
     nl++;
@@ -910,11 +910,9 @@ static int launch_step(dtmx_ctx* ctx) {
   else e_kernel<2><<<grd, blk, Pipe<2, false>::SMEM_BYTES, st>>>(P, ctx->maps);
   if (P.ade.Em[0] || ctx->has_gyro) {
     // dispersive and gyrotropic nodes of the E half step (e_kernel skipped them)
-    const long long na = (long long)P.ade.n[0] * P.ade.n[1] * P.ade.n[2];
-    const unsigned ag = (unsigned)std::min<long long>((na + 255) / 256, 148LL * 16);
     const bool box = c.geometry == DTMX_GEOM_BOX;
-    if (o4) { if (box) ade_node_kernel<4, true><<<ag, 256, 0, st>>>(P); else ade_node_kernel<4, false><<<ag, 256, 0, st>>>(P); }
-    else { if (box) ade_node_kernel<2, true><<<ag, 256, 0, st>>>(P); else ade_node_kernel<2, false><<<ag, 256, 0, st>>>(P); }
+    if (o4) { if (box) ade_node_kernel<4, true><<<agrd, ablk, 0, st>>>(P); else ade_node_kernel<4, false><<<agrd, ablk, 0, st>>>(P); }
+    else { if (box) ade_node_kernel<2, true><<<agrd, ablk, 0, st>>>(P); else ade_node_kernel<2, false><<<agrd, ablk, 0, st>>>(P); }
     nl++;
   }
   if (ctx->profiling) {

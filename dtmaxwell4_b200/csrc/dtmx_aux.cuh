@@ -372,13 +372,22 @@ __device__ __forceinline__ float gyro_old(const Params& p, int cur, int c, int i
   return p.ade.Jg[cur][c][((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk];
 }
 
+// Thread layout of the passes over the ADE box: (threadIdx.x, blockIdx.x) = z,
+// (threadIdx.y, blockIdx.y) = y, blockIdx.z = x (no index division).
+__device__ __forceinline__ bool ade_cell(const Params& p, int& bi, int& bj, int& bk, long long& q) {
+  bk = blockIdx.x * blockDim.x + threadIdx.x;
+  bj = blockIdx.y * blockDim.y + threadIdx.y;
+  bi = blockIdx.z;
+  if (bj >= p.ade.n[1] || bk >= p.ade.n[2]) return false;
+  q = ((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk;
+  return true;
+}
+
 __global__ void gyro_current_kernel(Params p, int cur) {
-  const long long na = (long long)p.ade.n[0] * p.ade.n[1] * p.ade.n[2];
   const MatTable& mt = *p.mt;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < na; q += (long long)gridDim.x * blockDim.x) {
-    const int bk = (int)(q % p.ade.n[2]);
-    const long long r = q / p.ade.n[2];
-    const int bj = (int)(r % p.ade.n[1]), bi = (int)(r / p.ade.n[1]);
+  int bi, bj, bk;
+  long long q;
+  if (ade_cell(p, bi, bj, bk, q)) {
     const int i = p.ade.lo[0] + bi, j = p.ade.lo[1] + bj, k = p.ade.lo[2] + bk;
     const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
 #pragma unroll
@@ -412,12 +421,10 @@ __global__ void gyro_current_kernel(Params p, int cur) {
 // the ADE box; BOX: zero-outside geometry (bounds-checked taps).
 template <int ORDER, bool BOX>
 __global__ void ade_node_kernel(Params p) {
-  const long long na = (long long)p.ade.n[0] * p.ade.n[1] * p.ade.n[2];
   const MatTable& mt = *p.mt;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < na; q += (long long)gridDim.x * blockDim.x) {
-    const int bk = (int)(q % p.ade.n[2]);
-    const long long rr = q / p.ade.n[2];
-    const int bj = (int)(rr % p.ade.n[1]), bi = (int)(rr / p.ade.n[1]);
+  int bi, bj, bk;
+  long long q;
+  if (ade_cell(p, bi, bj, bk, q)) {
     const int i = p.ade.lo[0] + bi, j = p.ade.lo[1] + bj, k = p.ade.lo[2] + bk;
     const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
     const int idx[3] = {i, j, k};
