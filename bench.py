@@ -380,6 +380,7 @@ def run_gyro_purcell(args):
     s = Simulation(sc["cfg"])
     scenarios.apply(s, sc)
     scenarios.apply_flux(s, sc)
+    tuned = s.autotune(4)
     s.step(3)
     s.sync()
     t0 = time.perf_counter()
@@ -394,6 +395,7 @@ def run_gyro_purcell(args):
     rate = ncell * args.gyro_steps / dt / 1e9
     hbm, kind = measured_peaks()
     out.update({"workload": sc["desc"] + ", %d timed steps (of 8000) after 3 warm-up steps" % args.gyro_steps,
+                "engine": "engine %d, x chunk %d, chosen by dtmx_autotune" % (tuned[0], tuned[2]),
                 "gcell_per_s": round(rate, 3), "ms_per_step": round(1e3 * dt / args.gyro_steps, 3),
                 "bytes_per_cell_update": round(b_cell, 2),
                 "hbm_frac": round(rate * 1e9 * b_cell / (hbm * 1e9), 4), "hbm_peak_gbs": hbm, "peak_kind": kind})

@@ -850,7 +850,9 @@ static int xchunk_for(const dtmx_ctx* ctx) {
   const long long target = 148LL * 8 * 3;   // about three waves of 8 CTAs per SM
   long long chunks = std::max<long long>(1, (target + tiles - 1) / tiles);
   long long xc = (c.nx + chunks - 1) / chunks;
-  return (int)std::max<long long>(4, xc);
+  // at most 10 planes per CTA: the autotuner picks 8-10 on 384^3 and
+  // 1024x1024x1536 grids (longer chunks leave the tail of each CTA alone on its SM)
+  return (int)std::min<long long>(10, std::max<long long>(4, xc));
 }
 
 static int set_kernel_attributes() {
