@@ -37,6 +37,9 @@ struct DftHost {
 // and the device buffer their flux reduction writes to.
 struct FluxHost {
   int face[6];              // DFT ids: x lo, x hi, y lo, y hi, z lo, z hi
+  // far field: tangential E and H of each face plane and H of the next plane,
+  // on windows [lo, hi] of the in-plane axes (one more point than the flux windows)
+  int ffe[6], ffh[6];
   double sgn_area[6];       // outward sign times the cell face area
   int nfreq;
   double* d_out = nullptr;  // [6][nfreq]
@@ -770,7 +773,7 @@ extern "C" int dtmx_add_flux_box(dtmx_ctx* ctx, const int lo[3], const int hi[3]
   const int n[3] = {ctx->cfg.nx, ctx->cfg.ny, ctx->cfg.nz};
   const double ds[3] = {ctx->cfg.dx, ctx->cfg.dy, ctx->cfg.dz};
   for (int a = 0; a < 3; a++)
-    if (lo[a] < 0 || hi[a] <= lo[a] || hi[a] >= n[a]) return fail(ctx, DTMX_ERR_INVALID, "flux box outside the grid");
+    if (lo[a] < 0 || hi[a] <= lo[a] || hi[a] + 1 >= n[a]) return fail(ctx, DTMX_ERR_INVALID, "flux box outside the grid");
   FluxHost fx{};
   fx.nfreq = nfreq;
   for (int a = 0; a < 3; a++) {
@@ -785,6 +788,16 @@ extern "C" int dtmx_add_flux_box(dtmx_ctx* ctx, const int lo[3], const int hi[3]
       if (rc) return rc;
       fx.face[2 * a + side] = id;
       fx.sgn_area[2 * a + side] = (side ? 1.0 : -1.0) * ds[s1] * ds[s2];
+      const int w = side ? hi[a] : lo[a];
+      const int n1 = hi[s1] - lo[s1] + 1, n2 = hi[s2] - lo[s2] + 1;
+      int eid = -1, hid = -1;
+      int rc2 = dtmx_add_dft_patch(ctx, a, w, lo[s1], n1, lo[s2], n2, mask, nfreq, omegas, &eid);
+      if (!rc2)
+        rc2 = dtmx_add_dft_patch(ctx, a, w + 1, lo[s1], n1, lo[s2], n2, (1 << (3 + b)) | (1 << (3 + c)), nfreq,
+                                 omegas, &hid);
+      if (rc2) return rc2;
+      fx.ffe[2 * a + side] = eid;
+      fx.ffh[2 * a + side] = hid;
     }
   }
   if (cudaMalloc(&fx.d_out, (size_t)6 * nfreq * sizeof(double)) != cudaSuccess)
@@ -839,6 +852,49 @@ extern "C" int dtmx_read_flux(dtmx_ctx* ctx, int id, double* out, size_t out_len
     for (int q = 0; q < 6; q++) t += out[(size_t)q * nf + f];
     out[(size_t)6 * nf + f] = t;
   }
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_ntff(dtmx_ctx* ctx, int id, int ndir, const double* theta, const double* phi, const double* origin,
+                         double* out, size_t out_len) {
+  if (!ctx || id < 0 || id >= (int)ctx->fluxes.size() || ndir < 1 || !theta || !phi || !out)
+    return fail(ctx, DTMX_ERR_INVALID, "bad far-field arguments");
+  FluxHost& fx = ctx->fluxes[id];
+  const int nf = fx.nfreq;
+  if (out_len < (size_t)ndir * nf * 5) return fail(ctx, DTMX_ERR_INVALID, "output buffer too small");
+  NtffFaces F{};
+  const double ds[3] = {ctx->cfg.dx, ctx->cfg.dy, ctx->cfg.dz};
+  for (int q = 0; q < 6; q++) {
+    DftHost& h = ctx->dfts[fx.ffe[q]];
+    dft_flush(ctx, h);
+    F.f[q] = h.d;
+    DftHost& h2 = ctx->dfts[fx.ffh[q]];
+    dft_flush(ctx, h2);
+    F.h[q] = h2.d;
+  }
+  for (int a = 0; a < 3; a++) {
+    F.ds[a] = ds[a];
+    F.lo[a] = F.f[2 * a].index;
+    F.hi[a] = F.f[2 * a + 1].index;
+    // default origin: the centre of the E surface (box lo + 1/2 .. hi + 1/2)
+    F.org[a] = origin ? origin[a] : (0.5 * (F.lo[a] + F.hi[a]) + 0.5) * ds[a];
+  }
+  double *dth = nullptr, *dph = nullptr, *dout = nullptr;
+  const size_t nout = (size_t)ndir * nf * 5;
+  if (cudaMalloc(&dth, ndir * 8) != cudaSuccess || cudaMalloc(&dph, ndir * 8) != cudaSuccess ||
+      cudaMalloc(&dout, nout * 8) != cudaSuccess) {
+    cudaFree(dth); cudaFree(dph); cudaFree(dout);
+    return fail(ctx, DTMX_ERR_OOM, "far-field allocation");
+  }
+  CK(cudaMemcpyAsync(dth, theta, ndir * 8, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(dph, phi, ndir * 8, cudaMemcpyHostToDevice, ctx->stream));
+  ntff_kernel<<<dim3(ndir, nf), FLUX_THREADS, 0, ctx->stream>>>(F, dth, dph, nf, dout);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, nout * 8, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(dth); cudaFree(dph); cudaFree(dout);
+  if (e != cudaSuccess) return fail(ctx, DTMX_ERR_CUDA, std::string("far field: ") + cudaGetErrorString(e));
   return DTMX_OK;
 }
 

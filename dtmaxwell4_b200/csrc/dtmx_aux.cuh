@@ -364,6 +364,133 @@ __global__ void __launch_bounds__(FLUX_THREADS) flux_face_kernel(DftDev d, doubl
   if (threadIdx.x == 0) out[f] = sgn_area * red[0];
 }
 
+// Near-to-far-field transform of a flux box (surface equivalence): on a face
+// with outward normal n = sgn e_a the equivalent currents are J = n x H and
+// M = -n x E, i.e. J_c = sgn H_b, J_b = -sgn H_c, M_c = -sgn E_b, M_b = sgn E_c
+// ((a, b, c) cyclic), and the radiation vectors are
+//   N = sum J(r') exp(i k rhat.r') dA,  L = sum M(r') exp(i k rhat.r') dA,
+// k = omega (c = 1).  Both currents must lie on one closed surface: the
+// tangential E of the face plane w sits at w + 1/2 along the normal and the
+// tangential H at w, so H is averaged over the planes w and w + 1 onto the E
+// surface, the box [lo + 1/2, hi + 1/2] on every axis.  In the plane every term
+// keeps its component's Yee position, and the sum over a face is a quadrature
+// over that box's face: along an in-plane axis, a component at integer
+// positions takes the midpoints lo+1 .. hi (weight 1), one at half-integer
+// positions the points lo+1/2 .. hi+1/2 with the trapezoid weights (1/2 at the
+// ends); the windows hold the indices lo .. hi.  The
+// DFT phasors follow x(t) = Re(X exp(i w t)), so an outgoing wave carries
+// exp(-i k r) and the far field is
+//   r E_theta = -i k/(4 pi) (L_phi + N_theta) e^{-ikr},  r E_phi = i k/(4 pi) (L_theta - N_phi) e^{-ikr},
+// with radiation intensity U = k^2/(16 pi^2) (|L_phi + N_theta|^2 + |L_theta - N_phi|^2),
+// normalised like the flux box (Re(E x H*) without the 1/2), so that the
+// integral of U over the sphere equals the box's power.  One block per
+// (direction, frequency); FP64 throughout, fixed-order reduction.
+struct NtffFaces {
+  DftDev f[6];              // tangential E and H of the face planes, windows [lo, hi] in the plane
+  DftDev h[6];              // tangential H of the planes one further along each normal
+  double org[3];            // the origin of r' (physical units)
+  double ds[3];
+  int lo[3], hi[3];         // the box (face plane indices)
+};
+// quadrature weight of in-plane index v for a component at v + o/2, box [lo + 1/2, hi + 1/2]
+__host__ __device__ __forceinline__ double ntff_weight(int v, int o, int lo, int hi) {
+  if (o == 0) return (v > lo && v <= hi) ? 1.0 : 0.0;
+  if (v == lo || v == hi) return 0.5;
+  return (v > lo && v < hi) ? 1.0 : 0.0;
+}
+__global__ void __launch_bounds__(FLUX_THREADS) ntff_kernel(NtffFaces F, const double* theta, const double* phi,
+                                                            int nfreq, double* out) {
+  __shared__ double red[12][FLUX_THREADS];
+  const int dir = blockIdx.x, f = blockIdx.y;
+  const double th = theta[dir], ph = phi[dir];
+  double sth, cth, sph, cph;
+  sincos(th, &sth, &cth);
+  sincos(ph, &sph, &cph);
+  const double rh[3] = {sth * cph, sth * sph, cth};
+  double acc[12];
+#pragma unroll
+  for (int q = 0; q < 12; q++) acc[q] = 0.0;
+  for (int q = 0; q < 6; q++) {
+    const DftDev& d = F.f[q];
+    const int a = d.axis, b = (a + 1) % 3, c = (a + 2) % 3;
+    const double sgn = (q & 1) ? 1.0 : -1.0;
+    const int s1 = a == 0 ? 1 : 0, s2 = a == 2 ? 1 : 2;
+    const double k = d.omega[f];
+    const double dA = F.ds[s1] * F.ds[s2];
+    const long long npts = (long long)d.n1 * d.n2;
+    const double2* Eb = d.acc + ((long long)dft_slot(d.comp_mask, b) * d.nfreq + f) * npts;
+    const double2* Ec = d.acc + ((long long)dft_slot(d.comp_mask, c) * d.nfreq + f) * npts;
+    const double2* Hb = d.acc + ((long long)dft_slot(d.comp_mask, 3 + b) * d.nfreq + f) * npts;
+    const double2* Hc = d.acc + ((long long)dft_slot(d.comp_mask, 3 + c) * d.nfreq + f) * npts;
+    const DftDev& d2 = F.h[q];
+    const double2* Hb2 = d2.acc + ((long long)dft_slot(d2.comp_mask, 3 + b) * d2.nfreq + f) * npts;
+    const double2* Hc2 = d2.acc + ((long long)dft_slot(d2.comp_mask, 3 + c) * d2.nfreq + f) * npts;
+    const int srcs[4] = {3 + b, 3 + c, b, c};       // terms J_c, J_b, M_c, M_b
+    for (long long pt = threadIdx.x; pt < npts; pt += FLUX_THREADS) {
+      int idx[3];
+      idx[a] = d.index;
+      idx[s1] = d.lo1 + (int)(pt / d.n2);
+      idx[s2] = d.lo2 + (int)(pt % d.n2);
+      const double2 hb = Hb[pt], hb2 = Hb2[pt], hc = Hc[pt], hc2 = Hc2[pt];
+      const double2 vals[4] = {make_double2(0.5 * (hb.x + hb2.x), 0.5 * (hb.y + hb2.y)),
+                               make_double2(0.5 * (hc.x + hc2.x), 0.5 * (hc.y + hc2.y)), Eb[pt], Ec[pt]};
+      const double wts[4] = {sgn, -sgn, -sgn, sgn};
+      const int dst[4] = {c, b, c, b};
+#pragma unroll
+      for (int t = 0; t < 4; t++) {
+        double proj = 0.0;
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+          // along the normal every term sits on the E surface w + 1/2
+          const double off = x == a ? 0.5 : 0.5 * comp_off(srcs[t], x);
+          proj += rh[x] * ((idx[x] + off) * F.ds[x] - F.org[x]);
+        }
+        const double qw = ntff_weight(idx[s1], comp_off(srcs[t], s1), F.lo[s1], F.hi[s1]) *
+                          ntff_weight(idx[s2], comp_off(srcs[t], s2), F.lo[s2], F.hi[s2]);
+        if (qw == 0.0) continue;
+        double sn, cs;
+        sincos(k * proj, &sn, &cs);
+        const double re = wts[t] * qw * dA * (vals[t].x * cs - vals[t].y * sn);
+        const double im = wts[t] * qw * dA * (vals[t].x * sn + vals[t].y * cs);
+        const int base = (t < 2 ? 0 : 6) + 2 * dst[t];
+        acc[base] += re;
+        acc[base + 1] += im;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 12; q++) red[q][threadIdx.x] = acc[q];
+  __syncthreads();
+  for (int w = FLUX_THREADS / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+#pragma unroll
+      for (int q = 0; q < 12; q++) red[q][threadIdx.x] += red[q][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    // N = red[0..5] (x, y, z complex), L = red[6..11]; theta/phi components
+    const double tv[3] = {cth * cph, cth * sph, -sth}, pv[3] = {-sph, cph, 0.0};
+    double Nt[2] = {0, 0}, Np[2] = {0, 0}, Lt[2] = {0, 0}, Lp[2] = {0, 0};
+    for (int x = 0; x < 3; x++)
+      for (int r = 0; r < 2; r++) {
+        Nt[r] += tv[x] * red[2 * x + r][0];
+        Np[r] += pv[x] * red[2 * x + r][0];
+        Lt[r] += tv[x] * red[6 + 2 * x + r][0];
+        Lp[r] += pv[x] * red[6 + 2 * x + r][0];
+      }
+    const double k = F.f[0].omega[f];
+    const double s = k / (4.0 * M_PI);
+    // r E_theta = -i s (Lp + Nt), r E_phi = i s (Lt - Np) (the e^{-ikr} dropped)
+    const double at[2] = {Lp[0] + Nt[0], Lp[1] + Nt[1]}, ap[2] = {Lt[0] - Np[0], Lt[1] - Np[1]};
+    double* o = out + ((long long)dir * nfreq + f) * 5;
+    o[0] = s * s * (at[0] * at[0] + at[1] * at[1] + ap[0] * ap[0] + ap[1] * ap[1]);
+    o[1] = s * at[1];
+    o[2] = -s * at[0];
+    o[3] = -s * ap[1];
+    o[4] = s * ap[0];
+  }
+}
+
 // Magnetised-Drude current over the ADE box (dtmx.h, dtmx_material):
 // J^{n+1/2} into buffer 1-cur from J^{n-1/2} (buffer cur) and E^n.
 __device__ __forceinline__ float gyro_old(const Params& p, int cur, int c, int i, int j, int k) {

@@ -26,7 +26,7 @@ EXPORTS = (
     "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
     "dtmx_write_arr", "dtmx_save_state", "dtmx_load_state",
     "dtmx_add_dft_patch", "dtmx_add_flux_box", "dtmx_read_flux", "dtmx_flux_faces",
-    "dtmx_set_adjoint_memory",
+    "dtmx_set_adjoint_memory", "dtmx_ntff",
 )
 
 
@@ -65,6 +65,7 @@ def load():
     L.dtmx_read_flux.argtypes = [vp, ip, vp, C.c_size_t]
     L.dtmx_flux_faces.argtypes = [vp, ip, C.POINTER(ip)]
     L.dtmx_set_adjoint_memory.argtypes = [vp, C.c_int64]
+    L.dtmx_ntff.argtypes = [vp, ip, ip, vp, vp, vp, vp, C.c_size_t]
     L.dtmx_step.argtypes = [vp, ip]
     L.dtmx_sync.argtypes = [vp]
     L.dtmx_get_step.argtypes = [vp, C.POINTER(C.c_int64)]
@@ -192,7 +193,9 @@ class Simulation:
         for a in range(3):
             n = [hi[q] - lo[q] for q in range(3) if q != a]
             for _ in range(2):
-                self._dft.append((4, len(om), n[0], n[1]))
+                self._dft.append((4, len(om), n[0], n[1]))              # the face window (flux)
+                self._dft.append((4, len(om), n[0] + 1, n[1] + 1))      # far field: E and H of the face plane
+                self._dft.append((2, len(om), n[0] + 1, n[1] + 1))      # far field: H one plane further
         self._flux.append((len(om), list(faces)))
         return fid.value
 
@@ -205,6 +208,23 @@ class Simulation:
         out = np.zeros(7 * nf, dtype=np.float64)
         self._ck(self._L.dtmx_read_flux(self._h, fid, out.ctypes.data, out.size))
         return out[: 6 * nf].reshape(6, nf), out[6 * nf:]
+
+    def far_field(self, fid, theta, phi, origin=None):
+        """Near-to-far-field transform of flux box fid at directions (theta, phi):
+        returns (U[ndir, nfreq], E_theta[ndir, nfreq], E_phi[ndir, nfreq]) with
+        r E as complex values (exp(-i k r) dropped); see dtmx_ntff."""
+        th = np.ascontiguousarray(np.ravel(theta), dtype=np.float64)
+        ph = np.ascontiguousarray(np.ravel(phi), dtype=np.float64)
+        if th.shape != ph.shape:
+            raise ValueError("theta and phi must have the same size")
+        nf = self._flux[fid][0]
+        out = np.zeros((th.size, nf, 5), dtype=np.float64)
+        org = None
+        if origin is not None:
+            org = np.ascontiguousarray(origin, dtype=np.float64)
+        self._ck(self._L.dtmx_ntff(self._h, fid, th.size, th.ctypes.data, ph.ctypes.data,
+                                   None if org is None else org.ctypes.data, out.ctypes.data, out.size))
+        return out[..., 0], out[..., 1] + 1j * out[..., 2], out[..., 3] + 1j * out[..., 4]
 
     def set_engine(self, engine, time_block=0):
         self._ck(self._L.dtmx_set_engine(self._h, engine, time_block))

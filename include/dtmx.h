@@ -217,7 +217,8 @@ int  dtmx_add_dft_patch(dtmx_ctx* ctx, int axis, int index, int lo1, int n1, int
  *   sign * d_b * d_c * sum Re(E_b conj(H_c) - E_c conj(H_b)),
  * (a, b, c) cyclic, sign -1 on the lo face and +1 on the hi face, accumulated
  * in FP64 on the device from the running DFTs (dtmx_add_dft_plane's
- * convention).  Requires 0 <= lo[a] < hi[a] < n[a]. */
+ * convention).  The box also records the tangential H one plane beyond each
+ * face, for dtmx_ntff.  Requires 0 <= lo[a] < hi[a] < n[a] - 1. */
 int  dtmx_add_flux_box(dtmx_ctx* ctx, const int lo[3], const int hi[3], int nfreq,
                        const double* omegas, int* id_out);
 /* out[7*nfreq]: the outward flux of the faces (x lo, x hi, y lo, y hi, z lo,
@@ -225,6 +226,21 @@ int  dtmx_add_flux_box(dtmx_ctx* ctx, const int lo[3], const int hi[3], int nfre
 int  dtmx_read_flux(dtmx_ctx* ctx, int id, double* out, size_t out_len);
 /* DFT ids of the six face windows (same order), for dtmx_read_dft. */
 int  dtmx_flux_faces(dtmx_ctx* ctx, int id, int faces[6]);
+/* Near-to-far-field transform of flux box id (surface equivalence, FP64 on
+ * the device; no reference counterpart).  For every direction (theta[d],
+ * phi[d]) (polar angle from +z, azimuth from +x) and frequency f:
+ *   out[(d*nfreq + f)*5 + 0]   radiation intensity U, normalised so that its
+ *                              integral over the sphere equals the box's
+ *                              dtmx_read_flux total in free space,
+ *   out[...+1 .. +4]           r E_theta and r E_phi (re, im) without the
+ *                              exp(-i k r) factor, phase referred to origin
+ *                              (physical units; NULL = the box centre).
+ * The currents lie on the surface of the tangential E (half a cell outside
+ * each face plane along its normal), with H averaged onto it from the face
+ * plane and the next one; in the plane every component enters at its own
+ * Yee position; k = omega. */
+int  dtmx_ntff(dtmx_ctx* ctx, int id, int ndir, const double* theta, const double* phi,
+               const double* origin, double* out, size_t out_len);
 
 /* Advance nsteps leapfrog steps (H half step then E half step each,
  * genAlg.py:420-501).  Asynchronous on the context stream.  Replaces

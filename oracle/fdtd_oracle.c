@@ -104,7 +104,7 @@ typedef struct {
   /* monitors */
   probe_t probes[4096]; int nprobes;
   int probe_cap; int nsamples; real* traces;
-  dft_t dft[16]; int ndft;
+  dft_t dft[64]; int ndft;
   int64_t step;
 } osim;
 
@@ -825,7 +825,7 @@ int PFX(add_probe)(void* h, int comp, int i, int j, int k, int mode) {
 
 int PFX(add_dft_plane)(void* h, int axis, int index, int comp_mask, int nfreq, const double* om) {
   osim* s = h;
-  if (s->ndft >= 16) return -1;
+  if (s->ndft >= 64) return -1;
   dft_t* d = &s->dft[s->ndft];
   d->axis = axis; d->index = index; d->comp_mask = comp_mask; d->nfreq = nfreq;
   d->ncomp = 0;

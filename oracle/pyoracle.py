@@ -96,6 +96,8 @@ class OracleSim:
     def add_dft_plane(self, axis, index, comp_mask, omegas):
         om = np.ascontiguousarray(omegas, dtype=np.float64)
         did = self._f("add_dft_plane")(self._h, axis, index, comp_mask, len(om), om.ctypes.data)
+        if did < 0:
+            raise ValueError("oracle: too many DFT planes")
         n = list(self.shape)
         del n[axis]
         ncomp = bin(comp_mask).count("1")
@@ -165,8 +167,11 @@ def add_flux_planes(sim, lo, hi, omegas):
     {(axis, side): dft id} with side 0 = lo face, 1 = hi face."""
     ids = {}
     for a in range(3):
+        b, c = (a + 1) % 3, (a + 2) % 3
         for side, v in enumerate((lo[a], hi[a])):
             ids[(a, side)] = sim.add_dft_plane(a, v, FLUX_MASK[a], omegas)
+            # tangential H one plane further along the normal (far-field transform)
+            ids[(a, side, "h")] = sim.add_dft_plane(a, v + 1, (1 << (3 + b)) | (1 << (3 + c)), omegas)
     return ids
 
 
@@ -188,3 +193,70 @@ def flux_box_from_planes(sim, ids, lo, hi, ds=(1.0, 1.0, 1.0)):
             faces.append((1.0 if side else -1.0) * ds[s1] * ds[s2] * s)
     faces = np.array(faces)
     return faces, faces.sum(axis=0)
+
+
+def _comp_off(c, x):
+    return int(x != c) if c < 3 else int(x == c - 3)
+
+
+def _ntff_weights(lo, hi, o):
+    """Quadrature weights of indices lo..hi over [lo + 1/2, hi + 1/2] for a
+    component at index + o/2: midpoints (o = 0) or trapezoid (o = 1)."""
+    v = np.arange(lo, hi + 1)
+    if o == 0:
+        return ((v > lo) & (v <= hi)).astype(np.float64)
+    w = ((v > lo) & (v < hi)).astype(np.float64)
+    w[0] = w[-1] = 0.5
+    return w
+
+
+def ntff_from_planes(sim, ids, lo, hi, omegas, theta, phi, ds=(1.0, 1.0, 1.0), origin=None):
+    """Near-to-far-field transform of a flux box from full-plane oracle DFTs:
+    J = n x H, M = -n x E on each face, N = sum J exp(i k rhat.r') dA and
+    L = sum M exp(i k rhat.r') dA on the surface of the tangential E (half a
+    cell beyond each face plane along its normal; H averaged onto it from the
+    face plane and the next one), every term at its component's in-plane Yee
+    position, U = k^2/(16 pi^2)(|L_phi + N_theta|^2 + |L_theta - N_phi|^2),
+    r E_theta = -i k/(4 pi)(L_phi + N_theta), r E_phi = i k/(4 pi)(L_theta - N_phi).
+    Returns (U, E_theta, E_phi), each [ndir, nfreq]."""
+    th = np.ravel(np.asarray(theta, dtype=np.float64))
+    ph = np.ravel(np.asarray(phi, dtype=np.float64))
+    k = np.asarray(omegas, dtype=np.float64)
+    rh = np.stack([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)], axis=1)
+    org = origin if origin is not None else [(0.5 * (lo[a] + hi[a]) + 0.5) * ds[a] for a in range(3)]
+    N = np.zeros((th.size, k.size, 3), np.complex128)
+    L = np.zeros_like(N)
+    for a in range(3):
+        b, c = (a + 1) % 3, (a + 2) % 3
+        s1, s2 = (1, 2) if a == 0 else ((0, 2) if a == 1 else (0, 1))
+        comps = [q for q in range(6) if FLUX_MASK[a] & (1 << q)]
+        dA = ds[s1] * ds[s2]
+        for side, w in enumerate((lo[a], hi[a])):
+            sgn = 1.0 if side else -1.0
+            F = sim.read_dft(ids[(a, side)])[:, :, lo[s1]:hi[s1] + 1, lo[s2]:hi[s2] + 1]
+            F2 = sim.read_dft(ids[(a, side, "h")])[:, :, lo[s1]:hi[s1] + 1, lo[s2]:hi[s2] + 1]
+            u = np.arange(lo[s1], hi[s1] + 1, dtype=np.float64)[:, None]
+            v = np.arange(lo[s2], hi[s2] + 1, dtype=np.float64)[None, :]
+            for t, (src, dst, wt) in enumerate(((3 + b, c, sgn), (3 + c, b, -sgn), (b, c, -sgn), (c, b, sgn))):
+                idx = {a: np.float64(w), s1: u, s2: v}
+                proj = 0.0
+                for x in range(3):
+                    off = 0.5 if x == a else 0.5 * _comp_off(src, x)
+                    px = (idx[x] + off) * ds[x] - org[x]
+                    proj = proj + rh[:, x][:, None, None] * px[None]
+                phase = np.exp(1j * k[None, :, None, None] * proj[:, None])
+                val = F[comps.index(src)]
+                if src >= 3:
+                    val = 0.5 * (val + F2[0 if src == 3 + min(b, c) else 1])
+                qw = (_ntff_weights(lo[s1], hi[s1], _comp_off(src, s1))[:, None] *
+                      _ntff_weights(lo[s2], hi[s2], _comp_off(src, s2))[None, :])
+                term = wt * dA * (val[None] * qw[None, None] * phase).sum(axis=(2, 3))
+                (N if t < 2 else L)[:, :, dst] += term
+    tv = np.stack([np.cos(th) * np.cos(ph), np.cos(th) * np.sin(ph), -np.sin(th)], axis=1)[:, None, :]
+    pv = np.stack([-np.sin(ph), np.cos(ph), np.zeros_like(ph)], axis=1)[:, None, :]
+    Nt, Np = (N * tv).sum(-1), (N * pv).sum(-1)
+    Lt, Lp = (L * tv).sum(-1), (L * pv).sum(-1)
+    s = k[None, :] / (4 * np.pi)
+    Et = -1j * s * (Lp + Nt)
+    Ep = 1j * s * (Lt - Np)
+    return np.abs(Et) ** 2 + np.abs(Ep) ** 2, Et, Ep

@@ -16,6 +16,11 @@ Tolerances:
                        staggering of E and H on a face is the residual)
   W/W0 homogeneous    |W/W0 - sqrt(eps)| <= 0.06 at 15 cells per wavelength in
                        the medium (grid dispersion of the discrete LDOS)
+  far field (dipole)   integral of U over the sphere = flux-box power within
+                       0.5 %; U(theta)/U(90 deg) = sin^2(theta) within 0.5 %
+                       of U(90 deg); azimuthal ripple < 0.5 % (the lattice's
+                       cos 4 phi anisotropy)
+  far field vs oracle  U within 2e-5 of max U (products of two DFTs)
 """
 import json
 import math
@@ -145,6 +150,12 @@ def test_flux_box_gyro_crystal_vs_oracle():
     assert np.abs(gf - of).max() <= 2e-5 * scale
     assert np.abs(gt - ot).max() <= 2e-5 * scale
     assert np.array_equal(gt, gf.sum(axis=0))
+    # far field of the same box (gyrotropic layer and slab inside the domain)
+    th, TH, PH = _sphere_grid(12, 24)
+    U, _, _ = g.far_field(fid, TH.ravel(), PH.ravel())
+    Uo, _, _ = pyoracle.ntff_from_planes(o, oid, lo, hi, om, TH.ravel(), PH.ravel())
+    print("far field max err / max U: %.2e" % (np.abs(U - Uo).max() / Uo.max()))
+    assert np.abs(U - Uo).max() <= 2e-5 * Uo.max()
 
 
 @pytest.mark.gpu
@@ -187,3 +198,56 @@ def test_engine_purcell_homogeneous_dielectric():
             assert np.max(np.abs(power[eps][0] - ot)) <= 2e-5 * np.abs(ot).max()
     w = purcell.purcell_flux(power[4.0][0], power[1.0][0], 4.0, 1.0)
     assert np.max(np.abs(w - 2.0)) < 0.06, w
+
+
+def _sphere_grid(nt=36, nph=72):
+    th = (np.arange(nt) + 0.5) * np.pi / nt
+    ph = (np.arange(nph) + 0.5) * 2 * np.pi / nph
+    TH, PH = np.meshgrid(th, ph, indexing="ij")
+    return th, TH, PH
+
+
+def _check_dipole_far_field(U, th, total):
+    """U[nt, nph, nf] of a z dipole against the flux-box total[nf]."""
+    nt, nph = U.shape[:2]
+    P = (U * np.sin(th)[:, None, None]).sum(axis=(0, 1)) * (np.pi / nt) * (2 * np.pi / nph)
+    assert np.max(np.abs(P / total - 1)) < 5e-3, (P, total)
+    eq = U[nt // 2 - 1: nt // 2 + 1].mean(axis=(0, 1))
+    shape = U.mean(axis=1) / eq
+    assert np.max(np.abs(shape - np.sin(th)[:, None] ** 2)) < 5e-3
+    ripple = np.abs(U - U.mean(axis=1, keepdims=True)).max(axis=(0, 1)) / U.max(axis=(0, 1))
+    assert np.max(ripple) < 5e-3, ripple
+
+
+def test_oracle_far_field_dipole_known_answers():
+    import pyoracle
+    o, boxes, om, steps = _homogeneous(1.0, lambda cfg: pyoracle.OracleSim(cfg, "f64"), halves=(8,))
+    (lo, hi), = boxes
+    ids = pyoracle.add_flux_planes(o, lo, hi, om)
+    o.step(steps)
+    _, total = pyoracle.flux_box_from_planes(o, ids, lo, hi)
+    th, TH, PH = _sphere_grid()
+    U, _, _ = pyoracle.ntff_from_planes(o, ids, lo, hi, om, TH.ravel(), PH.ravel())
+    _check_dipole_far_field(U.reshape(TH.shape + (len(om),)), th, total)
+
+
+@pytest.mark.gpu
+def test_engine_far_field_dipole_and_oracle():
+    """Engine near-to-far-field transform: dipole known answers, and the
+    same sums as the oracle's restatement on the same run."""
+    import pyoracle
+    from dtmaxwell4_b200 import Simulation
+    g, boxes, om, steps = _homogeneous(1.0, Simulation, halves=(8,))
+    (lo, hi), = boxes
+    fid = g.add_flux_box(lo, hi, om)
+    g.step(steps)
+    _, total = g.read_flux(fid)
+    th, TH, PH = _sphere_grid()
+    U, Et, Ep = g.far_field(fid, TH.ravel(), PH.ravel())
+    _check_dipole_far_field(U.reshape(TH.shape + (len(om),)), th, total)
+    o, _, _, _ = _homogeneous(1.0, lambda cfg: pyoracle.OracleSim(cfg, "f64"), halves=(8,))
+    ids = pyoracle.add_flux_planes(o, lo, hi, om)
+    o.step(steps)
+    Uo, Eto, Epo = pyoracle.ntff_from_planes(o, ids, lo, hi, om, TH.ravel(), PH.ravel())
+    assert np.max(np.abs(U - Uo)) <= 2e-5 * np.max(Uo)
+    assert np.allclose(np.abs(U), np.abs(Et) ** 2 + np.abs(Ep) ** 2, rtol=1e-12, atol=0)
