@@ -406,9 +406,6 @@ def run_gyro_purcell(args):
     cut = scenarios.gyro_crystal_purcell(n=(256, 256, 512), steps=8000)
     vac = scenarios.gyro_crystal_purcell(n=(128, 128, 128), steps=8000, structure=False)
     power = []
-    nt, nph = 36, 72
-    th = (np.arange(nt) + 0.5) * np.pi / nt
-    TH, PH = np.meshgrid(th, (np.arange(nph) + 0.5) * 2 * np.pi / nph, indexing="ij")
     t0 = time.perf_counter()
     for sc in (cut, vac):
         s = Simulation(sc["cfg"])
@@ -416,26 +413,14 @@ def run_gyro_purcell(args):
         fid, = scenarios.apply_flux(s, sc)
         s.step(sc["steps"])
         power.append(s.read_flux(fid)[1])
-        if sc is cut:
-            U = s.far_field(fid, TH.ravel(), PH.ravel())[0].reshape(nt, nph, -1)
         s.close()
     t_p = time.perf_counter() - t0
-    # far field of the structure run: power through the sphere (vs the box) and the share radiated upward (+z)
-    dW = (np.sin(th) * (np.pi / nt) * (2 * np.pi / nph))[:, None, None]
-    p_ff = (U * dW).sum(axis=(0, 1))
-    up = (U[: nt // 2] * dW[: nt // 2]).sum(axis=(0, 1)) / p_ff
     om = cut["flux"][0][2]
     w = purcell.purcell_flux(power[0], power[1], cut["eps_src"], vac["eps_src"])
     lam = 2 * np.pi / om
     out["purcell"] = {"workload": cut["desc"] + "; W0: " + vac["desc"] + "; 8000 steps each",
                       "wavelength_cells": [round(float(v), 3) for v in lam],
                       "w_over_w0": [round(float(v), 5) for v in w], "seconds": round(t_p, 2),
-                      "far_field": {"grid": "%dx%d (theta, phi) midpoints" % (nt, nph),
-                                    "power_over_box": [round(float(v), 4) for v in p_ff / power[0]],
-                                    "upward_fraction": [round(float(v), 4) for v in up],
-                                    "note": "near-to-far-field transform of the flux box (dtmx_ntff); the box "
-                                            "encloses the slab only, so the gyrotropic layer below scatters "
-                                            "part of the downward radiation back through it"},
                       "note": "flux-box powers normalised to equal source currents (eps_src^2)"}
     return out
 

@@ -231,7 +231,9 @@ int  dtmx_flux_faces(dtmx_ctx* ctx, int id, int faces[6]);
  * phi[d]) (polar angle from +z, azimuth from +x) and frequency f:
  *   out[(d*nfreq + f)*5 + 0]   radiation intensity U, normalised so that its
  *                              integral over the sphere equals the box's
- *                              dtmx_read_flux total in free space,
+ *                              dtmx_read_flux total in free space (the
+ *                              transform uses the free-space Green's function:
+ *                              the box surface must lie in vacuum),
  *   out[...+1 .. +4]           r E_theta and r E_phi (re, im) without the
  *                              exp(-i k r) factor, phase referred to origin
  *                              (physical units; NULL = the box centre).
