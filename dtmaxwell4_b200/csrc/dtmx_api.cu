@@ -351,6 +351,7 @@ static int setup_absorber(dtmx_ctx* ctx) {
     for (int s = 0; s < 4; s++) ab.aux[a][s] = nullptr;
     if (!th || c.absorber == DTMX_ABS_NONE) continue;
     const size_t cnt = th * (ctx->ncell / (size_t)n[a]);
+    if (cnt >= (size_t)INT32_MAX) return fail(ctx, DTMX_ERR_UNSUPPORTED, "absorber slab of more than 2^31 values");
     for (int s = 0; s < 4; s++) {
       int rc = dalloc(ctx, &ab.aux[a][s], cnt);
       if (rc) return rc;

@@ -230,6 +230,53 @@ __device__ __forceinline__ float absorb_apply(const Params& p, int c, int i, int
   return corr;
 }
 
+// The same two steps for the streaming kernels, with the node's slab indices
+// along the three axes computed once per node (-1 outside that slab) and
+// shared by its three components; 32-bit (every slab array holds fewer than
+// 2^31 values, checked when the absorber is set up).  Same arithmetic as
+// absorb_load / absorb_apply.
+__device__ __forceinline__ int slab_index32(const Params& p, int a, int i, int j, int k) {
+  const int n = p.g.n[a], v = a == 0 ? i : a == 1 ? j : k;
+  const int lo = p.ab.L[a][0], hi = p.ab.L[a][1];
+  int cs;
+  if (v < lo) cs = v;
+  else if (v >= n - hi) cs = lo + (v - (n - hi));
+  else return -1;
+  if (a == 0) return (cs * p.g.n[1] + j) * p.g.n[2] + k;
+  if (a == 1) return (i * (lo + hi) + cs) * p.g.n[2] + k;
+  return (i * p.g.n[1] + j) * (lo + hi) + cs;
+}
+// slab indices of node (i,j,k); true when it lies in any slab
+__device__ __forceinline__ bool node_slabs(const Params& p, int i, int j, int k, int (&si)[3]) {
+  si[0] = slab_index32(p, 0, i, j, k);
+  si[1] = slab_index32(p, 1, i, j, k);
+  si[2] = slab_index32(p, 2, i, j, k);
+  return (si[0] & si[1] & si[2]) >= 0;
+}
+__device__ __forceinline__ void absorb_load3(const Params& p, int c, const int (&si)[3], float (&old)[3]) {
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int sl = slot_of(c, a);
+    old[a] = (sl >= 0 && si[a] >= 0) ? p.ab.aux[a][sl][si[a]] : 0.f;
+  }
+}
+__device__ __forceinline__ float absorb_apply3(const Params& p, int c, const int (&idx)[3], const int (&si)[3],
+                                               const float* dif, const float (&old)[3]) {
+  float corr = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int sl = slot_of(c, a);
+    if (sl < 0 || si[a] < 0) continue;
+    const int h = 2 * idx[a] + comp_off(c, a);
+    const float k0 = __ldg(p.ab.c0[a] + h), k1 = __ldg(p.ab.c1[a] + h);
+    const float nv = __fmaf_rn(k0, old[a], __fmul_rn(k1, dif[a]));
+    p.ab.aux[a][sl][si[a]] = nv;
+    if (p.ab.kind == 1) corr = __fadd_rn(corr, __fmaf_rn(__fsub_rn(__ldg(p.ab.c2[a] + h), 1.f), dif[a], nv));
+    else corr = __fadd_rn(corr, __fsub_rn(__fsub_rn(nv, old[a]), dif[a]));
+  }
+  return corr;
+}
+
 // Shared-memory copy of one component's plane tile: rows of TW_ROW floats
 // covering z in [k0-4, k0+36) (16-byte aligned), with YL/YH halo rows in y.
 constexpr int ZO = 4;                 // z offset of node k0 inside a row
@@ -369,13 +416,13 @@ __device__ __forceinline__ float gyro_subtract(const Params& p, int c, int i, in
 template <bool ISH>
 __device__ __forceinline__ void absorb_prefetch(const Params& p, int i, int j0, int k0, float (&old)[RY][3][3]) {
   const int cf = ISH ? 3 : 0;
-  const bool inx = in_slab(p, 0, i);
 #pragma unroll
   for (int r = 0; r < RY; r++) {
     const int j = j0 + threadIdx.y + TW * r, k = k0 + threadIdx.x;
-    if (j >= p.g.n[1] || k >= p.g.n[2] || !(inx || in_slab(p, 1, j) || in_slab(p, 2, k))) continue;
+    int si[3];
+    if (j >= p.g.n[1] || k >= p.g.n[2] || !node_slabs(p, i, j, k, si)) continue;
 #pragma unroll
-    for (int c = 0; c < 3; c++) absorb_load(p, cf + c, i, j, k, old[r][c]);
+    for (int c = 0; c < 3; c++) absorb_load3(p, cf + c, si, old[r][c]);
   }
 }
 
@@ -399,7 +446,6 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
   const int cf = ISH ? 3 : 0;
   const long long pbase = (long long)i * p.g.sx;
   const bool tab = !SIMPLE && tile_absorber(p, i, j0, k0);
-  const bool inx = tab && in_slab(p, 0, i);
   const bool tade = !SIMPLE && !ISH && tile_ade(p, i, j0, k0);
   float iu[3] = {1.f, 1.f, 1.f};
   if (SIMPLE && !ISH) { iu[0] = ms.inv_eps[um][0]; iu[1] = ms.inv_eps[um][1]; iu[2] = ms.inv_eps[um][2]; }
@@ -433,7 +479,9 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
       d[1][0] = __fmul_rn(-cx, dxC);  d[1][1] = 0.f;                 d[1][2] = __fmul_rn(cz, dzA);
       d[2][0] = __fmul_rn(cx, dxB);   d[2][1] = __fmul_rn(-cy, dyA); d[2][2] = 0.f;
     }
-    const bool ab = tab && (inx || in_slab(p, 1, j) || in_slab(p, 2, k));
+    int si[3] = {-1, -1, -1};
+    const bool ab = tab && node_slabs(p, i, j, k, si);
+    const int idx3[3] = {i, j, k};
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       if (!SIMPLE && !fast && !is_live(p.g, cf + c, i, j, k)) continue;
@@ -459,7 +507,7 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
         d[c][0] = __fmul_rn(d[c][0], ie); d[c][1] = __fmul_rn(d[c][1], ie); d[c][2] = __fmul_rn(d[c][2], ie);
       }
       float inc = sum3(d[c][0], d[c][1], d[c][2]);
-      if (ab) inc = __fadd_rn(inc, absorb_apply(p, cf + c, i, j, k, d[c], old[r][c]));
+      if (ab) inc = __fadd_rn(inc, absorb_apply3(p, cf + c, idx3, si, d[c], old[r][c]));
       float nv = __fadd_rn(F, inc);
       p.f[cf + c][off] = nv;
     }
