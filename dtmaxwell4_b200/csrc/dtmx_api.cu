@@ -163,6 +163,7 @@ static void setup_grid(dtmx_ctx* ctx) {
   g.sx = (long long)c.ny * ctx->nzp;
   for (int a = 0; a < 3; a++)
     for (int s = 0; s < 2; s++) { g.btype[a][s] = 0; g.bsE[a][s] = 1; g.bsH[a][s] = 1; }
+  g.box = c.geometry == DTMX_GEOM_BOX;
   if (c.geometry == DTMX_GEOM_BOX) {
     for (int a = 0; a < 3; a++) { g.bplane[a][0] = -1; g.bplane[a][1] = 2 * n[a]; }
   } else {

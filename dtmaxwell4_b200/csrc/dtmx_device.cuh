@@ -40,6 +40,7 @@ struct Grid {
   int safe_lo[3], safe_hi[3];// index range whose taps need no mirror mapping (zero sides unbounded)
   int btype[3][2], bplane[3][2];
   int bsE[3][2], bsH[3][2];
+  int box;                   // box geometry: every node of the array is live, zero outside
 };
 
 struct Absorb {

@@ -181,7 +181,10 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
       for (int q = (i == xa ? 0 : AHEAD); q <= AHEAD; q++)
         mbar_wait(&bars[(i + q) % NST], (unsigned)(((i + q - xa) / NST) & 1), p.err);
     __syncthreads();
-    const bool fast = yz_in && i - 2 >= p.g.all_lo[0] && i + 2 <= p.g.all_hi[0];
+    // every node of the tile in the array and live, every tap in range or zero: in the box
+    // geometry a full tile (taps outside the array read the TMA zero fill)
+    const bool fast = p.g.box ? (j0 + TYT <= p.g.n[1] && k0 + TZ <= p.g.n[2])
+                              : (yz_in && i - 2 >= p.g.all_lo[0] && i + 2 <= p.g.all_hi[0]);
 #pragma unroll
     for (int r = 0; r < RY; r++) {
       const int y = w + TW * r;
