@@ -432,12 +432,15 @@ __device__ __forceinline__ void absorb_prefetch(const Params& p, int i, int j0, 
 // nodes add the absorber correction, dispersive nodes (E step, tiles touching
 // the ADE box) are replaced by the ADE recursion, non-live nodes are skipped.
 //   um >= 0: every E node of the tile has non-dispersive material um
-// SIMPLE: every node live, no absorber, no ADE, uniform material um (>= 0).
-template <int ORDER, bool ISH, bool SIMPLE>
+// MODE 1 (simple): every node live, no absorber, uniform material um (>= 0);
+// MODE 2 (absorber): the same with absorber slabs in the tile;
+// MODE 0: the general path.  All three evaluate the same expressions.
+template <int ORDER, bool ISH, int MODE>
 __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int k0, const float* sm,
                                              const float (&qb)[RY][4], const float (&qc)[RY][4], const float* so,
                                              const uint8_t* smat, const MatShared& ms, bool fast, int um,
                                              const float (&old)[RY][3][3]) {
+  constexpr bool SIMPLE = MODE == 1, ABSU = MODE == 2;
   using S = Stage<ORDER, ISH>;
   const float* sA = sm;
   const float* sB = sA + S::TA::N;
@@ -446,16 +449,16 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
   const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
   const int cf = ISH ? 3 : 0;
   const long long pbase = (long long)i * p.g.sx;
-  const bool tab = !SIMPLE && tile_absorber(p, i, j0, k0);
-  const bool tade = !SIMPLE && !ISH && tile_ade(p, i, j0, k0);
+  const bool tab = ABSU || (!SIMPLE && tile_absorber(p, i, j0, k0));
+  const bool tade = MODE == 0 && !ISH && tile_ade(p, i, j0, k0);
   float iu[3] = {1.f, 1.f, 1.f};
-  if (SIMPLE && !ISH) { iu[0] = ms.inv_eps[um][0]; iu[1] = ms.inv_eps[um][1]; iu[2] = ms.inv_eps[um][2]; }
+  if ((SIMPLE || ABSU) && !ISH) { iu[0] = ms.inv_eps[um][0]; iu[1] = ms.inv_eps[um][1]; iu[2] = ms.inv_eps[um][2]; }
   constexpr int o0 = ISH ? -2 : -1, o1 = o0 + 1, o2 = o0 + 2, o3 = o0 + 3;
 #pragma unroll
   for (int r = 0; r < RY; r++) {
     const int y = w + TW * r;
     const int j = j0 + y, k = k0 + tz;
-    if (!SIMPLE && !fast && (j >= p.g.n[1] || k >= p.g.n[2])) continue;
+    if (MODE == 0 && !fast && (j >= p.g.n[1] || k >= p.g.n[2])) continue;
     const long long off = pbase + (long long)j * p.g.sy + k;
     const float dyC = dstencil<ORDER>(ORDER == 4 ? S::TC::at(sC, y, tz, o0, 0) : 0.f, S::TC::at(sC, y, tz, o1, 0),
                                       S::TC::at(sC, y, tz, o2, 0), ORDER == 4 ? S::TC::at(sC, y, tz, o3, 0) : 0.f);
@@ -485,11 +488,13 @@ __device__ __forceinline__ void plane_update(const Params& p, int i, int j0, int
     const int idx3[3] = {i, j, k};
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      if (!SIMPLE && !fast && !is_live(p.g, cf + c, i, j, k)) continue;
+      if (MODE == 0 && !fast && !is_live(p.g, cf + c, i, j, k)) continue;
       float F = own_at(so, c, y, tz);
-      if (SIMPLE) {
+      if (SIMPLE || ABSU) {
         if (!ISH) { d[c][0] = __fmul_rn(d[c][0], iu[c]); d[c][1] = __fmul_rn(d[c][1], iu[c]); d[c][2] = __fmul_rn(d[c][2], iu[c]); }
-        p.f[cf + c][off] = __fadd_rn(F, sum3(d[c][0], d[c][1], d[c][2]));
+        float inc = sum3(d[c][0], d[c][1], d[c][2]);
+        if (ABSU && ab) inc = __fadd_rn(inc, absorb_apply3(p, cf + c, idx3, si, d[c], old[r][c]));
+        p.f[cf + c][off] = __fadd_rn(F, inc);
         continue;
       }
       int m = 0;

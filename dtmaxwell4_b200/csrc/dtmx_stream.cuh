@@ -198,9 +198,11 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
     const float* cur = dsm + (i % NST) * P::STAGE;
     const uint8_t* cmat = reinterpret_cast<const uint8_t*>(cur + P::OFF_MAT);
     if (fast && um >= 0 && !tab)
-      plane_update<ORDER, ISH, true>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
+      plane_update<ORDER, ISH, 1>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
+    else if (fast && um >= 0)
+      plane_update<ORDER, ISH, 2>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
     else
-      plane_update<ORDER, ISH, false>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
+      plane_update<ORDER, ISH, 0>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
 #pragma unroll
     for (int r = 0; r < RY; r++)
 #pragma unroll
