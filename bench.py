@@ -298,14 +298,22 @@ def run_adjoint(args):
     t_fwd = time.perf_counter() - t0
     s.close()
     res = {}
+    first = {}
     for mode, budget in (("history", -1), ("recompute", 0)):
-        s = make()
-        s.set_adjoint_memory(budget)
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        J, g = s.forward_adjoint(sc["steps"], sc["plane_x"], sc["omega"], 100)
-        res[mode] = (time.perf_counter() - t0, J, g)
-        s.close()
+        # the first call of a mode grows the device memory pool to the run's size
+        # (history or checkpoints); the second, timed call is the steady state of
+        # an optimisation loop, which takes its buffers from the pool
+        for rep in range(2):
+            s = make()
+            s.set_adjoint_memory(budget)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            J, g = s.forward_adjoint(sc["steps"], sc["plane_x"], sc["omega"], 100)
+            dt = time.perf_counter() - t0
+            s.close()
+            if rep == 0:
+                first[mode] = dt
+        res[mode] = (dt, J, g)
     t_fa, J, g = res["history"]
     t_rc, J_rc, g_rc = res["recompute"]
     c = sc["cfg"]
@@ -318,10 +326,13 @@ def run_adjoint(args):
             "forward_gcell_per_s": round(cells * sc["steps"] / t_fwd / 1e9, 3),
             "forward_adjoint_gcell_per_s": round(cells * sc["steps"] / t_fa / 1e9, 3),
             "cost_over_forward": round(t_fa / t_fwd, 2), "objective": J,
+            "first_call_seconds": round(first["history"], 3),
             "checkpointed": {"mode": "state checkpoint every 100 steps, each segment recomputed",
                              "grads_per_s": round(1.0 / t_rc, 4), "cost_over_forward": round(t_rc / t_fwd, 2),
+                             "first_call_seconds": round(first["recompute"], 3),
                              "identical": bool(J_rc == J and (g_rc == g).all())},
-            "note": "wall clock around the public-API calls, host-synchronised"}
+            "note": "wall clock around the public-API calls, host-synchronised; second call of each mode "
+                    "(the first grows the device memory pool, first_call_seconds)"}
 
 
 def run_batched(args):
