@@ -335,6 +335,35 @@ def run_adjoint(args):
                     "(the first grows the device memory pool, first_call_seconds)"}
 
 
+def run_point_dipole(args):
+    """The 128^3 point-dipole configuration at full length (1000 steps, 10-cell
+    CPML, dielectric sphere, 16 probe traces recorded every step): forward rate
+    with the engine configuration chosen by the autotuner, CUDA events on the
+    context stream."""
+    import torch
+    from dtmaxwell4_b200 import Simulation, scenarios
+    sc = scenarios.point_dipole_sphere()
+    s = Simulation(sc["cfg"])
+    scenarios.apply(s, sc)
+    tuned = s.autotune(20)
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.sync()
+    e0.record(stream)
+    s.step(sc["steps"])
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    tr = s.read_probes()
+    s.close()
+    c = sc["cfg"]
+    return {"workload": sc["desc"] + ", %d steps, %d probe traces" % (sc["steps"], tr.shape[0]),
+            "engine": "engine %d, x chunk %d, chosen by dtmx_autotune" % (tuned[0], tuned[2]),
+            "gcell_per_s": round(c.nx * c.ny * c.nz * sc["steps"] / (ms * 1e-3) / 1e9, 3),
+            "ms_per_step": round(ms / sc["steps"], 4),
+            "note": "50 MB of fields: L2-resident, issue/latency-bound (profiles/h_e_kernel_plain_cpml_128.md)"}
+
+
 def run_batched(args):
     """Independent design-block instances (edges from {64..256}, 8 blocks,
     one dipole, 10-cell CPML): one-at-a-time forward+adjoint loop against the
@@ -482,7 +511,8 @@ def main():
     import torch
     if args.extras_only:
         if rank == 0:
-            ex = {} if args.gyro_only else {"adjoint": run_adjoint(args), "batched": run_batched(args)}
+            ex = {} if args.gyro_only else {"point_dipole": run_point_dipole(args), "adjoint": run_adjoint(args),
+                                            "batched": run_batched(args)}
             if not args.no_gyro:
                 ex["gyro_purcell"] = run_gyro_purcell(args)
             print(json.dumps(ex))
@@ -497,6 +527,7 @@ def main():
                "sample": "%d time steps of the %d^3 workload (oracle FP32, %.1f s)" % (args.cpu_steps, args.n, dt)}
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
+        extras["point_dipole"] = run_point_dipole(args)
         extras["adjoint"] = run_adjoint(args)
         extras["batched"] = run_batched(args)
         if not args.no_gyro:
