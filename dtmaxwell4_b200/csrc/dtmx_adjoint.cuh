@@ -58,6 +58,8 @@ __global__ void adj_w_kernel(Params p, AdjDev A) {
   const int idx[3] = {i, j, k};
   const bool cpml = p.ab.kind == 1;
   const long long di = updH ? -1 : design_index(p, i, j, k);
+  int si[3] = {-1, -1, -1};
+  if (cpml) node_slabs(p, i, j, k, si);
   float lam[3];
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -74,10 +76,10 @@ __global__ void adj_w_kernel(Params p, AdjDev A) {
       float sg = t == 0 ? 1.f : -1.f;
       if (updH) sg = -sg;
       float ld = lam[c];
-      if (cpml && in_slab(p, a, idx[a])) {
+      if (si[a] >= 0) {
         const int h = 2 * idx[a] + comp_off(cu, a);
         const float al = __ldg(p.ab.c1[a] + h), gk = __fadd_rn(__ldg(p.ab.c2[a] + h), al);
-        ld = __fmaf_rn(gk, ld, __fmul_rn(al, A.lpsi[a][slot_of(cu, a)][slab_index(p, a, i, j, k)]));
+        ld = __fmaf_rn(gk, ld, __fmul_rn(al, A.lpsi[a][slot_of(cu, a)][si[a]]));
       }
       A.w[c][t][id] = __fmul_rn(__fmul_rn(sg * p.cdt[a], ie), ld);
     }
@@ -85,14 +87,13 @@ __global__ void adj_w_kernel(Params p, AdjDev A) {
   if (!cpml) return;
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    if (!in_slab(p, a, idx[a])) continue;
-    const long long si = slab_index(p, a, i, j, k);
+    if (si[a] < 0) continue;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const int cu = cu0 + c, sl = slot_of(cu, a);
       if (sl < 0) continue;
       const float b = __ldg(p.ab.c0[a] + 2 * idx[a] + comp_off(cu, a));
-      A.lpsi[a][sl][si] = __fmul_rn(b, __fadd_rn(lam[c], A.lpsi[a][sl][si]));
+      A.lpsi[a][sl][si[a]] = __fmul_rn(b, __fadd_rn(lam[c], A.lpsi[a][sl][si[a]]));
     }
   }
 }
