@@ -61,12 +61,18 @@ struct Pipe {
   static constexpr int OFF_MAT = OFF_OWN + 3 * OWN_N;
   static constexpr int STAGE = OFF_MAT + (ISH ? 0 : 3 * OWN_N / 4);   // floats, multiple of 32
   static constexpr unsigned BYTES = (S::TA::NV + S::TB::NV + S::TC::NV + 3 * OWN_N) * 4 + (ISH ? 0 : 3 * OWN_N);
-  // planes beyond i needed by plane i (x taps): H step order 4: +1; E step: +2 (order 4) / +1 (order 2)
-  static constexpr int AHEAD = ISH ? (ORDER == 4 ? 1 : 0) : (ORDER == 4 ? 2 : 1);
-  static constexpr int BEHIND = ISH ? (ORDER == 4 ? 2 : 1) : (ORDER == 4 ? 1 : 0);
-  static constexpr int LEAD = ISH ? 2 : 1;             // planes in flight beyond the resident ones
+  // The H step walks a chunk upwards in x, the E step downwards (the E update
+  // reads only H, so the order of its planes is free).  Plane i needs its own
+  // stage, AHEAD further planes along the walk (x taps not reached yet) and
+  // BEHIND planes already passed (kept in the register queue): H taps -R..R-1
+  // and E taps -(R-1)..R both give AHEAD = R-1 and BEHIND = R along their walk,
+  // so each keeps LEAD planes in flight beyond the resident ones.
+  static constexpr int DIR = ISH ? 1 : -1;             // direction of the walk along x
+  static constexpr int AHEAD = ORDER == 4 ? 1 : 0;
+  static constexpr int BEHIND = ORDER == 4 ? 2 : 1;
+  static constexpr int LEAD = 2;                       // planes in flight beyond the resident ones
   static constexpr int NST = AHEAD + 1 + LEAD;
-  static constexpr int BASE = ISH ? 2 : 1;             // queue slot of plane i (dstencil taps v0..v3)
+  static constexpr int BASE = ISH ? 2 : 1;             // queue slot of x offset 0 (dstencil taps v0..v3)
   static constexpr size_t SMEM_BYTES = (size_t)NST * STAGE * 4 + sizeof(MatShared) + NST * 8 + 128;
 };
 
@@ -126,13 +132,15 @@ template <int ORDER, bool ISH>
 __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, float* dsm) {
   using P = Pipe<ORDER, ISH>;
   using S = typename P::S;
-  constexpr int NST = P::NST, AHEAD = P::AHEAD, BEHIND = P::BEHIND, BASE = P::BASE, LEAD = P::LEAD;
+  constexpr int NST = P::NST, AHEAD = P::AHEAD, BEHIND = P::BEHIND, BASE = P::BASE, LEAD = P::LEAD, DIR = P::DIR;
   MatShared& ms = *reinterpret_cast<MatShared*>(dsm + NST * P::STAGE);
   uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(&ms) + sizeof(MatShared));
   const int tz = threadIdx.x, w = threadIdx.y, tid = w * TZ + tz;
   const int k0 = blockIdx.x * TZ, j0 = blockIdx.y * TYT;
   const int xa = p.x0 + blockIdx.z * p.xchunk;
   const int xb = min(xa + p.xchunk, p.x1);
+  const int len = xb - xa;
+  const int i0 = DIR > 0 ? xa : xb - 1;      // first plane of the walk; step t works on plane i0 + DIR t
   if (tid == 0) {
     for (int q = 0; q < NST; q++) mbar_init(&bars[q], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -149,24 +157,31 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
   for (int r = 0; r < RY; r++)
 #pragma unroll
     for (int q = 0; q < 4; q++) { qb[r][q] = 0.f; qc[r][q] = 0.f; }
-  for (int q = 0; q < BEHIND; q++) {
+  // the BEHIND planes before the first one of the walk, from global memory
+  for (int b = 1; b <= BEHIND; b++) {
     float tb[RY], tcv[RY];
-    const int ip = xa - BEHIND + q;
+    const int ip = i0 - DIR * b;
     const bool f = yz_in && ip >= p.g.all_lo[0] && ip <= p.g.all_hi[0];
     load_xtaps<0>(p, cb, ip, j0, k0, f, tb);
     load_xtaps<0>(p, cc, ip, j0, k0, f, tcv);
 #pragma unroll
-    for (int r = 0; r < RY; r++) { qb[r][BASE - BEHIND + q] = tb[r]; qc[r][BASE - BEHIND + q] = tcv[r]; }
+    for (int r = 0; r < RY; r++) { qb[r][BASE - DIR * b] = tb[r]; qc[r][BASE - DIR * b] = tcv[r]; }
   }
-  const int last = xb - 1 + AHEAD;    // last plane that has to be staged
-  for (int ip = xa; ip < xa + AHEAD + LEAD && ip <= last; ip++)
-    stage_plane<ORDER, ISH, 0>(p, m, dsm + (ip % NST) * P::STAGE, &bars[ip % NST], ip, j0, k0,
+  // stage number s holds plane i0 + DIR s in slot s % NST (its (s / NST)-th use)
+  const int slast = len - 1 + AHEAD;         // last stage number that has to be staged
+  for (int sq = 0; sq < AHEAD + LEAD && sq <= slast; sq++) {
+    const int ip = i0 + DIR * sq;
+    stage_plane<ORDER, ISH, 0>(p, m, dsm + (sq % NST) * P::STAGE, &bars[sq % NST], ip, j0, k0,
                                yz_safe && plane_safe_x(p.g, ip));
-  for (int i = xa; i < xb; i++) {
-    const int ipre = i + AHEAD + LEAD;
-    if (ipre <= last)
-      stage_plane<ORDER, ISH, 0>(p, m, dsm + (ipre % NST) * P::STAGE, &bars[ipre % NST], ipre, j0, k0,
+  }
+  for (int t = 0; t < len; t++) {
+    const int i = i0 + DIR * t;
+    const int spre = t + AHEAD + LEAD;
+    if (spre <= slast) {
+      const int ipre = i0 + DIR * spre;
+      stage_plane<ORDER, ISH, 0>(p, m, dsm + (spre % NST) * P::STAGE, &bars[spre % NST], ipre, j0, k0,
                                  yz_safe && plane_safe_x(p.g, ipre));
+    }
     // values that do not depend on the staged tiles are loaded before the stage
     // wait, so their latency overlaps it: the plane's uniform material and the
     // absorber auxiliaries of the thread's nodes
@@ -174,12 +189,12 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
     float old[RY][3][3];
     const bool tab = tile_absorber(p, i, j0, k0);
     if (tab) absorb_prefetch<ISH>(p, i, j0, k0, old);
-    // planes i..i+AHEAD-1 were waited for in earlier iterations (all of them at the
+    // stages t..t+AHEAD-1 were waited for in earlier steps (all of them at the
     // start); one thread polls the stage barriers and the CTA barrier then releases
     // everybody (and orders the staged data for them) without spinning issue slots
     if (tid == 0)
-      for (int q = (i == xa ? 0 : AHEAD); q <= AHEAD; q++)
-        mbar_wait(&bars[(i + q) % NST], (unsigned)(((i + q - xa) / NST) & 1), p.err);
+      for (int a = (t == 0 ? 0 : AHEAD); a <= AHEAD; a++)
+        mbar_wait(&bars[(t + a) % NST], (unsigned)(((t + a) / NST) & 1), p.err);
     __syncthreads();
     // every node of the tile in the array and live, every tap in range or zero: in the box
     // geometry a full tile (taps outside the array read the TMA zero fill)
@@ -189,13 +204,13 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
     for (int r = 0; r < RY; r++) {
       const int y = w + TW * r;
 #pragma unroll
-      for (int q = 0; q <= AHEAD; q++) {
-        const float* st = dsm + ((i + q) % NST) * P::STAGE;
-        qb[r][BASE + q] = S::TB::at(st + P::OFF_B, y, tz, 0, 0);
-        qc[r][BASE + q] = S::TC::at(st + P::OFF_C, y, tz, 0, 0);
+      for (int a = 0; a <= AHEAD; a++) {
+        const float* st = dsm + ((t + a) % NST) * P::STAGE;
+        qb[r][BASE + DIR * a] = S::TB::at(st + P::OFF_B, y, tz, 0, 0);
+        qc[r][BASE + DIR * a] = S::TC::at(st + P::OFF_C, y, tz, 0, 0);
       }
     }
-    const float* cur = dsm + (i % NST) * P::STAGE;
+    const float* cur = dsm + (t % NST) * P::STAGE;
     const uint8_t* cmat = reinterpret_cast<const uint8_t*>(cur + P::OFF_MAT);
     if (fast && um >= 0 && !tab)
       plane_update<ORDER, ISH, 1>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
@@ -203,10 +218,17 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
       plane_update<ORDER, ISH, 2>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
     else
       plane_update<ORDER, ISH, 0>(p, i, j0, k0, cur, qb, qc, cur + P::OFF_OWN, cmat, ms, fast, um, old);
+    // the queue moves one plane along the walk
 #pragma unroll
-    for (int r = 0; r < RY; r++)
+    for (int r = 0; r < RY; r++) {
+      if (DIR > 0) {
 #pragma unroll
-      for (int q = 0; q < 3; q++) { qb[r][q] = qb[r][q + 1]; qc[r][q] = qc[r][q + 1]; }
+        for (int q = 0; q < 3; q++) { qb[r][q] = qb[r][q + 1]; qc[r][q] = qc[r][q + 1]; }
+      } else {
+#pragma unroll
+        for (int q = 3; q > 0; q--) { qb[r][q] = qb[r][q - 1]; qc[r][q] = qc[r][q - 1]; }
+      }
+    }
     __syncthreads();
   }
 }
