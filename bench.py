@@ -237,7 +237,7 @@ def run_ours(args, rank, world):
         # kernels on the 256^3 case of this workload, scaled by cells
         traffic = None
         if args.workload == "drude":
-            traffic = int((38.6 if kname == "e_kernel" else 38.5) * ncell)
+            traffic = int((38.5 if kname == "e_kernel" else 38.6) * ncell)
         roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
                 "traffic_source": "profiles/e_h_kernel_drude_sphere_tfsf_256.md, dram bytes per cell x cells",
