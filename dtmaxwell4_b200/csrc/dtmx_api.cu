@@ -685,6 +685,7 @@ extern "C" int dtmx_set_tfsf(dtmx_ctx* ctx, const dtmx_tfsf* s) {
           }
           if (empty) continue;
           jb.cells = (long long)(jb.hi[0] - jb.lo[0] + 1) * (jb.hi[1] - jb.lo[1] + 1) * (jb.hi[2] - jb.lo[2] + 1);
+          if (jb.cells >= (long long)INT32_MAX) return fail(ctx, DTMX_ERR_UNSUPPORTED, "TF/SF correction shell of more than 2^31 nodes");
           T.job[hs][T.njob[hs]++] = jb;
         }
       }

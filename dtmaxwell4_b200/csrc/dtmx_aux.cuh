@@ -155,12 +155,14 @@ __global__ void tfsf_kernel(Params p, TfsfDev t, const long long* d_step, int is
   const int r = blockIdx.y;
   if (r >= t.njob[hs]) return;
   const TfsfJob& jb = t.job[hs][r];
-  const long long cell = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (cell >= jb.cells) return;
+  // a job is a thin shell (cells < 2^31, checked when the jobs are built): 32-bit indexing
+  const int cell = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= (int)jb.cells) return;
   const int ey = jb.hi[1] - jb.lo[1] + 1, ez = jb.hi[2] - jb.lo[2] + 1;
-  const int i = jb.lo[0] + (int)(cell / ((long long)ey * ez));
-  const int j = jb.lo[1] + (int)((cell / ez) % ey);
-  const int k = jb.lo[2] + (int)(cell % ez);
+  const int i = jb.lo[0] + cell / (ey * ez);
+  const int rest = cell - (i - jb.lo[0]) * (ey * ez);
+  const int j = jb.lo[1] + rest / ez;
+  const int k = jb.lo[2] + (rest - (j - jb.lo[1]) * ez);
   const int c = jb.c;
   if (!is_live(p.g, c, i, j, k)) return;
   for (int q = 0; q < r; q++)
