@@ -5,9 +5,10 @@
 // rows per thread).  The y/z taps of the derivatives come from shared-memory
 // copies of the neighbouring field's plane tile; the x taps come from the
 // caller (a register queue when a CTA streams along x, direct loads in the
-// wavefront engine).  Absorber (CPML or the reference split-field PML),
-// material coefficients and the Drude/Lorentz ADE (reference countDisp) are
-// applied in the same pass.
+// wavefront engine).  Absorber (CPML or the reference split-field PML) and
+// material coefficients are applied in the same pass; the Drude/Lorentz ADE
+// nodes (reference countDisp) and the gyrotropic current are finished by a
+// pass over the dispersive box after the E half step.
 //
 // Update equations (reference generator genAlg.py:182-301, defs.h:3-13):
 //   H -= dt * curl E,  E += dt/eps * curl H  (c = 1),

@@ -1,11 +1,12 @@
 // dtmx_stream.cuh -- TMA-fed streaming kernels (one launch per half step).
 //
-// A CTA owns one (z,y) tile column and an x chunk.  For every plane it needs
-// the three source-field tiles (with y/z halo), the own values of the three
-// updated components and, for the E step, their material indices.  One
+// A CTA owns one (z,y) tile column and an x chunk, which the H step walks
+// upwards and the E step downwards.  For every plane it needs the three
+// source-field tiles (with y/z halo), the own values of the three updated
+// components and, for the E step on mixed planes, their material indices.  One
 // elected thread fetches all of them with cp.async.bulk.tensor (TMA, no
 // multicast) into a ring of NST shared-memory stages, LEAD planes ahead of
-// the plane being updated; completion is tracked per stage by an mbarrier
+// the ones the update reads; completion is tracked per stage by an mbarrier
 // with a transaction count.  Out-of-array boxes are zero-filled by the TMA
 // unit, which is exactly the zero-outside boundary; planes whose taps reach a
 // mirror boundary are staged element-wise with the boundary rules instead.
