@@ -77,10 +77,11 @@ struct Pipe {
   static constexpr size_t SMEM_BYTES = (size_t)NST * STAGE * 4 + sizeof(MatShared) + NST * 8 + 128;
 };
 
-// Stage plane ip into stage buffer st (all threads call; uniform fast flag).
+// Stage plane ip into stage buffer st (all threads call; uniform fast flag);
+// um: the plane tile's uniform material (< 0: mixed, the material tile is staged too).
 template <int ORDER, bool ISH, int LD>
 __device__ __forceinline__ void stage_plane(const Params& p, const TmaMaps& m, float* st, uint64_t* bar, int ip, int j0,
-                                            int k0, bool fast) {
+                                            int k0, bool fast, int um) {
   using P = Pipe<ORDER, ISH>;
   using S = typename P::S;
   const int c0 = ISH ? 0 : 3;       // source components
@@ -89,8 +90,7 @@ __device__ __forceinline__ void stage_plane(const Params& p, const TmaMaps& m, f
   if (fast) {
     if (tid == 0) {
       // the material tile is needed only when this plane is updated with mixed materials
-      const bool want_mat = !ISH && ip >= 0 && ip < p.g.n[0] &&
-                            __ldg(p.umat + ((long long)ip * p.nty + blockIdx.y) * p.ntz + blockIdx.x) < 0;
+      const bool want_mat = !ISH && ip >= 0 && ip < p.g.n[0] && um < 0;
       mbar_arrive_expect_tx(bar, P::BYTES - (ISH || want_mat ? 0u : 3u * OWN_N));
       tma_load_3d(st + P::OFF_A, &m.src[c0], k0 - ZO, j0 - S::YL, ip, bar);
       tma_load_3d(st + P::OFF_B, &m.src[c0 + 1], k0 - ZO, j0, ip, bar);
@@ -142,12 +142,31 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
   const int xb = min(xa + p.xchunk, p.x1);
   const int len = xb - xa;
   const int i0 = DIR > 0 ? xa : xb - 1;      // first plane of the walk; step t works on plane i0 + DIR t
+  // the uniform-material entries of the planes this CTA stages (stage number s),
+  // read once so that the elected thread issues each stage without a dependent load
+  constexpr int UMC = 128;
+  __shared__ signed char umc[UMC];
+  const int slast = len - 1 + AHEAD;         // last stage number that has to be staged
   if (tid == 0) {
     for (int q = 0; q < NST; q++) mbar_init(&bars[q], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
-  if (!ISH) load_matshared(ms, p);
+  if (!ISH) {
+    load_matshared(ms, p);
+    for (int sq = tid; sq <= slast && sq < UMC; sq += NTHR) {
+      const int ip = i0 + DIR * sq;
+      umc[sq] = (ip >= 0 && ip < p.g.n[0]) ? __ldg(p.umat + ((long long)ip * p.nty + blockIdx.y) * p.ntz + blockIdx.x)
+                                          : (signed char)0;
+    }
+  }
   __syncthreads();
+  // uniform material of stage number sq (0 for planes outside the array)
+  auto um_of = [&](int sq) -> int {
+    if (ISH) return 0;
+    if (sq < UMC) return umc[sq];
+    const int ip = i0 + DIR * sq;
+    return (ip >= 0 && ip < p.g.n[0]) ? (int)__ldg(p.umat + ((long long)ip * p.nty + blockIdx.y) * p.ntz + blockIdx.x) : 0;
+  };
   const bool yz_safe = tile_safe_yz(p.g, j0, k0);
   // (fast path of the per-node update additionally needs every node and tap live)
   const bool yz_in = j0 - 2 >= p.g.all_lo[1] && j0 + TYT + 1 <= p.g.all_hi[1] && k0 - 2 >= p.g.all_lo[2] &&
@@ -169,11 +188,10 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
     for (int r = 0; r < RY; r++) { qb[r][BASE - DIR * b] = tb[r]; qc[r][BASE - DIR * b] = tcv[r]; }
   }
   // stage number s holds plane i0 + DIR s in slot s % NST (its (s / NST)-th use)
-  const int slast = len - 1 + AHEAD;         // last stage number that has to be staged
   for (int sq = 0; sq < AHEAD + LEAD && sq <= slast; sq++) {
     const int ip = i0 + DIR * sq;
     stage_plane<ORDER, ISH, 0>(p, m, dsm + (sq % NST) * P::STAGE, &bars[sq % NST], ip, j0, k0,
-                               yz_safe && plane_safe_x(p.g, ip));
+                               yz_safe && plane_safe_x(p.g, ip), um_of(sq));
   }
   for (int t = 0; t < len; t++) {
     const int i = i0 + DIR * t;
@@ -181,12 +199,12 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
     if (spre <= slast) {
       const int ipre = i0 + DIR * spre;
       stage_plane<ORDER, ISH, 0>(p, m, dsm + (spre % NST) * P::STAGE, &bars[spre % NST], ipre, j0, k0,
-                                 yz_safe && plane_safe_x(p.g, ipre));
+                                 yz_safe && plane_safe_x(p.g, ipre), um_of(spre));
     }
     // values that do not depend on the staged tiles are loaded before the stage
     // wait, so their latency overlaps it: the plane's uniform material and the
     // absorber auxiliaries of the thread's nodes
-    const int um = ISH ? 0 : (int)__ldg(p.umat + ((long long)i * p.nty + blockIdx.y) * p.ntz + blockIdx.x);
+    const int um = um_of(t);
     float old[RY][3][3];
     const bool tab = tile_absorber(p, i, j0, k0);
     if (tab) absorb_prefetch<ISH>(p, i, j0, k0, old);
