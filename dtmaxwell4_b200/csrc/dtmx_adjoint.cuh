@@ -66,8 +66,9 @@ __global__ void adj_w_kernel(Params p, AdjDev A) {
     const int cu = cu0 + c;
     float ie = 1.f;
     if (!updH) {
-      const int m = p.mat[cu] ? (int)p.mat[cu][id] : 0;
-      ie = di >= 0 ? p.des_ie[cu][di] : p.mt->inv_eps[m][cu];
+      // (material, design and table values are constant during the adjoint: read-only path)
+      const int m = p.mat[cu] ? (int)__ldg(p.mat[cu] + id) : 0;
+      ie = di >= 0 ? __ldg(p.des_ie[cu] + di) : __ldg(&p.mt->inv_eps[m][cu]);
     }
     lam[c] = A.lam[cu][id];
 #pragma unroll
