@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(FLUX_THREADS) ntff_kernel(NtffFaces F, const d
 __device__ __forceinline__ float gyro_old(const Params& p, int cur, int c, int i, int j, int k) {
   const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
   if (bi < 0 || bi >= p.ade.n[0] || bj < 0 || bj >= p.ade.n[1] || bk < 0 || bk >= p.ade.n[2]) return 0.f;
-  return p.ade.Jg[cur][c][((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk];
+  return __ldg(p.ade.Jg[cur][c] + ((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk);
 }
 
 // Thread layout of the passes over the ADE box: (threadIdx.x, blockIdx.x) = z,
@@ -521,24 +521,25 @@ __global__ void gyro_current_kernel(Params p, int cur) {
     const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const int m = p.mat[c] ? (int)p.mat[c][id] : 0;
-      if (mt.gjc[m] == 0.f) continue;
-      const float E = p.f[c][id], Jo = p.ade.Jg[cur][c][q];
+      // (E, the old current, materials and table are read-only in this pass)
+      const int m = p.mat[c] ? (int)__ldg(p.mat[c] + id) : 0;
+      if (__ldg(&mt.gjc[m]) == 0.f) continue;
+      const float E = __ldg(p.f[c] + id), Jo = __ldg(p.ade.Jg[cur][c] + q);
       float t;
       if (c == 0) {
         const float avg = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(__fadd_rn(gyro_old(p, cur, 1, i - 1, j, k), gyro_old(p, cur, 1, i, j, k)),
                                                                gyro_old(p, cur, 1, i - 1, j + 1, k)),
                                                      gyro_old(p, cur, 1, i, j + 1, k)));
-        t = __fmaf_rn(mt.gC[m], Jo, __fmul_rn(mt.gS[m], avg));
+        t = __fmaf_rn(__ldg(&mt.gC[m]), Jo, __fmul_rn(__ldg(&mt.gS[m]), avg));
       } else if (c == 1) {
         const float avg = __fmul_rn(0.25f, __fadd_rn(__fadd_rn(__fadd_rn(gyro_old(p, cur, 0, i, j - 1, k), gyro_old(p, cur, 0, i + 1, j - 1, k)),
                                                                gyro_old(p, cur, 0, i, j, k)),
                                                      gyro_old(p, cur, 0, i + 1, j, k)));
-        t = __fmaf_rn(mt.gC[m], Jo, -__fmul_rn(mt.gS[m], avg));
+        t = __fmaf_rn(__ldg(&mt.gC[m]), Jo, -__fmul_rn(__ldg(&mt.gS[m]), avg));
       } else {
         t = Jo;
       }
-      p.ade.Jg[1 - cur][c][q] = __fmaf_rn(mt.gA[m], t, __fmul_rn(mt.gB[m], E));
+      p.ade.Jg[1 - cur][c][q] = __fmaf_rn(__ldg(&mt.gA[m]), t, __fmul_rn(__ldg(&mt.gB[m]), E));
     }
   }
 }
@@ -560,8 +561,9 @@ __global__ void ade_node_kernel(Params p) {
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       if (!is_live(p.g, c, i, j, k)) continue;
-      const int m = p.mat[c] ? (int)p.mat[c][id] : 0;
-      const int np = mt.npoles[m];
+      // (materials, table, H and the new current are read-only in this pass)
+      const int m = p.mat[c] ? (int)__ldg(p.mat[c] + id) : 0;
+      const int np = __ldg(&mt.npoles[m]);
       if (np > 0) {
         float d[3] = {0.f, 0.f, 0.f};
 #pragma unroll
@@ -577,7 +579,7 @@ __global__ void ade_node_kernel(Params p) {
             m3[a] += o - 1;                          // E taps at -1..+2
             if (BOX) {
               const long long sa = a == 0 ? p.g.sx : a == 1 ? p.g.sy : 1;
-              v[o] = (m3[a] >= 0 && m3[a] < p.g.n[a]) ? p.f[g][id + (long long)(o - 1) * sa] : 0.f;
+              v[o] = (m3[a] >= 0 && m3[a] < p.g.n[a]) ? __ldg(p.f[g] + id + (long long)(o - 1) * sa) : 0.f;
             } else {
               v[o] = fetch<1>(p, g, m3[0], m3[1], m3[2]);
             }
@@ -586,8 +588,8 @@ __global__ void ade_node_kernel(Params p) {
         }
         (void)idx;
         p.f[c][id] = ade_update(p, c, m, np, q, sum3(d[0], d[1], d[2]), p.f[c][id]);
-      } else if (mt.gjc[m] != 0.f) {
-        p.f[c][id] = __fsub_rn(p.f[c][id], __fmul_rn(mt.gjc[m], p.ade.Jg[p.ade.gnew][c][q]));
+      } else if (__ldg(&mt.gjc[m]) != 0.f) {
+        p.f[c][id] = __fsub_rn(p.f[c][id], __fmul_rn(__ldg(&mt.gjc[m]), __ldg(p.ade.Jg[p.ade.gnew][c] + q)));
       }
     }
   }
