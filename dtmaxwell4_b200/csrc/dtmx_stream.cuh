@@ -252,14 +252,17 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
   }
 }
 
+// CTAs per SM that shared memory allows: order 2 (3-stage ring) 4, order 4 (4
+// stages) 3, which leaves the order-4 kernels up to 85 registers (no spills in
+// their plane loops)
 template <int ORDER>
-__global__ void __launch_bounds__(NTHR) h_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
+__global__ void __launch_bounds__(NTHR, ORDER == 4 ? 3 : 4) h_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
   extern __shared__ __align__(128) float dsm[];
   stream_body<ORDER, true>(p, m, dsm);
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(NTHR) e_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
+__global__ void __launch_bounds__(NTHR, ORDER == 4 ? 3 : 4) e_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
   extern __shared__ __align__(128) float dsm[];
   stream_body<ORDER, false>(p, m, dsm);
 }
