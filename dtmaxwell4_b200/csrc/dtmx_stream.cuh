@@ -71,7 +71,9 @@ struct Pipe {
   static constexpr int DIR = ISH ? 1 : -1;             // direction of the walk along x
   static constexpr int AHEAD = ORDER == 4 ? 1 : 0;
   static constexpr int BEHIND = ORDER == 4 ? 2 : 1;
-  static constexpr int LEAD = 2;                       // planes in flight beyond the resident ones
+  // planes in flight beyond the resident ones: order 4 keeps one, so that its
+  // 3-stage ring leaves room for 4 CTAs per SM (measured faster with absorbers)
+  static constexpr int LEAD = ORDER == 4 ? 1 : 2;
   static constexpr int NST = AHEAD + 1 + LEAD;
   static constexpr int BASE = ISH ? 2 : 1;             // queue slot of x offset 0 (dstencil taps v0..v3)
   static constexpr size_t SMEM_BYTES = (size_t)NST * STAGE * 4 + sizeof(MatShared) + NST * 8 + 128;
@@ -252,17 +254,15 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
   }
 }
 
-// CTAs per SM that shared memory allows: order 2 (3-stage ring) 4, order 4 (4
-// stages) 3, which leaves the order-4 kernels up to 85 registers (no spills in
-// their plane loops)
+// 4 CTAs per SM: what shared memory allows for the 3-stage rings (64 registers)
 template <int ORDER>
-__global__ void __launch_bounds__(NTHR, ORDER == 4 ? 3 : 4) h_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
+__global__ void __launch_bounds__(NTHR, 4) h_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
   extern __shared__ __align__(128) float dsm[];
   stream_body<ORDER, true>(p, m, dsm);
 }
 
 template <int ORDER>
-__global__ void __launch_bounds__(NTHR, ORDER == 4 ? 3 : 4) e_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
+__global__ void __launch_bounds__(NTHR, 4) e_kernel(const __grid_constant__ Params p, const __grid_constant__ TmaMaps m) {
   extern __shared__ __align__(128) float dsm[];
   stream_body<ORDER, false>(p, m, dsm);
 }
