@@ -9,7 +9,9 @@ ABI_VERSION = 1
 
 (OK, ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_NONFINITE, ERR_TIMEOUT, ERR_STATE, ERR_UNSUPPORTED, ERR_NODEVICE,
  ERR_TOO_LARGE) = range(10)
-NOALLOC_MAX_ELEMS = 1 << 24
+NOALLOC_BLOCK_ELEMS = 4096
+NOALLOC_MAX_BLOCKS = 4096
+NOALLOC_MAX_ELEMS = NOALLOC_BLOCK_ELEMS * NOALLOC_MAX_BLOCKS
 EX, EY, EZ, HX, HY, HZ = range(6)
 COMP_NAMES = ("Ex", "Ey", "Ez", "Hx", "Hy", "Hz")
 GEOM_BOX, GEOM_REFERENCE = 0, 1

@@ -8,12 +8,15 @@
 // the device).  Such a caller passes its own device arrays in and gets a host
 // count back; the scratch the reduction needs is a fixed array below.
 //
-// Scratch: g_partial holds one count per block plus the final total.  It is a
-// file-scope __device__ array, so every GPU that loads this library holds it
-// (DTMX_NOALLOC_MAX_ELEMS / 4096 + 1 eight-byte words, 32 KiB) until the
-// process exits.  Every call overwrites the entries it uses and the total, so
-// nothing carries over from the previous call; two calls whose kernels overlap
-// on the GPU (different host threads, same device) race on it.
+// Scratch: g_partial holds one count per block of DTMX_NOALLOC_BLOCK_ELEMS
+// elements plus the final total.  It is a file-scope __device__ array, so every
+// GPU that loads this library holds it (DTMX_NOALLOC_MAX_BLOCKS + 1 eight-byte
+// words, 32 KiB) until the process exits.  Each field is cut into its own
+// blocks (the last one partial), so the limit is on the block count:
+// nfields * ceil(nelem / DTMX_NOALLOC_BLOCK_ELEMS) <= DTMX_NOALLOC_MAX_BLOCKS.
+// Every call overwrites the entries it uses and the total, so nothing carries
+// over from the previous call; two calls whose kernels overlap on the GPU
+// (different host threads, same device) race on it.
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -24,7 +27,8 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kPerThread = 16;
 constexpr long long kBlockElems = (long long)kThreads * kPerThread;   // 4096 elements per block
-constexpr int kMaxBlocks = (int)(DTMX_NOALLOC_MAX_ELEMS / kBlockElems);
+static_assert(kBlockElems == DTMX_NOALLOC_BLOCK_ELEMS, "block size of the header");
+constexpr int kMaxBlocks = DTMX_NOALLOC_MAX_BLOCKS;
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned long long g_partial[kMaxBlocks + 1];
@@ -72,7 +76,9 @@ __global__ void sum_blocks(unsigned long long* partial, int nblocks) {
 extern "C" int dtmx_count_nonfinite_noalloc(const float* const* d_fields, int nfields, int64_t nelem,
                                             int64_t* count_out) {
   if (!d_fields || nfields < 1 || nelem < 0 || !count_out) return DTMX_ERR_INVALID;
-  if ((long long)nfields * nelem > DTMX_NOALLOC_MAX_ELEMS) return DTMX_ERR_TOO_LARGE;
+  // blocks per field, rounded up per field; divided before any product, so no overflow
+  const long long per_field = nelem / kBlockElems + (nelem % kBlockElems != 0);
+  if (per_field > kMaxBlocks / nfields) return DTMX_ERR_TOO_LARGE;
   for (int f = 0; f < nfields; f++)
     if (!d_fields[f] && nelem > 0) return DTMX_ERR_INVALID;
   int dev = 0;
@@ -85,7 +91,6 @@ extern "C" int dtmx_count_nonfinite_noalloc(const float* const* d_fields, int nf
     g_scratch[dev] = static_cast<unsigned long long*>(q);
   }
   unsigned long long* partial = g_scratch[dev];
-  const long long per_field = (nelem + kBlockElems - 1) / kBlockElems;
   int base = 0;
   for (int f = 0; f < nfields && per_field > 0; f++) {
     count_blocks<<<(unsigned)per_field, kThreads>>>(d_fields[f], nelem, base, partial);

@@ -377,15 +377,24 @@ int  dtmx_load_state(dtmx_ctx* ctx, const char* path);
  * allocating library routine).  For callers that cannot allocate: processes
  * whose device memory is reserved by another allocator, or health-check
  * threads that must stay out of the allocator.  No counterpart in the
- * reference.  The reduction's scratch is a fixed file-scope device array, so:
- *   - nfields*nelem must not exceed DTMX_NOALLOC_MAX_ELEMS, else
- *     DTMX_ERR_TOO_LARGE (nothing is launched);
+ * reference.  The reduction's scratch is a fixed file-scope device array of
+ * one count per block of DTMX_NOALLOC_BLOCK_ELEMS elements, so:
+ *   - each field is cut into ceil(nelem / DTMX_NOALLOC_BLOCK_ELEMS) blocks
+ *     and nfields times that must not exceed DTMX_NOALLOC_MAX_BLOCKS, else
+ *     DTMX_ERR_TOO_LARGE (nothing is launched).  That allows
+ *     DTMX_NOALLOC_MAX_ELEMS (2^24) floats in all when nelem is a multiple of
+ *     the block size, fewer otherwise;
  *   - the first call on a device looks up that array's device address with the
  *     device current; make that first call before any stream capture;
  *   - calls whose work overlaps on the GPU race on the shared array.
  * Kernels run on the legacy default stream and the count is copied back
- * synchronously into *count_out. */
-#define DTMX_NOALLOC_MAX_ELEMS (1LL << 24)
+ * synchronously into *count_out.  The legacy default stream does not wait for
+ * a context's own stream (created non-blocking): finish the work that writes
+ * the arrays first (dtmx_sync, or cudaStreamSynchronize of the writer's
+ * stream), else fields still being updated are counted. */
+#define DTMX_NOALLOC_BLOCK_ELEMS 4096LL
+#define DTMX_NOALLOC_MAX_BLOCKS 4096
+#define DTMX_NOALLOC_MAX_ELEMS (DTMX_NOALLOC_BLOCK_ELEMS * DTMX_NOALLOC_MAX_BLOCKS)
 int  dtmx_count_nonfinite_noalloc(const float* const* d_fields, int nfields, int64_t nelem, int64_t* count_out);
 
 /* Engine choice for dtmx_step: 0 = auto, 1 = one launch per half step,
