@@ -13,12 +13,20 @@ Unlike the SWIG build, the grid is not fixed at compile time: ``Np, Na, Nv``
 """
 import ctypes as C
 import math
+import struct
 
 from . import engine
 
 
+def _ftype(v):
+    """A value stored in one of the reference's ftype (float) variables."""
+    return struct.unpack("f", struct.pack("f", float(v)))[0]
+
+
 class TFSFsrc(C.Structure):
-    """TFSFsrc (py_consts.h:73-91) -- the dipole shotpoint."""
+    """TFSFsrc (py_consts.h:73-91) -- the dipole shotpoint.  Its real fields
+    are the reference's ftype (float): an assignment, and TFSFsrc::set, round
+    the value to float as the SWIG-wrapped struct does."""
     _fields_ = [
         ("tStop", C.c_double),
         ("srcXs", C.c_double), ("srcXa", C.c_double), ("srcXv", C.c_double), ("sphR", C.c_double),
@@ -32,12 +40,19 @@ class TFSFsrc(C.Structure):
         ("t0", C.c_double), ("tw", C.c_double), ("T", C.c_double),
     ]
 
+    def __setattr__(self, name, value):
+        if name in _REAL_FIELDS:
+            value = _ftype(value)
+        super().__setattr__(name, value)
+
     def set(self, c, imp, lmb):
         """TFSFsrc::set (signal.hpp:99-115)."""
         L = engine.load()
         L.dtmx_tfsfsrc_set.restype = None
         L.dtmx_tfsfsrc_set.argtypes = [C.POINTER(TFSFsrc), C.c_double, C.c_double, C.c_double]
         L.dtmx_tfsfsrc_set(C.byref(self), c, imp, lmb)
+        for name in _REAL_FIELDS:
+            setattr(self, name, getattr(self, name))
 
     def check(self):
         """TFSFsrc::check (signal.hpp:116-133); the shotpoint line prints srcXv
@@ -49,10 +64,13 @@ class TFSFsrc(C.Structure):
         print("TF/SF stops after %d steps" % int(self.tStop / cvar.dt))
 
 
+_REAL_FIELDS = tuple(n for n, t in TFSFsrc._fields_ if t is C.c_double)
+
+
 class RefGlobals(C.Structure):
     _fields_ = [("Np", C.c_int), ("Na", C.c_int), ("Nv", C.c_int), ("Ns", C.c_int), ("Ntime", C.c_int),
                 ("ds", C.c_double), ("da", C.c_double), ("dv", C.c_double), ("dt", C.c_double),
-                ("Tsteps", C.c_int)]
+                ("Tsteps", C.c_int), ("Npmlx", C.c_int), ("Npmly", C.c_int), ("Npmlz", C.c_int)]
 
 
 class _CVar:
@@ -65,8 +83,9 @@ class _CVar:
         self.Ntime = self.Ns - 3                 # params.h:50-52
         self.NyBloch = 1
         self.Npmlx, self.Npmly, self.Npmlz = 10, 10, 32
-        self.ds = self.da = self.dv = 0.005
-        self.dt = 0.002
+        # const ftype ds=0.005, da, dv, dt=0.002 (py_consts.h:71): float values
+        self.ds = self.da = self.dv = _ftype(0.005)
+        self.dt = _ftype(0.002)
         self.Tsteps = self.Ntime * 10             # DTmxw.cu:730
         self.shotpoint = TFSFsrc()
 
@@ -84,7 +103,7 @@ class _CVar:
 
     def globals(self):
         return RefGlobals(self.Np, self.Na, self.Nv, self.Ns, self.Ntime, self.ds, self.da, self.dv, self.dt,
-                          int(self.Tsteps))
+                          int(self.Tsteps), int(self.Npmlx), int(self.Npmly), int(self.Npmlz))
 
 
 cvar = _CVar()

@@ -310,14 +310,17 @@ static int setup_absorber(dtmx_ctx* ctx) {
     // K1 = K2 = 1 where gamma = 0
     for (int a = 0; a < 3; a++) t1[a].assign(2 * n[a] + 2, 1.f);
     const double V = c.spml_vmax;
-    const int KX = 60, KY = 60, KZ = 64;
+    // table lengths KNpmlx = 2 Npmlx NDT, KNpmly = 2 Npmly NDT, KNpmlz = 2 Npmlz (params.h:106-108);
+    // the slabs are Npmlx/2 and Npmly/2 rags of NDT cells and the Npmlz/2 top layers
+    const int KX = 4 * c.pml[0][0], KY = 4 * c.pml[1][0], KZ = 4 * c.pml[2][1];
+    const int XS = 2 * c.pml[0][0] - 3;                // inPMLsync (defs.h:45): Npmlx/2*2*NDT - NDT
     ab.L[0][0] = c.pml[0][0]; ab.L[0][1] = c.pml[0][1];
     ab.L[1][0] = c.pml[1][0]; ab.L[1][1] = c.pml[1][1];
     ab.L[2][0] = 0;           ab.L[2][1] = c.pml[2][1];
     for (int h = 0; h < 2 * n[0] + 2; h++) {
       int i = -1;
-      if (h < 27) i = h;                               // inPMLsync (defs.h:45)
-      else if (h >= 2 * n[0] - 27) i = h - 2 * n[0] + KX;
+      if (h < XS) i = h;
+      else if (h >= 2 * n[0] - XS) i = h - 2 * n[0] + KX;
       if (i < 0 || i >= KX) continue;
       const double k2 = 1.0 / (1.0 + 0.5 * c.dt * ref_gamma(KX / 2 - std::abs(i - KX / 2) - 3, KX / 2 - 3, c.dx, V));
       t1[0][h] = (float)k2; t0[0][h] = (float)(2.0 * k2 - 1.0);
@@ -387,6 +390,11 @@ extern "C" int dtmx_create(const dtmx_config* cfg, dtmx_ctx** out) {
   if (c.absorber == DTMX_ABS_CPML && c.geometry != DTMX_GEOM_BOX) return DTMX_ERR_UNSUPPORTED;
   if (c.absorber == DTMX_ABS_SPLIT_PML && c.geometry != DTMX_GEOM_REFERENCE) return DTMX_ERR_UNSUPPORTED;
   if (c.geometry == DTMX_GEOM_REFERENCE && (c.nx % 3 || c.ny % 3)) return DTMX_ERR_INVALID;  // DTmxw.cu:330-331
+  // split PML: whole rags along x and y on both faces, the top z face only (Npmlx/2, Npmly/2 rags, Npmlz/2 layers)
+  if (c.absorber == DTMX_ABS_SPLIT_PML &&
+      (c.pml[0][0] != c.pml[0][1] || c.pml[1][0] != c.pml[1][1] || c.pml[0][0] % 3 || c.pml[1][0] % 3 ||
+       c.pml[0][0] < 3 || c.pml[1][0] < 3 || c.pml[2][0] != 0 || c.pml[2][1] < 2))
+    return DTMX_ERR_INVALID;
   const int n[3] = {c.nx, c.ny, c.nz};
   for (int a = 0; a < 3; a++)
     for (int s = 0; s < 2; s++)

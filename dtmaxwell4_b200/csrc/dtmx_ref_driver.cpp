@@ -32,7 +32,7 @@ int ref_material(int ix, int iy, int iz, const dtmx_ref_globals* g) {
   const float dx = (float)g->ds, dy = (float)g->da, dz = (float)g->dv;
   float x = (float)(ix * 0.5 * (double)dx), y = (float)(iy * 0.5 * (double)dy), z = (float)(iz * 0.5 * (double)dz);
   const float Xc = (float)(0.5 * g->Np * NDT * (double)dx), Yc = (float)(0.5 * g->Na * NDT * (double)dy);
-  const int Npmlx = 10, Npmly = 10;
+  const int Npmlx = g->Npmlx > 0 ? g->Npmlx : 10, Npmly = g->Npmly > 0 ? g->Npmly : 10;
   if (x < (Npmlx * NDT + 100) * dx / 2 || x > g->Np * NDT * dx - (Npmlx * NDT + 100) * dx / 2 ||
       y < (Npmly * NDT + 100) * dy / 2 || y > g->Na * NDT * dy - (Npmly * NDT + 100) * dy / 2)
     return kOrg;
@@ -62,6 +62,27 @@ void ref_material_table(dtmx_material* mats) {
   mats[kAg].pole[0][3] = 0.0;
   mats[kAg].eps_inf = 1.0;                         // DispCoffsHost[IndAg].set(1, Agvec, 1, 0)
   mats[kAg].sigma = 0.0;
+}
+
+// SeismoDrops::drop (drop.cu:83-107) with DROP_DATA: Ez of the first V domain
+// of every rag, the node of cell (3x-1, 3y-1, z), z fastest within a rag.
+int write_rag_drop(const std::string& dir, int it, const dtmx_ref_globals* g, const std::vector<float>& ez) {
+  char fname[512];
+  snprintf(fname, sizeof(fname), "%s/ragEz_%05d.arr", dir.c_str(), it);
+  FILE* f = fopen(fname, "wb");
+  if (!f) return -1;
+  const int nx = 3 * g->Np, ny = 3 * g->Na, nz = g->Nv;
+  const int head[9] = {12, 0, 0, 0, 3, (int)sizeof(float), g->Nv, g->Na, g->Np};
+  bool ok = fwrite(head, sizeof(int), 9, f) == 9;
+  std::vector<float> row(nz);
+  for (int x = 0; x < g->Np && ok; x++)
+    for (int y = 0; y < g->Na && ok; y++) {
+      const int i = 3 * x - 1, j = 3 * y - 1;
+      for (int k = 0; k < nz; k++)
+        row[k] = (i >= 0 && i < nx && j >= 0 && j < ny) ? ez[((size_t)i * ny + j) * nz + k] : 0.f;
+      ok = fwrite(row.data(), sizeof(float), nz, f) == (size_t)nz;
+    }
+  return (fclose(f) == 0 && ok) ? 0 : -1;
 }
 
 struct SensorFile {
@@ -100,30 +121,38 @@ extern "C" int dtmx_ref_material_table(dtmx_material* out, int n) {
   return kNumMat;
 }
 
-// TFSFsrc::set (signal.hpp:99-115)
+// TFSFsrc::set (signal.hpp:99-115).  The reference's fields are ftype
+// (float): every assignment rounds to float and later lines read the rounded
+// value (kEnv = Omega/w is a float division); the values are returned in the
+// double fields of dtmx_tfsfsrc.
 extern "C" void dtmx_tfsfsrc_set(dtmx_tfsfsrc* s, double c, double impedance, double lmb) {
-  s->Imp = impedance;
-  s->V_max = c;
-  s->cSrc = c;
-  s->wavelength = lmb;
-  s->k = 2 * M_PI / s->wavelength;
-  s->w = c * s->k;
-  s->Omega = 0.05 * s->w;
-  s->kEnv = s->Omega / s->w;
-  s->theta = 0 + M_PI;
-  s->phi = M_PI / 2;
-  s->t0 = 25 * 0.02;
-  s->tw = 5 * 0.02;
-  s->T = 125 * 0.02;
+  s->Imp = (float)impedance;
+  s->V_max = (float)c;
+  s->cSrc = (float)c;
+  const float wl = (float)lmb;
+  const float k = (float)(2 * M_PI / wl);
+  const float w = (float)(c * k);
+  const float om = (float)(0.05 * w);
+  s->wavelength = wl;
+  s->k = k;
+  s->w = w;
+  s->Omega = om;
+  s->kEnv = om / w;
+  s->theta = (float)(0 + M_PI);
+  s->phi = (float)(M_PI / 2);
+  s->t0 = (float)(25 * 0.02);
+  s->tw = (float)(5 * 0.02);
+  s->T = (float)(125 * 0.02);
 }
 
 extern "C" int dtmx_ref_main(const dtmx_ref_globals* g, const dtmx_tfsfsrc* sp, int argc, char** argv) {
   if (!g || !sp) return -1;
-  bool test_only = false;
+  bool test_only = false, drop_data = false;
   std::string drop_dir = ".";
   for (int a = 1; a < argc; a++) {
     const std::string s = argv[a];
     if (s == "--test") test_only = true;
+    else if (s == "--drop_data") drop_data = true;
     else if (s == "--help") { printf("using: DTmxw._main([prog, '--test', '--drop_dir', dir])\n"); return 0; }
     else if (s == "--drop_dir" && a + 1 < argc) drop_dir = argv[++a];
     else if ((s == "--swap_dir" || s == "--sensor" || s == "--box" || s == "--mesh" || s == "--Dmesh" || s == "--zoom" ||
@@ -151,9 +180,12 @@ extern "C" int dtmx_ref_main(const dtmx_ref_globals* g, const dtmx_tfsfsrc* sp, 
   cfg.order = 4;                                   // genDT.py:8
   cfg.geometry = DTMX_GEOM_REFERENCE;
   cfg.absorber = DTMX_ABS_SPLIT_PML;
-  cfg.pml[0][0] = cfg.pml[0][1] = 15;              // Npmlx/2 rags of NDT cells
-  cfg.pml[1][0] = cfg.pml[1][1] = 15;              // Npmly/2 rags
-  cfg.pml[2][1] = 16;                              // Npmlz/2, top face only
+  const int Npmlx = g->Npmlx > 0 ? g->Npmlx : 10, Npmly = g->Npmly > 0 ? g->Npmly : 10;
+  const int Npmlz = g->Npmlz > 0 ? g->Npmlz : 32;  // py_consts.h:67-69
+  if (Npmlx % 2 || Npmly % 2 || Npmlz % 2) { printf("Error: Npmlx, Npmly and Npmlz must be even\n"); return -1; }
+  cfg.pml[0][0] = cfg.pml[0][1] = Npmlx / 2 * NDT; // Npmlx/2 rags of NDT cells
+  cfg.pml[1][0] = cfg.pml[1][1] = Npmly / 2 * NDT; // Npmly/2 rags
+  cfg.pml[2][1] = Npmlz / 2;                       // Npmlz/2, top face only
   cfg.spml_vmax = sp->V_max;
   cfg.probe_every = g->Ntime;                      // one sample per calcStep
   cfg.probe_capacity = g->Tsteps / g->Ntime + 2;
@@ -218,6 +250,14 @@ extern "C" int dtmx_ref_main(const dtmx_ref_globals* g, const dtmx_tfsfsrc* sp, 
     const double cells = (double)ncell * g->Ntime;
     printf("Step %d: Time %9.09f ms ||rate %9.09f GYee_cells/sec |total grid %dx%dx%d=%zu cells | isTFSF=%d\n", s, ms,
            1e-9 * cells / (ms * 1e-3), nx, ny, nz, ncell, (s + 1) * g->Ntime * g->dt < sp->tStop);
+    if (drop_data) {
+      std::vector<float> ez(ncell);
+      if (dtmx_get_field(ctx, DTMX_EZ, ez.data()) != DTMX_OK || write_rag_drop(drop_dir, s, g, ez) != 0) {
+        printf("Error: field drop %d: %s\n", s, dtmx_last_error(ctx));
+        status = -1;
+        break;
+      }
+    }
     if (!sensors.empty()) {
       const int cap = g->Tsteps / g->Ntime + 2;
       int ns = 0;

@@ -293,11 +293,15 @@ typedef struct dtmx_tfsfsrc {
 
 /* Compile-time constants of the reference (py_consts.h, params.h:44-62) as
  * run-time values: grid in rags (x = 3*Np, y = 3*Na cells, z = Nv cells),
- * window Ns and big-step length Ntime, steps, and the run length Tsteps. */
+ * window Ns and big-step length Ntime, steps, the run length Tsteps, and the
+ * split-PML sizes Npmlx, Npmly (in half rags: Npmlx/2 rags of NDT = 3 cells
+ * on each x face) and Npmlz (Npmlz/2 layers at the top z face),
+ * py_consts.h:67-69; values <= 0 select the reference's 10, 10, 32. */
 typedef struct dtmx_ref_globals {
   int Np, Na, Nv, Ns, Ntime;
   double ds, da, dv, dt;
   int Tsteps;
+  int Npmlx, Npmly, Npmlz;
 } dtmx_ref_globals;
 
 /* TFSFsrc::set (signal.hpp:99-115). */
@@ -314,7 +318,13 @@ int  dtmx_ref_material_table(dtmx_material* out, int n);
  * (get_mat_indev, defs.h:128-148) and materials (init_material), split PML,
  * TF/SF dipole from the shotpoint, the default sensor line of init_index
  * written to <drop_dir>/<fld>-xXXXXXyYYYYYzZZZZZ.dat once per Ntime steps, and
- * Tsteps/Ntime calls of dtmx_step(Ntime) (calcStep).  Returns 0 on success. */
+ * Tsteps/Ntime calls of dtmx_step(Ntime) (calcStep).  With --drop_data (the
+ * reference's compile-time DROP_DATA switch, py_consts.h:18) every big step
+ * also writes <drop_dir>/ragEz_NNNNN.arr like SeismoDrops::drop
+ * (drop.cu:83-107): int32 header {12,0,0,0,3,4,Nv,Na,Np}, then per rag
+ * (x < Np, y < Na) and z < Nv the Ez node of the rag's first V domain, the
+ * node of cell (3x-1, 3y-1, z) (0 where that cell lies outside the grid).
+ * Returns 0 on success. */
 int  dtmx_ref_main(const dtmx_ref_globals* g, const dtmx_tfsfsrc* shotpoint, int argc, char** argv);
 
 /* ---- differentiation (no reference counterpart: the reference has no

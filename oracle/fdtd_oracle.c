@@ -3,12 +3,15 @@
  * ONLY as test infrastructure (parity checker and the timed CPU baseline).
  * Nothing in the product links or calls this file.
  *
- * Parity status: the reference ships no tests, golden vectors or CPU path
- * (its kernels are generated at build time by a Python-2 generator), so
- * this oracle is pinned by analytic known answers (dispersion relation of
- * the stencils, Drude/Lorentz susceptibility of the ADE recursion) and by
- * stencil/sign tables extracted from the reference generator's own output
- * (tests/golden); full-field parity with the reference binary is unpinned.
+ * Parity status: the reference ships no tests, golden vectors or CPU path.
+ * This oracle is pinned (1) by analytic known answers (dispersion relation of
+ * the stencils, Drude/Lorentz resonances of the ADE recursion, CPML
+ * absorption; tests/test_cpu.py) and (2) against the reference itself: its
+ * own CUDA implementation, generated and compiled from its sources for
+ * sm_100a by oracle/refbuild/build_ref.py (oracle/_ref), whose FP64 build's
+ * field drops over the whole domain (Drude film, split PML, dipole TF/SF,
+ * mirror and zero boundaries) match this oracle's FP64 run
+ * (tests/test_reference_build.py).
  *
  * Built twice from this one source: REAL=double (prefix orc64_) and
  * REAL=float (prefix orc32_).  Dense SoA fields, z fastest, generic
@@ -209,16 +212,19 @@ static void setup_absorber(osim* s) {
     /* Reference grading (DTmxw.cu:250-265).  K2 = 1/(1+0.5*dt*gamma), K1 = 2*K2-1,
      * computed in double and stored in the field precision (ftype __constant__). */
     double V = cf->spml_vmax;
-    /* x: KNpmlx = 2*Npmlx*NDT with Npmlx/2 = 5 rags; index i = X (left) or
-     * X - 2nx + KNpmlx (right); gamma(KNpmlx/2-|i-KNpmlx/2|-3, KNpmlx/2-3) */
-    int KX = 60, KY = 60, KZ = 64;
+    /* x: KNpmlx = 2*Npmlx*NDT (params.h:106-108), the slab Npmlx/2 rags of
+     * NDT cells = pml[0] cells; index i = X (left) or X - 2nx + KNpmlx
+     * (right); gamma(KNpmlx/2-|i-KNpmlx/2|-3, KNpmlx/2-3).  KNpmly, KNpmlz
+     * likewise from the y slab and the Npmlz/2 top layers. */
+    int KX = 4 * cf->pml[0][0], KY = 4 * cf->pml[1][0], KZ = 4 * cf->pml[2][1];
+    int XS = 2 * cf->pml[0][0] - 3;                        /* inPMLsync: Npmlx/2*2*NDT - NDT (defs.h:45) */
     s->L[0][0] = cf->pml[0][0]; s->L[0][1] = cf->pml[0][1];
     s->L[1][0] = cf->pml[1][0]; s->L[1][1] = cf->pml[1][1];
     s->L[2][0] = 0;             s->L[2][1] = cf->pml[2][1];
     for (int h = 0; h < 2 * s->nx + 2; h++) {
       int i = -1;
-      if (h < 27) i = h;                                   /* inPMLsync left  (defs.h:45) */
-      else if (h >= 2 * s->nx - 27) i = h - 2 * s->nx + KX; /* inPMLsync right */
+      if (h < XS) i = h;                                   /* inPMLsync left */
+      else if (h >= 2 * s->nx - XS) i = h - 2 * s->nx + KX; /* inPMLsync right */
       if (i < 0 || i >= KX) continue;
       double g = ref_pml_gamma(KX / 2 - abs(i - KX / 2) - 3, KX / 2 - 3, cf->dx, V);
       double k2 = 1.0 / (1.0 + 0.5 * cf->dt * g);

@@ -51,10 +51,17 @@ def material_indices(Np, Na, Nv, ds, da, dv):
     return [mat_indev(2 * i + o[0], 2 * j + o[1], 2 * k + o[2], Np, Na, ds, da, dv) for o in offs]
 
 
-def tfsfsrc_set(c, imp, lmb):
-    """TFSFsrc::set (signal.hpp:99-115): the fields it writes."""
-    k = 2 * math.pi / lmb
-    w = c * k
-    Omega = 0.05 * w
-    return dict(Imp=imp, V_max=c, cSrc=c, wavelength=lmb, k=k, w=w, Omega=Omega, kEnv=Omega / w,
-                theta=math.pi, phi=math.pi / 2, t0=25 * 0.02, tw=5 * 0.02, T=125 * 0.02)
+def tfsfsrc_set(c, imp, lmb, ftype=np.float32):
+    """TFSFsrc::set (signal.hpp:99-115): the fields it writes.  They are
+    ftype (float unless the reference is built with USE_DOUBLE): each
+    assignment rounds, later lines read the rounded value, and kEnv = Omega/w
+    divides two ftype values."""
+    f = ftype
+    wl = f(lmb)
+    k = f(2 * math.pi / float(wl))
+    w = f(c * float(k))
+    Omega = f(0.05 * float(w))
+    kEnv = Omega / w                     # float / float
+    return {n: float(v) for n, v in dict(
+        Imp=f(imp), V_max=f(c), cSrc=f(c), wavelength=wl, k=k, w=w, Omega=Omega, kEnv=kEnv,
+        theta=f(math.pi), phi=f(math.pi / 2), t0=f(25 * 0.02), tw=f(5 * 0.02), T=f(125 * 0.02)).items()}

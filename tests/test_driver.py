@@ -110,9 +110,12 @@ def test_main_sensor_files_match_oracle(tmp_path):
     # line starts on the dipole axis, where Ex, Ey and the whole H field vanish
     # by symmetry up to the boundary asymmetry (|H| ~ 1e-5 |Ez| here), so each
     # trace is measured against max(its norm, 1% of the strongest trace).
+    # Ez, the field of the dipole on its axis, is held to 1e-5; the other five
+    # are symmetry-zero there and carry only FP32 round-off of the asymmetric
+    # boundaries (a few 1e-7 of |Ez|, i.e. up to a few 1e-5 of the 1% floor).
     norms = np.linalg.norm(ref, axis=1)
     assert norms[2] > 0
     floor = 1e-2 * norms.max()
     for c in range(6):
         err = np.linalg.norm(got[c] - ref[c]) / max(norms[c], floor)
-        assert err <= 2e-5, (abi.COMP_NAMES[c], err)
+        assert err <= (1e-5 if c == abi.EZ else 5e-5), (abi.COMP_NAMES[c], err)
