@@ -141,7 +141,23 @@ def algorithmic_bytes(sc):
                     disp += int((np.asarray(idx[c]) == m).sum())
     # ADE per dispersive node: Em, Jp, Jm read + write (4 B each) instead of the 1/eps path
     eb = 36 * ncell + 3 * ncell + 2 * 8 * slab + disp * 24
-    return hb, eb
+    # the single-sweep kernel reads E and H once and writes them once (the two
+    # passes each read the other field again); the ADE nodes are its side pass
+    fb = hb + eb - 24 * ncell - disp * 24
+    return hb, eb, fb
+
+
+def dram_bytes_per_cell(kernel, workload):
+    """DRAM bytes per cell of one launch of `kernel` on `workload`, from the ncu
+    captures summarised in profiles/ (None when there is no capture)."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "dram_bytes_per_cell.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.split()
+        if len(f) >= 3 and not line.startswith("#") and f[0] == kernel and f[1] == workload:
+            return float(f[2])
+    return None
 
 
 def max_over_ranks(ms, world, device):
@@ -215,9 +231,20 @@ def run_ours(args, rank, world):
     sim.step(max(20, args.tsteps // 5))
     h_ms, e_ms, cnt = sim.read_profile()
     sim.set_profiling(False)
-    hb, eb = algorithmic_bytes(sc)
+    hb, eb, fb = algorithmic_bytes(sc)
     peak, peak_kind = measured_peaks()
-    if args.engine == 2:
+    engine_used = args.engine if args.engine else run_ours.tuned[0]
+    if engine_used == 3:
+        kms = h_ms / cnt
+        achieved = fb / (kms * 1e-3) / 1e9
+        dpc = dram_bytes_per_cell("fused_kernel", args.workload)
+        roof = {"bound": "hbm", "kernel": "fused_kernel", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                "traffic": int(dpc * ncell) if dpc else None,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per cell (256^3 capture) x cells",
+                "algorithmic_bytes_per_launch": fb, "ms_per_launch": round(kms, 4),
+                "step_bytes_per_cell_update": round(fb / ncell, 2)}
+    elif args.engine == 2:
         # one wavefront launch reads and writes the state once for tblock steps
         T = max(1, args.tblock)
         kb = (hb + eb) - 36 * ncell - 3 * ncell          # the H and E reads/writes of one step ...
@@ -235,12 +262,11 @@ def run_ours(args, rank, world):
         achieved = kbytes / (kms * 1e-3) / 1e9
         # DRAM bytes per cell of one launch from the ncu capture of the same
         # kernels on the 256^3 case of this workload, scaled by cells
-        traffic = None
-        if args.workload == "drude":
-            traffic = int((38.5 if kname == "e_kernel" else 38.6) * ncell)
+        dpc = dram_bytes_per_cell(kname, args.workload)
+        traffic = int(dpc * ncell) if dpc else None
         roof = {"bound": "hbm", "kernel": kname, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind, "traffic": traffic,
-                "traffic_source": "profiles/e_h_kernel_drude_sphere_tfsf_256.md, dram bytes per cell x cells",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per cell (256^3 capture) x cells",
                 "algorithmic_bytes_per_launch": kbytes, "ms_per_launch": round(kms, 4),
                 "h_ms_per_launch": round(h_ms / cnt, 4), "e_ms_per_launch": round(e_ms / cnt, 4),
                 "step_bytes_per_cell_update": round((hb + eb) / ncell, 2)}
@@ -361,7 +387,7 @@ def run_point_dipole(args):
             "engine": "engine %d, x chunk %d, chosen by dtmx_autotune" % (tuned[0], tuned[2]),
             "gcell_per_s": round(c.nx * c.ny * c.nz * sc["steps"] / (ms * 1e-3) / 1e9, 3),
             "ms_per_step": round(ms / sc["steps"], 4),
-            "note": "50 MB of fields: L2-resident, issue/latency-bound (profiles/h_e_kernel_plain_cpml_128.md)"}
+            "note": "50 MB of fields: L2-resident, issue/latency-bound (ncu capture of the field kernels on this grid)"}
 
 
 def run_batched(args):

@@ -12,7 +12,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdtmx.so")
 SOURCES = ["dtmx_api.cu", "dtmx_noalloc.cu", "dtmx_ref_driver.cpp"]
-DEPS = ["dtmx_api.cu", "dtmx_noalloc.cu", "dtmx_ref_driver.cpp", "dtmx_device.cuh", "dtmx_aux.cuh", "dtmx_stream.cuh", "dtmx_torre.cuh", "dtmx_adjoint.cuh"]
+DEPS = ["dtmx_api.cu", "dtmx_noalloc.cu", "dtmx_ref_driver.cpp", "dtmx_device.cuh", "dtmx_aux.cuh", "dtmx_stream.cuh", "dtmx_torre.cuh", "dtmx_adjoint.cuh", "dtmx_fused.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

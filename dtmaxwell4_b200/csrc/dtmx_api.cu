@@ -20,6 +20,7 @@
 #include "dtmx_aux.cuh"
 #include "dtmx_torre.cuh"
 #include "dtmx_adjoint.cuh"
+#include "dtmx_fused.cuh"
 
 using namespace dtmx;
 
@@ -92,9 +93,23 @@ struct dtmx_ctx {
   bool prof_pending = false;
   int engine = 0, tblock = 0;
   int xchunk = 0;               // planes per CTA of the per-step kernels (0: automatic)
-  cudaGraphExec_t graph16 = nullptr;   // 16 captured per-step launch sequences
-  long long graph_launches = 0;
+  // 16 captured per-step launch sequences, one per field buffer holding the
+  // current state (the single-sweep engine alternates them)
+  cudaGraphExec_t graph16[2] = {};
+  long long graph_launches[2] = {};
   TmaMaps maps{};
+  // single-sweep engine (engine 3): the second field buffer and second set of
+  // H auxiliaries (allocated on first use), maps reading each buffer, and the
+  // uniform-material table of its 15-row tiles.  P.f / P.ab.aux always point
+  // at the current state; the other set is swapped in after every step.
+  float* f_alt[6] = {};
+  float* hax_alt[3][2] = {};
+  TmaMaps maps_alt{};
+  FusedMaps fmaps[2]{};               // [0] reads P.f, [1] reads f_alt (swapped with the buffers)
+  bool fused_ready = false;
+  int parity = 0;                     // 0: state in the buffers allocated first
+  signed char* d_umat_f = nullptr;
+  int fnty = 0;
   int* d_err = nullptr;
   bool has_gyro = false;
   // design region and the objective of dtmx_forward_adjoint
@@ -112,6 +127,16 @@ struct dtmx_ctx {
   signed char* d_umat = nullptr;
   std::string err;
 };
+
+// polls of one bounded device wait (mbarrier stages, wavefront neighbours / 16)
+constexpr long long kWaitPolls = 1LL << 26;
+
+static int upload_umat_fused(dtmx_ctx* ctx);
+
+static void drop_graphs(dtmx_ctx* ctx) {
+  for (auto& g : ctx->graph16)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
 
 static const char* kErrStr[] = {"ok", "invalid argument", "CUDA error", "out of device memory", "non-finite value",
                                 "device wait timed out", "invalid state", "unsupported", "no CUDA device",
@@ -424,6 +449,7 @@ extern "C" int dtmx_create(const dtmx_config* cfg, dtmx_ctx** out) {
   if (rc) { *out = ctx; return rc; }
   ctx->P.umat = ctx->d_umat;
   ctx->P.err = ctx->d_err;
+  ctx->P.wait_limit = kWaitPolls;
   for (int comp = 0; comp < 3; comp++) ctx->P.mat[comp] = ctx->d_mat[comp];
   ctx->P.cdt[0] = (float)(c.dt / c.dx); ctx->P.cdt[1] = (float)(c.dt / c.dy); ctx->P.cdt[2] = (float)(c.dt / c.dz);
   // default material 0: vacuum
@@ -442,7 +468,8 @@ extern "C" int dtmx_create(const dtmx_config* cfg, dtmx_ctx** out) {
 extern "C" void dtmx_destroy(dtmx_ctx* ctx) {
   if (!ctx) return;
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  if (ctx->graph16) cudaGraphExecDestroy(ctx->graph16);
+  for (auto& g : ctx->graph16)
+    if (g) cudaGraphExecDestroy(g);
   for (void* p : ctx->allocs) cudaFree(p);
   for (auto& d : ctx->dfts) { cudaFree(d.omega); cudaFree(d.acc); cudaFree(d.stage); cudaFree(d.sstep); }
   for (auto& fx : ctx->fluxes) cudaFree(fx.d_out);
@@ -570,6 +597,7 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
   int rc = upload_mattable(ctx);
   if (rc) return rc;
   if ((rc = upload_umat(ctx))) return rc;
+  if (ctx->fused_ready && (rc = upload_umat_fused(ctx))) return rc;
   Ade& A = ctx->P.ade;
   if (hi[0] >= 0) {
     size_t na = 1;
@@ -1179,15 +1207,228 @@ static int launch_torre(dtmx_ctx* ctx, int T) {
   return DTMX_OK;
 }
 
-// Capture (once) and launch 16 per-step launch sequences as one graph.  The
-// host-side bookkeeping of the 16 steps (staging slots, flushes, buffer
-// parity) is done during the capture; the captured kernels read the step
-// number from the device counter, so the graph is valid at every 16-step
-// boundary of an aligned run.
+// ---------------------------------------------------------------- single-sweep engine
+// Applies to the box geometry with the Yee stencil and a CPML or no absorber;
+// everything else the per-step engine covers.
+static bool fused_usable(const dtmx_ctx* ctx, std::string* why) {
+  const dtmx_config& c = ctx->cfg;
+  if (c.geometry != DTMX_GEOM_BOX) { if (why) *why = "box geometry only"; return false; }
+  if (c.order != 2) { if (why) *why = "order 2 only"; return false; }
+  if (c.absorber == DTMX_ABS_SPLIT_PML) { if (why) *why = "no split PML"; return false; }
+  return true;
+}
+
+// Uniform-material entries of the 15-row tiles (the rule of upload_umat).
+static int upload_umat_fused(dtmx_ctx* ctx) {
+  const dtmx_config& c = ctx->cfg;
+  const int nty = ctx->fnty, ntz = ctx->P.ntz;
+  const bool have = !ctx->h_mat[0].empty();
+  const Params& P = ctx->P;
+  std::vector<signed char> um((size_t)c.nx * nty * ntz);
+  for (int i = 0; i < c.nx; i++)
+    for (int ty = 0; ty < nty; ty++)
+      for (int tz = 0; tz < ntz; tz++) {
+        int m0 = have ? -2 : 0;
+        for (int j = ty * FTY; have && j < std::min(c.ny, ty * FTY + FTY) && m0 != -1; j++)
+          for (int comp = 0; comp < 3 && m0 != -1; comp++) {
+            const uint8_t* row = ctx->h_mat[comp].data() + store_index(ctx, i, j, 0);
+            for (int k = tz * FZ; k < std::min(c.nz, tz * FZ + FZ); k++) {
+              const int m = row[k];
+              if (m0 == -2) m0 = m;
+              if (m != m0 || ctx->mats[m].npoles > 0) { m0 = -1; break; }
+            }
+          }
+        const bool des = P.des_on && i >= P.des_lo[0] && i < P.des_lo[0] + P.des_n[0] &&
+                         ty * FTY < P.des_lo[1] + P.des_n[1] && ty * FTY + FTY > P.des_lo[1] &&
+                         tz * FZ < P.des_lo[2] + P.des_n[2] && tz * FZ + FZ > P.des_lo[2];
+        um[((size_t)i * nty + ty) * ntz + tz] = (signed char)(m0 < 0 || des ? -1 : m0);
+      }
+  CK(cudaMemcpyAsync(ctx->d_umat_f, um.data(), um.size(), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DTMX_OK;
+}
+
+static int build_fused_maps(dtmx_ctx* ctx, FusedMaps& fm, float* const* f) {
+  int rc;
+  for (int c = 0; c < 3; c++) {
+    if ((rc = make_map(ctx, &fm.e[c], f[c], false, FROW, FE_ROWS))) return rc;
+    if ((rc = make_map(ctx, &fm.h[c], f[3 + c], false, FROW, FH_ROWS))) return rc;
+    fm.mat[c] = ctx->maps.mat[c];
+  }
+  return DTMX_OK;
+}
+
+// First use: the second buffer set, the maps reading each set, the tile table.
+static int fused_prepare(dtmx_ctx* ctx) {
+  if (ctx->fused_ready) return DTMX_OK;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F_SMEM_BYTES);
+    attr = true;
+  }
+  const dtmx_config& c = ctx->cfg;
+  int rc = DTMX_OK;
+  for (int comp = 0; comp < 6 && !rc; comp++) rc = dalloc(ctx, &ctx->f_alt[comp], ctx->nstore + 64);
+  for (int a = 0; a < 3 && !rc; a++) {
+    const size_t th = (size_t)(ctx->P.ab.L[a][0] + ctx->P.ab.L[a][1]);
+    if (!ctx->P.ab.aux[a][2] || !th) continue;
+    const size_t cnt = th * (ctx->ncell / (size_t)(a == 0 ? c.nx : a == 1 ? c.ny : c.nz));
+    for (int q = 0; q < 2 && !rc; q++) rc = dalloc(ctx, &ctx->hax_alt[a][q], cnt);
+  }
+  // maps of the per-step kernels over the second set, so either engine runs from either buffer
+  if (!rc) {
+    TmaMaps save = ctx->maps;
+    float* fsave[6];
+    for (int comp = 0; comp < 6; comp++) { fsave[comp] = ctx->P.f[comp]; ctx->P.f[comp] = ctx->f_alt[comp]; }
+    rc = build_maps(ctx);
+    ctx->maps_alt = ctx->maps;
+    ctx->maps = save;
+    for (int comp = 0; comp < 6; comp++) ctx->P.f[comp] = fsave[comp];
+  }
+  if (!rc) rc = build_fused_maps(ctx, ctx->fmaps[0], ctx->P.f);
+  if (!rc) rc = build_fused_maps(ctx, ctx->fmaps[1], ctx->f_alt);
+  ctx->fnty = (c.ny + FTY - 1) / FTY;
+  if (!rc) rc = dalloc(ctx, &ctx->d_umat_f, (size_t)c.nx * ctx->fnty * ctx->P.ntz);
+  if (!rc) rc = upload_umat_fused(ctx);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->fused_ready = true;
+  return DTMX_OK;
+}
+
+// The state now lives in the other buffer set: swap the pointers (fields, H
+// auxiliaries, the maps reading them) so that P and every pass see it.
+static void fused_swap(dtmx_ctx* ctx) {
+  for (int comp = 0; comp < 6; comp++) std::swap(ctx->P.f[comp], ctx->f_alt[comp]);
+  for (int a = 0; a < 3; a++)
+    for (int q = 0; q < 2; q++) std::swap(ctx->P.ab.aux[a][2 + q], ctx->hax_alt[a][q]);
+  std::swap(ctx->maps, ctx->maps_alt);
+  std::swap(ctx->fmaps[0], ctx->fmaps[1]);
+  ctx->parity ^= 1;
+  ctx->tmaps_ok = false;          // the wavefront engine's maps are rebuilt for the current buffer
+}
+
+static int fused_xchunk_for(const dtmx_ctx* ctx) {
+  if (ctx->xchunk > 0) return ctx->xchunk;
+  const dtmx_config& c = ctx->cfg;
+  const long long tiles = (long long)((c.nz + FZ - 1) / FZ) * ((c.ny + FTY - 1) / FTY);
+  const long long target = 148LL * 3 * 6;   // about six waves of 3 CTAs per SM
+  const long long chunks = std::max<long long>(1, (target + tiles - 1) / tiles);
+  const long long xc = (c.nx + chunks - 1) / chunks;
+  return (int)std::min<long long>(32, std::max<long long>(8, xc));
+}
+
+// One time step of the single-sweep engine: the side passes that act on the
+// old state (TF/SF H correction, gyrotropic current), the sweep A -> B, the
+// passes on the new state (dispersive nodes, sources, TF/SF E correction,
+// monitors), then the buffer swap.
+static int launch_fused_step(dtmx_ctx* ctx) {
+  int rc = fused_prepare(ctx);
+  if (rc) return rc;
+  const dtmx_config& c = ctx->cfg;
+  Params PA = ctx->P;
+  PA.x0 = 0; PA.x1 = c.nx;
+  PA.xchunk = fused_xchunk_for(ctx);
+  Params PB = PA;
+  FusedArgs fa{};
+  for (int comp = 0; comp < 6; comp++) { PB.f[comp] = ctx->f_alt[comp]; fa.dst[comp] = ctx->f_alt[comp]; }
+  for (int a = 0; a < 3; a++)
+    for (int q = 0; q < 2; q++) {
+      fa.hsrc[a][q] = PA.ab.aux[a][2 + q];
+      fa.hdst[a][q] = ctx->hax_alt[a][q];
+      PB.ab.aux[a][2 + q] = ctx->hax_alt[a][q];
+    }
+  fa.umat = ctx->d_umat_f;
+  fa.nty = ctx->fnty;
+  fa.ntz = ctx->P.ntz;
+  cudaStream_t st = ctx->stream;
+  const bool pw = ctx->has_tfsf && ctx->tfsf.kind == DTMX_TFSF_PLANE_X;
+  long long nl = 0;
+  dim3 tgrid[2];
+  for (int hs = 0; hs < 2 && ctx->has_tfsf; hs++) {
+    long long mx = 1;
+    for (int r = 0; r < ctx->T.njob[hs]; r++) mx = std::max(mx, ctx->T.job[hs][r].cells);
+    tgrid[hs] = dim3((unsigned)((mx + 255) / 256), std::max(1, ctx->T.njob[hs]));
+  }
+  // TF/SF correction of H, added to the old H (the H update is linear in it)
+  if (ctx->has_tfsf) { tfsf_kernel<2><<<tgrid[1], 256, 0, st>>>(PA, ctx->T, ctx->d_step, 1); nl++; }
+  const double r1 = c.dt / c.dx;
+  if (pw) { line_h_kernel<2><<<8, 256, 0, st>>>(ctx->line_e, ctx->line_h, ctx->T.line_n, r1); nl++; }
+  const dim3 ablk(32, 8), agrd((PA.ade.n[2] + 31) / 32, (PA.ade.n[1] + 7) / 8, std::max(1, PA.ade.n[0]));
+  if (ctx->has_gyro) {
+    gyro_current_kernel<<<agrd, ablk, 0, st>>>(PA, ctx->gcur);
+    PA.ade.gnew = PB.ade.gnew = 1 - ctx->gcur;
+    ctx->gcur = 1 - ctx->gcur;
+    nl++;
+  }
+  const dim3 blk(FZ, FW), grd((c.nz + FZ - 1) / FZ, ctx->fnty, (c.nx + PA.xchunk - 1) / PA.xchunk);
+  if (ctx->profiling) cudaEventRecord(ctx->ev[0], st);
+  fused_kernel<<<grd, blk, F_SMEM_BYTES, st>>>(PA, fa, ctx->fmaps[0]);
+  if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
+  nl++;
+  if (PA.ade.Em[0] || ctx->has_gyro) {
+    // dispersive nodes (left by the sweep) from the old E in A; E -= dt/eps_inf J on gyrotropic nodes
+    for (int comp = 0; comp < 3; comp++) PB.fe_old[comp] = PA.f[comp];
+    ade_node_kernel<2, true><<<agrd, ablk, 0, st>>>(PB);
+    nl++;
+  }
+  if (ctx->profiling) {
+    cudaEventSynchronize(ctx->ev[1]);
+    float a = 0;
+    cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+    ctx->prof_ms_h += a; ctx->prof_count++;
+  }
+  if (!ctx->psrc.empty()) {
+    point_source_kernel<<<((int)ctx->psrc.size() + 63) / 64, 64, 0, st>>>(PB, ctx->d_psrc, (int)ctx->psrc.size(), ctx->d_step, c.dt);
+    nl++;
+  }
+  if (ctx->has_tfsf) { tfsf_kernel<2><<<tgrid[0], 256, 0, st>>>(PB, ctx->T, ctx->d_step, 0); nl++; }
+  if (pw) {
+    const dtmx_tfsf& s = ctx->tfsf;
+    line_e_kernel<2><<<8, 256, 0, st>>>(ctx->line_e, ctx->line_h, ctx->T.line_n, r1, ctx->line_src, ctx->d_step, c.dt, s.amp, s.f0, s.tau, s.t0);
+    nl++;
+  }
+  if (!ctx->probes.empty() && !ctx->monitors_off) {
+    const int every = c.probe_every > 0 ? c.probe_every : 1;
+    probe_kernel<<<((int)ctx->probes.size() + 127) / 128, 128, 0, st>>>(PB, ctx->d_probes, (int)ctx->probes.size(), ctx->d_traces,
+                                                                       ctx->probe_cap, ctx->d_step, every);
+    nl++;
+  }
+  for (auto& d : ctx->dfts) {
+    if (ctx->monitors_off) break;
+    const long long npts = (long long)d.d.n1 * d.d.n2;
+    dft_capture_kernel<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(PB, d.d, ctx->d_step, d.nstaged);
+    nl++;
+    if (++d.nstaged == DFT_STAGE) dft_flush(ctx, d);
+  }
+  if (ctx->obj_on) {
+    DftHost& d = ctx->obj;
+    const long long npts = (long long)d.d.n1 * d.d.n2;
+    dft_capture_kernel<<<(unsigned)((npts + 255) / 256), 256, 0, st>>>(PB, d.d, ctx->d_step, d.nstaged);
+    nl++;
+    if (++d.nstaged == DFT_STAGE) dft_flush(ctx, d);
+  }
+  advance_step_kernel<<<1, 1, 0, st>>>(ctx->d_step);
+  nl++;
+  ctx->launches += nl;
+  fused_swap(ctx);
+  return DTMX_OK;
+}
+
+// one time step of the selected per-step engine (per-step or single sweep)
+static int launch_one(dtmx_ctx* ctx) { return ctx->engine == 3 ? launch_fused_step(ctx) : launch_step(ctx); }
+
+// Capture (once per field buffer) and launch 16 per-step launch sequences as
+// one graph.  The host-side bookkeeping of the 16 steps (staging slots,
+// flushes, buffer parities) is done during the capture; the captured kernels
+// read the step number from the device counter, so the graph is valid at
+// every 16-step boundary of an aligned run that starts from the same buffer
+// (16 single-sweep steps come back to it).
 static int graph_steps16(dtmx_ctx* ctx) {
-  if (!ctx->graph16) {
+  const int par = ctx->parity;
+  if (!ctx->graph16[par]) {
     set_kernel_attributes();
-    const long long step0 = ctx->step;
+    if (ctx->engine == 3) { int rc = fused_prepare(ctx); if (rc) return rc; }
     const long long launches0 = ctx->launches;
     const int gcur0 = ctx->gcur;
     std::vector<int> staged0;
@@ -1196,23 +1437,21 @@ static int graph_steps16(dtmx_ctx* ctx) {
     if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
       return fail(ctx, DTMX_ERR_CUDA, "graph capture could not start");
     int rc = DTMX_OK;
-    for (int q = 0; q < 16 && !rc; q++) rc = launch_step(ctx);
+    for (int q = 0; q < 16 && !rc; q++) rc = launch_one(ctx);
     cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
     if (rc || e != cudaSuccess) { if (g) cudaGraphDestroy(g); cudaGetLastError(); return rc ? rc : fail(ctx, DTMX_ERR_CUDA, "graph capture failed"); }
-    e = cudaGraphInstantiate(&ctx->graph16, g, 0);
+    e = cudaGraphInstantiate(&ctx->graph16[par], g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) { ctx->graph16 = nullptr; cudaGetLastError(); return fail(ctx, DTMX_ERR_CUDA, "graph instantiation failed"); }
+    if (e != cudaSuccess) { ctx->graph16[par] = nullptr; cudaGetLastError(); return fail(ctx, DTMX_ERR_CUDA, "graph instantiation failed"); }
     // the capture ran the bookkeeping of 16 steps; the graph below executes them
-    if (ctx->gcur != gcur0) return fail(ctx, DTMX_ERR_STATE, "graph capture: unexpected buffer parity");
+    if (ctx->gcur != gcur0 || ctx->parity != par) return fail(ctx, DTMX_ERR_STATE, "graph capture: unexpected buffer parity");
     for (size_t q = 0; q < ctx->dfts.size(); q++)
       if (ctx->dfts[q].nstaged != staged0[q]) return fail(ctx, DTMX_ERR_STATE, "graph capture: staging not aligned");
-    ctx->launches = launches0 + (ctx->launches - launches0);
-    ctx->graph_launches = ctx->launches - launches0;
-    (void)step0;
+    ctx->graph_launches[par] = ctx->launches - launches0;
   } else {
-    ctx->launches += ctx->graph_launches;
+    ctx->launches += ctx->graph_launches[par];
   }
-  CK(cudaGraphLaunch(ctx->graph16, ctx->stream));
+  CK(cudaGraphLaunch(ctx->graph16[par], ctx->stream));
   ctx->step += 16;
   return DTMX_OK;
 }
@@ -1231,6 +1470,10 @@ extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
       left -= ctx->tblock;
     }
   }
+  if (ctx->engine == 3) {
+    std::string why;
+    if (!fused_usable(ctx, &why)) return fail(ctx, DTMX_ERR_UNSUPPORTED, "single-sweep engine: " + why);
+  }
   while (left > 0) {
     // 16 steps as one CUDA graph when every DFT staging cycle is at its start
     // (the captured sequence then repeats exactly: staging slots, the flush
@@ -1244,7 +1487,7 @@ extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
       left -= 16;
       continue;
     }
-    int rc = launch_step(ctx);
+    int rc = ctx->engine == 2 ? launch_step(ctx) : launch_one(ctx);
     if (rc) return rc;
     ctx->step++;
     left--;
@@ -1280,7 +1523,9 @@ extern "C" int dtmx_set_design(dtmx_ctx* ctx, const int* lo, const int* n, const
   }
   for (int a = 0; a < 3; a++) { ctx->P.des_lo[a] = lo[a]; ctx->P.des_n[a] = n[a]; }
   ctx->P.des_on = 1;
-  return upload_umat(ctx);
+  int rc = upload_umat(ctx);
+  if (!rc && ctx->fused_ready) rc = upload_umat_fused(ctx);
+  return rc;
 }
 
 // device buffers that make up the restartable state of a context
@@ -1692,6 +1937,9 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
     std::vector<TuneVal> cand;
     for (int xc : {0, 4, 6, 8, 10, 12, 16, 24, 32, 64})
       if (xc <= c.nx) cand.push_back({1, 0, xc, 0});
+    if (fused_usable(ctx, nullptr) && fused_prepare(ctx) == DTMX_OK)
+      for (int xc : {0, 8, 12, 16, 24, 32, 48, 64})
+        if (xc <= c.nx) cand.push_back({3, 0, xc, 0});
     std::string why;
     if (torre_features_ok(ctx, &why))
       for (int T : {1, 2, 4})
@@ -1699,13 +1947,14 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
     ctx->monitors_off = true;
     for (auto& cd : cand) {
       ctx->xchunk = cd.xchunk;
+      ctx->engine = cd.engine;
       int r = DTMX_OK;
       const int n = cd.engine == 2 ? (trial_steps / cd.tblock) * cd.tblock : trial_steps;
       cudaEventRecord(e0, ctx->stream);
       if (cd.engine == 2) {
         for (int q = 0; q < n && !r; q += cd.tblock) r = launch_torre(ctx, cd.tblock);
       } else {
-        for (int q = 0; q < n && !r; q++) { r = launch_step(ctx); ctx->step++; }
+        for (int q = 0; q < n && !r; q++) { r = launch_one(ctx); ctx->step++; }
       }
       cudaEventRecord(e1, ctx->stream);
       cudaEventSynchronize(e1);
@@ -1729,7 +1978,7 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
   ctx->engine = best.engine;
   ctx->tblock = best.tblock;
   ctx->xchunk = best.xchunk;
-  if (ctx->graph16) { cudaGraphExecDestroy(ctx->graph16); ctx->graph16 = nullptr; }
+  drop_graphs(ctx);
   if (engine_out) *engine_out = best.engine;
   if (tblock_out) *tblock_out = best.tblock;
   if (xchunk_out) *xchunk_out = best.xchunk;
@@ -1894,8 +2143,12 @@ extern "C" int dtmx_kernel_launches(const dtmx_ctx* ctx, int64_t* n) {
 }
 
 extern "C" int dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block) {
-  if (!ctx || engine < 0 || engine > 2 || time_block < 0) return fail(ctx, DTMX_ERR_INVALID, "bad engine");
-  if (engine == 2) {
+  if (!ctx || engine < 0 || engine > 3 || time_block < 0) return fail(ctx, DTMX_ERR_INVALID, "bad engine");
+  if (engine == 3) {
+    std::string why;
+    if (!fused_usable(ctx, &why)) return fail(ctx, DTMX_ERR_UNSUPPORTED, "single-sweep engine: " + why);
+    ctx->tblock = 0;
+  } else if (engine == 2) {
     const int T = time_block > 0 ? time_block : 2;
     std::string why;
     if (!torre_usable(ctx, T, &why)) return fail(ctx, DTMX_ERR_UNSUPPORTED, "wavefront engine: " + why);
@@ -1904,7 +2157,13 @@ extern "C" int dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block) {
     ctx->tblock = time_block;
   }
   ctx->engine = engine;
-  if (ctx->graph16) { cudaGraphExecDestroy(ctx->graph16); ctx->graph16 = nullptr; }
+  drop_graphs(ctx);
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_set_wait_limit(dtmx_ctx* ctx, int64_t polls) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  ctx->P.wait_limit = polls > 0 ? (long long)polls : kWaitPolls;
   return DTMX_OK;
 }
 

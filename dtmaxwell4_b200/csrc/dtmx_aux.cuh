@@ -587,7 +587,8 @@ __global__ void ade_node_kernel(Params p) {
           d[a] = __fmul_rn(t == 0 ? p.cdt[a] : -p.cdt[a], dstencil<ORDER>(v[0], v[1], v[2], v[3]));
         }
         (void)idx;
-        p.f[c][id] = ade_update(p, c, m, np, q, sum3(d[0], d[1], d[2]), p.f[c][id]);
+        const float E0 = p.fe_old[c] ? __ldg(p.fe_old[c] + id) : p.f[c][id];
+        p.f[c][id] = ade_update(p, c, m, np, q, sum3(d[0], d[1], d[2]), E0);
       } else if (__ldg(&mt.gjc[m]) != 0.f) {
         p.f[c][id] = __fsub_rn(p.f[c][id], __fmul_rn(__ldg(&mt.gjc[m]), __ldg(p.ade.Jg[p.ade.gnew][c] + q)));
       }

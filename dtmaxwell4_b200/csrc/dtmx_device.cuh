@@ -83,10 +83,14 @@ struct Params {
   int x0, x1;                // planes [x0, x1) processed by a streaming launch
   int xchunk;                // planes per CTA along x
   int* err;                  // device error word (bounded waits that gave up)
+  long long wait_limit;      // polls of one bounded wait (2^26; lowered only to test the timeout paths)
   // per (plane, y tile, z tile): the single non-dispersive material of all E
   // nodes of that plane tile, or -1 when mixed/dispersive
   const signed char* umat;
   int ntz, nty;              // tiles along z and y
+  // E of the previous step when a pass reads it from another buffer than the
+  // one it writes (the single-sweep engine's ADE pass); nullptr: in place
+  const float* fe_old[3];
   // design region: per-node 1/eps of the E components over a cell box
   const float* des_ie[3];
   int des_lo[3], des_n[3];

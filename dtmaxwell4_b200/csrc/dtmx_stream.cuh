@@ -35,15 +35,21 @@ __device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after ~2^26 polls, records the failure in *err and returns.
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, int* err) {
+// Bounded wait: gives up after `limit` polls (2^26 unless a test lowers it),
+// records the failure in *err and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int* err, long long limit = 1LL << 26) {
   for (long long it = 0; !mbar_test(bar, parity); it++) {
-    if (it > (1LL << 26)) {
+    if (it > limit) {
       if (err) atomicExch(err, 1);
-      return;
+      return false;
     }
   }
+  return true;
 }
+// Polls allowed while draining the copies of a CTA that gave up: TMA copies
+// that were issued always complete, so this bound only guards a broken
+// transaction count.
+constexpr long long DRAIN_POLLS = 1LL << 20;
 __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int c0, int c1, int c2, uint64_t* bar) {
   asm volatile(
       "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(
@@ -148,10 +154,14 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
   // read once so that the elected thread issues each stage without a dependent load
   constexpr int UMC = 128;
   __shared__ signed char umc[UMC];
+  // set by the thread that waits for the stages when a wait gave up: the CTA
+  // then stops issuing and computing, drains its copies in flight and returns
+  __shared__ int gave_up;
   const int slast = len - 1 + AHEAD;         // last stage number that has to be staged
   if (tid == 0) {
     for (int q = 0; q < NST; q++) mbar_init(&bars[q], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    gave_up = 0;
   }
   if (!ISH) {
     load_matshared(ms, p);
@@ -215,8 +225,15 @@ __device__ __forceinline__ void stream_body(const Params& p, const TmaMaps& m, f
     // everybody (and orders the staged data for them) without spinning issue slots
     if (tid == 0)
       for (int a = (t == 0 ? 0 : AHEAD); a <= AHEAD; a++)
-        mbar_wait(&bars[(t + a) % NST], (unsigned)(((t + a) / NST) & 1), p.err);
+        if (!mbar_wait(&bars[(t + a) % NST], (unsigned)(((t + a) / NST) & 1), p.err, p.wait_limit)) gave_up = 1;
     __syncthreads();
+    if (gave_up) {
+      // stages t .. the last one issued may still be landing: wait for them (bounded) before leaving
+      if (tid == 0)
+        for (int sq = t; sq <= min(slast, t + AHEAD + LEAD); sq++)
+          mbar_wait(&bars[sq % NST], (unsigned)((sq / NST) & 1), nullptr, DRAIN_POLLS);
+      return;
+    }
     // every node of the tile in the array and live, every tap in range or zero: in the box
     // geometry a full tile (taps outside the array read the TMA zero fill)
     const bool fast = p.g.box ? (j0 + TYT <= p.g.n[1] && k0 + TZ <= p.g.n[2])

@@ -124,8 +124,8 @@ __device__ __forceinline__ bool item_live(int s, int l, int nx, int& x) {
 // Producer warp: wait until this tile and its four neighbours have completed
 // at least `need` wave steps.  Lane q watches tile q; the five counters are
 // read in parallel and a lane re-reads only while its cached value is short.
-// Bounded: gives up after ~2^22 rounds and records the timeout.
-__device__ __forceinline__ void wait_tiles(const Params& p, const TorreArgs& ta, int ty, int tz, int need, int& seen) {
+// Bounded: gives up after wait_limit/16 rounds (2^22) and records the timeout.
+__device__ __forceinline__ bool wait_tiles(const Params& p, const TorreArgs& ta, int ty, int tz, int need, int& seen) {
   const int lane = threadIdx.x & 31;
   const int* c = nullptr;
   if (lane < 5) {
@@ -134,16 +134,19 @@ __device__ __forceinline__ void wait_tiles(const Params& p, const TorreArgs& ta,
     if (y >= 0 && y < ta.nty && z >= 0 && z < ta.ntz) c = ta.ctr + y * ta.ntz + z;
   }
   if (!c) seen = 1 << 30;
+  bool ok = true;
   for (long long it = 0;; it++) {
     if (seen < need) seen = ld_acquire(c);
     if (__all_sync(0xffffffffu, seen >= need)) break;
-    if (it > (1LL << 22)) {
+    if (it > (p.wait_limit >> 4)) {
       if (lane == 0) atomicExch(p.err, 2);
+      ok = false;
       break;
     }
     __nanosleep(32);
   }
   __syncwarp();
+  return ok;
 }
 
 template <int ORDER, int TY>
@@ -383,10 +386,16 @@ __global__ void __launch_bounds__(TorreLayout<ORDER, TY>::NTHR, 1)
   const int z0 = tz * TT_Z, y0 = ty * TY;
   const int nx = p.g.n[0];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // Set when any wait of this CTA gave up.  From then on the producer issues
+  // no copy (it never re-arms a stage whose copy may still be landing), every
+  // warp leaves its loop, and the producer waits for its copies in flight
+  // before it returns; the timeout is reported through p.err.
+  __shared__ volatile int gave_up;
   if (threadIdx.x == 0) {
     for (int q = 0; q < TT_NS; q++) { mbar_init(&full[q], 1); mbar_init(&empty[q], L::NCW); }
     for (int q = 0; q < TT_NPUB; q++) mbar_init(&done[q], L::NCW);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    gave_up = 0;
   }
   for (int q = threadIdx.x; q < MAXMAT * 3; q += L::NTHR) (&ms.inv_eps[0][0])[q] = __ldg(&p.mt->inv_eps[0][0] + q);
   for (int q = threadIdx.x; q < MAXMAT; q += L::NTHR) ms.npoles[q] = __ldg(&p.mt->npoles[q]);
@@ -397,15 +406,18 @@ __global__ void __launch_bounds__(TorreLayout<ORDER, TY>::NTHR, 1)
     int it = 0, seen = 0;
     for (int s = 0; s < ta.nsteps; s++) {
       // step s reads values produced up to step s - TT_K - 1 (own and neighbours)
-      if (s - TT_K > 0) wait_tiles(p, ta, ty, tz, s - TT_K, seen);
+      if (s - TT_K > 0 && !wait_tiles(p, ta, ty, tz, s - TT_K, seen)) gave_up = 1;
       if (lane == 0) {
         fence_proxy_async_global();
 #pragma unroll 1
-        for (int l = 0; l < NL; l++) {
+        for (int l = 0; l < NL && !gave_up; l++) {
           int x;
           if (!item_live<ORDER>(s, l, nx, x)) continue;
           const int st = it % TT_NS;
-          if (it >= TT_NS) mbar_wait(&empty[st], (unsigned)(((it / TT_NS) - 1) & 1), p.err);
+          if (it >= TT_NS && !mbar_wait(&empty[st], (unsigned)(((it / TT_NS) - 1) & 1), p.err, p.wait_limit)) {
+            gave_up = 1;
+            break;
+          }
           const int um = ((l & 1) && x >= 0) ? torre_umat<TY>(p, x, ty, tz) : 0;
           stage_um[st] = um;
           const bool want_mat = (l & 1) && x >= 0 && um < 0;
@@ -413,16 +425,25 @@ __global__ void __launch_bounds__(TorreLayout<ORDER, TY>::NTHR, 1)
           it++;
         }
       }
+      if (__shfl_sync(0xffffffffu, gave_up, 0)) break;
       __syncwarp();
     }
+    // no copy of this CTA may still be landing when it exits: after a wait
+    // that gave up, the consumers may have moved past items still in flight
+    if (lane == 0)
+      for (int q = it - 1; q >= 0 && q >= it - TT_NS; q--)
+        mbar_wait(&full[q % TT_NS], (unsigned)((q / TT_NS) & 1), nullptr, DRAIN_POLLS);
     return;
   }
   if (warp == L::NCW + 1) {
     // ---------------- publisher warp: release each completed wave step
     if (lane == 0) {
       int* mine = ta.ctr + ty * ta.ntz + tz;
-      for (int s = 0; s < ta.nsteps; s++) {
-        mbar_wait(&done[s % TT_NPUB], (unsigned)((s / TT_NPUB) & 1), p.err);
+      for (int s = 0; s < ta.nsteps && !gave_up; s++) {
+        if (!mbar_wait(&done[s % TT_NPUB], (unsigned)((s / TT_NPUB) & 1), p.err, p.wait_limit)) {
+          gave_up = 1;
+          break;
+        }
         __threadfence();
         st_release(mine, s + 1);
       }
@@ -440,12 +461,15 @@ __global__ void __launch_bounds__(TorreLayout<ORDER, TY>::NTHR, 1)
       for (int e = 0; e < 4; e++) { qb[l][q][e] = 0.f; qc[l][q][e] = 0.f; }
   int it = 0;
   for (int s = 0; s < ta.nsteps; s++) {
+    if (gave_up) break;
 #pragma unroll
     for (int l = 0; l < NL; l++) {
       int x;
       if (!item_live<ORDER>(s, l, nx, x)) continue;
       const int st = it % TT_NS;
-      mbar_wait(&full[st], (unsigned)((it / TT_NS) & 1), p.err);
+      // (all lanes poll; warp-uniform outcome, the stage completes for all of them at once)
+      if (!mbar_wait(&full[st], (unsigned)((it / TT_NS) & 1), p.err, p.wait_limit)) gave_up = 1;
+      if (__any_sync(0xffffffffu, gave_up != 0)) return;
       const unsigned char* stg = stages + st * L::STAGE;
       const bool isE = l & 1;
       const int um = stage_um[st];

@@ -26,7 +26,7 @@ EXPORTS = (
     "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
     "dtmx_write_arr", "dtmx_save_state", "dtmx_load_state",
     "dtmx_add_dft_patch", "dtmx_add_flux_box", "dtmx_read_flux", "dtmx_flux_faces",
-    "dtmx_set_adjoint_memory", "dtmx_ntff",
+    "dtmx_set_adjoint_memory", "dtmx_ntff", "dtmx_set_wait_limit",
 )
 
 
@@ -88,6 +88,7 @@ def load():
     L.dtmx_batch_forward_adjoint.argtypes = [C.POINTER(vp), ip, ip, ip, C.POINTER(ip), C.POINTER(C.c_double),
                                              C.POINTER(C.c_double), C.POINTER(vp)]
     L.dtmx_count_nonfinite_noalloc.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int64, C.POINTER(C.c_int64)]
+    L.dtmx_set_wait_limit.argtypes = [vp, C.c_int64]
     _lib = L
     return L
 
@@ -274,6 +275,10 @@ class Simulation:
 
     def sync(self):
         self._ck(self._L.dtmx_sync(self._h))
+
+    def set_wait_limit(self, polls):
+        """Bound of the device-side waits (polls); <= 0 restores the default."""
+        self._ck(self._L.dtmx_set_wait_limit(self._h, int(polls)))
 
     @property
     def nstep(self):

@@ -264,6 +264,14 @@ int  dtmx_check_finite(dtmx_ctx* ctx);
 /* Number of kernels this context has launched so far. */
 int  dtmx_kernel_launches(const dtmx_ctx* ctx, int64_t* n);
 
+/* Bound of every device-side wait of this context's kernels (staged copies,
+ * wavefront neighbours), in polls; polls <= 0 restores the default 2^26.
+ * A wait that runs out sets an error word, the CTA stops issuing copies,
+ * waits for those in flight and returns, and the next dtmx_sync reports
+ * DTMX_ERR_TIMEOUT (the results of that step are not valid).  Lowering it
+ * exists to exercise that path in tests without a hang. */
+int  dtmx_set_wait_limit(dtmx_ctx* ctx, int64_t polls);
+
 /* The context's CUDA stream (cudaStream_t), for event timing by the caller. */
 int  dtmx_get_stream(dtmx_ctx* ctx, void** stream);
 
