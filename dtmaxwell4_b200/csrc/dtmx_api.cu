@@ -99,17 +99,16 @@ struct dtmx_ctx {
   long long graph_launches[2] = {};
   TmaMaps maps{};
   // single-sweep engine (engine 3): the second field buffer and second set of
-  // H auxiliaries (allocated on first use), maps reading each buffer, and the
-  // uniform-material table of its 15-row tiles.  P.f / P.ab.aux always point
-  // at the current state; the other set is swapped in after every step.
+  // H auxiliaries (allocated on first use) and the maps reading each buffer
+  // (its tiles are the per-step kernels' tiles and share their uniform-material
+  // table).  P.f / P.ab.aux always point at the current state; the other set
+  // is swapped in after every step.
   float* f_alt[6] = {};
   float* hax_alt[3][2] = {};
   TmaMaps maps_alt{};
   FusedMaps fmaps[2]{};               // [0] reads P.f, [1] reads f_alt (swapped with the buffers)
   bool fused_ready = false;
   int parity = 0;                     // 0: state in the buffers allocated first
-  signed char* d_umat_f = nullptr;
-  int fnty = 0;
   int* d_err = nullptr;
   bool has_gyro = false;
   // design region and the objective of dtmx_forward_adjoint
@@ -131,7 +130,6 @@ struct dtmx_ctx {
 // polls of one bounded device wait (mbarrier stages, wavefront neighbours / 16)
 constexpr long long kWaitPolls = 1LL << 26;
 
-static int upload_umat_fused(dtmx_ctx* ctx);
 
 static void drop_graphs(dtmx_ctx* ctx) {
   for (auto& g : ctx->graph16)
@@ -597,7 +595,6 @@ extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int
   int rc = upload_mattable(ctx);
   if (rc) return rc;
   if ((rc = upload_umat(ctx))) return rc;
-  if (ctx->fused_ready && (rc = upload_umat_fused(ctx))) return rc;
   Ade& A = ctx->P.ade;
   if (hi[0] >= 0) {
     size_t na = 1;
@@ -1218,44 +1215,15 @@ static bool fused_usable(const dtmx_ctx* ctx, std::string* why) {
   return true;
 }
 
-// Uniform-material entries of the 15-row tiles (the rule of upload_umat).
-static int upload_umat_fused(dtmx_ctx* ctx) {
-  const dtmx_config& c = ctx->cfg;
-  const int nty = ctx->fnty, ntz = ctx->P.ntz;
-  const bool have = !ctx->h_mat[0].empty();
-  const Params& P = ctx->P;
-  std::vector<signed char> um((size_t)c.nx * nty * ntz);
-  for (int i = 0; i < c.nx; i++)
-    for (int ty = 0; ty < nty; ty++)
-      for (int tz = 0; tz < ntz; tz++) {
-        int m0 = have ? -2 : 0;
-        for (int j = ty * FTY; have && j < std::min(c.ny, ty * FTY + FTY) && m0 != -1; j++)
-          for (int comp = 0; comp < 3 && m0 != -1; comp++) {
-            const uint8_t* row = ctx->h_mat[comp].data() + store_index(ctx, i, j, 0);
-            for (int k = tz * FZ; k < std::min(c.nz, tz * FZ + FZ); k++) {
-              const int m = row[k];
-              if (m0 == -2) m0 = m;
-              if (m != m0 || ctx->mats[m].npoles > 0) { m0 = -1; break; }
-            }
-          }
-        const bool des = P.des_on && i >= P.des_lo[0] && i < P.des_lo[0] + P.des_n[0] &&
-                         ty * FTY < P.des_lo[1] + P.des_n[1] && ty * FTY + FTY > P.des_lo[1] &&
-                         tz * FZ < P.des_lo[2] + P.des_n[2] && tz * FZ + FZ > P.des_lo[2];
-        um[((size_t)i * nty + ty) * ntz + tz] = (signed char)(m0 < 0 || des ? -1 : m0);
-      }
-  CK(cudaMemcpyAsync(ctx->d_umat_f, um.data(), um.size(), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  return DTMX_OK;
-}
-
 static int build_fused_maps(dtmx_ctx* ctx, FusedMaps& fm, float* const* f) {
   int rc;
   for (int c = 0; c < 3; c++) {
-    if ((rc = make_map(ctx, &fm.e[c], f[c], false, FROW, FE_ROWS))) return rc;
-    if ((rc = make_map(ctx, &fm.h[c], f[3 + c], false, FROW, FH_ROWS))) return rc;
+    if ((rc = make_map(ctx, &fm.e[c], f[c], false, FE_W, FE_R))) return rc;
     fm.mat[c] = ctx->maps.mat[c];
   }
-  return DTMX_OK;
+  if ((rc = make_map(ctx, &fm.hx, f[3], false, FHX_W, FHX_R))) return rc;
+  if ((rc = make_map(ctx, &fm.hy, f[4], false, FHY_W, FHY_R))) return rc;
+  return make_map(ctx, &fm.hz, f[5], false, FHZ_W, FHZ_R);
 }
 
 // First use: the second buffer set, the maps reading each set, the tile table.
@@ -1287,9 +1255,6 @@ static int fused_prepare(dtmx_ctx* ctx) {
   }
   if (!rc) rc = build_fused_maps(ctx, ctx->fmaps[0], ctx->P.f);
   if (!rc) rc = build_fused_maps(ctx, ctx->fmaps[1], ctx->f_alt);
-  ctx->fnty = (c.ny + FTY - 1) / FTY;
-  if (!rc) rc = dalloc(ctx, &ctx->d_umat_f, (size_t)c.nx * ctx->fnty * ctx->P.ntz);
-  if (!rc) rc = upload_umat_fused(ctx);
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->fused_ready = true;
@@ -1308,11 +1273,13 @@ static void fused_swap(dtmx_ctx* ctx) {
   ctx->tmaps_ok = false;          // the wavefront engine's maps are rebuilt for the current buffer
 }
 
+// planes per CTA (at most FX_MAX): about eight waves of 3 CTAs per SM, and
+// at least 8 planes (each chunk stages one plane and updates one H plane more)
 static int fused_xchunk_for(const dtmx_ctx* ctx) {
-  if (ctx->xchunk > 0) return ctx->xchunk;
+  if (ctx->xchunk > 0) return std::min(ctx->xchunk, FX_MAX);
   const dtmx_config& c = ctx->cfg;
-  const long long tiles = (long long)((c.nz + FZ - 1) / FZ) * ((c.ny + FTY - 1) / FTY);
-  const long long target = 148LL * 3 * 6;   // about six waves of 3 CTAs per SM
+  const long long tiles = (long long)((c.nz + TZ - 1) / TZ) * ((c.ny + TYT - 1) / TYT);
+  const long long target = 148LL * 3 * 8;
   const long long chunks = std::max<long long>(1, (target + tiles - 1) / tiles);
   const long long xc = (c.nx + chunks - 1) / chunks;
   return (int)std::min<long long>(32, std::max<long long>(8, xc));
@@ -1338,9 +1305,6 @@ static int launch_fused_step(dtmx_ctx* ctx) {
       fa.hdst[a][q] = ctx->hax_alt[a][q];
       PB.ab.aux[a][2 + q] = ctx->hax_alt[a][q];
     }
-  fa.umat = ctx->d_umat_f;
-  fa.nty = ctx->fnty;
-  fa.ntz = ctx->P.ntz;
   cudaStream_t st = ctx->stream;
   const bool pw = ctx->has_tfsf && ctx->tfsf.kind == DTMX_TFSF_PLANE_X;
   long long nl = 0;
@@ -1361,7 +1325,7 @@ static int launch_fused_step(dtmx_ctx* ctx) {
     ctx->gcur = 1 - ctx->gcur;
     nl++;
   }
-  const dim3 blk(FZ, FW), grd((c.nz + FZ - 1) / FZ, ctx->fnty, (c.nx + PA.xchunk - 1) / PA.xchunk);
+  const dim3 blk(TZ, TW), grd((c.nz + TZ - 1) / TZ, (c.ny + TYT - 1) / TYT, (c.nx + PA.xchunk - 1) / PA.xchunk);
   if (ctx->profiling) cudaEventRecord(ctx->ev[0], st);
   fused_kernel<<<grd, blk, F_SMEM_BYTES, st>>>(PA, fa, ctx->fmaps[0]);
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
@@ -1523,9 +1487,7 @@ extern "C" int dtmx_set_design(dtmx_ctx* ctx, const int* lo, const int* n, const
   }
   for (int a = 0; a < 3; a++) { ctx->P.des_lo[a] = lo[a]; ctx->P.des_n[a] = n[a]; }
   ctx->P.des_on = 1;
-  int rc = upload_umat(ctx);
-  if (!rc && ctx->fused_ready) rc = upload_umat_fused(ctx);
-  return rc;
+  return upload_umat(ctx);
 }
 
 // device buffers that make up the restartable state of a context
@@ -2157,6 +2119,13 @@ extern "C" int dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block) {
     ctx->tblock = time_block;
   }
   ctx->engine = engine;
+  drop_graphs(ctx);
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_set_xchunk(dtmx_ctx* ctx, int planes) {
+  if (!ctx || planes < 0) return fail(ctx, DTMX_ERR_INVALID, "bad x chunk");
+  ctx->xchunk = planes;
   drop_graphs(ctx);
   return DTMX_OK;
 }

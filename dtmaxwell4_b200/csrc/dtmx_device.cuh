@@ -113,10 +113,15 @@ struct TmaMaps {
 };
 
 // storage slot of component c for derivative axis a (-1: c has no derivative along a)
-__host__ __device__ __forceinline__ int slot_of(int c, int a) {
+__host__ __device__ __forceinline__ constexpr int slot_of(int c, int a) {
   // Ex: y->0 z->0 ; Ey: x->0 z->1 ; Ez: x->1 y->1 ; Hx: y->2 z->2 ; Hy: x->2 z->3 ; Hz: x->3 y->3
-  const int S[6][3] = {{-1, 0, 0}, {0, -1, 1}, {1, 1, -1}, {-1, 2, 2}, {2, -1, 3}, {3, 3, -1}};
-  return S[c][a];
+  // (a conditional expression: a table indexed by a run-time c would live in local memory)
+  return c == 0 ? (a == 0 ? -1 : 0)
+       : c == 1 ? (a == 0 ? 0 : a == 1 ? -1 : 1)
+       : c == 2 ? (a == 2 ? -1 : 1)
+       : c == 3 ? (a == 0 ? -1 : 2)
+       : c == 4 ? (a == 0 ? 2 : a == 1 ? -1 : 3)
+                : (a == 2 ? -1 : 3);
 }
 
 // Loads: LD = 0 read-only path (field not written during the launch),

@@ -11,19 +11,25 @@
 // (H, then E), each reading the field the other one writes; this engine makes
 // one.
 //
-// Tile: a CTA owns 15 y rows x 32 z columns of an x chunk, walked upwards.
-// Its 8 warps compute the new H on 16 rows (the 15 own rows and the halo row
-// above), 32 lanes per row; the halo column beyond the tile (Hy and Hx of
-// z = k0+32, needed by the E update of the last lane) is shared out over the
-// warps.  For plane i of the walk:
-//   H(i+1) on the 16 x 33 region  <- E_old(i+1), E_old(i) (staged), H_old(i+1)
-//   E(i)   on the 15 x 32 tile    <- E_old(i), H(i) and H(i+1) (shared memory)
-// One thread issues the TMA copies (cp.async.bulk.tensor, no multicast) of each
-// plane's E (17 rows: the row below the tile for the H taps), old H (16 rows)
-// and, on mixed planes, material tiles into a 3-stage ring; the new H of two
-// planes sits in a shared-memory double buffer.  Everything outside the grid
-// reads as zero (TMA fill, or forced for the new H), which is the box
-// geometry; other geometries use the per-step engine.
+// Tile: the per-step kernels' 32 (z, lanes) x 16 (y, 8 warps x 2 rows) node
+// tile, walked upwards along an x chunk.  Iteration t of the walk consumes the
+// stage of plane pc = x0 + t and
+//   * computes the new H of plane pc on the own nodes (and, split over warps
+//     0-3, the halo: Hz and Hx of row 16, Hy and Hx of column 32) from the old
+//     E of planes pc (staged) and pc - 1 (registers) and the old H of plane pc
+//     (staged); the own values go to B and, with the halo, to a shared-memory
+//     plane buffer;
+//   * computes the new E of plane pc - 1 on the own nodes from its old E
+//     (registers), the new H of plane pc - 1 (the other shared-memory plane
+//     buffer; own nodes from registers) and of plane pc (registers).
+// Each old value is therefore read from HBM once per step (the halo rows and
+// columns of the TMA boxes come from L2), and every plane costs one CTA
+// barrier.  One elected thread issues the TMA copies (cp.async.bulk.tensor,
+// no multicast) of a plane's E box (18 rows x 40 floats per component), old-H
+// boxes and, when the E update of the previous plane needs them, that plane's
+// material tiles, into a 3-stage ring (two planes in flight).  Everything
+// outside the grid reads as zero (TMA fill; new H forced to zero outside),
+// which is the box geometry; other geometries use the per-step engine.
 //
 // The node updates are the expressions of plane_update (dtmx_device.cuh), in
 // the same order with the same explicitly rounded operations, so without a
@@ -35,193 +41,298 @@
 
 namespace dtmx {
 
-constexpr int FZ = 32;                      // tile columns (lanes)
-constexpr int FW = 8;                       // warps
-constexpr int FTY = 15;                     // own rows of a tile
-constexpr int FHR = 16;                     // rows with a new H: own + the halo row
-constexpr int FNTHR = FZ * FW;
-constexpr int FROW = 40;                    // staged row: z in [k0-4, k0+36), 16-byte aligned
-constexpr int FZO = 4;                      // z offset of k0 in a staged row
-constexpr int FE_ROWS = FHR + 1;            // E rows j0-1 .. j0+15
-constexpr int FH_ROWS = FHR;                // old H rows j0 .. j0+15
-constexpr int FE_N = 704;                   // 17 x 40 = 680 floats, rounded to 128 bytes
-constexpr int FH_N = 640;                   // 16 x 40
-constexpr int FM_N = 3 * FHR * FZ / 4;      // material tiles (bytes as floats): 3 x 16 x 32
-constexpr int F_OFF_E = 0, F_OFF_H = 3 * FE_N, F_OFF_M = F_OFF_H + 3 * FH_N;
-constexpr int F_STAGE = F_OFF_M + FM_N;     // 4416 floats = 17664 bytes (138 x 128)
-constexpr unsigned F_BYTES = (3 * FE_ROWS * FROW + 3 * FH_ROWS * FROW) * 4;
-constexpr unsigned F_BYTES_MAT = 3 * FHR * FZ;
+constexpr int FE_W = 40;                     // E box: z in [k0-4, k0+36) (16-byte aligned start)
+constexpr int FE_R = TYT + 2;                // ... y in [j0-1, j0+17)
+constexpr int FE_N = 736;                    // 18 x 40 = 720 floats, rounded up to 128 bytes
+constexpr int FHX_W = 36, FHX_R = TYT + 1;   // old Hx: z [k0, k0+36), y [j0, j0+17)
+constexpr int FHY_W = 36, FHY_R = TYT;       // old Hy: z [k0, k0+36), y [j0, j0+16)
+constexpr int FHZ_W = 32, FHZ_R = TYT + 1;   // old Hz: z [k0, k0+32), y [j0, j0+17)
+constexpr int F_OFF_HX = 3 * FE_N;                        // 2208
+constexpr int F_OFF_HY = F_OFF_HX + 640;                  // 612 floats, rounded up
+constexpr int F_OFF_HZ = F_OFF_HY + FHY_W * FHY_R;        // 576
+constexpr int F_OFF_M = F_OFF_HZ + FHZ_W * FHZ_R;         // 544
+constexpr int F_STAGE = F_OFF_M + 3 * TYT * TZ / 4;       // material: 3 x 16 x 32 bytes; 4352 floats
+constexpr unsigned F_BYTES = (3 * FE_W * FE_R + FHX_W * FHX_R + FHY_W * FHY_R + FHZ_W * FHZ_R) * 4;
+constexpr unsigned F_BYTES_MAT = 3 * TYT * TZ;
 constexpr int F_NST = 3;
-constexpr int HN_P = 33;                    // new-H row pitch: z in [k0, k0+33)
-constexpr int HN_N = FHR * HN_P;            // per component
+constexpr int HN_P = TZ + 1;                 // new-H plane buffer: z in [k0, k0+33) ...
+constexpr int HN_N = (TYT + 1) * HN_P;       // ... y in [j0, j0+17), per component (Hx, Hy, Hz)
 constexpr int F_HN = ((3 * HN_N + 31) / 32) * 32;
+constexpr int FX_MAX = 64;                   // longest x chunk
 constexpr size_t F_SMEM_BYTES = (size_t)(F_NST * F_STAGE + 2 * F_HN) * 4 + sizeof(MatShared) + F_NST * 8 + 128;
+static_assert(F_OFF_HY % 32 == 0 && F_OFF_HZ % 32 == 0 && F_OFF_M % 32 == 0 && F_STAGE % 32 == 0, "128-byte boxes");
 
-// TMA descriptors of one buffer set: E tiles (40 x 17) and old H tiles (40 x 16)
+// TMA descriptors of one buffer set
 struct FusedMaps {
-  CUtensorMap e[3];
-  CUtensorMap h[3];
-  CUtensorMap mat[3];                       // 32 x 16 material tiles (rows j0 .. j0+15)
+  CUtensorMap e[3];                          // 40 x 18 E boxes
+  CUtensorMap hx, hy, hz;                    // old-H boxes
+  CUtensorMap mat[3];                        // 32 x 16 material tiles (the per-step kernels' maps)
 };
 
 // Per-launch arguments beyond Params (which describes the source buffer A)
 struct FusedArgs {
-  float* dst[6];                            // buffer B
-  float* hsrc[3][2];                        // CPML auxiliaries of H (slots 2, 3) in A
-  float* hdst[3][2];                        // ... and in B
-  const signed char* umat;                  // uniform material per (plane, 15-row tile, z tile)
-  int nty, ntz;
+  float* dst[6];                             // buffer B
+  float* hsrc[3][2];                         // CPML auxiliaries of H (slots 2, 3) in A
+  float* hdst[3][2];                         // ... and in B
 };
 
-// CPML correction of component c at a slab node (absorb_apply3 with the H
-// auxiliaries read from A and written to B; E auxiliaries in place).
-template <bool STORE>
-__device__ __forceinline__ float fused_absorb(const Params& p, const FusedArgs& fa, int c, const int (&idx)[3],
-                                              const int (&si)[3], const float* dif) {
+// staged-tile accessors (tile-local y, z)
+__device__ __forceinline__ float fE(const float* st, int c, int y, int z) { return st[c * FE_N + (y + 1) * FE_W + z + 4]; }
+__device__ __forceinline__ float fHx(const float* st, int y, int z) { return st[F_OFF_HX + y * FHX_W + z]; }
+__device__ __forceinline__ float fHy(const float* st, int y, int z) { return st[F_OFF_HY + y * FHY_W + z]; }
+__device__ __forceinline__ float fHz(const float* st, int y, int z) { return st[F_OFF_HZ + y * FHZ_W + z]; }
+__device__ __forceinline__ int fM(const float* st, int c, int y, int z) {
+  return reinterpret_cast<const uint8_t*>(st + F_OFF_M)[c * TYT * TZ + y * TZ + z];
+}
+__device__ __forceinline__ float& fN(float* hn, int q, int y, int z) { return hn[q * HN_N + y * HN_P + z]; }
+__device__ __forceinline__ float fN(const float* hn, int q, int y, int z) { return hn[q * HN_N + y * HN_P + z]; }
+
+// CPML correction of component C at node (i, j, k) with slab indices si
+// (absorb_apply3 of the CPML form); H auxiliaries read from A and written to
+// B, E auxiliaries in place.  store false: a node whose new value this CTA
+// does not own (halo, the plane after the chunk) reads its auxiliaries only.
+template <int C>
+__device__ __forceinline__ float fused_cpml(const Params& p, const FusedArgs& fa, const int (&idx)[3], const int (&si)[3],
+                                            const float (&dif)[3], bool store) {
   float corr = 0.f;
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    const int sl = slot_of(c, a);
+    const int sl = slot_of(C, a);
     if (sl < 0 || si[a] < 0) continue;
-    const float* src = c >= 3 ? fa.hsrc[a][sl - 2] : p.ab.aux[a][sl];
-    const float old = src[si[a]];
-    const int h = 2 * idx[a] + comp_off(c, a);
+    const int h = 2 * idx[a] + comp_off(C, a);
     const float k0 = __ldg(p.ab.c0[a] + h), k1 = __ldg(p.ab.c1[a] + h);
+    const float old = C >= 3 ? __ldg(fa.hsrc[a][sl - 2] + si[a]) : p.ab.aux[a][sl][si[a]];
     const float nv = __fmaf_rn(k0, old, __fmul_rn(k1, dif[a]));
-    if (STORE) (c >= 3 ? fa.hdst[a][sl - 2] : p.ab.aux[a][sl])[si[a]] = nv;
+    if (store) (C >= 3 ? fa.hdst[a][sl - 2] : p.ab.aux[a][sl])[si[a]] = nv;
     corr = __fadd_rn(corr, __fmaf_rn(__fsub_rn(__ldg(p.ab.c2[a] + h), 1.f), dif[a], nv));
   }
   return corr;
 }
 
-// staged-tile accessors: E rows y in [-1, 15], old H rows y in [0, 15], z in [-4, 35]
-__device__ __forceinline__ float fE(const float* st, int c, int y, int z) {
-  return st[F_OFF_E + c * FE_N + (y + 1) * FROW + z + FZO];
-}
-__device__ __forceinline__ float fH(const float* st, int c, int y, int z) {
-  return st[F_OFF_H + c * FH_N + y * FROW + z + FZO];
-}
-__device__ __forceinline__ int fM(const float* st, int c, int y, int z) {
-  return reinterpret_cast<const uint8_t*>(st + F_OFF_M)[c * FHR * FZ + y * FZ + z];
+// new H component C (3..5) = old + sum of the derivative terms d (+ CPML)
+template <int C, bool ABS>
+__device__ __forceinline__ float fused_hnode(const Params& p, const FusedArgs& fa, float old, float d0, float d1, float d2,
+                                             bool slab, const int (&idx)[3], const int (&si)[3], bool store) {
+  float inc = sum3(d0, d1, d2);
+  if (ABS && slab) {
+    const float dif[3] = {d0, d1, d2};
+    inc = __fadd_rn(inc, fused_cpml<C>(p, fa, idx, si, dif, store));
+  }
+  return __fadd_rn(old, inc);
 }
 
-// New H of component hc (3..5) at tile node (y, z) of plane i (stage cur, plane
-// i-1 in stage prv): the H expressions of plane_update, H taps at -1..0.
-// CPML slab nodes add the absorber correction (ABS).
-template <bool ABS, bool STORE>
-__device__ __forceinline__ float fused_h(const Params& p, const FusedArgs& fa, const float* cur, const float* prv,
-                                         int hc, int y, int z, int i, int j, int k) {
-  const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
-  float d[3];
-  if (hc == 3) {        // Hx -= dt (dy Ez - dz Ey)
-    d[0] = 0.f;
-    d[1] = __fmul_rn(-cy, __fsub_rn(fE(cur, 2, y, z), fE(cur, 2, y - 1, z)));
-    d[2] = __fmul_rn(cz, __fsub_rn(fE(cur, 1, y, z), fE(cur, 1, y, z - 1)));
-  } else if (hc == 4) { // Hy -= dt (dz Ex - dx Ez)
-    d[0] = __fmul_rn(cx, __fsub_rn(fE(cur, 2, y, z), fE(prv, 2, y, z)));
-    d[1] = 0.f;
-    d[2] = __fmul_rn(-cz, __fsub_rn(fE(cur, 0, y, z), fE(cur, 0, y, z - 1)));
-  } else {              // Hz -= dt (dx Ey - dy Ex)
-    d[0] = __fmul_rn(-cx, __fsub_rn(fE(cur, 1, y, z), fE(prv, 1, y, z)));
-    d[1] = __fmul_rn(cy, __fsub_rn(fE(cur, 0, y, z), fE(cur, 0, y - 1, z)));
-    d[2] = 0.f;
-  }
-  float inc = sum3(d[0], d[1], d[2]);
-  if (ABS) {
-    int si[3];
-    if (node_slabs(p, i, j, k, si)) {
-      const int idx[3] = {i, j, k};
-      inc = __fadd_rn(inc, fused_absorb<STORE>(p, fa, hc, idx, si, d));
-    }
-  }
-  return __fadd_rn(fH(cur, hc - 3, y, z), inc);
+// ---- absorber tiles
+// CPML coefficients are staged per CTA in shared memory, 6 floats per node
+// coordinate v of an axis: b, a, 1/kappa - 1 at half-coordinate 2v (the H
+// components' offset along a derivative axis) and at 2v + 1 (the E
+// components').  Rows: x planes x0-1 .. x0+FX_MAX, y rows j0 .. j0+16, z
+// columns k0 .. k0+32.
+constexpr int FCO_X = 0, FCO_Y = (FX_MAX + 2) * 6, FCO_Z = FCO_Y + (TYT + 1) * 6, FCO_N = FCO_Z + (TZ + 1) * 6;
+
+// index of coordinate v in the slab of its axis (-1 outside)
+__device__ __forceinline__ int slab_cs(const Params& p, int a, int v) {
+  const int n = p.g.n[a], lo = p.ab.L[a][0], hi = p.ab.L[a][1];
+  return v < lo ? v : (v >= n - hi ? lo + v - (n - hi) : -1);
 }
 
-// New H of plane i over the 16 x 33 region into hn (and the own nodes into B).
-// cur: stage of plane i, prv: stage of plane i-1.  Values outside the grid are
-// zero; STORE_B: plane i belongs to this chunk.
-template <bool ABS>
-__device__ __forceinline__ void fused_h_plane(const Params& p, const FusedArgs& fa, const float* cur, const float* prv,
-                                              float* hn, int i, int j0, int k0, bool store_b) {
+// slab indices of node (i, j, k) along the axes of AXM (bit a: axis a may hold
+// a slab), from its slab coordinates xs, ys, zs (-1 outside); the slab_index32 layouts
+template <int AXM>
+__device__ __forceinline__ void fused_slabs(const Params& p, int i, int j, int k, int xs, int ys, int zs, int (&si)[3]) {
+  si[0] = ((AXM & 1) && xs >= 0) ? (xs * p.g.n[1] + j) * p.g.n[2] + k : -1;
+  si[1] = ((AXM & 2) && ys >= 0) ? (i * (p.ab.L[1][0] + p.ab.L[1][1]) + ys) * p.g.n[2] + k : -1;
+  si[2] = ((AXM & 4) && zs >= 0) ? (i * p.g.n[1] + j) * (p.ab.L[2][0] + p.ab.L[2][1]) + zs : -1;
+}
+
+// the old auxiliaries of one node for one half of the update: per slab axis a
+// the two slots of that axis (H: slots 2, 3 from A; E: slots 0, 1 in place)
+template <int AXM, bool ISH>
+__device__ __forceinline__ void fused_aux_load(const Params& p, const FusedArgs& fa, const int (&si)[3], float (&old)[3][2]) {
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    old[a][0] = 0.f; old[a][1] = 0.f;
+    if (!((AXM >> a) & 1) || si[a] < 0) continue;
+    if (ISH) { old[a][0] = __ldg(fa.hsrc[a][0] + si[a]); old[a][1] = __ldg(fa.hsrc[a][1] + si[a]); }
+    else { old[a][0] = p.ab.aux[a][0][si[a]]; old[a][1] = p.ab.aux[a][1][si[a]]; }
+  }
+}
+
+// CPML correction of component C from preloaded auxiliaries and staged
+// coefficients (the arithmetic of absorb_apply3, CPML form); store: the new
+// auxiliaries belong to this CTA.  Every axis of AXM takes part without a
+// branch: off its slab a node reads 0 and the coefficients there are b = 1,
+// a = 0, 1/kappa - 1 = 0, so its term is exactly zero and nothing is stored.
+template <int C, int AXM>
+__device__ __forceinline__ float fused_aux_apply(const Params& p, const FusedArgs& fa, const int (&si)[3],
+                                                 const float (&old)[3][2], const float (&dif)[3], const float* cx,
+                                                 const float* cy, const float* cz, bool store) {
+  float corr = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const int sl = slot_of(C, a);
+    if (sl < 0 || !((AXM >> a) & 1)) continue;
+    const int q = sl & 1;
+    const float* cf = (a == 0 ? cx : a == 1 ? cy : cz) + (C >= 3 ? 0 : 3);
+    const float nv = __fmaf_rn(cf[0], old[a][q], __fmul_rn(cf[1], dif[a]));
+    if (store && si[a] >= 0) (C >= 3 ? fa.hdst[a][q] : p.ab.aux[a][q])[si[a]] = nv;
+    corr = __fadd_rn(corr, __fmaf_rn(cf[2], dif[a], nv));
+  }
+  return corr;
+}
+
+// New H of plane i on the thread's own nodes: hc (registers), hn (shared
+// plane buffer), B (when the chunk owns plane i).  ec gets the old E of the
+// own nodes (the next plane's x taps and its E update); ep holds those of
+// plane i - 1.  AXM: the slab axes of the tile-plane (0: no absorber); the
+// slab coordinates xs (plane), ys (rows), zs (column) are per-thread constants.
+template <int AXM>
+__device__ __forceinline__ void fused_h_own(const Params& p, const FusedArgs& fa, const float* st, float* hn, int i,
+                                            int j0, int k0, bool store, const bool (&ok)[RY], const float (&ep)[RY][3],
+                                            float (&hc)[RY][3], float (&ec)[RY][3], const float* fco, int xs,
+                                            const int (&ys)[RY], int zs) {
   const int lane = threadIdx.x, w = threadIdx.y;
-  const int k = k0 + lane;
-  const bool in_x = i < p.g.n[0];
+  const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
   const long long pb = (long long)i * p.g.sx;
+  int si[RY][3];
+  float old[RY][3][2];
+  if (AXM) {
+    // every auxiliary of the thread's nodes is requested before any is used
 #pragma unroll
-  for (int r = 0; r < 2; r++) {
-    const int y = w + FW * r, j = j0 + y;
-    const bool ok = in_x && j < p.g.n[1] && k < p.g.n[2];
-    const bool own = y < FTY && store_b && ok;
-    const long long off = pb + (long long)j * p.g.sy + k;
-#pragma unroll
-    for (int hc = 3; hc < 6; hc++) {
-      float v = 0.f;
-      if (ok) {
-        v = own ? fused_h<ABS, true>(p, fa, cur, prv, hc, y, lane, i, j, k)
-                : fused_h<ABS, false>(p, fa, cur, prv, hc, y, lane, i, j, k);
-        if (own) fa.dst[hc][off] = v;
-      }
-      hn[(hc - 3) * HN_N + y * HN_P + lane] = v;
+    for (int r = 0; r < RY; r++) {
+      fused_slabs<AXM>(p, i, j0 + w + TW * r, k0 + lane, xs, ys[r], zs, si[r]);
+      if (!ok[r]) si[r][0] = si[r][1] = si[r][2] = -1;
+      fused_aux_load<AXM, true>(p, fa, si[r], old[r]);
     }
   }
-  // the halo column z = k0+32: Hy on rows 0-14 by warps 0-3, Hx by warps 4-7 (lanes 0-3)
-  {
-    const int hc = w < 4 ? 4 : 3;
-    const int y = (w & 3) * 4 + lane;
-    if (lane < 4 && y < FTY) {
-      const int j = j0 + y, kk = k0 + FZ;
-      const bool ok = in_x && j < p.g.n[1] && kk < p.g.n[2];
-      hn[(hc - 3) * HN_N + y * HN_P + FZ] = ok ? fused_h<ABS, false>(p, fa, cur, prv, hc, y, FZ, i, j, kk) : 0.f;
+#pragma unroll
+  for (int r = 0; r < RY; r++) {
+    const int y = w + TW * r, j = j0 + y, k = k0 + lane;
+    const float ez = fE(st, 2, y, lane), ey = fE(st, 1, y, lane), ex = fE(st, 0, y, lane);
+    ec[r][0] = ex; ec[r][1] = ey; ec[r][2] = ez;
+    // Hx -= dt(dy Ez - dz Ey); Hy -= dt(dz Ex - dx Ez); Hz -= dt(dx Ey - dy Ex)
+    const float dhx[3] = {0.f, __fmul_rn(-cy, __fsub_rn(ez, fE(st, 2, y - 1, lane))),
+                         __fmul_rn(cz, __fsub_rn(ey, fE(st, 1, y, lane - 1)))};
+    const float dhy[3] = {__fmul_rn(cx, __fsub_rn(ez, ep[r][2])), 0.f,
+                         __fmul_rn(-cz, __fsub_rn(ex, fE(st, 0, y, lane - 1)))};
+    const float dhz[3] = {__fmul_rn(-cx, __fsub_rn(ey, ep[r][1])), __fmul_rn(cy, __fsub_rn(ex, fE(st, 0, y - 1, lane))),
+                         0.f};
+    float ix = sum3(dhx[0], dhx[1], dhx[2]), iy = sum3(dhy[0], dhy[1], dhy[2]), iz = sum3(dhz[0], dhz[1], dhz[2]);
+    if (AXM && (si[r][0] & si[r][1] & si[r][2]) >= 0) {
+      const float* fx = fco + FCO_X + (i - p.x0 - blockIdx.z * p.xchunk + 1) * 6;
+      const float* fy = fco + FCO_Y + y * 6;
+      const float* fz = fco + FCO_Z + lane * 6;
+      ix = __fadd_rn(ix, fused_aux_apply<3, AXM>(p, fa, si[r], old[r], dhx, fx, fy, fz, store));
+      iy = __fadd_rn(iy, fused_aux_apply<4, AXM>(p, fa, si[r], old[r], dhy, fx, fy, fz, store));
+      iz = __fadd_rn(iz, fused_aux_apply<5, AXM>(p, fa, si[r], old[r], dhz, fx, fy, fz, store));
+    }
+    float vx = __fadd_rn(fHx(st, y, lane), ix), vy = __fadd_rn(fHy(st, y, lane), iy), vz = __fadd_rn(fHz(st, y, lane), iz);
+    if (!ok[r]) { vx = 0.f; vy = 0.f; vz = 0.f; }
+    hc[r][0] = vx; hc[r][1] = vy; hc[r][2] = vz;
+    fN(hn, 0, y, lane) = vx;
+    fN(hn, 1, y, lane) = vy;
+    fN(hn, 2, y, lane) = vz;
+    if (store && ok[r]) {
+      const long long off = pb + (long long)j * p.g.sy + k;
+      fa.dst[3][off] = vx;
+      fa.dst[4][off] = vy;
+      fa.dst[5][off] = vz;
     }
   }
 }
 
-// New E of plane i on the own nodes: the E expressions of plane_update, E taps
-// at 0..+1, from the new H of planes i (h0) and i+1 (h1).
-//   MODE 1: uniform non-dispersive material um, no absorber
-//   MODE 2: uniform material um, absorber slabs in the tile
-//   MODE 0: general (mixed materials, dispersive nodes left to the ADE pass,
-//           design region, absorber)
-template <int MODE>
-__device__ __forceinline__ void fused_e_plane(const Params& p, const FusedArgs& fa, const float* cur, const float* h0,
-                                              const float* h1, const MatShared& ms, int um, int i, int j0, int k0) {
+// The halo of the new-H plane buffer (values the E update of the tile reads
+// beyond its own nodes), one component per warp:
+//   warp 0: Hz of row 16      warp 1: Hx of row 16
+//   warp 2: Hy of column 32   warp 3: Hx of column 32 (lanes 0-15)
+// xe: the warp's old E of the previous plane at its halo node (x tap), updated.
+// A CPML slab node takes the correction with the auxiliaries read, not written.
+template <bool ABS>
+__device__ __forceinline__ void fused_h_halo(const Params& p, const FusedArgs& fa, const float* st, float* hn, int i,
+                                             int j0, int k0, float& xe) {
   const int lane = threadIdx.x, w = threadIdx.y;
-  const int k = k0 + lane;
+  if (w > 3 || (w > 1 && lane >= TYT)) return;
   const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
-  if (i >= p.g.n[0] || k >= p.g.n[2]) return;
+  const bool row = w < 2;
+  const int y = row ? TYT : lane, z = row ? lane : TZ;
+  const int j = j0 + y, k = k0 + z;
+  const bool ok = j < p.g.n[1] && k < p.g.n[2];
+  int si[3] = {-1, -1, -1};
+  const int idx[3] = {i, j, k};
+  const bool slab = ABS && ok && node_slabs(p, i, j, k, si);
+  float v;
+  if (w == 0) {
+    const float ey = fE(st, 1, y, z);
+    const float d0 = __fmul_rn(-cx, __fsub_rn(ey, xe));
+    const float d1 = __fmul_rn(cy, __fsub_rn(fE(st, 0, y, z), fE(st, 0, y - 1, z)));
+    v = fused_hnode<5, ABS>(p, fa, fHz(st, y, z), d0, d1, 0.f, slab, idx, si, false);
+    xe = ey;
+  } else if (w == 2) {
+    const float ez = fE(st, 2, y, z);
+    const float d0 = __fmul_rn(cx, __fsub_rn(ez, xe));
+    const float d2 = __fmul_rn(-cz, __fsub_rn(fE(st, 0, y, z), fE(st, 0, y, z - 1)));
+    v = fused_hnode<4, ABS>(p, fa, fHy(st, y, z), d0, 0.f, d2, slab, idx, si, false);
+    xe = ez;
+  } else {
+    const float d1 = __fmul_rn(-cy, __fsub_rn(fE(st, 2, y, z), fE(st, 2, y - 1, z)));
+    const float d2 = __fmul_rn(cz, __fsub_rn(fE(st, 1, y, z), fE(st, 1, y, z - 1)));
+    v = fused_hnode<3, ABS>(p, fa, fHx(st, y, z), 0.f, d1, d2, slab, idx, si, false);
+  }
+  fN(hn, w == 0 ? 2 : w == 2 ? 1 : 0, y, z) = ok ? v : 0.f;
+}
+
+// New E of plane i on the own nodes.  ep: old E (registers), hn: new H of
+// plane i (shared), hc: new H of plane i + 1 (own nodes).
+//   MODE 1: uniform non-dispersive material um
+//   MODE 0: general (mixed materials, dispersive nodes left to the ADE pass,
+//           design region)
+// AXM: the slab axes of the tile-plane (0: no absorber).
+template <int MODE, int AXM>
+__device__ __forceinline__ void fused_e_own(const Params& p, const FusedArgs& fa, const float* st, const float* hn,
+                                            const MatShared& ms, int um, int i, int j0, int k0, const bool (&ok)[RY],
+                                            const float (&ep)[RY][3], const float (&hc)[RY][3], const float* fco, int xs,
+                                            const int (&ys)[RY], int zs) {
+  const int lane = threadIdx.x, w = threadIdx.y;
+  const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
   float iu[3] = {1.f, 1.f, 1.f};
   if (MODE != 0) { iu[0] = ms.inv_eps[um][0]; iu[1] = ms.inv_eps[um][1]; iu[2] = ms.inv_eps[um][2]; }
   const long long pb = (long long)i * p.g.sx;
+  int si[RY][3];
+  float old[RY][3][2];
+  if (AXM) {
 #pragma unroll
-  for (int r = 0; r < 2; r++) {
-    const int y = w + FW * r, j = j0 + y;
-    if (y >= FTY || j >= p.g.n[1]) continue;
+    for (int r = 0; r < RY; r++) {
+      fused_slabs<AXM>(p, i, j0 + w + TW * r, k0 + lane, xs, ys[r], zs, si[r]);
+      if (!ok[r]) si[r][0] = si[r][1] = si[r][2] = -1;
+      fused_aux_load<AXM, false>(p, fa, si[r], old[r]);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < RY; r++) {
+    if (!ok[r]) continue;
+    const int y = w + TW * r, j = j0 + y, k = k0 + lane;
     const long long off = pb + (long long)j * p.g.sy + k;
-    const float* hx = h0;
-    const float* hy = h0 + HN_N;
-    const float* hz = h0 + 2 * HN_N;
-    const int q = y * HN_P + lane;
+    const float hx = fN(hn, 0, y, lane), hy = fN(hn, 1, y, lane), hz = fN(hn, 2, y, lane);
+    // Ex += dt/eps(dy Hz - dz Hy); Ey += dt/eps(dz Hx - dx Hz); Ez += dt/eps(dx Hy - dy Hx)
     float d[3][3];
-    // Ex += dt/eps (dy Hz - dz Hy); Ey += dt/eps (dz Hx - dx Hz); Ez += dt/eps (dx Hy - dy Hx)
     d[0][0] = 0.f;
-    d[0][1] = __fmul_rn(cy, __fsub_rn(hz[q + HN_P], hz[q]));
-    d[0][2] = __fmul_rn(-cz, __fsub_rn(hy[q + 1], hy[q]));
-    d[1][0] = __fmul_rn(-cx, __fsub_rn(h1[2 * HN_N + q], hz[q]));
+    d[0][1] = __fmul_rn(cy, __fsub_rn(fN(hn, 2, y + 1, lane), hz));
+    d[0][2] = __fmul_rn(-cz, __fsub_rn(fN(hn, 1, y, lane + 1), hy));
+    d[1][0] = __fmul_rn(-cx, __fsub_rn(hc[r][2], hz));
     d[1][1] = 0.f;
-    d[1][2] = __fmul_rn(cz, __fsub_rn(hx[q + 1], hx[q]));
-    d[2][0] = __fmul_rn(cx, __fsub_rn(h1[HN_N + q], hy[q]));
-    d[2][1] = __fmul_rn(-cy, __fsub_rn(hx[q + HN_P], hx[q]));
+    d[1][2] = __fmul_rn(cz, __fsub_rn(fN(hn, 0, y, lane + 1), hx));
+    d[2][0] = __fmul_rn(cx, __fsub_rn(hc[r][1], hy));
+    d[2][1] = __fmul_rn(-cy, __fsub_rn(fN(hn, 0, y + 1, lane), hx));
     d[2][2] = 0.f;
-    int si[3] = {-1, -1, -1};
-    const bool ab = (MODE != 1) && p.ab.kind != 0 && node_slabs(p, i, j, k, si);
-    const int idx3[3] = {i, j, k};
+    const bool slab = AXM && (si[r][0] & si[r][1] & si[r][2]) >= 0;
+    const float* fx = fco + FCO_X + (i - p.x0 - blockIdx.z * p.xchunk + 1) * 6;
+    const float* fy = fco + FCO_Y + y * 6;
+    const float* fz = fco + FCO_Z + lane * 6;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const float F = fE(cur, c, y, lane);
       float ie = iu[c];
       if (MODE == 0) {
-        const int m = um >= 0 ? um : fM(cur, c, y, lane);
-        if (ms.npoles[m] > 0) continue;               // dispersive node: the ADE pass writes it
+        const int m = um >= 0 ? um : fM(st, c, y, lane);
+        if (ms.npoles[m] > 0) continue;              // dispersive node: the ADE pass writes it
         ie = ms.inv_eps[m][c];
         if (p.des_on) {
           const long long di = design_index(p, i, j, k);
@@ -230,108 +341,173 @@ __device__ __forceinline__ void fused_e_plane(const Params& p, const FusedArgs& 
       }
       d[c][0] = __fmul_rn(d[c][0], ie); d[c][1] = __fmul_rn(d[c][1], ie); d[c][2] = __fmul_rn(d[c][2], ie);
       float inc = sum3(d[c][0], d[c][1], d[c][2]);
-      if (ab) inc = __fadd_rn(inc, fused_absorb<true>(p, fa, c, idx3, si, d[c]));
-      fa.dst[c][off] = __fadd_rn(F, inc);
+      if (slab) {
+        if (c == 0) inc = __fadd_rn(inc, fused_aux_apply<0, AXM>(p, fa, si[r], old[r], d[0], fx, fy, fz, true));
+        else if (c == 1) inc = __fadd_rn(inc, fused_aux_apply<1, AXM>(p, fa, si[r], old[r], d[1], fx, fy, fz, true));
+        else inc = __fadd_rn(inc, fused_aux_apply<2, AXM>(p, fa, si[r], old[r], d[2], fx, fy, fz, true));
+      }
+      fa.dst[c][off] = __fadd_rn(ep[r][c], inc);
     }
   }
 }
 
-// Issue the copies of plane ip into a stage (one thread).
-__device__ __forceinline__ void fused_stage(const FusedMaps& m, float* st, uint64_t* bar, int ip, int j0, int k0,
+// Issue the copies of stage s (plane x0 - 1 + s; the material tiles of the
+// plane before it, whose E update runs while this stage is current).
+__device__ __forceinline__ void fused_issue(const FusedMaps& m, float* st, uint64_t* bar, int ip, int j0, int k0,
                                             bool want_mat) {
   mbar_arrive_expect_tx(bar, F_BYTES + (want_mat ? F_BYTES_MAT : 0u));
 #pragma unroll
-  for (int c = 0; c < 3; c++) tma_load_3d(st + F_OFF_E + c * FE_N, &m.e[c], k0 - FZO, j0 - 1, ip, bar);
-#pragma unroll
-  for (int c = 0; c < 3; c++) tma_load_3d(st + F_OFF_H + c * FH_N, &m.h[c], k0 - FZO, j0, ip, bar);
+  for (int c = 0; c < 3; c++) tma_load_3d(st + c * FE_N, &m.e[c], k0 - 4, j0 - 1, ip, bar);
+  tma_load_3d(st + F_OFF_HX, &m.hx, k0, j0, ip, bar);
+  tma_load_3d(st + F_OFF_HY, &m.hy, k0, j0, ip, bar);
+  tma_load_3d(st + F_OFF_HZ, &m.hz, k0, j0, ip, bar);
   if (want_mat)
 #pragma unroll
     for (int c = 0; c < 3; c++)
-      tma_load_3d(reinterpret_cast<uint8_t*>(st + F_OFF_M) + c * FHR * FZ, &m.mat[c], k0, j0, ip, bar);
+      tma_load_3d(reinterpret_cast<uint8_t*>(st + F_OFF_M) + c * TYT * TZ, &m.mat[c], k0, j0, ip - 1, bar);
 }
 
-// the plane's absorber test over the region whose new H the CTA computes (y
-// up to j0+15, z up to k0+32) -- a superset of the E tile
-__device__ __forceinline__ bool fused_tile_abs(const Params& p, int i, int j0, int k0) {
-  if (p.ab.kind == 0) return false;
-  return in_slab(p, 0, i) || j0 < p.ab.L[1][0] || j0 + FHR > p.g.n[1] - p.ab.L[1][1] || k0 < p.ab.L[2][0] ||
-         k0 + FZ + 1 > p.g.n[2] - p.ab.L[2][1];
+// H of plane i over the own nodes for the tile-plane's slab axes m (bit 0: x
+// slab plane, bit 1: y slab rows, bit 2: z slab columns).  Tile-planes with
+// any slab take one general variant: variants per slab combination were
+// measured slower on every workload (a larger kernel).
+__device__ __forceinline__ void fused_h_dispatch(int m, const Params& p, const FusedArgs& fa, const float* st, float* hn,
+                                                 int i, int j0, int k0, bool store, const bool (&ok)[RY],
+                                                 const float (&ep)[RY][3], float (&hc)[RY][3], float (&ec)[RY][3],
+                                                 const float* fco, int xs, const int (&ys)[RY], int zs) {
+  switch (m) {
+    case 0: fused_h_own<0>(p, fa, st, hn, i, j0, k0, store, ok, ep, hc, ec, fco, xs, ys, zs); break;
+    default: fused_h_own<7>(p, fa, st, hn, i, j0, k0, store, ok, ep, hc, ec, fco, xs, ys, zs); break;
+  }
+}
+template <int MODE>
+__device__ __forceinline__ void fused_e_dispatch(int m, const Params& p, const FusedArgs& fa, const float* st,
+                                                 const float* hn, const MatShared& ms, int um, int i, int j0, int k0,
+                                                 const bool (&ok)[RY], const float (&ep)[RY][3], const float (&hc)[RY][3],
+                                                 const float* fco, int xs, const int (&ys)[RY], int zs) {
+  switch (m) {
+    case 0: fused_e_own<MODE, 0>(p, fa, st, hn, ms, um, i, j0, k0, ok, ep, hc, fco, xs, ys, zs); break;
+    default: fused_e_own<MODE, 7>(p, fa, st, hn, ms, um, i, j0, k0, ok, ep, hc, fco, xs, ys, zs); break;
+  }
 }
 
-// 3 CTAs per SM (68 KB of shared memory each)
-__global__ void __launch_bounds__(FNTHR, 3)
+// 3 CTAs per SM (shared memory: a 3-stage ring and two new-H planes)
+__global__ void __launch_bounds__(NTHR, 3)
     fused_kernel(const __grid_constant__ Params p, const __grid_constant__ FusedArgs fa,
                  const __grid_constant__ FusedMaps m) {
   extern __shared__ __align__(128) float fsm[];
   float* hnb = fsm + F_NST * F_STAGE;                      // two new-H planes
   MatShared& ms = *reinterpret_cast<MatShared*>(hnb + 2 * F_HN);
   uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(&ms) + sizeof(MatShared));
+  __shared__ signed char umc[FX_MAX];
+  __shared__ float fco[FCO_N];
   __shared__ int gave_up;
-  const int lane = threadIdx.x, w = threadIdx.y, tid = w * FZ + lane;
-  const int k0 = blockIdx.x * FZ, ty = blockIdx.y, j0 = ty * FTY;
+  const int lane = threadIdx.x, w = threadIdx.y, tid = w * TZ + lane;
+  const int k0 = blockIdx.x * TZ, j0 = blockIdx.y * TYT;
   const int x0 = p.x0 + blockIdx.z * p.xchunk;
   const int x1 = min(x0 + p.xchunk, p.x1);
   const int len = x1 - x0;
-  // stage number s holds plane x0 - 1 + s; planes x0-1 .. x1 (len + 2 stages)
-  const int slast = len + 1;
-  auto umat = [&](int ip) -> int {
-    return (ip >= 0 && ip < p.g.n[0]) ? (int)__ldg(fa.umat + ((long long)ip * fa.nty + ty) * fa.ntz + blockIdx.x) : 0;
-  };
+  const int slast = len + 1;                               // stages 0 .. len + 1: planes x0 - 1 .. x1
+  const bool cpml = p.ab.kind == 1;
   if (tid == 0) {
     for (int q = 0; q < F_NST; q++) mbar_init(&bars[q], 1);
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     gave_up = 0;
   }
   load_matshared(ms, p);
+  for (int q = tid; q < len; q += NTHR)
+    umc[q] = __ldg(p.umat + ((long long)(x0 + q) * p.nty + blockIdx.y) * p.ntz + blockIdx.x);
+  if (cpml)
+    for (int q = tid; q < FCO_N / 6; q += NTHR) {
+      // row q: x plane x0 - 1 + q, y row j0 + q - (FX_MAX + 2), z column k0 + q - (FX_MAX + TYT + 3)
+      const int a = q < FX_MAX + 2 ? 0 : q < FX_MAX + TYT + 3 ? 1 : 2;
+      const int v = a == 0 ? x0 - 1 + q : a == 1 ? j0 + q - (FX_MAX + 2) : k0 + q - (FX_MAX + TYT + 3);
+#pragma unroll
+      for (int o = 0; o < 2; o++) {
+        const int h = 2 * v + o;
+        const bool in = h >= 0 && h < 2 * p.g.n[a] + 2;
+        fco[q * 6 + 3 * o + 0] = in ? __ldg(p.ab.c0[a] + h) : 1.f;
+        fco[q * 6 + 3 * o + 1] = in ? __ldg(p.ab.c1[a] + h) : 0.f;
+        fco[q * 6 + 3 * o + 2] = in ? __fsub_rn(__ldg(p.ab.c2[a] + h), 1.f) : 0.f;
+      }
+    }
   __syncthreads();
+  auto issue = [&](int s) {
+    const int ip = x0 - 1 + s;
+    fused_issue(m, fsm + (s % F_NST) * F_STAGE, &bars[s % F_NST], ip, j0, k0, ip - 1 >= x0 && umc[ip - 1 - x0] < 0);
+  };
+  int issued = -1;
   if (tid == 0)
-    for (int s = 0; s <= 2 && s <= slast; s++) {
-      const int ip = x0 - 1 + s;
-      fused_stage(m, fsm + (s % F_NST) * F_STAGE, &bars[s % F_NST], ip, j0, k0, ip >= x0 && ip < x1 && umat(ip) < 0);
-    }
-  // prologue: the new H of plane x0 (needs planes x0-1 and x0)
-  const bool ok = mbar_wait(&bars[0], 0u, p.err, p.wait_limit) && mbar_wait(&bars[1], 0u, p.err, p.wait_limit);
-  if (__syncthreads_or(!ok)) gave_up = 1;
-  int issued = min(2, slast);
+    for (int s = 0; s < F_NST && s <= slast; s++) { issue(s); issued = s; }
+  // per-thread constants of the walk
+  bool ok[RY];
+  int ys[RY];
+#pragma unroll
+  for (int r = 0; r < RY; r++) {
+    ok[r] = j0 + w + TW * r < p.g.n[1] && k0 + lane < p.g.n[2];
+    ys[r] = cpml ? slab_cs(p, 1, j0 + w + TW * r) : -1;
+  }
+  const int zs = cpml ? slab_cs(p, 2, k0 + lane) : -1;
+  // slab axes of the own nodes (y, z: fixed for the walk) and of the halo (row 16, column 32)
+  const int myz = cpml ? ((j0 < p.ab.L[1][0] || j0 + TYT > p.g.n[1] - p.ab.L[1][1]) ? 2 : 0) |
+                             ((k0 < p.ab.L[2][0] || k0 + TZ > p.g.n[2] - p.ab.L[2][1]) ? 4 : 0)
+                       : 0;
+  const bool halo_yz = cpml && (j0 < p.ab.L[1][0] || j0 + TYT + 1 > p.g.n[1] - p.ab.L[1][1] || k0 < p.ab.L[2][0] ||
+                                k0 + TZ + 1 > p.g.n[2] - p.ab.L[2][1]);
+  float ep[RY][3], hc[RY][3], ec[RY][3];
+  float xe = 0.f;
+  // stage 0 (plane x0 - 1): the old E of the own nodes and of the halo nodes (x taps)
+  if (tid == 0 && !mbar_wait(&bars[0], 0u, p.err, p.wait_limit)) gave_up = 1;
+  __syncthreads();
+  int t = 0, swait = 0;                                    // swait: the stage waited for last
   if (!gave_up) {
-    const float* prv = fsm;
-    const float* cur = fsm + F_STAGE;
-    if (fused_tile_abs(p, x0, j0, k0)) fused_h_plane<true>(p, fa, cur, prv, hnb, x0, j0, k0, true);
-    else fused_h_plane<false>(p, fa, cur, prv, hnb, x0, j0, k0, true);
-  }
-  for (int t = 0; t < len && !gave_up; t++) {
-    const int i = x0 + t;
-    // the stage of plane i+1 (every thread waits: the barrier phase completes for all at once)
-    const int sw = t + 2;
-    const bool got = mbar_wait(&bars[sw % F_NST], (unsigned)((sw / F_NST) & 1), p.err, p.wait_limit);
-    // every thread is past step t-1 here: the stage of plane i-1 and new-H buffer t+1 are free
-    if (__syncthreads_or(!got)) { gave_up = 1; break; }
-    const int s_next = t + 3;                               // stage of plane i+2
-    if (tid == 0 && s_next <= slast) {
-      const int ip = x0 - 1 + s_next;
-      fused_stage(m, fsm + (s_next % F_NST) * F_STAGE, &bars[s_next % F_NST], ip, j0, k0, ip < x1 && umat(ip) < 0);
-      issued = s_next;
+#pragma unroll
+    for (int r = 0; r < RY; r++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) ep[r][c] = fE(fsm, c, w + TW * r, lane);
+    if (w == 0) xe = fE(fsm, 1, TYT, lane);
+    else if (w == 2 && lane < TYT) xe = fE(fsm, 2, lane, TZ);
+    for (; t <= len; t++) {
+      const int s = t + 1, pc = x0 + t;
+      swait = s;
+      if (tid == 0 && !mbar_wait(&bars[s % F_NST], (unsigned)((s / F_NST) & 1), p.err, p.wait_limit)) gave_up = 1;
+      // every thread is past iteration t - 1: the slot of stage t and the new-H
+      // plane written two iterations ago are free
+      __syncthreads();
+      if (gave_up) break;
+      if (tid == 0 && t + F_NST <= slast) { issue(t + F_NST); issued = t + F_NST; }
+      const float* st = fsm + (s % F_NST) * F_STAGE;
+      float* hn1 = hnb + (t & 1) * F_HN;                   // new H of plane pc
+      const float* hn0 = hnb + ((t + 1) & 1) * F_HN;       // new H of plane pc - 1
+      if (pc < p.g.n[0]) {
+        const int xs = cpml ? slab_cs(p, 0, pc) : -1;
+        fused_h_dispatch(myz | (xs >= 0 ? 1 : 0), p, fa, st, hn1, pc, j0, k0, t < len, ok, ep, hc, ec, fco, xs, ys, zs);
+        if (halo_yz || xs >= 0) fused_h_halo<true>(p, fa, st, hn1, pc, j0, k0, xe);
+        else fused_h_halo<false>(p, fa, st, hn1, pc, j0, k0, xe);
+      } else {
+        // beyond the last plane of the grid: H is zero there
+#pragma unroll
+        for (int r = 0; r < RY; r++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) { hc[r][c] = 0.f; ec[r][c] = 0.f; }
+      }
+      if (t >= 1) {
+        const int pe = pc - 1;
+        const int um = umc[pe - x0];
+        const int xs = cpml ? slab_cs(p, 0, pe) : -1;
+        const int mm = myz | (xs >= 0 ? 1 : 0);
+        if (um >= 0) fused_e_dispatch<1>(mm, p, fa, st, hn0, ms, um, pe, j0, k0, ok, ep, hc, fco, xs, ys, zs);
+        else fused_e_dispatch<0>(mm, p, fa, st, hn0, ms, um, pe, j0, k0, ok, ep, hc, fco, xs, ys, zs);
+      }
+#pragma unroll
+      for (int r = 0; r < RY; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) ep[r][c] = ec[r][c];
     }
-    const float* sti = fsm + ((t + 1) % F_NST) * F_STAGE;  // plane i
-    const float* st1 = fsm + (sw % F_NST) * F_STAGE;       // plane i+1
-    const float* h0 = hnb + (t & 1) * F_HN;                 // new H of plane i
-    float* h1 = hnb + ((t + 1) & 1) * F_HN;                 // new H of plane i+1
-    // new H of plane i+1 (stored to B only when the chunk owns it)
-    if (fused_tile_abs(p, i + 1, j0, k0)) fused_h_plane<true>(p, fa, st1, sti, h1, i + 1, j0, k0, i + 1 < x1);
-    else fused_h_plane<false>(p, fa, st1, sti, h1, i + 1, j0, k0, i + 1 < x1);
-    __syncthreads();
-    const int um = umat(i);
-    const bool eab = p.ab.kind != 0 && (in_slab(p, 0, i) || j0 < p.ab.L[1][0] || j0 + FTY > p.g.n[1] - p.ab.L[1][1] ||
-                                        k0 < p.ab.L[2][0] || k0 + FZ > p.g.n[2] - p.ab.L[2][1]);
-    if (um >= 0 && !eab) fused_e_plane<1>(p, fa, sti, h0, h1, ms, um, i, j0, k0);
-    else if (um >= 0) fused_e_plane<2>(p, fa, sti, h0, h1, ms, um, i, j0, k0);
-    else fused_e_plane<0>(p, fa, sti, h0, h1, ms, um, i, j0, k0);
   }
-  if (gave_up) {
+  if (gave_up && tid == 0) {
     // a wait gave up: no further copies were issued; wait (bounded) for those in flight, then leave
-    if (tid == 0)
-      for (int s = max(0, issued - 2); s <= issued; s++)
-        mbar_wait(&bars[s % F_NST], (unsigned)((s / F_NST) & 1), nullptr, DRAIN_POLLS);
+    for (int s = swait; s <= issued; s++) mbar_wait(&bars[s % F_NST], (unsigned)((s / F_NST) & 1), nullptr, DRAIN_POLLS);
   }
 }
 

@@ -416,8 +416,16 @@ int  dtmx_load_state(dtmx_ctx* ctx, const char* path);
 int  dtmx_count_nonfinite_noalloc(const float* const* d_fields, int nfields, int64_t nelem, int64_t* count_out);
 
 /* Engine choice for dtmx_step: 0 = auto, 1 = one launch per half step,
- * 2 = L2-resident wavefront (several time steps per launch). */
+ * 2 = L2-resident wavefront (several time steps per launch), 3 = single sweep
+ * (one launch per time step updating H and then E over two field buffers; box
+ * geometry, order 2, CPML or no absorber).  The reference compiles its kernel
+ * families per build (chooseV.h:3-38); here the choice is made at run time. */
 int  dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block);
+
+/* Planes of the x walk per CTA for engines 1 and 3 (0: automatic; engine 3
+ * uses at most 64).  The reference fixes its block shape per build
+ * (params.h:50-52); dtmx_autotune searches this value. */
+int  dtmx_set_xchunk(dtmx_ctx* ctx, int planes);
 
 /* Time every applicable engine configuration for trial_steps steps from the
  * current state (probes and DFT planes paused; the state is restored after

@@ -77,6 +77,21 @@ def test_single_sweep_bitwise_equal_to_per_step(gyro, design):
     b.close()
 
 
+@pytest.mark.parametrize("xchunk", [1, 5, 13, 64])
+def test_single_sweep_x_chunks(xchunk):
+    """Chunk boundaries anywhere along x (one plane per CTA up to the longest
+    chunk, 64 planes, which here is the whole grid) give the same fields."""
+    case = _case()
+    a = _sim(case, 1)
+    b = _sim(case, 3)
+    b.set_xchunk(xchunk)
+    a.step(11)
+    b.step(11)
+    _same(_fields(b), _fields(a))
+    a.close()
+    b.close()
+
+
 def test_engines_switch_mid_run_and_state_files(tmp_path):
     case = _case()
     ref = _sim(case, 1)
