@@ -2,7 +2,7 @@
 // respect to per-node permittivity (no reference counterpart: the reference
 // has no differentiation path).
 //
-// Forward step (box geometry, CPML or no absorber, non-dispersive nodes):
+// Forward step (box geometry, CPML or no absorber):
 //   H' = H + sum_a g_a d_a + sum_slab b_a psi_a,   psi_a' = b_a psi_a + al_a d_a,
 //   d_a = s_a D_a(E) for H, d_a = ie s_a D_a(H') for E,
 // with g_a = 1 outside the axis-a slab and 1/kappa_a + al_a inside.  The
@@ -11,8 +11,11 @@
 // (lam_E += D^T w_H, lam_psiH <- b (lam_H + lam_psiH)), where w = s ie (g lam
 // + al lam_psi) is the adjoint of d.  D^T is gathered tap by tap with the
 // forward stencil weights; outside the grid every value is zero, as in the
-// forward box geometry.  Each kernel is a plain per-node gather: the adjoint
-// is run on the recomputed segments of a checkpointed forward run.
+// forward box geometry.  Dispersive (Drude/Lorentz) E nodes follow the ADE
+// recursion instead (adj_ade_kernel: its transpose replaces their w and
+// carries the adjoint of the ADE state).  Each kernel is a plain per-node
+// gather: the adjoint is run on the recomputed segments of a checkpointed
+// forward run.
 #pragma once
 #include "dtmx_device.cuh"
 
@@ -25,6 +28,9 @@ struct AdjDev {
   const float* hist;        // [K+1][3][nd] design-region E of the recomputed segment
   int nd;
   float* w[3][2];           // adjoint of the scaled derivative terms d of the updated field, field layout
+  float* lEm[3];            // adjoint of the ADE state (Em, Jp, Jm) over the ADE box
+  float* lJp[3][MAXPOLE];
+  float* lJm[3][MAXPOLE];
 };
 
 // curl table: updated component -> {axis, source component} of its + and - terms
@@ -159,7 +165,52 @@ __global__ void adj_source_kernel(Params p, AdjDev A, const double* F, long long
   A.lam[4][id] -= (float)(ez[0] * phr + ez[1] * phi);
 }
 
-// grad += lam_E (E^s - E^{s-1}) / ie over the design region (hist slots st, st-1)
+// Transposed ADE recursion on the dispersive E nodes, between adj_w_kernel<.,0>
+// and adj_curl_kernel<.,0>.  The forward update of such a node (ade_update,
+// countDisp of dispersion.cpp:85-99, no absorber terms) is linear:
+//   E' = kE0 Em + kE1 E + kE2 rot - sum_q (kEJ0 Jp_q + kEJ1 Jm_q),  rot = sum_a d_a,
+//   Jp_q' = kJ0 Jp_q + kJ1 Jm_q + kJ2 E' + kJ3 Em + kJ4 E,   Jm_q' = Jp_q,   Em' = E.
+// With mu = lam_E' + sum_q kJ2 lam_Jp_q' (the adjoint of the intermediate E'):
+//   w_{c,t} = s_t cdt_a kE2 mu   (replaces the w adj_w_kernel wrote for the node),
+//   lam_E  = kE1 mu + sum_q kJ4 lam_Jp_q' + lam_Em',   lam_Em = kE0 mu + sum_q kJ3 lam_Jp_q',
+//   lam_Jp_q = -kEJ0 mu + kJ0 lam_Jp_q' + lam_Jm_q',   lam_Jm_q = -kEJ1 mu + kJ1 lam_Jp_q'.
+// One thread per cell of the ADE box (the ade_node_kernel layout).
+__global__ void adj_ade_kernel(Params p, AdjDev A) {
+  const MatTable& mt = *p.mt;
+  int bi, bj, bk;
+  long long q;
+  if (!ade_cell(p, bi, bj, bk, q)) return;
+  const int i = p.ade.lo[0] + bi, j = p.ade.lo[1] + bj, k = p.ade.lo[2] + bk;
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int m = p.mat[c] ? (int)__ldg(p.mat[c] + id) : 0;
+    const int np = __ldg(&mt.npoles[m]);
+    if (np <= 0) continue;
+    float mu = A.lam[c][id];
+    for (int r = 0; r < np; r++) mu = __fmaf_rn(__ldg(&mt.kJ[m][c][r][2]), A.lJp[c][r][q], mu);
+    const float wk = __fmul_rn(__ldg(&mt.kE[m][c][2]), mu);
+#pragma unroll
+    for (int t = 0; t < 2; t++) {
+      const int a = curl_axis(c, t);
+      A.w[c][t][id] = __fmul_rn(t == 0 ? p.cdt[a] : -p.cdt[a], wk);
+    }
+    float nE = __fmaf_rn(__ldg(&mt.kE[m][c][1]), mu, A.lEm[c][q]);
+    float nEm = __fmul_rn(__ldg(&mt.kE[m][c][0]), mu);
+    for (int r = 0; r < np; r++) {
+      const float lp = A.lJp[c][r][q], lm = A.lJm[c][r][q];
+      nE = __fmaf_rn(__ldg(&mt.kJ[m][c][r][4]), lp, nE);
+      nEm = __fmaf_rn(__ldg(&mt.kJ[m][c][r][3]), lp, nEm);
+      A.lJp[c][r][q] = __fmaf_rn(__ldg(&mt.kJ[m][c][r][0]), lp, __fmaf_rn(-__ldg(&mt.kEJ[m][c][r][0]), mu, lm));
+      A.lJm[c][r][q] = __fmaf_rn(__ldg(&mt.kJ[m][c][r][1]), lp, -__fmul_rn(__ldg(&mt.kEJ[m][c][r][1]), mu));
+    }
+    A.lam[c][id] = nE;
+    A.lEm[c][q] = nEm;
+  }
+}
+
+// grad += lam_E (E^s - E^{s-1}) / ie over the design region (hist slots st, st-1);
+// a design node whose material is dispersive takes no design permittivity: 0
 __global__ void adj_grad_kernel(Params p, AdjDev A, int st) {
   const int nd = A.nd;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
@@ -169,6 +220,7 @@ __global__ void adj_grad_kernel(Params p, AdjDev A, int st) {
   const int j = p.des_lo[1] + (di / p.des_n[2]) % p.des_n[1];
   const int k = p.des_lo[2] + di % p.des_n[2];
   const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+  if (p.mat[c] && __ldg(&p.mt->npoles[__ldg(p.mat[c] + id)]) > 0) return;
   const double dE = (double)A.hist[((long long)st * 3 + c) * nd + di] - (double)A.hist[((long long)(st - 1) * 3 + c) * nd + di];
   A.grad[q] += (double)A.lam[c][id] * dE / (double)p.des_ie[c][di];
 }

@@ -1601,7 +1601,7 @@ static int fa_begin(dtmx_ctx* ctx, FaRun& R, int nsteps, int checkpoint_every, i
   if (plane_x < 0 || plane_x >= c.nx) return fail(ctx, DTMX_ERR_INVALID, "objective plane outside the grid");
   if (c.geometry != DTMX_GEOM_BOX || c.absorber == DTMX_ABS_SPLIT_PML)
     return fail(ctx, DTMX_ERR_UNSUPPORTED, "the adjoint needs the box geometry with CPML or no absorber");
-  if (P.ade.Em[0] || ctx->has_gyro) return fail(ctx, DTMX_ERR_UNSUPPORTED, "the adjoint supports non-dispersive materials only");
+  if (ctx->has_gyro) return fail(ctx, DTMX_ERR_UNSUPPORTED, "the adjoint does not carry gyrotropic materials");
   for (const auto& q : ctx->psrc) {
     const long long sz = ctx->nzp, sy = (long long)c.ny * sz;
     const int i = (int)(q.id / sy), j = (int)((q.id % sy) / sz), k = (int)(q.id % sz);
@@ -1702,6 +1702,15 @@ static int fa_forward_done(dtmx_ctx* ctx, FaRun& R) {
   }
   for (int c3 = 0; c3 < 3; c3++)
     for (int t = 0; t < 2; t++) ok = ok && talloc((void**)&A.w[c3][t], (ctx->nstore + 64) * 4);
+  if (P.ade.Em[0]) {
+    // adjoint of the ADE state, over the ADE box
+    const size_t na = (size_t)P.ade.n[0] * P.ade.n[1] * P.ade.n[2];
+    for (int c3 = 0; c3 < 3; c3++) {
+      ok = ok && talloc((void**)&A.lEm[c3], na * 4);
+      for (int r = 0; r < MAXPOLE; r++)
+        if (P.ade.Jp[c3][r]) ok = ok && talloc((void**)&A.lJp[c3][r], na * 4) && talloc((void**)&A.lJm[c3][r], na * 4);
+    }
+  }
   ok = ok && talloc((void**)&A.grad, (size_t)3 * R.nd * 8) && talloc((void**)&R.dF, F.size() * 8);
   if (!R.full) ok = ok && talloc((void**)&R.hist, (size_t)(R.K + 1) * 3 * R.nd * 4);
   if (!ok) { R.release(); return fail(ctx, DTMX_ERR_OOM, "adjoint allocation"); }
@@ -1744,18 +1753,23 @@ static int fa_adjoint(dtmx_ctx* ctx, FaRun& R, int q) {
   adj_source_kernel<<<(R.npl + 255) / 256, 256, 0, st>>>(P, A, R.dF, R.s0 + (long long)R.seg * R.K + q, R.plane_x, R.omega, c.dt);
   adj_grad_kernel<<<design_blocks(R), 256, 0, st>>>(P, A, q);
   const dim3 blk(32, 8), grd((c.nz + 31) / 32, (c.ny + 7) / 8, c.nx);
+  // the dispersive nodes' transposed ADE recursion replaces their w (after adj_w, before adj_curl)
+  const bool ade = P.ade.Em[0] != nullptr;
+  const dim3 ablk(32, 8), agrd((P.ade.n[2] + 31) / 32, (P.ade.n[1] + 7) / 8, std::max(1, P.ade.n[0]));
   if (c.order == 4) {
     adj_w_kernel<4, 0><<<grd, blk, 0, st>>>(P, A);
+    if (ade) adj_ade_kernel<<<agrd, ablk, 0, st>>>(P, A);
     adj_curl_kernel<4, 0><<<grd, blk, 0, st>>>(P, A);
     adj_w_kernel<4, 1><<<grd, blk, 0, st>>>(P, A);
     adj_curl_kernel<4, 1><<<grd, blk, 0, st>>>(P, A);
   } else {
     adj_w_kernel<2, 0><<<grd, blk, 0, st>>>(P, A);
+    if (ade) adj_ade_kernel<<<agrd, ablk, 0, st>>>(P, A);
     adj_curl_kernel<2, 0><<<grd, blk, 0, st>>>(P, A);
     adj_w_kernel<2, 1><<<grd, blk, 0, st>>>(P, A);
     adj_curl_kernel<2, 1><<<grd, blk, 0, st>>>(P, A);
   }
-  ctx->launches += 6;
+  ctx->launches += ade ? 7 : 6;
   return DTMX_OK;
 }
 

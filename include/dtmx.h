@@ -340,8 +340,9 @@ int  dtmx_ref_main(const dtmx_ref_globals* g, const dtmx_tfsfsrc* shotpoint, int
 
 /* Per-node permittivity of the three E components over the cell box
  * [lo, lo+n): eps holds 3*n0*n1*n2 values (component-major, z fastest).  Inside
- * the box it replaces the material permittivity (the materials there must be
- * non-dispersive).  Set before the first step. */
+ * the box it replaces the permittivity of non-dispersive materials; a node
+ * whose material is dispersive keeps its ADE update (and its gradient in
+ * dtmx_forward_adjoint is 0).  Set before the first step. */
 int  dtmx_set_design(dtmx_ctx* ctx, const int lo[3], const int n[3], const float* eps);
 
 /* Advance nsteps from the current state and return the objective
@@ -349,14 +350,15 @@ int  dtmx_set_design(dtmx_ctx* ctx, const int lo[3], const int n[3], const float
  * the Poynting flux of the running DFTs at omega (E^ = sum_s E^s e^{-i w s dt} dt,
  * H^ with t = (s - 1/2) dt), and dJ/d eps at every design node (3*nd floats,
  * the layout of dtmx_set_design).  The gradient is the discrete adjoint of the
- * update (transposed stencils and CPML recursions), run backward over the
+ * update (transposed stencils, CPML recursions and Drude/Lorentz ADE
+ * recursions of countDisp, dispersion.cpp:85-99), run backward over the
  * steps; the accumulation is in double precision.  The adjoint needs, of the
  * forward run, only E in the design region at every step: when that history
  * ((nsteps+1) * 3 * nd floats) fits the budget of dtmx_set_adjoint_memory the
  * forward pass records it and nothing is recomputed; otherwise the state is
  * checkpointed every checkpoint_every steps in device memory and each segment
  * is recomputed before its adjoint.  Both modes give bit-identical results.
- * Box geometry, CPML or no absorber, non-dispersive materials, no point source
+ * Box geometry, CPML or no absorber, no gyrotropic material, no point source
  * inside the design region.  On return the context holds the state after
  * nsteps, as after dtmx_step(nsteps).  The run's device buffers (adjoint
  * fields, history or checkpoints) come from the device's stream-ordered memory

@@ -96,6 +96,8 @@ typedef struct {
   real gjc[DTMX_MAX_MATERIALS];
   int has_gyro, gcur;
   real* Jg[2][3];
+  /* adjoint runs: the adjoint of the intermediate E' of the dispersive nodes */
+  real* amu[3];
   /* design region: per-node 1/eps of each E component over a cell box */
   int des_on, des_lo[3], des_n[3];
   real* des_ie[3];
@@ -969,6 +971,14 @@ int PFX(threads)(void) {
  * staggered difference operators satisfy D_E^T = -D_H (zero outside the box).
  * The adjoint step applies the transposes in reverse order.
  *
+ * Dispersive (Drude/Lorentz) E nodes follow countDisp instead (no absorber
+ * terms, as in the forward step):
+ *   E' = kE0 Em + kE1 E + kE2 rot - sum_q (kEJ0 Jp_q + kEJ1 Jm_q),  rot = sum_a d_a,
+ *   Jp_q' = kJ0 Jp_q + kJ1 Jm_q + kJ2 E' + kJ3 Em + kJ4 E,  Jm_q' = Jp_q,  Em' = E;
+ * with mu = lam_E' + sum_q kJ2 lam_Jp_q' their adjoint is w_a = s_a kE2 mu and
+ *   lam_E = kE1 mu + sum_q kJ4 lam_Jp_q' + lam_Em',  lam_Em = kE0 mu + sum_q kJ3 lam_Jp_q',
+ *   lam_Jp_q = -kEJ0 mu + kJ0 lam_Jp_q' + lam_Jm_q',  lam_Jm_q = -kEJ1 mu + kJ1 lam_Jp_q'.
+ * The design permittivity does not enter a dispersive node: its gradient is 0.
  * Objective: J = sum over the plane x = X of Re(Ey^ conj(Hz^) - Ez^ conj(Hy^)),
  * with E^ = sum_s E^s exp(-i w s dt) dt and H^ = sum_s H^{s-1/2} exp(-i w (s-1/2) dt) dt
  * (the engine's DFT convention).  Gradient: dJ/d ie_c(p) =
@@ -1000,8 +1010,17 @@ static real lget(const osim* s, real* const* arr, int c, int i, int j, int k) {
   return arr[c][IDX(s, i, j, k)];
 }
 
+/* material of E component c at node (i,j,k) when it is dispersive and in the ADE box, else -1 */
+static int ade_mat(const osim* s, int c, int i, int j, int k, long* ai) {
+  int mi = s->midx[c] ? s->midx[c][IDX(s, i, j, k)] : 0;
+  if (s->mat[mi].npoles <= 0) return -1;
+  *ai = ade_index(s, i, j, k);
+  return *ai >= 0 ? mi : -1;
+}
+
 /* w_{c,a}(p) = s_a ie(p) (g lam(p) + al lampsi(p)) for updated component c at
- * node p (the adjoint of d_a), zero outside the grid */
+ * node p (the adjoint of d_a), zero outside the grid; s_a kE2 mu(p) at a
+ * dispersive node */
 static double adj_w(const osim* s, real* const* lam, real* const lpsi[3][4], int c, int t, int i, int j, int k) {
   if (i < 0 || i >= s->nx || j < 0 || j >= s->ny || k < 0 || k >= s->nz) return 0;
   const dtmx_config* cf = &s->cfg;
@@ -1012,6 +1031,11 @@ static double adj_w(const osim* s, real* const* lam, real* const lpsi[3][4], int
   if (isH) sg = -sg;
   double sa = sg * cf->dt / dd[a];
   size_t id = IDX(s, i, j, k);
+  if (!isH && s->ade_n) {
+    long ai;
+    int mi = ade_mat(s, c, i, j, k, &ai);
+    if (mi >= 0) return sa * (double)s->kE[mi][c][2] * (double)s->amu[c][ai];
+  }
   double ie = 1;
   if (!isH) ie = node_ie(s, c, s->midx[c] ? s->midx[c][id] : 0, i, j, k);
   int sl = slot_of(c, a);
@@ -1075,10 +1099,50 @@ static void adj_half(osim* s, real** lam, real* lpsi[3][4], int updH) {
   }
 }
 
+/* mu = lam_E' + sum_q kJ2 lam_Jp_q' on the dispersive nodes */
+static void ade_adjoint_mu(osim* s, real* const* lam, real* const lJp[3][DTMX_MAX_POLES]) {
+  for (int c = 0; c < 3; c++)
+    for (int i = s->ade_box[0][0]; i < s->ade_box[0][1]; i++)
+      for (int j = s->ade_box[1][0]; j < s->ade_box[1][1]; j++)
+        for (int k = s->ade_box[2][0]; k < s->ade_box[2][1]; k++) {
+          long ai;
+          int mi = ade_mat(s, c, i, j, k, &ai);
+          if (mi < 0) continue;
+          double mu = lam[c][IDX(s, i, j, k)];
+          for (int q = 0; q < s->mat[mi].npoles; q++) mu += (double)s->kJ[mi][c][q][2] * lJp[c][q][ai];
+          s->amu[c][ai] = (real)mu;
+        }
+}
+
+/* lam_E and the adjoint ADE state of the dispersive nodes (after the E-update transposition) */
+static void ade_adjoint_state(const osim* s, real** lam, real** lEm, real* lJp[3][DTMX_MAX_POLES],
+                              real* lJm[3][DTMX_MAX_POLES]) {
+  for (int c = 0; c < 3; c++)
+    for (int i = s->ade_box[0][0]; i < s->ade_box[0][1]; i++)
+      for (int j = s->ade_box[1][0]; j < s->ade_box[1][1]; j++)
+        for (int k = s->ade_box[2][0]; k < s->ade_box[2][1]; k++) {
+          long ai;
+          int mi = ade_mat(s, c, i, j, k, &ai);
+          if (mi < 0) continue;
+          const double mu = s->amu[c][ai];
+          double nE = (double)s->kE[mi][c][1] * mu + lEm[c][ai];
+          double nEm = (double)s->kE[mi][c][0] * mu;
+          for (int q = 0; q < s->mat[mi].npoles; q++) {
+            const double lp = lJp[c][q][ai], lm = lJm[c][q][ai];
+            nE += (double)s->kJ[mi][c][q][4] * lp;
+            nEm += (double)s->kJ[mi][c][q][3] * lp;
+            lJp[c][q][ai] = (real)(-(double)s->kEJ[mi][c][q][0] * mu + (double)s->kJ[mi][c][q][0] * lp + lm);
+            lJm[c][q][ai] = (real)(-(double)s->kEJ[mi][c][q][1] * mu + (double)s->kJ[mi][c][q][1] * lp);
+          }
+          lam[c][IDX(s, i, j, k)] = (real)nE;
+          lEm[c][ai] = (real)nEm;
+        }
+}
+
 int PFX(forward_adjoint)(void* h, int nsteps, int X, double omega, double* J_out, double* grad_out) {
   osim* s = h;
   if (!s->des_on || X < 0 || X >= s->nx || nsteps < 1) return DTMX_ERR_INVALID;
-  if (s->cfg.geometry != DTMX_GEOM_BOX || s->cfg.absorber == DTMX_ABS_SPLIT_PML || s->ade_n) return DTMX_ERR_UNSUPPORTED;
+  if (s->cfg.geometry != DTMX_GEOM_BOX || s->cfg.absorber == DTMX_ABS_SPLIT_PML || s->has_gyro) return DTMX_ERR_UNSUPPORTED;
   const double dt = s->cfg.dt;
   const size_t nd = (size_t)s->des_n[0] * s->des_n[1] * s->des_n[2];
   const size_t npl = (size_t)s->ny * s->nz;
@@ -1124,6 +1188,13 @@ int PFX(forward_adjoint)(void* h, int nsteps, int X, double omega, double* J_out
     for (int q = 0; q < 4; q++) lpsi[a][q] = calloc(ns ? ns : 1, sizeof(real));
   }
   double* grad = calloc(3 * nd, sizeof(double));
+  /* adjoint of the ADE state over the ADE box */
+  real *lEm[3] = {0}, *lJp[3][DTMX_MAX_POLES] = {{0}}, *lJm[3][DTMX_MAX_POLES] = {{0}};
+  for (int c = 0; c < 3 && s->ade_n; c++) {
+    lEm[c] = calloc(s->ade_n, sizeof(real));
+    s->amu[c] = calloc(s->ade_n, sizeof(real));
+    for (int q = 0; q < DTMX_MAX_POLES; q++) { lJp[c][q] = calloc(s->ade_n, sizeof(real)); lJm[c][q] = calloc(s->ade_n, sizeof(real)); }
+  }
   for (int st = nsteps; st >= 1; st--) {
     double sE = (double)(s0 + st), sH = sE - 0.5;
     double pe[2] = {cos(omega * sE * dt) * dt, -sin(omega * sE * dt) * dt};
@@ -1144,12 +1215,20 @@ int PFX(forward_adjoint)(void* h, int nsteps, int X, double omega, double* J_out
           for (int k = 0; k < s->des_n[2]; k++) {
             size_t di = ((size_t)i * s->des_n[1] + j) * s->des_n[2] + k;
             size_t id = IDX(s, s->des_lo[0] + i, s->des_lo[1] + j, s->des_lo[2] + k);
+            long ai;
+            if (s->ade_n && ade_mat(s, c, s->des_lo[0] + i, s->des_lo[1] + j, s->des_lo[2] + k, &ai) >= 0) continue;
             double dE = (double)hist[((size_t)st * 3 + c) * nd + di] - (double)hist[((size_t)(st - 1) * 3 + c) * nd + di];
             grad[c * nd + di] += (double)lam[c][id] * dE / (double)s->des_ie[c][di];
           }
     /* lam^{st-1} = A^T lam^{st}: E update transposed, then H update transposed */
+    if (s->ade_n) ade_adjoint_mu(s, lam, lJp);
     adj_half(s, lam, lpsi, 0);
+    if (s->ade_n) ade_adjoint_state(s, lam, lEm, lJp, lJm);
     adj_half(s, lam, lpsi, 1);
+  }
+  for (int c = 0; c < 3 && s->ade_n; c++) {
+    free(lEm[c]); free(s->amu[c]); s->amu[c] = NULL;
+    for (int q = 0; q < DTMX_MAX_POLES; q++) { free(lJp[c][q]); free(lJm[c][q]); }
   }
   for (int c = 0; c < 3; c++)
     for (size_t q = 0; q < nd; q++) {

@@ -55,6 +55,55 @@ def test_oracle_adjoint_matches_finite_differences(order):
         assert abs(g[cell] - fd) <= 1e-6 * abs(fd), (cell, g[cell], fd)
 
 
+def _disp_materials(nx=22, ny=18, nz=18, overlap=False):
+    """A Drude block across the objective plane and a two-pole (Lorentz +
+    Drude) block near the source; overlap: one Drude node inside the design
+    region."""
+    from dtmaxwell4_b200 import abi
+    wp = 2 * math.pi / 8
+    mats = [abi.make_material(1.0),
+            abi.make_material(1.0, poles=[(abi.POLE_DRUDE, 1.0, wp, wp / 40, 0.0)], eps_inf=1.5),
+            abi.make_material(1.0, poles=[(abi.POLE_LORENTZ, 1.5, 0.5, 0.05, 0.0), (abi.POLE_DRUDE, 1.0, 0.8, 0.02, 0.0)],
+                              eps_inf=2.0)]
+    idx = np.zeros((nx, ny, nz), np.uint8)
+    idx[13:18, 4:13, 5:13] = 1
+    idx[3:6, 7:12, 6:12] = 2
+    if overlap:
+        idx[LO[0] + 1, LO[1], LO[2] + 2] = 1
+    return mats, idx
+
+
+def _oracle_disp(eps, overlap=False):
+    import pyoracle
+    o = _setup(pyoracle.OracleSim(_cfg(2)), 2)
+    mats, idx = _disp_materials(overlap=overlap)
+    o.set_materials(mats, idx, idx, idx)
+    o.set_design(LO, eps)
+    return o.forward_adjoint(N_STEPS, PLANE_X, OMEGA)
+
+
+@pytest.mark.parametrize("overlap", [False, True])
+def test_oracle_adjoint_dispersive_matches_finite_differences(overlap):
+    """The transposed ADE recursion (Drude and Lorentz poles): the FP64
+    adjoint equals central differences of the FP64 forward; a design node
+    whose material is dispersive has gradient 0 (its permittivity is the
+    material's, not the design's), and so does J's difference quotient."""
+    eps = _eps()
+    J, g = _oracle_disp(eps, overlap)
+    assert J != 0
+    cells = [(2, 1, 1, 1), (0, 0, 2, 1), (1, 2, 0, 2)]
+    if overlap:
+        cells.append((0, 1, 0, 2))
+        assert g[0, 1, 0, 2] == 0.0
+    for cell in cells:
+        h = 1e-4
+        ep, em = eps.copy(), eps.copy()
+        ep[cell] += h
+        em[cell] -= h
+        fd = (_oracle_disp(ep, overlap)[0] - _oracle_disp(em, overlap)[0]) / (2 * h)
+        assert abs(g[cell] - fd) <= 1e-6 * max(abs(fd), 1e-12 * abs(J)), (cell, g[cell], fd)
+
+
 def _gpu(order, eps, K=100, budget=-1):
     from dtmaxwell4_b200 import Simulation
     s = _setup(Simulation(_cfg(order)), order)
@@ -144,7 +193,9 @@ def test_full_size_gradient_directional_difference():
     design region, 2000 steps): the directional central difference of J along
     d = sign(dJ/deps) with h = 1e-3 on every design node equals sum |dJ/deps|.
     (Per-node differences at this size change J by less than its FP32 rounding;
-    they are checked at the small size above.)"""
+    they are checked at the small size above.)  Measured agreement 7.2e-6;
+    held to 1e-4 (the FP32 rounding of J itself sets the noise of the
+    difference quotient)."""
     from dtmaxwell4_b200 import Simulation, scenarios
     sc = scenarios.design_region()
     lo, eps = sc["design"]
@@ -167,4 +218,62 @@ def test_full_size_gradient_directional_difference():
     fd = (Jp - Jm) / (2 * h)
     ad = float((np.abs(g).astype(np.float64) * (hp + hm) / (2 * h)).sum())
     print("J %.9g  directional FD %.9g  adjoint %.9g  rel %.2e" % (J, fd, ad, abs(fd - ad) / abs(ad)))
-    assert abs(fd - ad) <= 1e-2 * abs(ad)
+    assert abs(fd - ad) <= 1e-4 * abs(ad)
+
+
+def _gpu_disp(eps, K=100, budget=-1, overlap=False):
+    from dtmaxwell4_b200 import Simulation
+    s = _setup(Simulation(_cfg(2)), 2)
+    mats, idx = _disp_materials(overlap=overlap)
+    s.set_materials(mats, idx, idx, idx)
+    s.set_design(LO, eps)
+    s.set_adjoint_memory(budget)
+    J, g = s.forward_adjoint(N_STEPS, PLANE_X, OMEGA, K)
+    return J, g, s
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("overlap", [False, True])
+def test_gpu_adjoint_dispersive_against_fp64_adjoint(overlap):
+    """Drude and two-pole Lorentz+Drude blocks (one Drude node in the design
+    region with overlap): the GPU adjoint of the ADE recursion against the
+    FP64 adjoint, recorded history and checkpointed recompute bit-identical."""
+    eps = _eps()
+    J, g, s = _gpu_disp(eps, overlap=overlap)
+    s.close()
+    J2, g2, s2 = _gpu_disp(eps, K=7, budget=0, overlap=overlap)
+    s2.close()
+    assert J2 == J and np.array_equal(g2, g)
+    Jo, go = _oracle_disp(eps.astype(np.float32).astype(np.float64), overlap)
+    assert abs(J - Jo) <= 1e-5 * abs(Jo), (J, Jo)
+    cos = float((g * go).sum() / (np.linalg.norm(g) * np.linalg.norm(go)))
+    rel = float(np.linalg.norm(g - go) / np.linalg.norm(go))
+    print("dispersive adjoint: J %.9g vs %.9g, cos %.8f, rel %.2e" % (J, Jo, cos, rel))
+    assert cos >= 0.9999 and rel <= 1e-3, (cos, rel)
+    if overlap:
+        assert g[0, 1, 0, 2] == 0.0
+
+
+@pytest.mark.gpu
+def test_gpu_adjoint_dispersive_against_central_differences():
+    """8 seeded design cells, h = 1e-3, with the dispersive blocks present."""
+    eps = _eps().astype(np.float32)
+    J, g, s = _gpu_disp(eps)
+    s.close()
+    rng = np.random.default_rng(9)
+    cells = [tuple(int(v) for v in (rng.integers(3), *rng.integers(0, 3, size=3))) for _ in range(8)]
+    fd, ad = [], []
+    for cell in cells:
+        h = 1e-3
+        ep, em = eps.copy(), eps.copy()
+        ep[cell] += h
+        em[cell] -= h
+        Jp, _, sp = _gpu_disp(ep)
+        sp.close()
+        Jm, _, sm = _gpu_disp(em)
+        sm.close()
+        fd.append((Jp - Jm) / (2 * h))
+        ad.append(float(g[cell]))
+    fd, ad = np.array(fd), np.array(ad)
+    cos = float(fd @ ad / (np.linalg.norm(fd) * np.linalg.norm(ad)))
+    assert cos >= 0.999, (cos, fd, ad)
