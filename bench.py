@@ -43,8 +43,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched measurements")
     ap.add_argument("--extras-only", action="store_true", help="print only the adjoint and batched measurements")
     ap.add_argument("--adj-steps", type=int, default=2000)
-    ap.add_argument("--batch-instances", type=int, default=16)
-    ap.add_argument("--batch-steps", type=int, default=300)
+    ap.add_argument("--batch-instances", type=int, default=64)
+    ap.add_argument("--batch-steps", type=int, default=1500)
     ap.add_argument("--gyro-steps", type=int, default=100, help="timed steps of the 1024x1024x1536 gyrotropic run")
     ap.add_argument("--gyro-n", type=int, nargs=3, default=[1024, 1024, 1536])
     ap.add_argument("--no-gyro", action="store_true", help="skip the gyrotropic / Purcell measurement")
@@ -295,7 +295,9 @@ def run_ours(args, rank, world):
     e2e_val = aggregate_rate(ncell * args.tsteps * e_steps, world, max_over_ranks(e0.elapsed_time(e1), world, "cuda"))
     nb = 6 * ncell * 4
     e2e = {"value": round(e2e_val, 3), "unit": UNIT, "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb,
-           "steps": e_steps}
+           "steps": e_steps,
+           "cadence": "the six fields uploaded and downloaded once per bench step (%d time steps) through "
+                      "dtmx_set_field / dtmx_get_field; CPML, ADE and DFT state stay on the device" % args.tsteps}
     sim.close()
     return value, ms_max, launches, roof, e2e, clk, sc
 
@@ -309,9 +311,11 @@ def run_adjoint(args):
     sc = scenarios.design_region(steps=args.adj_steps)
 
     def make():
+        # forward and recomputed segments step with the single-sweep engine
         s = Simulation(sc["cfg"])
         scenarios.apply(s, sc)
         s.set_design(*sc["design"])
+        s.set_engine(3, 0)
         return s
     w = make()
     w.forward_adjoint(40, sc["plane_x"], sc["omega"], 20)
@@ -401,9 +405,11 @@ def run_batched(args):
     scs = [scenarios.design_block_instance(seed, steps=steps) for seed in range(n)]
 
     def make(sc):
+        # both arms step with the single-sweep engine (its automatic x chunk)
         s = Simulation(sc["cfg"])
         scenarios.apply(s, sc)
         s.set_design(*sc["design"])
+        s.set_engine(3, 0)
         return s
     w = make(scs[0])
     w.forward_adjoint(20, scs[0]["plane_x"], scs[0]["omega"], 10)
@@ -454,10 +460,12 @@ def run_gyro_purcell(args):
     s.sync()
     dt = time.perf_counter() - t0
     s.close()
-    hb, eb = algorithmic_bytes(sc)
+    hb, eb, fb = algorithmic_bytes(sc)
     gyro = sum(int((sc["materials"][1][c] == 2).sum()) for c in range(3))
     ncell = n[0] * n[1] * n[2]
-    b_cell = (hb + eb + 8 * gyro) / ncell
+    # the field bytes of the engine the autotuner chose (one sweep or two passes), plus the
+    # gyrotropic current (read and written by its pass)
+    b_cell = ((fb if tuned[0] == 3 else hb + eb) + 8 * gyro) / ncell
     rate = ncell * args.gyro_steps / dt / 1e9
     hbm, kind = measured_peaks()
     out.update({"workload": sc["desc"] + ", %d timed steps (of 8000) after 3 warm-up steps" % args.gyro_steps,
@@ -508,6 +516,53 @@ def cpu_sample(args, n, tsteps):
     return ncell * tsteps / dt / 1e9, pyoracle.threads(), dt
 
 
+def cpu_check_fp64(args, n=64, steps=4000):
+    """Part of the CPU leg: the headline workload at its full length (4000
+    steps, 16 DFT frequencies, 12-cell CPML) on an n^3 grid, run through the
+    library with the engine configuration the timed run used and by the FP64
+    oracle on the host (the oracle only checks: it is not what is measured).
+    Returns the relative L2 errors of the probe traces, the DFT plane and the
+    final fields against FP64."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from dtmaxwell4_b200 import Simulation, scenarios
+    sc = scenarios.drude_sphere_tfsf(n=n, steps=steps, pml=12, inset=4, nfreq=16)
+    eng, tb, xc = run_ours.tuned[:3]
+    g = Simulation(sc["cfg"])
+    gid = scenarios.apply(g, sc)
+    if eng in (1, 3):
+        g.set_engine(eng, tb)
+    g.step(steps)
+    g.sync()
+    o = pyoracle.OracleSim(sc["cfg"], "f64")
+    oid = scenarios.apply(o, sc)
+    t0 = time.perf_counter()
+    o.step(steps)
+    dt = time.perf_counter() - t0
+    # each trace against max(|trace|, 1% of the strongest trace of its field type)
+    tg, to = g.read_probes(), o.read_probes(100000)
+    comps = [p[0] for p in sc["probes"]]
+    norms = np.linalg.norm(to, axis=1)
+    floor = {t: 1e-2 * max([norms[q] for q in range(len(comps)) if comps[q] // 3 == t] or [0.0]) for t in (0, 1)}
+    pe = max(float(np.linalg.norm(tg[q] - to[q]) / max(norms[q], floor[comps[q] // 3], 1e-300)) for q in range(len(to)))
+    dg, do = g.read_dft(gid[0]).view(np.float64), o.read_dft(oid[0]).view(np.float64)
+    de = float(np.linalg.norm(dg - do) / np.linalg.norm(do))
+    fe = 0.0
+    for grp in ((0, 1, 2), (3, 4, 5)):
+        want = [o.get_field(c) for c in grp]
+        ref = float(np.sqrt(sum(np.linalg.norm(w) ** 2 for w in want)))
+        for c, w in zip(grp, want):
+            fe = max(fe, float(np.linalg.norm(g.get_field(c).astype(np.float64) - w) / ref))
+    g.close()
+    o.close()
+    return {"workload": sc["desc"] + ", %d steps" % steps, "engine": eng, "probe_rel_l2_max": float("%.3g" % pe),
+            "dft_rel_l2": float("%.3g" % de), "field_rel_l2_max": float("%.3g" % fe),
+            "oracle_seconds": round(dt, 1),
+            "note": "relative L2 against the FP64 oracle of the same update equations (the fields: each "
+                    "component against the norm of its whole E or H field)"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -547,10 +602,13 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     value, ms, launches, roof, e2e, clk, sc = run_ours(args, rank, world)
     cpu = None
+    err_fp64 = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, dt = cpu_sample(args, args.n, args.cpu_steps)
         cpu = {"value": round(v, 5), "unit": UNIT, "cores": cores, "kind": "port",
                "sample": "%d time steps of the %d^3 workload (oracle FP32, %.1f s)" % (args.cpu_steps, args.n, dt)}
+        if args.workload == "drude":
+            err_fp64 = cpu_check_fp64(args)
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
         extras["point_dipole"] = run_point_dipole(args)
@@ -573,7 +631,8 @@ def main():
                            "desc": sc["desc"], "time_steps_per_step": args.tsteps,
                            "l2": "inputs larger than L2 (%.2f GB of fields)" % (6 * args.n ** 3 * 4 / 1e9),
                            "parallelism": "replicas%d" % world},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+                "err_vs_fp64": err_fp64}
         line.update(extras)
         print(json.dumps(line))
     return 0

@@ -31,6 +31,8 @@ struct AdjDev {
   float* lEm[3];            // adjoint of the ADE state (Em, Jp, Jm) over the ADE box
   float* lJp[3][MAXPOLE];
   float* lJm[3][MAXPOLE];
+  float* lJg[3];            // adjoint of the gyrotropic current, ADE box
+  float* lT[3];             // muJ of the gyrotropic nodes during one adjoint step, ADE box
 };
 
 // curl table: updated component -> {axis, source component} of its + and - terms
@@ -206,6 +208,75 @@ __global__ void adj_ade_kernel(Params p, AdjDev A) {
     }
     A.lam[c][id] = nE;
     A.lEm[c][q] = nEm;
+  }
+}
+
+// Transposed magnetised-Drude current (gyro_current_kernel, then E -= gjc J'):
+//   J' = gA t + gB E,  t_x = gC Jx + gS avg4(Jy),  t_y = gC Jy - gS avg4(Jx),  t_z = Jz.
+// adj_gyro_mu_kernel (after adj_w_kernel<.,0>, which reads lam_E'): muJ =
+// lam_J' - gjc lam_E' on the gyrotropic nodes (0 elsewhere) into lT, and
+// lam_E += gB muJ.  adj_gyro_j_kernel: the adjoint of the old current,
+// lam_J = gC gA muJ (own node) -/+ gS/4 gA muJ of the nodes whose 4-node average
+// holds it; a non-gyrotropic node's current is identically zero, so is its adjoint.
+__global__ void adj_gyro_mu_kernel(Params p, AdjDev A) {
+  const MatTable& mt = *p.mt;
+  int bi, bj, bk;
+  long long q;
+  if (!ade_cell(p, bi, bj, bk, q)) return;
+  const int i = p.ade.lo[0] + bi, j = p.ade.lo[1] + bj, k = p.ade.lo[2] + bk;
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int m = p.mat[c] ? (int)__ldg(p.mat[c] + id) : 0;
+    const float gjc = __ldg(&mt.gjc[m]);
+    if (gjc == 0.f) { A.lT[c][q] = 0.f; continue; }
+    const float lE = A.lam[c][id];
+    const float mu = __fmaf_rn(-gjc, lE, A.lJg[c][q]);
+    A.lT[c][q] = mu;
+    A.lam[c][id] = __fmaf_rn(__ldg(&mt.gB[m]), mu, lE);
+  }
+}
+
+// gA gS / 4 muJ of component c at node (i, j, k) when it is gyrotropic (0 outside the box or grid)
+__device__ __forceinline__ float adj_gyro_term(const Params& p, const AdjDev& A, int c, int i, int j, int k) {
+  const int bi = i - p.ade.lo[0], bj = j - p.ade.lo[1], bk = k - p.ade.lo[2];
+  if (bi < 0 || bi >= p.ade.n[0] || bj < 0 || bj >= p.ade.n[1] || bk < 0 || bk >= p.ade.n[2]) return 0.f;
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+  const int m = p.mat[c] ? (int)__ldg(p.mat[c] + id) : 0;
+  if (__ldg(&p.mt->gjc[m]) == 0.f) return 0.f;
+  const float mu = A.lT[c][((long long)bi * p.ade.n[1] + bj) * p.ade.n[2] + bk];
+  return __fmul_rn(__fmul_rn(0.25f, __fmul_rn(__ldg(&p.mt->gS[m]), __ldg(&p.mt->gA[m]))), mu);
+}
+
+__global__ void adj_gyro_j_kernel(Params p, AdjDev A) {
+  const MatTable& mt = *p.mt;
+  int bi, bj, bk;
+  long long q;
+  if (!ade_cell(p, bi, bj, bk, q)) return;
+  const int i = p.ade.lo[0] + bi, j = p.ade.lo[1] + bj, k = p.ade.lo[2] + bk;
+  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int m = p.mat[c] ? (int)__ldg(p.mat[c] + id) : 0;
+    if (__ldg(&mt.gjc[m]) == 0.f) { A.lJg[c][q] = 0.f; continue; }
+    const float t = __fmul_rn(__ldg(&mt.gA[m]), A.lT[c][q]);
+    float v;
+    if (c == 0) {
+      // Jx(i,j) enters the averages of the y nodes (i,j+1), (i-1,j+1), (i,j), (i-1,j)
+      const float acc = __fadd_rn(__fadd_rn(__fadd_rn(adj_gyro_term(p, A, 1, i, j + 1, k), adj_gyro_term(p, A, 1, i - 1, j + 1, k)),
+                                            adj_gyro_term(p, A, 1, i, j, k)),
+                                  adj_gyro_term(p, A, 1, i - 1, j, k));
+      v = __fsub_rn(__fmul_rn(__ldg(&mt.gC[m]), t), acc);
+    } else if (c == 1) {
+      // Jy(i,j) enters the averages of the x nodes (i+1,j), (i,j), (i+1,j-1), (i,j-1)
+      const float acc = __fadd_rn(__fadd_rn(__fadd_rn(adj_gyro_term(p, A, 0, i + 1, j, k), adj_gyro_term(p, A, 0, i, j, k)),
+                                            adj_gyro_term(p, A, 0, i + 1, j - 1, k)),
+                                  adj_gyro_term(p, A, 0, i, j - 1, k));
+      v = __fmaf_rn(__ldg(&mt.gC[m]), t, acc);
+    } else {
+      v = t;
+    }
+    A.lJg[c][q] = v;
   }
 }
 

@@ -1543,6 +1543,7 @@ struct FaRun {
   int N = 0, K = 0, nseg = 0, nd = 0, npl = 0, plane_x = 0;
   double omega = 0, J = 0;
   long long s0 = 0;
+  int gcur0 = 0;              // gyrotropic current buffer at the start (it alternates every step)
   std::vector<char*> ck;
   AdjDev A{};
   float* hist = nullptr;
@@ -1601,7 +1602,15 @@ static int fa_begin(dtmx_ctx* ctx, FaRun& R, int nsteps, int checkpoint_every, i
   if (plane_x < 0 || plane_x >= c.nx) return fail(ctx, DTMX_ERR_INVALID, "objective plane outside the grid");
   if (c.geometry != DTMX_GEOM_BOX || c.absorber == DTMX_ABS_SPLIT_PML)
     return fail(ctx, DTMX_ERR_UNSUPPORTED, "the adjoint needs the box geometry with CPML or no absorber");
-  if (ctx->has_gyro) return fail(ctx, DTMX_ERR_UNSUPPORTED, "the adjoint does not carry gyrotropic materials");
+  if (ctx->has_gyro && !ctx->h_mat[0].empty()) {
+    // the design permittivity of a gyrotropic node would enter next to its current: not carried
+    for (int comp = 0; comp < 3; comp++)
+      for (int i = P.des_lo[0]; i < P.des_lo[0] + P.des_n[0]; i++)
+        for (int j = P.des_lo[1]; j < P.des_lo[1] + P.des_n[1]; j++)
+          for (int k = P.des_lo[2]; k < P.des_lo[2] + P.des_n[2]; k++)
+            if (ctx->mats[ctx->h_mat[comp][store_index(ctx, i, j, k)]].gyro_wp > 0)
+              return fail(ctx, DTMX_ERR_UNSUPPORTED, "the design region holds a gyrotropic node");
+  }
   for (const auto& q : ctx->psrc) {
     const long long sz = ctx->nzp, sy = (long long)c.ny * sz;
     const int i = (int)(q.id / sy), j = (int)((q.id % sy) / sz), k = (int)(q.id % sz);
@@ -1643,6 +1652,7 @@ static int fa_begin(dtmx_ctx* ctx, FaRun& R, int nsteps, int checkpoint_every, i
       if (!(q = (char*)R.take(ctx, sb))) { R.release(); return fail(ctx, DTMX_ERR_OOM, "checkpoint allocation"); }
   }
   R.s0 = ctx->step;
+  R.gcur0 = ctx->gcur;
   ctx->obj_on = true;
   return DTMX_OK;
 }
@@ -1659,7 +1669,7 @@ static int fa_forward(dtmx_ctx* ctx, FaRun& R, int st) {
   } else if (st % R.K == 0) {
     state_copy(ctx, R.ck[st / R.K], true);
   }
-  int rc = launch_step(ctx);
+  int rc = launch_one(ctx);
   if (rc) return rc;
   ctx->step++;
   if (R.full) {
@@ -1702,6 +1712,10 @@ static int fa_forward_done(dtmx_ctx* ctx, FaRun& R) {
   }
   for (int c3 = 0; c3 < 3; c3++)
     for (int t = 0; t < 2; t++) ok = ok && talloc((void**)&A.w[c3][t], (ctx->nstore + 64) * 4);
+  if (ctx->has_gyro) {
+    const size_t na = (size_t)P.ade.n[0] * P.ade.n[1] * P.ade.n[2];
+    for (int c3 = 0; c3 < 3; c3++) ok = ok && talloc((void**)&A.lJg[c3], na * 4) && talloc((void**)&A.lT[c3], na * 4);
+  }
   if (P.ade.Em[0]) {
     // adjoint of the ADE state, over the ADE box
     const size_t na = (size_t)P.ade.n[0] * P.ade.n[1] * P.ade.n[2];
@@ -1730,6 +1744,7 @@ static int fa_segment_begin(dtmx_ctx* ctx, FaRun& R, int seg) {
   if (R.full) return DTMX_OK;
   state_copy(ctx, R.ck[seg], false);
   ctx->step = R.s0 + start;
+  ctx->gcur = R.gcur0 ^ (start & 1);
   design_capture_kernel<<<design_blocks(R), 256, 0, ctx->stream>>>(ctx->P, R.hist, 0, R.nd);
   return DTMX_OK;
 }
@@ -1737,7 +1752,7 @@ static int fa_segment_begin(dtmx_ctx* ctx, FaRun& R, int seg) {
 // recompute step q (1..len) of the current segment
 static int fa_recompute(dtmx_ctx* ctx, FaRun& R, int q) {
   if (R.full) return DTMX_OK;
-  int rc = launch_step(ctx);
+  int rc = launch_one(ctx);
   if (rc) return rc;
   ctx->step++;
   design_capture_kernel<<<design_blocks(R), 256, 0, ctx->stream>>>(ctx->P, R.hist, q, R.nd);
@@ -1753,23 +1768,28 @@ static int fa_adjoint(dtmx_ctx* ctx, FaRun& R, int q) {
   adj_source_kernel<<<(R.npl + 255) / 256, 256, 0, st>>>(P, A, R.dF, R.s0 + (long long)R.seg * R.K + q, R.plane_x, R.omega, c.dt);
   adj_grad_kernel<<<design_blocks(R), 256, 0, st>>>(P, A, q);
   const dim3 blk(32, 8), grd((c.nz + 31) / 32, (c.ny + 7) / 8, c.nx);
-  // the dispersive nodes' transposed ADE recursion replaces their w (after adj_w, before adj_curl)
+  // the dispersive nodes' transposed ADE recursion replaces their w (after adj_w, before adj_curl);
+  // the gyrotropic current's transposition reads lam_E' (after adj_w) and gathers over the box
   const bool ade = P.ade.Em[0] != nullptr;
+  const bool gyro = ctx->has_gyro;
   const dim3 ablk(32, 8), agrd((P.ade.n[2] + 31) / 32, (P.ade.n[1] + 7) / 8, std::max(1, P.ade.n[0]));
   if (c.order == 4) {
     adj_w_kernel<4, 0><<<grd, blk, 0, st>>>(P, A);
     if (ade) adj_ade_kernel<<<agrd, ablk, 0, st>>>(P, A);
+    if (gyro) { adj_gyro_mu_kernel<<<agrd, ablk, 0, st>>>(P, A); adj_gyro_j_kernel<<<agrd, ablk, 0, st>>>(P, A); }
     adj_curl_kernel<4, 0><<<grd, blk, 0, st>>>(P, A);
     adj_w_kernel<4, 1><<<grd, blk, 0, st>>>(P, A);
     adj_curl_kernel<4, 1><<<grd, blk, 0, st>>>(P, A);
+    ctx->launches += 6 + (ade ? 1 : 0) + (gyro ? 2 : 0);
   } else {
     adj_w_kernel<2, 0><<<grd, blk, 0, st>>>(P, A);
     if (ade) adj_ade_kernel<<<agrd, ablk, 0, st>>>(P, A);
+    if (gyro) { adj_gyro_mu_kernel<<<agrd, ablk, 0, st>>>(P, A); adj_gyro_j_kernel<<<agrd, ablk, 0, st>>>(P, A); }
     adj_curl_kernel<2, 0><<<grd, blk, 0, st>>>(P, A);
     adj_w_kernel<2, 1><<<grd, blk, 0, st>>>(P, A);
     adj_curl_kernel<2, 1><<<grd, blk, 0, st>>>(P, A);
+    ctx->launches += 6 + (ade ? 1 : 0) + (gyro ? 2 : 0);
   }
-  ctx->launches += ade ? 7 : 6;
   return DTMX_OK;
 }
 
@@ -1778,6 +1798,7 @@ static int fa_finish(dtmx_ctx* ctx, FaRun& R, double* objective, float* grad_eps
   ctx->monitors_off = false;
   if (!R.full) state_copy(ctx, R.ck[R.nseg], false);
   ctx->step = R.s0 + R.N;
+  ctx->gcur = R.gcur0 ^ (R.N & 1);
   std::vector<double> g((size_t)3 * R.nd);
   CK(cudaMemcpyAsync(g.data(), R.A.grad, g.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
@@ -1914,7 +1935,7 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
     for (int xc : {0, 4, 6, 8, 10, 12, 16, 24, 32, 64})
       if (xc <= c.nx) cand.push_back({1, 0, xc, 0});
     if (fused_usable(ctx, nullptr) && fused_prepare(ctx) == DTMX_OK)
-      for (int xc : {0, 8, 12, 16, 24, 32, 48, 64})
+      for (int xc : {0, 2, 4, 6, 8, 12, 16, 24, 32, 48, 64})
         if (xc <= c.nx) cand.push_back({3, 0, xc, 0});
     std::string why;
     if (torre_features_ok(ctx, &why))

@@ -119,7 +119,11 @@ typedef struct dtmx_material {
    * stepped as J_x <- a (cos th J_x + sin th <J_y>) + b E_x,
    *            J_y <- a (cos th J_y - sin th <J_x>) + b E_y,  J_z <- a J_z + b E_z,
    * a = exp(-gamma dt), th = wc dt, b = wp^2 dt, <.> the 4-node average of
-   * the other component around the node; then E += dt/eps_inf (curl H - J). */
+   * the other component around the node; then E += dt/eps_inf (curl H - J).
+   * Keep these nodes out of the CPML slabs: the CPML recursion does not
+   * account for the current, and a gyrotropic layer running through the
+   * absorber was measured to grow without bound after some thousands of
+   * steps (use a plain dielectric of the same diagonal permittivity there). */
   double gyro_wp, gyro_gamma, gyro_wc;
   double reserved[4];
 } dtmx_material;
@@ -358,7 +362,7 @@ int  dtmx_set_design(dtmx_ctx* ctx, const int lo[3], const int n[3], const float
  * forward pass records it and nothing is recomputed; otherwise the state is
  * checkpointed every checkpoint_every steps in device memory and each segment
  * is recomputed before its adjoint.  Both modes give bit-identical results.
- * Box geometry, CPML or no absorber, no gyrotropic material, no point source
+ * Box geometry, CPML or no absorber, no gyrotropic node in the design region, no point source
  * inside the design region.  On return the context holds the state after
  * nsteps, as after dtmx_step(nsteps).  The run's device buffers (adjoint
  * fields, history or checkpoints) come from the device's stream-ordered memory

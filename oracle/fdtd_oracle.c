@@ -979,6 +979,12 @@ int PFX(threads)(void) {
  *   lam_E = kE1 mu + sum_q kJ4 lam_Jp_q' + lam_Em',  lam_Em = kE0 mu + sum_q kJ3 lam_Jp_q',
  *   lam_Jp_q = -kEJ0 mu + kJ0 lam_Jp_q' + lam_Jm_q',  lam_Jm_q = -kEJ1 mu + kJ1 lam_Jp_q'.
  * The design permittivity does not enter a dispersive node: its gradient is 0.
+ * Gyrotropic nodes: the current J' = gA t + gB E (t_x = gC Jx + gS avg4(Jy),
+ * t_y = gC Jy - gS avg4(Jx), t_z = Jz, from the old J and E) is subtracted as
+ * E' -= gjc J'.  With muJ = lam_J' - gjc lam_E' and lam_t = gA muJ:
+ *   lam_E += gB muJ,  lam_J = gC lam_t (own node) -/+ gS/4 lam_t of the nodes
+ *   whose average holds it (x and y), lam_Jz = lam_tz;
+ * the adjoint of a non-gyrotropic node's current (identically zero) is zero.
  * Objective: J = sum over the plane x = X of Re(Ey^ conj(Hz^) - Ez^ conj(Hy^)),
  * with E^ = sum_s E^s exp(-i w s dt) dt and H^ = sum_s H^{s-1/2} exp(-i w (s-1/2) dt) dt
  * (the engine's DFT convention).  Gradient: dJ/d ie_c(p) =
@@ -1139,10 +1145,81 @@ static void ade_adjoint_state(const osim* s, real** lam, real** lEm, real* lJp[3
         }
 }
 
+/* muJ = lam_J' - gjc lam_E' on the gyrotropic nodes (0 elsewhere); uses lam_E' */
+static void gyro_adjoint_t(const osim* s, real* const* lam, real* const* lJg, real** lT) {
+  for (int i = s->ade_box[0][0]; i < s->ade_box[0][1]; i++)
+    for (int j = s->ade_box[1][0]; j < s->ade_box[1][1]; j++)
+      for (int k = s->ade_box[2][0]; k < s->ade_box[2][1]; k++) {
+        size_t id = IDX(s, i, j, k);
+        long ai = ade_index(s, i, j, k);
+        for (int c = 0; c < 3; c++) {
+          int mi = s->midx[c] ? s->midx[c][id] : 0;
+          lT[c][ai] = s->gyro[mi] ? (real)((double)lJg[c][ai] - (double)s->gjc[mi] * lam[c][id]) : 0;
+        }
+      }
+}
+
+static real adj_t_at(const osim* s, real* const* lT, int c, int i, int j, int k) {
+  long ai = ade_index(s, i, j, k);
+  return ai < 0 ? 0 : lT[c][ai];
+}
+
+/* lam_E += gB muJ and lam_J of the old current from lam_t = gA muJ (gathered
+ * over the nodes whose 4-node average holds each current) */
+static void gyro_adjoint_state(const osim* s, real** lam, real** lJg, real* const* lT) {
+  for (int i = s->ade_box[0][0]; i < s->ade_box[0][1]; i++)
+    for (int j = s->ade_box[1][0]; j < s->ade_box[1][1]; j++)
+      for (int k = s->ade_box[2][0]; k < s->ade_box[2][1]; k++) {
+        size_t id = IDX(s, i, j, k);
+        long ai = ade_index(s, i, j, k);
+        for (int c = 0; c < 3; c++) {
+          int mi = s->midx[c] ? s->midx[c][id] : 0;
+          if (!s->gyro[mi]) { lJg[c][ai] = 0; continue; }
+          const double mu = lT[c][ai], t = (double)s->gA[mi] * mu;
+          lam[c][id] += (real)((double)s->gB[mi] * mu);
+          double v;
+          if (c == 0) {
+            /* Jx(i,j) enters the averages of the y nodes (i,j+1), (i-1,j+1), (i,j), (i-1,j) */
+            int nb[4][2] = {{i, j + 1}, {i - 1, j + 1}, {i, j}, {i - 1, j}};
+            double acc = 0;
+            for (int q = 0; q < 4; q++) {
+              int ii = nb[q][0], jj = nb[q][1];
+              if (ii < 0 || ii >= s->nx || jj < 0 || jj >= s->ny) continue;
+              int mq = s->midx[1] ? s->midx[1][IDX(s, ii, jj, k)] : 0;
+              if (s->gyro[mq]) acc += 0.25 * (double)s->gS[mq] * (double)s->gA[mq] * adj_t_at(s, lT, 1, ii, jj, k);
+            }
+            v = (double)s->gC[mi] * t - acc;
+          } else if (c == 1) {
+            /* Jy(i,j) enters the averages of the x nodes (i+1,j), (i,j), (i+1,j-1), (i,j-1) */
+            int nb[4][2] = {{i + 1, j}, {i, j}, {i + 1, j - 1}, {i, j - 1}};
+            double acc = 0;
+            for (int q = 0; q < 4; q++) {
+              int ii = nb[q][0], jj = nb[q][1];
+              if (ii < 0 || ii >= s->nx || jj < 0 || jj >= s->ny) continue;
+              int mq = s->midx[0] ? s->midx[0][IDX(s, ii, jj, k)] : 0;
+              if (s->gyro[mq]) acc += 0.25 * (double)s->gS[mq] * (double)s->gA[mq] * adj_t_at(s, lT, 0, ii, jj, k);
+            }
+            v = (double)s->gC[mi] * t + acc;
+          } else {
+            v = t;
+          }
+          lJg[c][ai] = (real)v;
+        }
+      }
+}
+
 int PFX(forward_adjoint)(void* h, int nsteps, int X, double omega, double* J_out, double* grad_out) {
   osim* s = h;
   if (!s->des_on || X < 0 || X >= s->nx || nsteps < 1) return DTMX_ERR_INVALID;
-  if (s->cfg.geometry != DTMX_GEOM_BOX || s->cfg.absorber == DTMX_ABS_SPLIT_PML || s->has_gyro) return DTMX_ERR_UNSUPPORTED;
+  if (s->cfg.geometry != DTMX_GEOM_BOX || s->cfg.absorber == DTMX_ABS_SPLIT_PML) return DTMX_ERR_UNSUPPORTED;
+  /* the design permittivity of a gyrotropic node would enter next to its current: not carried */
+  for (int c = 0; c < 3 && s->has_gyro; c++)
+    for (int i = 0; i < s->des_n[0]; i++)
+      for (int j = 0; j < s->des_n[1]; j++)
+        for (int k = 0; k < s->des_n[2]; k++) {
+          size_t id = IDX(s, s->des_lo[0] + i, s->des_lo[1] + j, s->des_lo[2] + k);
+          if (s->gyro[s->midx[c] ? s->midx[c][id] : 0]) return DTMX_ERR_UNSUPPORTED;
+        }
   const double dt = s->cfg.dt;
   const size_t nd = (size_t)s->des_n[0] * s->des_n[1] * s->des_n[2];
   const size_t npl = (size_t)s->ny * s->nz;
@@ -1195,6 +1272,8 @@ int PFX(forward_adjoint)(void* h, int nsteps, int X, double omega, double* J_out
     s->amu[c] = calloc(s->ade_n, sizeof(real));
     for (int q = 0; q < DTMX_MAX_POLES; q++) { lJp[c][q] = calloc(s->ade_n, sizeof(real)); lJm[c][q] = calloc(s->ade_n, sizeof(real)); }
   }
+  real *lJg[3] = {0}, *lT[3] = {0};
+  for (int c = 0; c < 3 && s->has_gyro && s->ade_n; c++) { lJg[c] = calloc(s->ade_n, sizeof(real)); lT[c] = calloc(s->ade_n, sizeof(real)); }
   for (int st = nsteps; st >= 1; st--) {
     double sE = (double)(s0 + st), sH = sE - 0.5;
     double pe[2] = {cos(omega * sE * dt) * dt, -sin(omega * sE * dt) * dt};
@@ -1222,10 +1301,13 @@ int PFX(forward_adjoint)(void* h, int nsteps, int X, double omega, double* J_out
           }
     /* lam^{st-1} = A^T lam^{st}: E update transposed, then H update transposed */
     if (s->ade_n) ade_adjoint_mu(s, lam, lJp);
+    if (lJg[0]) gyro_adjoint_t(s, lam, lJg, lT);
     adj_half(s, lam, lpsi, 0);
     if (s->ade_n) ade_adjoint_state(s, lam, lEm, lJp, lJm);
+    if (lJg[0]) gyro_adjoint_state(s, lam, lJg, lT);
     adj_half(s, lam, lpsi, 1);
   }
+  for (int c = 0; c < 3; c++) { free(lJg[c]); free(lT[c]); }
   for (int c = 0; c < 3 && s->ade_n; c++) {
     free(lEm[c]); free(s->amu[c]); s->amu[c] = NULL;
     for (int q = 0; q < DTMX_MAX_POLES; q++) { free(lJp[c][q]); free(lJm[c][q]); }

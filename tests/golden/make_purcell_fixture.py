@@ -48,4 +48,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_purcell_fixture.py <path of the DTmaxwell4 source tree>")
+    main(sys.argv[1])

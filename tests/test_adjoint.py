@@ -104,6 +104,47 @@ def test_oracle_adjoint_dispersive_matches_finite_differences(overlap):
         assert abs(g[cell] - fd) <= 1e-6 * max(abs(fd), 1e-12 * abs(J)), (cell, g[cell], fd)
 
 
+def _gyro_materials(nx=22, ny=18, nz=18, overlap=False):
+    """A magnetised-Drude block (eps_diag 4, off-diagonal 0.3 at the source
+    frequency) across the objective plane, next to the design region;
+    overlap: one gyrotropic node inside the design region (refused)."""
+    from dtmaxwell4_b200 import abi
+    einf, g = abi.gyro_for(4.0, 0.3, OMEGA)
+    mats = [abi.make_material(1.0), abi.make_material(1.0, eps_inf=einf, gyro=g)]
+    idx = np.zeros((nx, ny, nz), np.uint8)
+    idx[13:18, 4:13, 5:13] = 1
+    if overlap:
+        idx[LO[0] + 1, LO[1], LO[2] + 2] = 1
+    return mats, idx
+
+
+def _oracle_gyro(eps, overlap=False):
+    import pyoracle
+    o = _setup(pyoracle.OracleSim(_cfg(2)), 2)
+    mats, idx = _gyro_materials(overlap=overlap)
+    o.set_materials(mats, idx, idx, idx)
+    o.set_design(LO, eps)
+    return o.forward_adjoint(N_STEPS, PLANE_X, OMEGA)
+
+
+def test_oracle_adjoint_gyrotropic_matches_finite_differences():
+    """The transposed magnetised-Drude current (4-node averages gathered
+    back): the FP64 adjoint equals central differences of the FP64 forward;
+    a design region holding a gyrotropic node is refused."""
+    eps = _eps()
+    J, g = _oracle_gyro(eps)
+    assert J != 0
+    for cell in [(2, 1, 1, 1), (0, 0, 2, 1), (1, 2, 0, 2), (0, 2, 2, 0)]:
+        h = 1e-4
+        ep, em = eps.copy(), eps.copy()
+        ep[cell] += h
+        em[cell] -= h
+        fd = (_oracle_gyro(ep)[0] - _oracle_gyro(em)[0]) / (2 * h)
+        assert abs(g[cell] - fd) <= 1e-6 * abs(fd), (cell, g[cell], fd)
+    with pytest.raises(ValueError):
+        _oracle_gyro(eps, overlap=True)
+
+
 def _gpu(order, eps, K=100, budget=-1):
     from dtmaxwell4_b200 import Simulation
     s = _setup(Simulation(_cfg(order)), order)
@@ -277,3 +318,49 @@ def test_gpu_adjoint_dispersive_against_central_differences():
     fd, ad = np.array(fd), np.array(ad)
     cos = float(fd @ ad / (np.linalg.norm(fd) * np.linalg.norm(ad)))
     assert cos >= 0.999, (cos, fd, ad)
+
+
+def _gpu_gyro(eps, K=100, budget=-1, overlap=False):
+    from dtmaxwell4_b200 import Simulation
+    s = _setup(Simulation(_cfg(2)), 2)
+    mats, idx = _gyro_materials(overlap=overlap)
+    s.set_materials(mats, idx, idx, idx)
+    s.set_design(LO, eps)
+    s.set_adjoint_memory(budget)
+    J, g = s.forward_adjoint(N_STEPS, PLANE_X, OMEGA, K)
+    return J, g, s
+
+
+@pytest.mark.gpu
+def test_gpu_adjoint_gyrotropic_against_fp64_adjoint():
+    """A magnetised-Drude block: the GPU adjoint of the gyrotropic current
+    against the FP64 adjoint; recorded history and checkpointed recompute
+    (odd interval: segments start on either current buffer) bit-identical
+    with the final state of a plain run; a design region holding a
+    gyrotropic node is refused."""
+    from dtmaxwell4_b200 import DtmxError, Simulation
+    eps = _eps()
+    J, g, s = _gpu_gyro(eps)
+    fin = [s.get_field(c) for c in range(6)]
+    s.close()
+    J2, g2, s2 = _gpu_gyro(eps, K=7, budget=0)
+    fin2 = [s2.get_field(c) for c in range(6)]
+    s2.step(5)
+    s2.close()
+    assert J2 == J and np.array_equal(g2, g)
+    ref = _setup(Simulation(_cfg(2)), 2)
+    mats, idx = _gyro_materials()
+    ref.set_materials(mats, idx, idx, idx)
+    ref.set_design(LO, eps)
+    ref.step(N_STEPS)
+    for c in range(6):
+        assert np.array_equal(fin[c], ref.get_field(c)) and np.array_equal(fin2[c], fin[c])
+    ref.close()
+    Jo, go = _oracle_gyro(eps.astype(np.float32).astype(np.float64))
+    assert abs(J - Jo) <= 1e-5 * abs(Jo), (J, Jo)
+    cos = float((g * go).sum() / (np.linalg.norm(g) * np.linalg.norm(go)))
+    rel = float(np.linalg.norm(g - go) / np.linalg.norm(go))
+    print("gyrotropic adjoint: J %.9g vs %.9g, cos %.8f, rel %.2e" % (J, Jo, cos, rel))
+    assert cos >= 0.9999 and rel <= 1e-3, (cos, rel)
+    with pytest.raises(DtmxError):
+        _gpu_gyro(eps, overlap=True)

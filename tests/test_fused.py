@@ -169,3 +169,20 @@ def test_single_sweep_tfsf_against_oracle(kind, engine):
             err = np.linalg.norm(got[c] - want[c]) / ref
             assert err <= 1e-5, (c, err)
     g.close()
+
+
+@pytest.mark.parametrize("budget", [-1, 0])
+def test_single_sweep_forward_adjoint_matches_per_step(budget):
+    """dtmx_forward_adjoint steps its forward pass and recomputed segments with
+    the selected engine: the single sweep (Drude sphere, CPML, design region)
+    gives the objective, gradient and final state of the per-step engine."""
+    case = _case(design=True)
+    res = []
+    for eng in (1, 3):
+        s = _sim(case, eng)
+        s.set_adjoint_memory(budget)
+        J, g = s.forward_adjoint(25, 40, 2 * np.pi / 10, 7)
+        res.append((J, g, _fields(s)))
+        s.close()
+    assert res[0][0] == res[1][0] and np.array_equal(res[0][1], res[1][1])
+    _same(res[1][2], res[0][2])

@@ -79,8 +79,11 @@ def test_triangular_lattice_geometry():
     sc = scenarios.gyro_crystal_purcell(n=(64, 64, 64), slab=8, layer=12, period=12, radius=4, box_half=5, nfreq=3,
                                         steps=10, pml=6)
     mats, idx = sc["materials"]
-    assert len(mats) == 3 and idx[2][32, 32, 32] == 1           # dipole node in the slab (the defect)
-    assert (idx[0][:, :, 16:28] == 2).all() and (idx[0][:, :, 40:] == 0).all()
+    assert len(mats) == 4 and idx[2][32, 32, 32] == 1           # dipole node in the slab (the defect)
+    # the gyrotropic layer (2) inside the absorber-free interior, the plain dielectric (3) in the CPML slabs
+    assert (idx[0][6:58, 6:58, 16:28] == 2).all() and (idx[0][:, :, 40:] == 0).all()
+    assert (idx[0][:6, :, 16:28] == 3).all() and (idx[0][:, 58:, 16:28] == 3).all()
+    assert mats[3].gyro_wp == 0 and mats[3].npoles == 0 and tuple(mats[3].eps) == (4.0, 4.0, 4.0)
     assert sc["flux"][0][0] == [27, 27, 27] and sc["flux"][0][1] == [37, 37, 37]
 
 
