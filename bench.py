@@ -201,6 +201,7 @@ def run_ours(args, rank, world):
         # engine configuration chosen by the library's autotuner (state is restored after the trials)
         tuned = sim.autotune(12)
         run_ours.tuned = tuned
+    run_ours.rows = sim.engine_config()[3]
     ncell = sc["cfg"].nx * sc["cfg"].ny * sc["cfg"].nz
     stream = torch.cuda.ExternalStream(sim.stream_handle())
     for _ in range(args.warmup):
@@ -376,6 +377,7 @@ def run_point_dipole(args):
     s = Simulation(sc["cfg"])
     scenarios.apply(s, sc)
     tuned = s.autotune(20)
+    s_rows = s.engine_config()[3]
     stream = torch.cuda.ExternalStream(s.stream_handle())
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s.sync()
@@ -388,7 +390,7 @@ def run_point_dipole(args):
     s.close()
     c = sc["cfg"]
     return {"workload": sc["desc"] + ", %d steps, %d probe traces" % (sc["steps"], tr.shape[0]),
-            "engine": "engine %d, x chunk %d, chosen by dtmx_autotune" % (tuned[0], tuned[2]),
+            "engine": "engine %d, x chunk %d, %d-row tiles, chosen by dtmx_autotune" % (tuned[0], tuned[2], s_rows),
             "gcell_per_s": round(c.nx * c.ny * c.nz * sc["steps"] / (ms * 1e-3) / 1e9, 3),
             "ms_per_step": round(ms / sc["steps"], 4),
             "note": "50 MB of fields: L2-resident, issue/latency-bound (ncu capture of the field kernels on this grid)"}
@@ -453,6 +455,7 @@ def run_gyro_purcell(args):
     scenarios.apply(s, sc)
     scenarios.apply_flux(s, sc)
     tuned = s.autotune(4)
+    s_rows = s.engine_config()[3]
     s.step(3)
     s.sync()
     t0 = time.perf_counter()
@@ -469,7 +472,7 @@ def run_gyro_purcell(args):
     rate = ncell * args.gyro_steps / dt / 1e9
     hbm, kind = measured_peaks()
     out.update({"workload": sc["desc"] + ", %d timed steps (of 8000) after 3 warm-up steps" % args.gyro_steps,
-                "engine": "engine %d, x chunk %d, chosen by dtmx_autotune" % (tuned[0], tuned[2]),
+                "engine": "engine %d, x chunk %d, %d-row tiles, chosen by dtmx_autotune" % (tuned[0], tuned[2], s_rows),
                 "gcell_per_s": round(rate, 3), "ms_per_step": round(1e3 * dt / args.gyro_steps, 3),
                 "bytes_per_cell_update": round(b_cell, 2),
                 "hbm_frac": round(rate * 1e9 * b_cell / (hbm * 1e9), 4), "hbm_peak_gbs": hbm, "peak_kind": kind})
@@ -535,6 +538,7 @@ def cpu_check_fp64(args, n=64, steps=4000):
     gid = scenarios.apply(g, sc)
     if eng in (1, 3):
         g.set_engine(eng, tb)
+        g.set_tile_rows(getattr(run_ours, "rows", 16))
     g.step(steps)
     g.sync()
     o = pyoracle.OracleSim(sc["cfg"], "f64")
@@ -624,8 +628,8 @@ def main():
                 "config": {"workload": "%s %d^3, %d time steps per step" % (
                                "drude_sphere_tfsf" if args.workload == "drude" else "plain_cpml", args.n, args.tsteps),
                            "engine": ("wavefront T=%d" % max(1, args.tblock)) if args.engine == 2 else
-                                     "engine %d, T %d, x chunk %d (0: automatic)%s" % (tuple(run_ours.tuned[:3]) + (
-                                         ", chosen by dtmx_autotune" if not args.engine else "",)),
+                                     "engine %d, T %d, x chunk %d (0: automatic), %d-row tiles%s" % (tuple(run_ours.tuned[:3]) + (
+                                         run_ours.rows, ", chosen by dtmx_autotune" if not args.engine else "",)),
                            "desc": sc["desc"], "time_steps_per_step": args.tsteps,
                            "l2": "inputs larger than L2 (%.2f GB of fields)" % (6 * args.n ** 3 * 4 / 1e9),
                            "parallelism": "replicas%d" % world},

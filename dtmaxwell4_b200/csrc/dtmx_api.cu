@@ -106,7 +106,9 @@ struct dtmx_ctx {
   float* f_alt[6] = {};
   float* hax_alt[3][2] = {};
   TmaMaps maps_alt{};
-  FusedMaps fmaps[2]{};               // [0] reads P.f, [1] reads f_alt (swapped with the buffers)
+  FusedMaps fmaps[2]{};               // 16-row tiles: [0] reads P.f, [1] reads f_alt (swapped with the buffers)
+  FusedMaps fmaps8[2]{};              // the same for 8-row tiles
+  int frows = 16;                     // tile rows of the single sweep (16 or 8; dtmx_set_tile_rows, dtmx_autotune)
   bool fused_ready = false;
   int parity = 0;                     // 0: state in the buffers allocated first
   int* d_err = nullptr;
@@ -1215,15 +1217,17 @@ static bool fused_usable(const dtmx_ctx* ctx, std::string* why) {
   return true;
 }
 
+template <int NR>
 static int build_fused_maps(dtmx_ctx* ctx, FusedMaps& fm, float* const* f) {
+  using L = FL<NR>;
   int rc;
   for (int c = 0; c < 3; c++) {
-    if ((rc = make_map(ctx, &fm.e[c], f[c], false, FE_W, FE_R))) return rc;
+    if ((rc = make_map(ctx, &fm.e[c], f[c], false, FE_W, L::FE_R))) return rc;
     fm.mat[c] = ctx->maps.mat[c];
   }
-  if ((rc = make_map(ctx, &fm.hx, f[3], false, FHX_W, FHX_R))) return rc;
-  if ((rc = make_map(ctx, &fm.hy, f[4], false, FHY_W, FHY_R))) return rc;
-  return make_map(ctx, &fm.hz, f[5], false, FHZ_W, FHZ_R);
+  if ((rc = make_map(ctx, &fm.hx, f[3], false, FHX_W, L::FHX_R))) return rc;
+  if ((rc = make_map(ctx, &fm.hy, f[4], false, FHY_W, L::FHY_R))) return rc;
+  return make_map(ctx, &fm.hz, f[5], false, FHZ_W, L::FHZ_R);
 }
 
 // First use: the second buffer set, the maps reading each set, the tile table.
@@ -1231,7 +1235,8 @@ static int fused_prepare(dtmx_ctx* ctx) {
   if (ctx->fused_ready) return DTMX_OK;
   static bool attr = false;
   if (!attr) {
-    cudaFuncSetAttribute(fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)F_SMEM_BYTES);
+    cudaFuncSetAttribute(fused_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FL<2>::SMEM);
+    cudaFuncSetAttribute(fused_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FL<1>::SMEM);
     attr = true;
   }
   const dtmx_config& c = ctx->cfg;
@@ -1253,8 +1258,10 @@ static int fused_prepare(dtmx_ctx* ctx) {
     ctx->maps = save;
     for (int comp = 0; comp < 6; comp++) ctx->P.f[comp] = fsave[comp];
   }
-  if (!rc) rc = build_fused_maps(ctx, ctx->fmaps[0], ctx->P.f);
-  if (!rc) rc = build_fused_maps(ctx, ctx->fmaps[1], ctx->f_alt);
+  if (!rc) rc = build_fused_maps<2>(ctx, ctx->fmaps[0], ctx->P.f);
+  if (!rc) rc = build_fused_maps<2>(ctx, ctx->fmaps[1], ctx->f_alt);
+  if (!rc) rc = build_fused_maps<1>(ctx, ctx->fmaps8[0], ctx->P.f);
+  if (!rc) rc = build_fused_maps<1>(ctx, ctx->fmaps8[1], ctx->f_alt);
   if (rc) return rc;
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->fused_ready = true;
@@ -1269,6 +1276,7 @@ static void fused_swap(dtmx_ctx* ctx) {
     for (int q = 0; q < 2; q++) std::swap(ctx->P.ab.aux[a][2 + q], ctx->hax_alt[a][q]);
   std::swap(ctx->maps, ctx->maps_alt);
   std::swap(ctx->fmaps[0], ctx->fmaps[1]);
+  std::swap(ctx->fmaps8[0], ctx->fmaps8[1]);
   ctx->parity ^= 1;
   ctx->tmaps_ok = false;          // the wavefront engine's maps are rebuilt for the current buffer
 }
@@ -1278,7 +1286,7 @@ static void fused_swap(dtmx_ctx* ctx) {
 static int fused_xchunk_for(const dtmx_ctx* ctx) {
   if (ctx->xchunk > 0) return std::min(ctx->xchunk, FX_MAX);
   const dtmx_config& c = ctx->cfg;
-  const long long tiles = (long long)((c.nz + TZ - 1) / TZ) * ((c.ny + TYT - 1) / TYT);
+  const long long tiles = (long long)((c.nz + TZ - 1) / TZ) * ((c.ny + ctx->frows - 1) / ctx->frows);
   const long long target = 148LL * 3 * 8;
   const long long chunks = std::max<long long>(1, (target + tiles - 1) / tiles);
   const long long xc = (c.nx + chunks - 1) / chunks;
@@ -1325,9 +1333,10 @@ static int launch_fused_step(dtmx_ctx* ctx) {
     ctx->gcur = 1 - ctx->gcur;
     nl++;
   }
-  const dim3 blk(TZ, TW), grd((c.nz + TZ - 1) / TZ, (c.ny + TYT - 1) / TYT, (c.nx + PA.xchunk - 1) / PA.xchunk);
+  const dim3 blk(TZ, TW), grd((c.nz + TZ - 1) / TZ, (c.ny + ctx->frows - 1) / ctx->frows, (c.nx + PA.xchunk - 1) / PA.xchunk);
   if (ctx->profiling) cudaEventRecord(ctx->ev[0], st);
-  fused_kernel<<<grd, blk, F_SMEM_BYTES, st>>>(PA, fa, ctx->fmaps[0]);
+  if (ctx->frows == 8) fused_kernel<1><<<grd, blk, FL<1>::SMEM, st>>>(PA, fa, ctx->fmaps8[0]);
+  else fused_kernel<2><<<grd, blk, FL<2>::SMEM, st>>>(PA, fa, ctx->fmaps[0]);
   if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
   nl++;
   if (PA.ade.Em[0] || ctx->has_gyro) {
@@ -1902,7 +1911,7 @@ struct TuneKey {
     return std::tie(nx, ny, nz, order, absorber, geometry, feats) < std::tie(o.nx, o.ny, o.nz, o.order, o.absorber, o.geometry, o.feats);
   }
 };
-struct TuneVal { int engine, tblock, xchunk; double ms; };
+struct TuneVal { int engine, tblock, xchunk; double ms; int rows = 16; };
 static std::map<TuneKey, TuneVal>& tune_cache() {
   static std::map<TuneKey, TuneVal> m;
   return m;
@@ -1927,7 +1936,7 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
     if (cudaMalloc(&ck, state_bytes(ctx)) != cudaSuccess) return fail(ctx, DTMX_ERR_OOM, "autotune state copy");
     state_copy(ctx, ck, true);
     const long long step0 = ctx->step;
-    const int gcur0 = ctx->gcur, eng0 = ctx->engine, tb0 = ctx->tblock, xc0 = ctx->xchunk;
+    const int gcur0 = ctx->gcur, eng0 = ctx->engine, tb0 = ctx->tblock, xc0 = ctx->xchunk, fr0 = ctx->frows;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -1935,8 +1944,9 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
     for (int xc : {0, 4, 6, 8, 10, 12, 16, 24, 32, 64})
       if (xc <= c.nx) cand.push_back({1, 0, xc, 0});
     if (fused_usable(ctx, nullptr) && fused_prepare(ctx) == DTMX_OK)
-      for (int xc : {0, 2, 4, 6, 8, 12, 16, 24, 32, 48, 64})
-        if (xc <= c.nx) cand.push_back({3, 0, xc, 0});
+      for (int rows : {16, 8})
+        for (int xc : {0, 2, 4, 6, 8, 12, 16, 24, 32, 48, 64})
+          if (xc <= c.nx) cand.push_back({3, 0, xc, 0, rows});
     std::string why;
     if (torre_features_ok(ctx, &why))
       for (int T : {1, 2, 4})
@@ -1945,6 +1955,7 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
     for (auto& cd : cand) {
       ctx->xchunk = cd.xchunk;
       ctx->engine = cd.engine;
+      ctx->frows = cd.rows;
       int r = DTMX_OK;
       const int n = cd.engine == 2 ? (trial_steps / cd.tblock) * cd.tblock : trial_steps;
       cudaEventRecord(e0, ctx->stream);
@@ -1969,12 +1980,13 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
     cudaFree(ck);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx->engine = eng0; ctx->tblock = tb0; ctx->xchunk = xc0;
+    ctx->engine = eng0; ctx->tblock = tb0; ctx->xchunk = xc0; ctx->frows = fr0;
     tune_cache()[key] = best;
   }
   ctx->engine = best.engine;
   ctx->tblock = best.tblock;
   ctx->xchunk = best.xchunk;
+  ctx->frows = best.rows;
   drop_graphs(ctx);
   if (engine_out) *engine_out = best.engine;
   if (tblock_out) *tblock_out = best.tblock;
@@ -2155,6 +2167,22 @@ extern "C" int dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block) {
   }
   ctx->engine = engine;
   drop_graphs(ctx);
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_set_tile_rows(dtmx_ctx* ctx, int rows) {
+  if (!ctx || (rows != 0 && rows != 8 && rows != 16)) return fail(ctx, DTMX_ERR_INVALID, "tile rows must be 8 or 16");
+  ctx->frows = rows ? rows : 16;
+  drop_graphs(ctx);
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_get_engine(dtmx_ctx* ctx, int* engine, int* time_block, int* xchunk, int* tile_rows) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  if (engine) *engine = ctx->engine;
+  if (time_block) *time_block = ctx->tblock;
+  if (xchunk) *xchunk = ctx->xchunk;
+  if (tile_rows) *tile_rows = ctx->frows;
   return DTMX_OK;
 }
 

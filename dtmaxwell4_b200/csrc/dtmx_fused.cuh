@@ -42,29 +42,36 @@
 namespace dtmx {
 
 constexpr int FE_W = 40;                     // E box: z in [k0-4, k0+36) (16-byte aligned start)
-constexpr int FE_R = TYT + 2;                // ... y in [j0-1, j0+17)
-constexpr int FE_N = 736;                    // 18 x 40 = 720 floats, rounded up to 128 bytes
-constexpr int FHX_W = 36, FHX_R = TYT + 1;   // old Hx: z [k0, k0+36), y [j0, j0+17)
-constexpr int FHY_W = 36, FHY_R = TYT;       // old Hy: z [k0, k0+36), y [j0, j0+16)
-constexpr int FHZ_W = 32, FHZ_R = TYT + 1;   // old Hz: z [k0, k0+32), y [j0, j0+17)
-constexpr int F_OFF_HX = 3 * FE_N;                        // 2208
-constexpr int F_OFF_HY = F_OFF_HX + 640;                  // 612 floats, rounded up
-constexpr int F_OFF_HZ = F_OFF_HY + FHY_W * FHY_R;        // 576
-constexpr int F_OFF_M = F_OFF_HZ + FHZ_W * FHZ_R;         // 544
-constexpr int F_STAGE = F_OFF_M + 3 * TYT * TZ / 4;       // material: 3 x 16 x 32 bytes; 4352 floats
-constexpr unsigned F_BYTES = (3 * FE_W * FE_R + FHX_W * FHX_R + FHY_W * FHY_R + FHZ_W * FHZ_R) * 4;
-constexpr unsigned F_BYTES_MAT = 3 * TYT * TZ;
+constexpr int FHX_W = 36, FHY_W = 36, FHZ_W = 32;
 constexpr int F_NST = 3;
-constexpr int HN_P = TZ + 1;                 // new-H plane buffer: z in [k0, k0+33) ...
-constexpr int HN_N = (TYT + 1) * HN_P;       // ... y in [j0, j0+17), per component (Hx, Hy, Hz)
-constexpr int F_HN = ((3 * HN_N + 31) / 32) * 32;
+constexpr int HN_P = TZ + 1;                 // new-H plane buffer: z in [k0, k0+33)
 constexpr int FX_MAX = 64;                   // longest x chunk
-constexpr size_t F_SMEM_BYTES = (size_t)(F_NST * F_STAGE + 2 * F_HN) * 4 + sizeof(MatShared) + F_NST * 8 + 128;
-static_assert(F_OFF_HY % 32 == 0 && F_OFF_HZ % 32 == 0 && F_OFF_M % 32 == 0 && F_STAGE % 32 == 0, "128-byte boxes");
+constexpr int F_MROWS = 16;                  // material tiles: the per-step kernels' 32 x 16 boxes
+__host__ __device__ constexpr int f_up32(int v) { return (v + 31) / 32 * 32; }
 
-// TMA descriptors of one buffer set
+// Shared-memory layout of a tile of NR rows per warp (8 NR rows), in floats.
+template <int NR>
+struct FL {
+  static constexpr int TY = TW * NR;                 // own rows of a tile (16 or 8)
+  static constexpr int FE_R = TY + 2;                // E box rows: y in [j0-1, j0+TY+1)
+  static constexpr int FE_N = f_up32(FE_R * FE_W);
+  static constexpr int FHX_R = TY + 1, FHY_R = TY, FHZ_R = TY + 1;   // old-H boxes
+  static constexpr int OFF_HX = 3 * FE_N;
+  static constexpr int OFF_HY = OFF_HX + f_up32(FHX_W * FHX_R);
+  static constexpr int OFF_HZ = OFF_HY + f_up32(FHY_W * FHY_R);
+  static constexpr int OFF_M = OFF_HZ + f_up32(FHZ_W * FHZ_R);
+  static constexpr int STAGE = OFF_M + 3 * F_MROWS * TZ / 4;
+  static constexpr unsigned BYTES = (3 * FE_W * FE_R + FHX_W * FHX_R + FHY_W * FHY_R + FHZ_W * FHZ_R) * 4;
+  static constexpr unsigned BYTES_MAT = 3 * F_MROWS * TZ;
+  static constexpr int HN_N = (TY + 1) * HN_P;       // new-H plane, per component: y in [j0, j0+TY+1)
+  static constexpr int HN = f_up32(3 * HN_N);
+  static constexpr size_t SMEM = (size_t)(F_NST * STAGE + 2 * HN) * 4 + sizeof(MatShared) + F_NST * 8 + 128;
+};
+static_assert(FL<2>::STAGE == 4352 && FL<2>::OFF_HX == 2208, "16-row layout");
+
+// TMA descriptors of one buffer set for one tile height
 struct FusedMaps {
-  CUtensorMap e[3];                          // 40 x 18 E boxes
+  CUtensorMap e[3];                          // 40 x (TY+2) E boxes
   CUtensorMap hx, hy, hz;                    // old-H boxes
   CUtensorMap mat[3];                        // 32 x 16 material tiles (the per-step kernels' maps)
 };
@@ -77,15 +84,21 @@ struct FusedArgs {
 };
 
 // staged-tile accessors (tile-local y, z)
-__device__ __forceinline__ float fE(const float* st, int c, int y, int z) { return st[c * FE_N + (y + 1) * FE_W + z + 4]; }
-__device__ __forceinline__ float fHx(const float* st, int y, int z) { return st[F_OFF_HX + y * FHX_W + z]; }
-__device__ __forceinline__ float fHy(const float* st, int y, int z) { return st[F_OFF_HY + y * FHY_W + z]; }
-__device__ __forceinline__ float fHz(const float* st, int y, int z) { return st[F_OFF_HZ + y * FHZ_W + z]; }
-__device__ __forceinline__ int fM(const float* st, int c, int y, int z) {
-  return reinterpret_cast<const uint8_t*>(st + F_OFF_M)[c * TYT * TZ + y * TZ + z];
+template <int NR>
+__device__ __forceinline__ float fE(const float* st, int c, int y, int z) {
+  return st[c * FL<NR>::FE_N + (y + 1) * FE_W + z + 4];
 }
-__device__ __forceinline__ float& fN(float* hn, int q, int y, int z) { return hn[q * HN_N + y * HN_P + z]; }
-__device__ __forceinline__ float fN(const float* hn, int q, int y, int z) { return hn[q * HN_N + y * HN_P + z]; }
+template <int NR> __device__ __forceinline__ float fHx(const float* st, int y, int z) { return st[FL<NR>::OFF_HX + y * FHX_W + z]; }
+template <int NR> __device__ __forceinline__ float fHy(const float* st, int y, int z) { return st[FL<NR>::OFF_HY + y * FHY_W + z]; }
+template <int NR> __device__ __forceinline__ float fHz(const float* st, int y, int z) { return st[FL<NR>::OFF_HZ + y * FHZ_W + z]; }
+template <int NR>
+__device__ __forceinline__ int fM(const float* st, int c, int y, int z) {
+  return reinterpret_cast<const uint8_t*>(st + FL<NR>::OFF_M)[c * F_MROWS * TZ + y * TZ + z];
+}
+template <int NR>
+__device__ __forceinline__ float& fN(float* hn, int q, int y, int z) { return hn[q * FL<NR>::HN_N + y * HN_P + z]; }
+template <int NR>
+__device__ __forceinline__ float fN(const float* hn, int q, int y, int z) { return hn[q * FL<NR>::HN_N + y * HN_P + z]; }
 
 // CPML correction of component C at node (i, j, k) with slab indices si
 // (absorb_apply3 of the CPML form); H auxiliaries read from A and written to
@@ -127,7 +140,7 @@ __device__ __forceinline__ float fused_hnode(const Params& p, const FusedArgs& f
 // components' offset along a derivative axis) and at 2v + 1 (the E
 // components').  Rows: x planes x0-1 .. x0+FX_MAX, y rows j0 .. j0+16, z
 // columns k0 .. k0+32.
-constexpr int FCO_X = 0, FCO_Y = (FX_MAX + 2) * 6, FCO_Z = FCO_Y + (TYT + 1) * 6, FCO_N = FCO_Z + (TZ + 1) * 6;
+constexpr int FCO_X = 0, FCO_Y = (FX_MAX + 2) * 6, FCO_Z = FCO_Y + (F_MROWS + 1) * 6, FCO_N = FCO_Z + (TZ + 1) * 6;
 
 // index of coordinate v in the slab of its axis (-1 outside)
 __device__ __forceinline__ int slab_cs(const Params& p, int a, int v) {
@@ -185,36 +198,36 @@ __device__ __forceinline__ float fused_aux_apply(const Params& p, const FusedArg
 // own nodes (the next plane's x taps and its E update); ep holds those of
 // plane i - 1.  AXM: the slab axes of the tile-plane (0: no absorber); the
 // slab coordinates xs (plane), ys (rows), zs (column) are per-thread constants.
-template <int AXM>
+template <int NR, int AXM>
 __device__ __forceinline__ void fused_h_own(const Params& p, const FusedArgs& fa, const float* st, float* hn, int i,
-                                            int j0, int k0, bool store, const bool (&ok)[RY], const float (&ep)[RY][3],
-                                            float (&hc)[RY][3], float (&ec)[RY][3], const float* fco, int xs,
-                                            const int (&ys)[RY], int zs) {
+                                            int j0, int k0, bool store, const bool (&ok)[NR], const float (&ep)[NR][3],
+                                            float (&hc)[NR][3], float (&ec)[NR][3], const float* fco, int xs,
+                                            const int (&ys)[NR], int zs) {
   const int lane = threadIdx.x, w = threadIdx.y;
   const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
   const long long pb = (long long)i * p.g.sx;
-  int si[RY][3];
-  float old[RY][3][2];
+  int si[NR][3];
+  float old[NR][3][2];
   if (AXM) {
     // every auxiliary of the thread's nodes is requested before any is used
 #pragma unroll
-    for (int r = 0; r < RY; r++) {
+    for (int r = 0; r < NR; r++) {
       fused_slabs<AXM>(p, i, j0 + w + TW * r, k0 + lane, xs, ys[r], zs, si[r]);
       if (!ok[r]) si[r][0] = si[r][1] = si[r][2] = -1;
       fused_aux_load<AXM, true>(p, fa, si[r], old[r]);
     }
   }
 #pragma unroll
-  for (int r = 0; r < RY; r++) {
+  for (int r = 0; r < NR; r++) {
     const int y = w + TW * r, j = j0 + y, k = k0 + lane;
-    const float ez = fE(st, 2, y, lane), ey = fE(st, 1, y, lane), ex = fE(st, 0, y, lane);
+    const float ez = fE<NR>(st, 2, y, lane), ey = fE<NR>(st, 1, y, lane), ex = fE<NR>(st, 0, y, lane);
     ec[r][0] = ex; ec[r][1] = ey; ec[r][2] = ez;
     // Hx -= dt(dy Ez - dz Ey); Hy -= dt(dz Ex - dx Ez); Hz -= dt(dx Ey - dy Ex)
-    const float dhx[3] = {0.f, __fmul_rn(-cy, __fsub_rn(ez, fE(st, 2, y - 1, lane))),
-                         __fmul_rn(cz, __fsub_rn(ey, fE(st, 1, y, lane - 1)))};
+    const float dhx[3] = {0.f, __fmul_rn(-cy, __fsub_rn(ez, fE<NR>(st, 2, y - 1, lane))),
+                         __fmul_rn(cz, __fsub_rn(ey, fE<NR>(st, 1, y, lane - 1)))};
     const float dhy[3] = {__fmul_rn(cx, __fsub_rn(ez, ep[r][2])), 0.f,
-                         __fmul_rn(-cz, __fsub_rn(ex, fE(st, 0, y, lane - 1)))};
-    const float dhz[3] = {__fmul_rn(-cx, __fsub_rn(ey, ep[r][1])), __fmul_rn(cy, __fsub_rn(ex, fE(st, 0, y - 1, lane))),
+                         __fmul_rn(-cz, __fsub_rn(ex, fE<NR>(st, 0, y, lane - 1)))};
+    const float dhz[3] = {__fmul_rn(-cx, __fsub_rn(ey, ep[r][1])), __fmul_rn(cy, __fsub_rn(ex, fE<NR>(st, 0, y - 1, lane))),
                          0.f};
     float ix = sum3(dhx[0], dhx[1], dhx[2]), iy = sum3(dhy[0], dhy[1], dhy[2]), iz = sum3(dhz[0], dhz[1], dhz[2]);
     if (AXM && (si[r][0] & si[r][1] & si[r][2]) >= 0) {
@@ -225,12 +238,12 @@ __device__ __forceinline__ void fused_h_own(const Params& p, const FusedArgs& fa
       iy = __fadd_rn(iy, fused_aux_apply<4, AXM>(p, fa, si[r], old[r], dhy, fx, fy, fz, store));
       iz = __fadd_rn(iz, fused_aux_apply<5, AXM>(p, fa, si[r], old[r], dhz, fx, fy, fz, store));
     }
-    float vx = __fadd_rn(fHx(st, y, lane), ix), vy = __fadd_rn(fHy(st, y, lane), iy), vz = __fadd_rn(fHz(st, y, lane), iz);
+    float vx = __fadd_rn(fHx<NR>(st, y, lane), ix), vy = __fadd_rn(fHy<NR>(st, y, lane), iy), vz = __fadd_rn(fHz<NR>(st, y, lane), iz);
     if (!ok[r]) { vx = 0.f; vy = 0.f; vz = 0.f; }
     hc[r][0] = vx; hc[r][1] = vy; hc[r][2] = vz;
-    fN(hn, 0, y, lane) = vx;
-    fN(hn, 1, y, lane) = vy;
-    fN(hn, 2, y, lane) = vz;
+    fN<NR>(hn, 0, y, lane) = vx;
+    fN<NR>(hn, 1, y, lane) = vy;
+    fN<NR>(hn, 2, y, lane) = vz;
     if (store && ok[r]) {
       const long long off = pb + (long long)j * p.g.sy + k;
       fa.dst[3][off] = vx;
@@ -246,14 +259,14 @@ __device__ __forceinline__ void fused_h_own(const Params& p, const FusedArgs& fa
 //   warp 2: Hy of column 32   warp 3: Hx of column 32 (lanes 0-15)
 // xe: the warp's old E of the previous plane at its halo node (x tap), updated.
 // A CPML slab node takes the correction with the auxiliaries read, not written.
-template <bool ABS>
+template <int NR, bool ABS>
 __device__ __forceinline__ void fused_h_halo(const Params& p, const FusedArgs& fa, const float* st, float* hn, int i,
                                              int j0, int k0, float& xe) {
   const int lane = threadIdx.x, w = threadIdx.y;
-  if (w > 3 || (w > 1 && lane >= TYT)) return;
+  if (w > 3 || (w > 1 && lane >= FL<NR>::TY)) return;
   const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
   const bool row = w < 2;
-  const int y = row ? TYT : lane, z = row ? lane : TZ;
+  const int y = row ? FL<NR>::TY : lane, z = row ? lane : TZ;
   const int j = j0 + y, k = k0 + z;
   const bool ok = j < p.g.n[1] && k < p.g.n[2];
   int si[3] = {-1, -1, -1};
@@ -261,23 +274,23 @@ __device__ __forceinline__ void fused_h_halo(const Params& p, const FusedArgs& f
   const bool slab = ABS && ok && node_slabs(p, i, j, k, si);
   float v;
   if (w == 0) {
-    const float ey = fE(st, 1, y, z);
+    const float ey = fE<NR>(st, 1, y, z);
     const float d0 = __fmul_rn(-cx, __fsub_rn(ey, xe));
-    const float d1 = __fmul_rn(cy, __fsub_rn(fE(st, 0, y, z), fE(st, 0, y - 1, z)));
-    v = fused_hnode<5, ABS>(p, fa, fHz(st, y, z), d0, d1, 0.f, slab, idx, si, false);
+    const float d1 = __fmul_rn(cy, __fsub_rn(fE<NR>(st, 0, y, z), fE<NR>(st, 0, y - 1, z)));
+    v = fused_hnode<5, ABS>(p, fa, fHz<NR>(st, y, z), d0, d1, 0.f, slab, idx, si, false);
     xe = ey;
   } else if (w == 2) {
-    const float ez = fE(st, 2, y, z);
+    const float ez = fE<NR>(st, 2, y, z);
     const float d0 = __fmul_rn(cx, __fsub_rn(ez, xe));
-    const float d2 = __fmul_rn(-cz, __fsub_rn(fE(st, 0, y, z), fE(st, 0, y, z - 1)));
-    v = fused_hnode<4, ABS>(p, fa, fHy(st, y, z), d0, 0.f, d2, slab, idx, si, false);
+    const float d2 = __fmul_rn(-cz, __fsub_rn(fE<NR>(st, 0, y, z), fE<NR>(st, 0, y, z - 1)));
+    v = fused_hnode<4, ABS>(p, fa, fHy<NR>(st, y, z), d0, 0.f, d2, slab, idx, si, false);
     xe = ez;
   } else {
-    const float d1 = __fmul_rn(-cy, __fsub_rn(fE(st, 2, y, z), fE(st, 2, y - 1, z)));
-    const float d2 = __fmul_rn(cz, __fsub_rn(fE(st, 1, y, z), fE(st, 1, y, z - 1)));
-    v = fused_hnode<3, ABS>(p, fa, fHx(st, y, z), 0.f, d1, d2, slab, idx, si, false);
+    const float d1 = __fmul_rn(-cy, __fsub_rn(fE<NR>(st, 2, y, z), fE<NR>(st, 2, y - 1, z)));
+    const float d2 = __fmul_rn(cz, __fsub_rn(fE<NR>(st, 1, y, z), fE<NR>(st, 1, y, z - 1)));
+    v = fused_hnode<3, ABS>(p, fa, fHx<NR>(st, y, z), 0.f, d1, d2, slab, idx, si, false);
   }
-  fN(hn, w == 0 ? 2 : w == 2 ? 1 : 0, y, z) = ok ? v : 0.f;
+  fN<NR>(hn, w == 0 ? 2 : w == 2 ? 1 : 0, y, z) = ok ? v : 0.f;
 }
 
 // New E of plane i on the own nodes.  ep: old E (registers), hn: new H of
@@ -286,42 +299,42 @@ __device__ __forceinline__ void fused_h_halo(const Params& p, const FusedArgs& f
 //   MODE 0: general (mixed materials, dispersive nodes left to the ADE pass,
 //           design region)
 // AXM: the slab axes of the tile-plane (0: no absorber).
-template <int MODE, int AXM>
+template <int NR, int MODE, int AXM>
 __device__ __forceinline__ void fused_e_own(const Params& p, const FusedArgs& fa, const float* st, const float* hn,
-                                            const MatShared& ms, int um, int i, int j0, int k0, const bool (&ok)[RY],
-                                            const float (&ep)[RY][3], const float (&hc)[RY][3], const float* fco, int xs,
-                                            const int (&ys)[RY], int zs) {
+                                            const MatShared& ms, int um, int i, int j0, int k0, const bool (&ok)[NR],
+                                            const float (&ep)[NR][3], const float (&hc)[NR][3], const float* fco, int xs,
+                                            const int (&ys)[NR], int zs) {
   const int lane = threadIdx.x, w = threadIdx.y;
   const float cx = p.cdt[0], cy = p.cdt[1], cz = p.cdt[2];
   float iu[3] = {1.f, 1.f, 1.f};
   if (MODE != 0) { iu[0] = ms.inv_eps[um][0]; iu[1] = ms.inv_eps[um][1]; iu[2] = ms.inv_eps[um][2]; }
   const long long pb = (long long)i * p.g.sx;
-  int si[RY][3];
-  float old[RY][3][2];
+  int si[NR][3];
+  float old[NR][3][2];
   if (AXM) {
 #pragma unroll
-    for (int r = 0; r < RY; r++) {
+    for (int r = 0; r < NR; r++) {
       fused_slabs<AXM>(p, i, j0 + w + TW * r, k0 + lane, xs, ys[r], zs, si[r]);
       if (!ok[r]) si[r][0] = si[r][1] = si[r][2] = -1;
       fused_aux_load<AXM, false>(p, fa, si[r], old[r]);
     }
   }
 #pragma unroll
-  for (int r = 0; r < RY; r++) {
+  for (int r = 0; r < NR; r++) {
     if (!ok[r]) continue;
     const int y = w + TW * r, j = j0 + y, k = k0 + lane;
     const long long off = pb + (long long)j * p.g.sy + k;
-    const float hx = fN(hn, 0, y, lane), hy = fN(hn, 1, y, lane), hz = fN(hn, 2, y, lane);
+    const float hx = fN<NR>(hn, 0, y, lane), hy = fN<NR>(hn, 1, y, lane), hz = fN<NR>(hn, 2, y, lane);
     // Ex += dt/eps(dy Hz - dz Hy); Ey += dt/eps(dz Hx - dx Hz); Ez += dt/eps(dx Hy - dy Hx)
     float d[3][3];
     d[0][0] = 0.f;
-    d[0][1] = __fmul_rn(cy, __fsub_rn(fN(hn, 2, y + 1, lane), hz));
-    d[0][2] = __fmul_rn(-cz, __fsub_rn(fN(hn, 1, y, lane + 1), hy));
+    d[0][1] = __fmul_rn(cy, __fsub_rn(fN<NR>(hn, 2, y + 1, lane), hz));
+    d[0][2] = __fmul_rn(-cz, __fsub_rn(fN<NR>(hn, 1, y, lane + 1), hy));
     d[1][0] = __fmul_rn(-cx, __fsub_rn(hc[r][2], hz));
     d[1][1] = 0.f;
-    d[1][2] = __fmul_rn(cz, __fsub_rn(fN(hn, 0, y, lane + 1), hx));
+    d[1][2] = __fmul_rn(cz, __fsub_rn(fN<NR>(hn, 0, y, lane + 1), hx));
     d[2][0] = __fmul_rn(cx, __fsub_rn(hc[r][1], hy));
-    d[2][1] = __fmul_rn(-cy, __fsub_rn(fN(hn, 0, y + 1, lane), hx));
+    d[2][1] = __fmul_rn(-cy, __fsub_rn(fN<NR>(hn, 0, y + 1, lane), hx));
     d[2][2] = 0.f;
     const bool slab = AXM && (si[r][0] & si[r][1] & si[r][2]) >= 0;
     const float* fx = fco + FCO_X + (i - p.x0 - blockIdx.z * p.xchunk + 1) * 6;
@@ -331,7 +344,7 @@ __device__ __forceinline__ void fused_e_own(const Params& p, const FusedArgs& fa
     for (int c = 0; c < 3; c++) {
       float ie = iu[c];
       if (MODE == 0) {
-        const int m = um >= 0 ? um : fM(st, c, y, lane);
+        const int m = um >= 0 ? um : fM<NR>(st, c, y, lane);
         if (ms.npoles[m] > 0) continue;              // dispersive node: the ADE pass writes it
         ie = ms.inv_eps[m][c];
         if (p.des_on) {
@@ -353,57 +366,60 @@ __device__ __forceinline__ void fused_e_own(const Params& p, const FusedArgs& fa
 
 // Issue the copies of stage s (plane x0 - 1 + s; the material tiles of the
 // plane before it, whose E update runs while this stage is current).
+template <int NR>
 __device__ __forceinline__ void fused_issue(const FusedMaps& m, float* st, uint64_t* bar, int ip, int j0, int k0,
                                             bool want_mat) {
-  mbar_arrive_expect_tx(bar, F_BYTES + (want_mat ? F_BYTES_MAT : 0u));
+  mbar_arrive_expect_tx(bar, FL<NR>::BYTES + (want_mat ? FL<NR>::BYTES_MAT : 0u));
 #pragma unroll
-  for (int c = 0; c < 3; c++) tma_load_3d(st + c * FE_N, &m.e[c], k0 - 4, j0 - 1, ip, bar);
-  tma_load_3d(st + F_OFF_HX, &m.hx, k0, j0, ip, bar);
-  tma_load_3d(st + F_OFF_HY, &m.hy, k0, j0, ip, bar);
-  tma_load_3d(st + F_OFF_HZ, &m.hz, k0, j0, ip, bar);
+  for (int c = 0; c < 3; c++) tma_load_3d(st + c * FL<NR>::FE_N, &m.e[c], k0 - 4, j0 - 1, ip, bar);
+  tma_load_3d(st + FL<NR>::OFF_HX, &m.hx, k0, j0, ip, bar);
+  tma_load_3d(st + FL<NR>::OFF_HY, &m.hy, k0, j0, ip, bar);
+  tma_load_3d(st + FL<NR>::OFF_HZ, &m.hz, k0, j0, ip, bar);
   if (want_mat)
 #pragma unroll
     for (int c = 0; c < 3; c++)
-      tma_load_3d(reinterpret_cast<uint8_t*>(st + F_OFF_M) + c * TYT * TZ, &m.mat[c], k0, j0, ip - 1, bar);
+      tma_load_3d(reinterpret_cast<uint8_t*>(st + FL<NR>::OFF_M) + c * F_MROWS * TZ, &m.mat[c], k0, j0, ip - 1, bar);
 }
 
 // H of plane i over the own nodes for the tile-plane's slab axes m (bit 0: x
 // slab plane, bit 1: y slab rows, bit 2: z slab columns).  Tile-planes with
 // any slab take one general variant: variants per slab combination were
 // measured slower on every workload (a larger kernel).
+template <int NR>
 __device__ __forceinline__ void fused_h_dispatch(int m, const Params& p, const FusedArgs& fa, const float* st, float* hn,
-                                                 int i, int j0, int k0, bool store, const bool (&ok)[RY],
-                                                 const float (&ep)[RY][3], float (&hc)[RY][3], float (&ec)[RY][3],
-                                                 const float* fco, int xs, const int (&ys)[RY], int zs) {
+                                                 int i, int j0, int k0, bool store, const bool (&ok)[NR],
+                                                 const float (&ep)[NR][3], float (&hc)[NR][3], float (&ec)[NR][3],
+                                                 const float* fco, int xs, const int (&ys)[NR], int zs) {
   switch (m) {
-    case 0: fused_h_own<0>(p, fa, st, hn, i, j0, k0, store, ok, ep, hc, ec, fco, xs, ys, zs); break;
-    default: fused_h_own<7>(p, fa, st, hn, i, j0, k0, store, ok, ep, hc, ec, fco, xs, ys, zs); break;
+    case 0: fused_h_own<NR, 0>(p, fa, st, hn, i, j0, k0, store, ok, ep, hc, ec, fco, xs, ys, zs); break;
+    default: fused_h_own<NR, 7>(p, fa, st, hn, i, j0, k0, store, ok, ep, hc, ec, fco, xs, ys, zs); break;
   }
 }
-template <int MODE>
+template <int NR, int MODE>
 __device__ __forceinline__ void fused_e_dispatch(int m, const Params& p, const FusedArgs& fa, const float* st,
                                                  const float* hn, const MatShared& ms, int um, int i, int j0, int k0,
-                                                 const bool (&ok)[RY], const float (&ep)[RY][3], const float (&hc)[RY][3],
-                                                 const float* fco, int xs, const int (&ys)[RY], int zs) {
+                                                 const bool (&ok)[NR], const float (&ep)[NR][3], const float (&hc)[NR][3],
+                                                 const float* fco, int xs, const int (&ys)[NR], int zs) {
   switch (m) {
-    case 0: fused_e_own<MODE, 0>(p, fa, st, hn, ms, um, i, j0, k0, ok, ep, hc, fco, xs, ys, zs); break;
-    default: fused_e_own<MODE, 7>(p, fa, st, hn, ms, um, i, j0, k0, ok, ep, hc, fco, xs, ys, zs); break;
+    case 0: fused_e_own<NR, MODE, 0>(p, fa, st, hn, ms, um, i, j0, k0, ok, ep, hc, fco, xs, ys, zs); break;
+    default: fused_e_own<NR, MODE, 7>(p, fa, st, hn, ms, um, i, j0, k0, ok, ep, hc, fco, xs, ys, zs); break;
   }
 }
 
 // 3 CTAs per SM (shared memory: a 3-stage ring and two new-H planes)
-__global__ void __launch_bounds__(NTHR, 3)
+template <int NR>
+__global__ void __launch_bounds__(NTHR, NR == 2 ? 3 : 4)
     fused_kernel(const __grid_constant__ Params p, const __grid_constant__ FusedArgs fa,
                  const __grid_constant__ FusedMaps m) {
   extern __shared__ __align__(128) float fsm[];
-  float* hnb = fsm + F_NST * F_STAGE;                      // two new-H planes
-  MatShared& ms = *reinterpret_cast<MatShared*>(hnb + 2 * F_HN);
+  float* hnb = fsm + F_NST * FL<NR>::STAGE;                      // two new-H planes
+  MatShared& ms = *reinterpret_cast<MatShared*>(hnb + 2 * FL<NR>::HN);
   uint64_t* bars = reinterpret_cast<uint64_t*>(reinterpret_cast<char*>(&ms) + sizeof(MatShared));
   __shared__ signed char umc[FX_MAX];
   __shared__ float fco[FCO_N];
   __shared__ int gave_up;
   const int lane = threadIdx.x, w = threadIdx.y, tid = w * TZ + lane;
-  const int k0 = blockIdx.x * TZ, j0 = blockIdx.y * TYT;
+  const int k0 = blockIdx.x * TZ, j0 = blockIdx.y * FL<NR>::TY;
   const int x0 = p.x0 + blockIdx.z * p.xchunk;
   const int x1 = min(x0 + p.xchunk, p.x1);
   const int len = x1 - x0;
@@ -416,12 +432,12 @@ __global__ void __launch_bounds__(NTHR, 3)
   }
   load_matshared(ms, p);
   for (int q = tid; q < len; q += NTHR)
-    umc[q] = __ldg(p.umat + ((long long)(x0 + q) * p.nty + blockIdx.y) * p.ntz + blockIdx.x);
+    umc[q] = __ldg(p.umat + ((long long)(x0 + q) * p.nty + j0 / F_MROWS) * p.ntz + blockIdx.x);
   if (cpml)
     for (int q = tid; q < FCO_N / 6; q += NTHR) {
-      // row q: x plane x0 - 1 + q, y row j0 + q - (FX_MAX + 2), z column k0 + q - (FX_MAX + TYT + 3)
-      const int a = q < FX_MAX + 2 ? 0 : q < FX_MAX + TYT + 3 ? 1 : 2;
-      const int v = a == 0 ? x0 - 1 + q : a == 1 ? j0 + q - (FX_MAX + 2) : k0 + q - (FX_MAX + TYT + 3);
+      // row q: x plane x0 - 1 + q, y row j0 + q - (FX_MAX + 2), z column k0 + q - (FX_MAX + F_MROWS + 3)
+      const int a = q < FX_MAX + 2 ? 0 : q < FX_MAX + F_MROWS + 3 ? 1 : 2;
+      const int v = a == 0 ? x0 - 1 + q : a == 1 ? j0 + q - (FX_MAX + 2) : k0 + q - (FX_MAX + F_MROWS + 3);
 #pragma unroll
       for (int o = 0; o < 2; o++) {
         const int h = 2 * v + o;
@@ -434,27 +450,27 @@ __global__ void __launch_bounds__(NTHR, 3)
   __syncthreads();
   auto issue = [&](int s) {
     const int ip = x0 - 1 + s;
-    fused_issue(m, fsm + (s % F_NST) * F_STAGE, &bars[s % F_NST], ip, j0, k0, ip - 1 >= x0 && umc[ip - 1 - x0] < 0);
+    fused_issue<NR>(m, fsm + (s % F_NST) * FL<NR>::STAGE, &bars[s % F_NST], ip, j0, k0, ip - 1 >= x0 && umc[ip - 1 - x0] < 0);
   };
   int issued = -1;
   if (tid == 0)
     for (int s = 0; s < F_NST && s <= slast; s++) { issue(s); issued = s; }
   // per-thread constants of the walk
-  bool ok[RY];
-  int ys[RY];
+  bool ok[NR];
+  int ys[NR];
 #pragma unroll
-  for (int r = 0; r < RY; r++) {
+  for (int r = 0; r < NR; r++) {
     ok[r] = j0 + w + TW * r < p.g.n[1] && k0 + lane < p.g.n[2];
     ys[r] = cpml ? slab_cs(p, 1, j0 + w + TW * r) : -1;
   }
   const int zs = cpml ? slab_cs(p, 2, k0 + lane) : -1;
   // slab axes of the own nodes (y, z: fixed for the walk) and of the halo (row 16, column 32)
-  const int myz = cpml ? ((j0 < p.ab.L[1][0] || j0 + TYT > p.g.n[1] - p.ab.L[1][1]) ? 2 : 0) |
+  const int myz = cpml ? ((j0 < p.ab.L[1][0] || j0 + FL<NR>::TY > p.g.n[1] - p.ab.L[1][1]) ? 2 : 0) |
                              ((k0 < p.ab.L[2][0] || k0 + TZ > p.g.n[2] - p.ab.L[2][1]) ? 4 : 0)
                        : 0;
-  const bool halo_yz = cpml && (j0 < p.ab.L[1][0] || j0 + TYT + 1 > p.g.n[1] - p.ab.L[1][1] || k0 < p.ab.L[2][0] ||
+  const bool halo_yz = cpml && (j0 < p.ab.L[1][0] || j0 + FL<NR>::TY + 1 > p.g.n[1] - p.ab.L[1][1] || k0 < p.ab.L[2][0] ||
                                 k0 + TZ + 1 > p.g.n[2] - p.ab.L[2][1]);
-  float ep[RY][3], hc[RY][3], ec[RY][3];
+  float ep[NR][3], hc[NR][3], ec[NR][3];
   float xe = 0.f;
   // stage 0 (plane x0 - 1): the old E of the own nodes and of the halo nodes (x taps)
   if (tid == 0 && !mbar_wait(&bars[0], 0u, p.err, p.wait_limit)) gave_up = 1;
@@ -462,11 +478,11 @@ __global__ void __launch_bounds__(NTHR, 3)
   int t = 0, swait = 0;                                    // swait: the stage waited for last
   if (!gave_up) {
 #pragma unroll
-    for (int r = 0; r < RY; r++)
+    for (int r = 0; r < NR; r++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) ep[r][c] = fE(fsm, c, w + TW * r, lane);
-    if (w == 0) xe = fE(fsm, 1, TYT, lane);
-    else if (w == 2 && lane < TYT) xe = fE(fsm, 2, lane, TZ);
+      for (int c = 0; c < 3; c++) ep[r][c] = fE<NR>(fsm, c, w + TW * r, lane);
+    if (w == 0) xe = fE<NR>(fsm, 1, FL<NR>::TY, lane);
+    else if (w == 2 && lane < FL<NR>::TY) xe = fE<NR>(fsm, 2, lane, TZ);
     for (; t <= len; t++) {
       const int s = t + 1, pc = x0 + t;
       swait = s;
@@ -476,18 +492,18 @@ __global__ void __launch_bounds__(NTHR, 3)
       __syncthreads();
       if (gave_up) break;
       if (tid == 0 && t + F_NST <= slast) { issue(t + F_NST); issued = t + F_NST; }
-      const float* st = fsm + (s % F_NST) * F_STAGE;
-      float* hn1 = hnb + (t & 1) * F_HN;                   // new H of plane pc
-      const float* hn0 = hnb + ((t + 1) & 1) * F_HN;       // new H of plane pc - 1
+      const float* st = fsm + (s % F_NST) * FL<NR>::STAGE;
+      float* hn1 = hnb + (t & 1) * FL<NR>::HN;                   // new H of plane pc
+      const float* hn0 = hnb + ((t + 1) & 1) * FL<NR>::HN;       // new H of plane pc - 1
       if (pc < p.g.n[0]) {
         const int xs = cpml ? slab_cs(p, 0, pc) : -1;
-        fused_h_dispatch(myz | (xs >= 0 ? 1 : 0), p, fa, st, hn1, pc, j0, k0, t < len, ok, ep, hc, ec, fco, xs, ys, zs);
-        if (halo_yz || xs >= 0) fused_h_halo<true>(p, fa, st, hn1, pc, j0, k0, xe);
-        else fused_h_halo<false>(p, fa, st, hn1, pc, j0, k0, xe);
+        fused_h_dispatch<NR>(myz | (xs >= 0 ? 1 : 0), p, fa, st, hn1, pc, j0, k0, t < len, ok, ep, hc, ec, fco, xs, ys, zs);
+        if (halo_yz || xs >= 0) fused_h_halo<NR, true>(p, fa, st, hn1, pc, j0, k0, xe);
+        else fused_h_halo<NR, false>(p, fa, st, hn1, pc, j0, k0, xe);
       } else {
         // beyond the last plane of the grid: H is zero there
 #pragma unroll
-        for (int r = 0; r < RY; r++)
+        for (int r = 0; r < NR; r++)
 #pragma unroll
           for (int c = 0; c < 3; c++) { hc[r][c] = 0.f; ec[r][c] = 0.f; }
       }
@@ -496,11 +512,11 @@ __global__ void __launch_bounds__(NTHR, 3)
         const int um = umc[pe - x0];
         const int xs = cpml ? slab_cs(p, 0, pe) : -1;
         const int mm = myz | (xs >= 0 ? 1 : 0);
-        if (um >= 0) fused_e_dispatch<1>(mm, p, fa, st, hn0, ms, um, pe, j0, k0, ok, ep, hc, fco, xs, ys, zs);
-        else fused_e_dispatch<0>(mm, p, fa, st, hn0, ms, um, pe, j0, k0, ok, ep, hc, fco, xs, ys, zs);
+        if (um >= 0) fused_e_dispatch<NR, 1>(mm, p, fa, st, hn0, ms, um, pe, j0, k0, ok, ep, hc, fco, xs, ys, zs);
+        else fused_e_dispatch<NR, 0>(mm, p, fa, st, hn0, ms, um, pe, j0, k0, ok, ep, hc, fco, xs, ys, zs);
       }
 #pragma unroll
-      for (int r = 0; r < RY; r++)
+      for (int r = 0; r < NR; r++)
 #pragma unroll
         for (int c = 0; c < 3; c++) ep[r][c] = ec[r][c];
     }

@@ -433,12 +433,24 @@ int  dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block);
  * (params.h:50-52); dtmx_autotune searches this value. */
 int  dtmx_set_xchunk(dtmx_ctx* ctx, int planes);
 
+/* Tile height (y rows) of the single-sweep engine: 16 (default) or 8 (more
+ * CTAs for grids of a few million cells; 0 restores 16).  The reference's
+ * block shape is a per-build parameter (params.h:50-52); dtmx_autotune
+ * searches this value. */
+int  dtmx_set_tile_rows(dtmx_ctx* ctx, int rows);
+
+/* The engine configuration dtmx_step uses (as set or as chosen by
+ * dtmx_autotune); any pointer may be NULL.  No reference counterpart. */
+int  dtmx_get_engine(dtmx_ctx* ctx, int* engine, int* time_block, int* xchunk, int* tile_rows);
+
 /* Time every applicable engine configuration for trial_steps steps from the
  * current state (probes and DFT planes paused; the state is restored after
  * each trial) and keep the fastest: the per-step engine with x chunks of 4 to 64
- * planes per CTA and the wavefront engine with 1, 2 and 4 steps per launch (the
- * reference's torre height, chosen at run time instead of compiled in,
- * params.h:50-52).  Results are cached per grid shape and feature set. */
+ * planes per CTA, the single-sweep engine with x chunks of 2 to 64 planes and
+ * tiles of 16 or 8 rows, and the wavefront engine with 1, 2 and 4 steps per
+ * launch (the reference's block shape and torre height, chosen at run time
+ * instead of compiled in, params.h:50-52).  Results are cached per grid shape
+ * and feature set. */
 int  dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, int* time_block_out, int* xchunk_out,
                    double* ms_per_step_out);
 

@@ -186,3 +186,22 @@ def test_single_sweep_forward_adjoint_matches_per_step(budget):
         s.close()
     assert res[0][0] == res[1][0] and np.array_equal(res[0][1], res[1][1])
     _same(res[1][2], res[0][2])
+
+
+@pytest.mark.parametrize("gyro,design,xchunk", [(False, False, 0), (True, False, 3), (False, True, 7)])
+def test_single_sweep_8_row_tiles(gyro, design, xchunk):
+    """8-row tiles (the autotuner's choice for small grids): bit-identical to
+    the per-step engine, including partial tiles, CPML slabs, materials,
+    design region and gyrotropic layer."""
+    case = _case(gyro=gyro, design=design)
+    a = _sim(case, 1)
+    b = _sim(case, 3)
+    b.set_tile_rows(8)
+    b.set_xchunk(xchunk)
+    assert b.engine_config()[3] == 8
+    for n in (5, 16):
+        a.step(n)
+        b.step(n)
+        _same(_fields(b), _fields(a))
+    a.close()
+    b.close()
