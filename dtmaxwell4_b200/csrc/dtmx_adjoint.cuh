@@ -53,56 +53,76 @@ __device__ __forceinline__ void curl_pair(int c, int t, int& a, int& g) {
 //   w_{c,t} = sg_t cdt_a ie_c (g_a lam_c + al_a lam_psi)   (a = curl axis of term t;
 //   g_a lam + al lam_psi only inside the axis-a slab, lam elsewhere),
 // then the slab recursion lam_psi <- b (lam + lam_psi) (w uses the old lam_psi).
-// The node's 1/eps, design index and lam are loaded once per component.
-// One thread per node: blockIdx.z = x plane, (threadIdx.x, blockIdx.x) = z,
-// (threadIdx.y, blockIdx.y) = y.
+// One thread per ADJ_XP nodes along x: their lam, materials and 1/eps are
+// requested together before any is used (measured on the differentiation
+// workload: 2 nodes 3 % faster than 1, 4 nodes 1 %, 8 nodes 8 % slower).
+// Thread layout: (threadIdx.x, blockIdx.x) = z,
+// (threadIdx.y, blockIdx.y) = y, blockIdx.z = x planes [ADJ_XP z, ADJ_XP (z + 1)).
+constexpr int ADJ_XP = 2;
 template <int ORDER, int UPDH>
 __global__ void adj_w_kernel(Params p, AdjDev A) {
   constexpr bool updH = UPDH != 0;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, i = blockIdx.z;
+  const int k = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i0 = blockIdx.z * ADJ_XP;
   if (j >= p.g.n[1] || k >= p.g.n[2]) return;
-  const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
   constexpr int cu0 = updH ? 3 : 0;
-  const int idx[3] = {i, j, k};
   const bool cpml = p.ab.kind == 1;
-  const long long di = updH ? -1 : design_index(p, i, j, k);
-  int si[3] = {-1, -1, -1};
-  if (cpml) node_slabs(p, i, j, k, si);
-  float lam[3];
+  float lam[ADJ_XP][3], ie[ADJ_XP][3];
 #pragma unroll
-  for (int c = 0; c < 3; c++) {
-    const int cu = cu0 + c;
-    float ie = 1.f;
-    if (!updH) {
-      // (material, design and table values are constant during the adjoint: read-only path)
-      const int m = p.mat[cu] ? (int)__ldg(p.mat[cu] + id) : 0;
-      ie = di >= 0 ? __ldg(p.des_ie[cu] + di) : __ldg(&p.mt->inv_eps[m][cu]);
-    }
-    lam[c] = A.lam[cu][id];
+  for (int q = 0; q < ADJ_XP; q++) {
+    const int i = i0 + q;
 #pragma unroll
-    for (int t = 0; t < 2; t++) {
-      const int a = curl_axis(cu, t);
-      float sg = t == 0 ? 1.f : -1.f;
-      if (updH) sg = -sg;
-      float ld = lam[c];
-      if (si[a] >= 0) {
-        const int h = 2 * idx[a] + comp_off(cu, a);
-        const float al = __ldg(p.ab.c1[a] + h), gk = __fadd_rn(__ldg(p.ab.c2[a] + h), al);
-        ld = __fmaf_rn(gk, ld, __fmul_rn(al, A.lpsi[a][slot_of(cu, a)][si[a]]));
-      }
-      A.w[c][t][id] = __fmul_rn(__fmul_rn(sg * p.cdt[a], ie), ld);
-    }
-  }
-  if (!cpml) return;
-#pragma unroll
-  for (int a = 0; a < 3; a++) {
-    if (si[a] < 0) continue;
+    for (int c = 0; c < 3; c++) { lam[q][c] = 0.f; ie[q][c] = 1.f; }
+    if (i >= p.g.n[0]) continue;
+    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+    const long long di = updH ? -1 : design_index(p, i, j, k);
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const int cu = cu0 + c, sl = slot_of(cu, a);
-      if (sl < 0) continue;
-      const float b = __ldg(p.ab.c0[a] + 2 * idx[a] + comp_off(cu, a));
-      A.lpsi[a][sl][si[a]] = __fmul_rn(b, __fadd_rn(lam[c], A.lpsi[a][sl][si[a]]));
+      const int cu = cu0 + c;
+      if (!updH) {
+        // (material, design and table values are constant during the adjoint: read-only path)
+        const int m = p.mat[cu] ? (int)__ldg(p.mat[cu] + id) : 0;
+        ie[q][c] = di >= 0 ? __ldg(p.des_ie[cu] + di) : __ldg(&p.mt->inv_eps[m][cu]);
+      }
+      lam[q][c] = A.lam[cu][id];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < ADJ_XP; q++) {
+    const int i = i0 + q;
+    if (i >= p.g.n[0]) break;
+    const long long id = (long long)i * p.g.sx + (long long)j * p.g.sy + k;
+    const int idx[3] = {i, j, k};
+    int si[3] = {-1, -1, -1};
+    if (cpml) node_slabs(p, i, j, k, si);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int cu = cu0 + c;
+#pragma unroll
+      for (int t = 0; t < 2; t++) {
+        const int a = curl_axis(cu, t);
+        float sg = t == 0 ? 1.f : -1.f;
+        if (updH) sg = -sg;
+        float ld = lam[q][c];
+        if (si[a] >= 0) {
+          const int h = 2 * idx[a] + comp_off(cu, a);
+          const float al = __ldg(p.ab.c1[a] + h), gk = __fadd_rn(__ldg(p.ab.c2[a] + h), al);
+          ld = __fmaf_rn(gk, ld, __fmul_rn(al, A.lpsi[a][slot_of(cu, a)][si[a]]));
+        }
+        A.w[c][t][id] = __fmul_rn(__fmul_rn(sg * p.cdt[a], ie[q][c]), ld);
+      }
+    }
+    if (!cpml) continue;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      if (si[a] < 0) continue;
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const int cu = cu0 + c, sl = slot_of(cu, a);
+        if (sl < 0) continue;
+        const float b = __ldg(p.ab.c0[a] + 2 * idx[a] + comp_off(cu, a));
+        A.lpsi[a][sl][si[a]] = __fmul_rn(b, __fadd_rn(lam[q][c], A.lpsi[a][sl][si[a]]));
+      }
     }
   }
 }

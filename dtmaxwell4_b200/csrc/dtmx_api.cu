@@ -1777,25 +1777,26 @@ static int fa_adjoint(dtmx_ctx* ctx, FaRun& R, int q) {
   adj_source_kernel<<<(R.npl + 255) / 256, 256, 0, st>>>(P, A, R.dF, R.s0 + (long long)R.seg * R.K + q, R.plane_x, R.omega, c.dt);
   adj_grad_kernel<<<design_blocks(R), 256, 0, st>>>(P, A, q);
   const dim3 blk(32, 8), grd((c.nz + 31) / 32, (c.ny + 7) / 8, c.nx);
+  const dim3 wgrd((c.nz + 31) / 32, (c.ny + 7) / 8, (c.nx + ADJ_XP - 1) / ADJ_XP);   // adj_w: ADJ_XP planes per thread
   // the dispersive nodes' transposed ADE recursion replaces their w (after adj_w, before adj_curl);
   // the gyrotropic current's transposition reads lam_E' (after adj_w) and gathers over the box
   const bool ade = P.ade.Em[0] != nullptr;
   const bool gyro = ctx->has_gyro;
   const dim3 ablk(32, 8), agrd((P.ade.n[2] + 31) / 32, (P.ade.n[1] + 7) / 8, std::max(1, P.ade.n[0]));
   if (c.order == 4) {
-    adj_w_kernel<4, 0><<<grd, blk, 0, st>>>(P, A);
+    adj_w_kernel<4, 0><<<wgrd, blk, 0, st>>>(P, A);
     if (ade) adj_ade_kernel<<<agrd, ablk, 0, st>>>(P, A);
     if (gyro) { adj_gyro_mu_kernel<<<agrd, ablk, 0, st>>>(P, A); adj_gyro_j_kernel<<<agrd, ablk, 0, st>>>(P, A); }
     adj_curl_kernel<4, 0><<<grd, blk, 0, st>>>(P, A);
-    adj_w_kernel<4, 1><<<grd, blk, 0, st>>>(P, A);
+    adj_w_kernel<4, 1><<<wgrd, blk, 0, st>>>(P, A);
     adj_curl_kernel<4, 1><<<grd, blk, 0, st>>>(P, A);
     ctx->launches += 6 + (ade ? 1 : 0) + (gyro ? 2 : 0);
   } else {
-    adj_w_kernel<2, 0><<<grd, blk, 0, st>>>(P, A);
+    adj_w_kernel<2, 0><<<wgrd, blk, 0, st>>>(P, A);
     if (ade) adj_ade_kernel<<<agrd, ablk, 0, st>>>(P, A);
     if (gyro) { adj_gyro_mu_kernel<<<agrd, ablk, 0, st>>>(P, A); adj_gyro_j_kernel<<<agrd, ablk, 0, st>>>(P, A); }
     adj_curl_kernel<2, 0><<<grd, blk, 0, st>>>(P, A);
-    adj_w_kernel<2, 1><<<grd, blk, 0, st>>>(P, A);
+    adj_w_kernel<2, 1><<<wgrd, blk, 0, st>>>(P, A);
     adj_curl_kernel<2, 1><<<grd, blk, 0, st>>>(P, A);
     ctx->launches += 6 + (ade ? 1 : 0) + (gyro ? 2 : 0);
   }
