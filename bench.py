@@ -41,6 +41,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched measurements")
+    ap.add_argument("--no-point-dipole", action="store_true", help="skip the 128^3 point-dipole measurement")
     ap.add_argument("--extras-only", action="store_true", help="print only the adjoint and batched measurements")
     ap.add_argument("--adj-steps", type=int, default=2000)
     ap.add_argument("--batch-instances", type=int, default=64)
@@ -594,7 +595,8 @@ def main():
     import torch
     if args.extras_only:
         if rank == 0:
-            ex = {} if args.gyro_only else {"point_dipole": run_point_dipole(args), "adjoint": run_adjoint(args),
+            ex = {} if args.gyro_only else {"point_dipole": None if args.no_point_dipole else run_point_dipole(args),
+                                            "adjoint": run_adjoint(args),
                                             "batched": run_batched(args)}
             if not args.no_gyro:
                 ex["gyro_purcell"] = run_gyro_purcell(args)
@@ -613,7 +615,8 @@ def main():
             err_fp64 = cpu_check_fp64(args)
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
-        extras["point_dipole"] = run_point_dipole(args)
+        if not args.no_point_dipole:
+            extras["point_dipole"] = run_point_dipole(args)
         extras["adjoint"] = run_adjoint(args)
         extras["batched"] = run_batched(args)
         if not args.no_gyro:
