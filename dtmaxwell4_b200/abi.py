@@ -37,7 +37,8 @@ class Config(C.Structure):
         ("spml_vmax", C.c_double),
         ("probe_every", C.c_int),
         ("probe_capacity", C.c_int),
-        ("reserved", C.c_int * 8),
+        ("parkable", C.c_int),
+        ("reserved", C.c_int * 7),
     ]
 
 
@@ -77,7 +78,7 @@ class TFSF(C.Structure):
 def make_config(nx, ny, nz, dx=1.0, dy=None, dz=None, dt=None, courant=0.5, order=2,
                 geometry=GEOM_BOX, absorber=ABS_CPML, pml=10, cpml_m=3.0, cpml_sigma_factor=1.0,
                 cpml_kappa_max=1.0, cpml_alpha_max=0.0, spml_vmax=1.0, probe_every=1,
-                probe_capacity=0):
+                probe_capacity=0, parkable=False):
     """Build a Config.  dt defaults to courant*dx (c = 1); pml is an int for all
     six faces or a ((xlo,xhi),(ylo,yhi),(zlo,zhi)) tuple."""
     dy = dx if dy is None else dy
@@ -100,6 +101,7 @@ def make_config(nx, ny, nz, dx=1.0, dy=None, dz=None, dt=None, courant=0.5, orde
     cfg.spml_vmax = spml_vmax
     cfg.probe_every = probe_every
     cfg.probe_capacity = probe_capacity
+    cfg.parkable = 1 if parkable else 0
     return cfg
 
 

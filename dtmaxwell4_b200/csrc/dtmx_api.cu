@@ -46,6 +46,17 @@ struct FluxHost {
   double* d_out = nullptr;  // [6][nfreq]
 };
 
+// A device array of a parkable context: a CUDA virtual-address reservation
+// with its own physical allocation, so that dtmx_park can release the physical
+// memory while the address (held in Params, TMA descriptors and graphs) stays
+// reserved, and dtmx_unpark can map new memory at the same address.
+struct VmmBlock {
+  CUdeviceptr va = 0;
+  size_t size = 0;
+  CUmemGenericAllocationHandle h = 0;
+  void* host = nullptr;       // pinned copy while parked
+};
+
 struct dtmx_ctx {
   dtmx_config cfg{};
   int dev = 0;
@@ -55,6 +66,8 @@ struct dtmx_ctx {
   size_t nstore = 0;            // elements per component array (padded)
   size_t ncell = 0;             // nx*ny*nz
   std::vector<void*> allocs;
+  std::vector<VmmBlock> vmm;    // the arrays of a parkable context (instead of allocs)
+  bool parked = false;
   // coefficient tables
   float* ctab[3][3] = {};
   // materials
@@ -156,8 +169,74 @@ static int fail(dtmx_ctx* ctx, int code, const std::string& msg) {
   return code;
 }
 
+// ---- parkable device memory (no reference counterpart) -----------------------
+struct VmmApi {
+  PFN_cuMemGetAllocationGranularity_v10020 gran = nullptr;
+  PFN_cuMemAddressReserve_v10020 reserve = nullptr;
+  PFN_cuMemAddressFree_v10020 vfree = nullptr;
+  PFN_cuMemCreate_v10020 create = nullptr;
+  PFN_cuMemRelease_v10020 release = nullptr;
+  PFN_cuMemMap_v10020 map = nullptr;
+  PFN_cuMemUnmap_v10020 unmap = nullptr;
+  PFN_cuMemSetAccess_v10020 access = nullptr;
+  bool ok = false;
+};
+static const VmmApi& vmm_api() {
+  static const VmmApi api = [] {
+    VmmApi v;
+    auto get = [](const char* name, void** q) {
+      cudaDriverEntryPointQueryResult qr;
+      return cudaGetDriverEntryPoint(name, q, cudaEnableDefault, &qr) == cudaSuccess && qr == cudaDriverEntryPointSuccess;
+    };
+    v.ok = get("cuMemGetAllocationGranularity", (void**)&v.gran) && get("cuMemAddressReserve", (void**)&v.reserve) &&
+           get("cuMemAddressFree", (void**)&v.vfree) && get("cuMemCreate", (void**)&v.create) &&
+           get("cuMemRelease", (void**)&v.release) && get("cuMemMap", (void**)&v.map) &&
+           get("cuMemUnmap", (void**)&v.unmap) && get("cuMemSetAccess", (void**)&v.access);
+    return v;
+  }();
+  return api;
+}
+static CUmemAllocationProp vmm_prop(int dev) {
+  CUmemAllocationProp prop{};
+  prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+  prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+  prop.location.id = dev;
+  return prop;
+}
+// physical memory for block b, mapped read-write at its reserved address
+static CUresult vmm_back(int dev, VmmBlock& b) {
+  const VmmApi& A = vmm_api();
+  const CUmemAllocationProp prop = vmm_prop(dev);
+  CUresult r = A.create(&b.h, b.size, &prop, 0);
+  if (r != CUDA_SUCCESS) return r;
+  if ((r = A.map(b.va, b.size, 0, b.h, 0)) != CUDA_SUCCESS) { A.release(b.h); return r; }
+  CUmemAccessDesc acc{};
+  acc.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+  acc.location.id = dev;
+  acc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+  if ((r = A.access(b.va, b.size, &acc, 1)) != CUDA_SUCCESS) { A.unmap(b.va, b.size); A.release(b.h); }
+  return r;
+}
+
 template <class T>
 static int dalloc(dtmx_ctx* ctx, T** p, size_t count) {
+  if (ctx->cfg.parkable) {
+    const VmmApi& A = vmm_api();
+    if (!A.ok) return fail(ctx, DTMX_ERR_CUDA, "CUDA virtual memory management is unavailable");
+    const CUmemAllocationProp prop = vmm_prop(ctx->dev);
+    size_t g = 0;
+    if (A.gran(&g, &prop, CU_MEM_ALLOC_GRANULARITY_MINIMUM) != CUDA_SUCCESS || g == 0)
+      return fail(ctx, DTMX_ERR_CUDA, "allocation granularity");
+    VmmBlock b;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    b.size = (bytes + g - 1) / g * g;
+    if (A.reserve(&b.va, b.size, 0, 0, 0) != CUDA_SUCCESS) return fail(ctx, DTMX_ERR_OOM, "address reservation");
+    if (vmm_back(ctx->dev, b) != CUDA_SUCCESS) { A.vfree(b.va, b.size); return fail(ctx, DTMX_ERR_OOM, "device memory"); }
+    ctx->vmm.push_back(b);
+    CK(cudaMemsetAsync((void*)b.va, 0, b.size, ctx->stream));
+    *p = (T*)b.va;
+    return DTMX_OK;
+  }
   void* q = nullptr;
   cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
   if (e != cudaSuccess) {
@@ -471,6 +550,12 @@ extern "C" void dtmx_destroy(dtmx_ctx* ctx) {
   for (auto& g : ctx->graph16)
     if (g) cudaGraphExecDestroy(g);
   for (void* p : ctx->allocs) cudaFree(p);
+  for (auto& b : ctx->vmm) {
+    const VmmApi& A = vmm_api();
+    if (!ctx->parked) { A.unmap(b.va, b.size); A.release(b.h); }
+    A.vfree(b.va, b.size);
+    if (b.host) cudaFreeHost(b.host);
+  }
   for (auto& d : ctx->dfts) { cudaFree(d.omega); cudaFree(d.acc); cudaFree(d.stage); cudaFree(d.sstep); }
   for (auto& fx : ctx->fluxes) cudaFree(fx.d_out);
   cudaFree(ctx->obj.omega); cudaFree(ctx->obj.acc); cudaFree(ctx->obj.stage); cudaFree(ctx->obj.sstep);
@@ -543,6 +628,7 @@ static int upload_umat(dtmx_ctx* ctx) {
 
 extern "C" int dtmx_set_materials(dtmx_ctx* ctx, const dtmx_material* table, int nmat, const uint8_t* idx_x,
                                   const uint8_t* idx_y, const uint8_t* idx_z) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || !table || nmat < 1 || nmat > DTMX_MAX_MATERIALS || !idx_x) return fail(ctx, DTMX_ERR_INVALID, "bad material arguments");
   if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "materials must be set before the first step");
   const uint8_t* src[3] = {idx_x, idx_y ? idx_y : idx_x, idx_z ? idx_z : idx_x};
@@ -628,6 +714,7 @@ static bool node_live(const dtmx_ctx* ctx, int comp, int i, int j, int k) {
 }
 
 extern "C" int dtmx_add_point_source(dtmx_ctx* ctx, const dtmx_point_source* s) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || !s || s->comp < 0 || s->comp > 2) return fail(ctx, DTMX_ERR_INVALID, "bad point source");
   if (!node_live(ctx, s->comp, s->i, s->j, s->k)) return fail(ctx, DTMX_ERR_INVALID, "point source outside the live domain");
   if (!(s->tau > 0)) return fail(ctx, DTMX_ERR_INVALID, "point source tau must be > 0");
@@ -652,6 +739,7 @@ static void sf_range(double dstep, double bm, double bp, int hmax, int* lo, int*
 }
 
 extern "C" int dtmx_set_tfsf(dtmx_ctx* ctx, const dtmx_tfsf* s) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || !s || (s->kind != DTMX_TFSF_DIPOLE && s->kind != DTMX_TFSF_PLANE_X)) return fail(ctx, DTMX_ERR_INVALID, "bad TF/SF source");
   if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "TF/SF source must be set before the first step");
   const dtmx_config& c = ctx->cfg;
@@ -744,6 +832,7 @@ extern "C" int dtmx_set_tfsf(dtmx_ctx* ctx, const dtmx_tfsf* s) {
 }
 
 extern "C" int dtmx_add_probe(dtmx_ctx* ctx, int comp, int i, int j, int k, int mode, int* id_out) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || comp < 0 || comp > 5 || (mode != DTMX_PROBE_NODE && mode != DTMX_PROBE_REFERENCE)) return fail(ctx, DTMX_ERR_INVALID, "bad probe");
   if (i < 0 || i >= ctx->cfg.nx || j < 0 || j >= ctx->cfg.ny || k < 0 || k >= ctx->cfg.nz) return fail(ctx, DTMX_ERR_INVALID, "probe outside the grid");
   if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "probes must be added before the first step");
@@ -754,6 +843,7 @@ extern "C" int dtmx_add_probe(dtmx_ctx* ctx, int comp, int i, int j, int k, int 
 }
 
 extern "C" int dtmx_read_probes(dtmx_ctx* ctx, float* out, int max_samples, int* nsamples) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || !out || max_samples < 0) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
   const int every = ctx->cfg.probe_every > 0 ? ctx->cfg.probe_every : 1;
   const long long have = std::min<long long>(ctx->step / every, ctx->probe_cap);
@@ -768,6 +858,7 @@ extern "C" int dtmx_read_probes(dtmx_ctx* ctx, float* out, int max_samples, int*
 
 extern "C" int dtmx_add_dft_patch(dtmx_ctx* ctx, int axis, int index, int lo1, int n1, int lo2, int n2, int comp_mask,
                                   int nfreq, const double* omegas, int* id_out) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || axis < 0 || axis > 2 || nfreq < 1 || nfreq > 64 || !omegas || (comp_mask & ~63) || !comp_mask)
     return fail(ctx, DTMX_ERR_INVALID, "bad DFT plane");
   const int n[3] = {ctx->cfg.nx, ctx->cfg.ny, ctx->cfg.nz};
@@ -799,6 +890,7 @@ extern "C" int dtmx_add_dft_patch(dtmx_ctx* ctx, int axis, int index, int lo1, i
 }
 
 extern "C" int dtmx_add_dft_plane(dtmx_ctx* ctx, int axis, int index, int comp_mask, int nfreq, const double* omegas, int* id_out) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || axis < 0 || axis > 2) return fail(ctx, DTMX_ERR_INVALID, "bad DFT plane");
   const int n[3] = {ctx->cfg.nx, ctx->cfg.ny, ctx->cfg.nz};
   return dtmx_add_dft_patch(ctx, axis, index, 0, n[axis == 0 ? 1 : 0], 0, n[axis == 2 ? 1 : 2], comp_mask, nfreq, omegas,
@@ -807,6 +899,7 @@ extern "C" int dtmx_add_dft_plane(dtmx_ctx* ctx, int axis, int index, int comp_m
 
 extern "C" int dtmx_add_flux_box(dtmx_ctx* ctx, const int lo[3], const int hi[3], int nfreq, const double* omegas,
                                  int* id_out) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || !lo || !hi) return fail(ctx, DTMX_ERR_INVALID, "bad flux box");
   const int n[3] = {ctx->cfg.nx, ctx->cfg.ny, ctx->cfg.nz};
   const double ds[3] = {ctx->cfg.dx, ctx->cfg.dy, ctx->cfg.dz};
@@ -846,6 +939,7 @@ extern "C" int dtmx_add_flux_box(dtmx_ctx* ctx, const int lo[3], const int hi[3]
 }
 
 extern "C" int dtmx_flux_faces(dtmx_ctx* ctx, int id, int faces[6]) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || id < 0 || id >= (int)ctx->fluxes.size() || !faces) return fail(ctx, DTMX_ERR_INVALID, "bad flux box id");
   for (int q = 0; q < 6; q++) faces[q] = ctx->fluxes[id].face[q];
   return DTMX_OK;
@@ -861,6 +955,7 @@ static void dft_flush(dtmx_ctx* ctx, DftHost& h) {
 }
 
 extern "C" int dtmx_read_dft(dtmx_ctx* ctx, int id, double* out, size_t out_len) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || id < 0 || id >= (int)ctx->dfts.size() || !out) return fail(ctx, DTMX_ERR_INVALID, "bad DFT id");
   DftHost& h = ctx->dfts[id];
   const size_t n = (size_t)h.ncomp * h.d.nfreq * h.d.n1 * h.d.n2 * 2;
@@ -872,6 +967,7 @@ extern "C" int dtmx_read_dft(dtmx_ctx* ctx, int id, double* out, size_t out_len)
 }
 
 extern "C" int dtmx_read_flux(dtmx_ctx* ctx, int id, double* out, size_t out_len) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || id < 0 || id >= (int)ctx->fluxes.size() || !out) return fail(ctx, DTMX_ERR_INVALID, "bad flux box id");
   FluxHost& fx = ctx->fluxes[id];
   const int nf = fx.nfreq;
@@ -895,6 +991,7 @@ extern "C" int dtmx_read_flux(dtmx_ctx* ctx, int id, double* out, size_t out_len
 
 extern "C" int dtmx_ntff(dtmx_ctx* ctx, int id, int ndir, const double* theta, const double* phi, const double* origin,
                          double* out, size_t out_len) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || id < 0 || id >= (int)ctx->fluxes.size() || ndir < 1 || !theta || !phi || !out)
     return fail(ctx, DTMX_ERR_INVALID, "bad far-field arguments");
   FluxHost& fx = ctx->fluxes[id];
@@ -1430,6 +1527,7 @@ static int graph_steps16(dtmx_ctx* ctx) {
 }
 
 extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || nsteps < 0) return fail(ctx, DTMX_ERR_INVALID, "bad step count");
   int rc0 = prepare(ctx);
   if (rc0) return rc0;
@@ -1472,6 +1570,7 @@ extern "C" int dtmx_step(dtmx_ctx* ctx, int nsteps) {
 
 // ---------------------------------------------------------------- design region and adjoint
 extern "C" int dtmx_set_design(dtmx_ctx* ctx, const int* lo, const int* n, const float* eps) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || !lo || !n || !eps) return fail(ctx, DTMX_ERR_INVALID, "bad design region");
   const dtmx_config& c = ctx->cfg;
   const int dim[3] = {c.nx, c.ny, c.nz};
@@ -1832,6 +1931,7 @@ static void fa_abort(dtmx_ctx* ctx, FaRun& R) {
 
 extern "C" int dtmx_forward_adjoint(dtmx_ctx* ctx, int nsteps, int checkpoint_every, int plane_x, double omega,
                                     double* objective, float* grad_eps) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || !objective || !grad_eps) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
   FaRun R;
   if (nsteps < 1 || checkpoint_every < 1) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
@@ -1862,6 +1962,8 @@ extern "C" int dtmx_batch_forward_adjoint(dtmx_ctx* const* ctxs, int n, int nste
                                           const int* plane_x, const double* omega, double* objectives,
                                           float* const* grads) {
   if (!ctxs || n < 1 || !plane_x || !omega || !objectives || !grads) return DTMX_ERR_INVALID;
+  for (int b = 0; b < n; b++)
+    if (ctxs[b] && ctxs[b]->parked) return fail(ctxs[b], DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   std::vector<FaRun> R(n);
   int rc = DTMX_OK;
   auto abort_all = [&](int upto) {
@@ -1920,6 +2022,7 @@ static std::map<TuneKey, TuneVal>& tune_cache() {
 
 extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, int* tblock_out, int* xchunk_out,
                              double* ms_per_step_out) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || trial_steps < 1) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
   int rc = prepare(ctx);
   if (rc) return rc;
@@ -2003,6 +2106,7 @@ extern "C" int dtmx_autotune(dtmx_ctx* ctx, int trial_steps, int* engine_out, in
 // with z fastest and x slowest; dense cells instead of the reference's one
 // value per rag.
 extern "C" int dtmx_write_arr(dtmx_ctx* ctx, int comp, const char* path) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || comp < 0 || comp > 5 || !path) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
   const dtmx_config& c = ctx->cfg;
   std::vector<float> buf((size_t)c.nx * c.ny * c.nz);
@@ -2028,6 +2132,7 @@ struct StateHeader {
 };
 
 extern "C" int dtmx_save_state(dtmx_ctx* ctx, const char* path) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || !path) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
   int rc = prepare(ctx);
   if (rc) return rc;
@@ -2053,6 +2158,7 @@ extern "C" int dtmx_save_state(dtmx_ctx* ctx, const char* path) {
 }
 
 extern "C" int dtmx_load_state(dtmx_ctx* ctx, const char* path) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || !path) return fail(ctx, DTMX_ERR_INVALID, "bad arguments");
   int rc = prepare(ctx);
   if (rc) return rc;
@@ -2106,6 +2212,7 @@ extern "C" int dtmx_get_step(const dtmx_ctx* ctx, int64_t* n) {
 }
 
 extern "C" int dtmx_get_field(dtmx_ctx* ctx, int comp, float* host_out) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || comp < 0 || comp > 5 || !host_out) return fail(ctx, DTMX_ERR_INVALID, "bad field request");
   const dtmx_config& c = ctx->cfg;
   CK(cudaStreamSynchronize(ctx->stream));
@@ -2115,6 +2222,7 @@ extern "C" int dtmx_get_field(dtmx_ctx* ctx, int comp, float* host_out) {
 }
 
 extern "C" int dtmx_set_field(dtmx_ctx* ctx, int comp, const float* host_in) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || comp < 0 || comp > 5 || !host_in) return fail(ctx, DTMX_ERR_INVALID, "bad field request");
   const dtmx_config& c = ctx->cfg;
   CK(cudaMemcpy2DAsync(ctx->P.f[comp], (size_t)ctx->nzp * 4, host_in, (size_t)c.nz * 4, (size_t)c.nz * 4,
@@ -2127,6 +2235,7 @@ extern "C" int dtmx_set_field(dtmx_ctx* ctx, int comp, const float* host_in) {
 }
 
 extern "C" int dtmx_field_device_ptr(dtmx_ctx* ctx, int comp, void** dptr, int64_t strides[3]) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx || comp < 0 || comp > 5 || !dptr) return fail(ctx, DTMX_ERR_INVALID, "bad field request");
   *dptr = ctx->P.f[comp];
   if (strides) { strides[0] = ctx->P.g.sx; strides[1] = ctx->P.g.sy; strides[2] = 1; }
@@ -2134,6 +2243,7 @@ extern "C" int dtmx_field_device_ptr(dtmx_ctx* ctx, int comp, void** dptr, int64
 }
 
 extern "C" int dtmx_check_finite(dtmx_ctx* ctx) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx) return DTMX_ERR_INVALID;
   CK(cudaMemsetAsync(ctx->d_flag, 0, sizeof(int), ctx->stream));
   for (int comp = 0; comp < 6; comp++) {
@@ -2168,6 +2278,44 @@ extern "C" int dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block) {
   }
   ctx->engine = engine;
   drop_graphs(ctx);
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_park(dtmx_ctx* ctx) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  if (!ctx->cfg.parkable) return fail(ctx, DTMX_ERR_STATE, "the context was not created parkable");
+  if (ctx->parked) return DTMX_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  const VmmApi& A = vmm_api();
+  for (auto& b : ctx->vmm) {
+    if (!b.host) CK(cudaMallocHost(&b.host, b.size));
+    CK(cudaMemcpy(b.host, (void*)b.va, b.size, cudaMemcpyDeviceToHost));
+  }
+  for (auto& b : ctx->vmm) {
+    if (A.unmap(b.va, b.size) != CUDA_SUCCESS || A.release(b.h) != CUDA_SUCCESS)
+      return fail(ctx, DTMX_ERR_CUDA, "releasing the device memory of a parked context");
+    b.h = 0;
+  }
+  ctx->parked = true;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_unpark(dtmx_ctx* ctx) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  if (!ctx->parked) return DTMX_OK;
+  CK(cudaSetDevice(ctx->dev));
+  for (size_t q = 0; q < ctx->vmm.size(); q++) {
+    VmmBlock& b = ctx->vmm[q];
+    if (vmm_back(ctx->dev, b) != CUDA_SUCCESS) {
+      // keep the context consistent: release what was mapped again and stay parked
+      const VmmApi& A = vmm_api();
+      for (size_t r = 0; r < q; r++) { A.unmap(ctx->vmm[r].va, ctx->vmm[r].size); A.release(ctx->vmm[r].h); }
+      return fail(ctx, DTMX_ERR_OOM, "device memory for an unparked context");
+    }
+  }
+  for (auto& b : ctx->vmm) CK(cudaMemcpyAsync((void*)b.va, b.host, b.size, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->parked = false;
   return DTMX_OK;
 }
 
@@ -2207,6 +2355,7 @@ extern "C" int dtmx_get_stream(dtmx_ctx* ctx, void** stream) {
 }
 
 extern "C" int dtmx_set_profiling(dtmx_ctx* ctx, int enable) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx) return DTMX_ERR_INVALID;
   if (enable && !ctx->ev[0])
     for (int q = 0; q < 4; q++) CK(cudaEventCreate(&ctx->ev[q]));
@@ -2219,6 +2368,7 @@ extern "C" int dtmx_set_profiling(dtmx_ctx* ctx, int enable) {
 }
 
 extern "C" int dtmx_read_profile(dtmx_ctx* ctx, double* ms_h, double* ms_e, int64_t* count) {
+  if (ctx && ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (!ctx) return DTMX_ERR_INVALID;
   CK(cudaStreamSynchronize(ctx->stream));
   if (ms_h) *ms_h = ctx->prof_ms_h;

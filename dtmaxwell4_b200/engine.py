@@ -20,7 +20,7 @@ EXPORTS = (
     "dtmx_set_materials", "dtmx_add_point_source", "dtmx_set_tfsf", "dtmx_add_probe",
     "dtmx_read_probes", "dtmx_add_dft_plane", "dtmx_read_dft", "dtmx_step", "dtmx_sync",
     "dtmx_get_step", "dtmx_get_field", "dtmx_set_field", "dtmx_field_device_ptr",
-    "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_set_xchunk", "dtmx_set_tile_rows", "dtmx_get_engine", "dtmx_get_stream",
+    "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_set_xchunk", "dtmx_park", "dtmx_unpark", "dtmx_set_tile_rows", "dtmx_get_engine", "dtmx_get_stream",
     "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
     "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
     "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
@@ -76,6 +76,8 @@ def load():
     L.dtmx_kernel_launches.argtypes = [vp, C.POINTER(C.c_int64)]
     L.dtmx_set_engine.argtypes = [vp, ip, ip]
     L.dtmx_set_xchunk.argtypes = [vp, ip]
+    L.dtmx_park.argtypes = [vp]
+    L.dtmx_unpark.argtypes = [vp]
     L.dtmx_set_tile_rows.argtypes = [vp, ip]
     L.dtmx_get_engine.argtypes = [vp, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), C.POINTER(ip)]
     L.dtmx_get_stream.argtypes = [vp, C.POINTER(vp)]
@@ -232,6 +234,15 @@ class Simulation:
 
     def set_engine(self, engine, time_block=0):
         self._ck(self._L.dtmx_set_engine(self._h, engine, time_block))
+
+    def park(self):
+        """Move the device state to pinned host memory and free the device
+        memory (contexts made with make_config(..., parkable=True))."""
+        self._ck(self._L.dtmx_park(self._h))
+
+    def unpark(self):
+        """Bring a parked context's state back to the device."""
+        self._ck(self._L.dtmx_unpark(self._h))
 
     def set_xchunk(self, planes):
         """Planes of the x walk per CTA (0: automatic)."""

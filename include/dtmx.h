@@ -90,7 +90,11 @@ typedef struct dtmx_config {
   int probe_every;
   /* Capacity of the probe trace buffer in samples per probe (0 = 4096). */
   int probe_capacity;
-  int reserved[8];
+  /* 1: the context's device arrays can be parked (dtmx_park) -- each is a
+   * CUDA virtual-memory reservation with its own physical allocation, rounded
+   * up to the allocation granularity.  0: plain device allocations. */
+  int parkable;
+  int reserved[7];
 } dtmx_config;
 
 /* ---- materials ----------------------------------------------------------- */
@@ -432,6 +436,18 @@ int  dtmx_set_engine(dtmx_ctx* ctx, int engine, int time_block);
  * uses at most 64).  The reference fixes its block shape per build
  * (params.h:50-52); dtmx_autotune searches this value. */
 int  dtmx_set_xchunk(dtmx_ctx* ctx, int planes);
+
+/* Parking (contexts created with cfg.parkable = 1; no reference counterpart,
+ * the reference's out-of-core window streams its domain through the device,
+ * window.hpp:177-267): dtmx_park waits for the context's stream, copies every
+ * device array to pinned host memory and releases the device memory, keeping
+ * the addresses reserved; dtmx_unpark maps device memory at the same
+ * addresses again and copies the arrays back.  While parked, every call that
+ * touches the context's device state returns DTMX_ERR_STATE.  Several parked
+ * contexts then share one GPU's memory, one resident at a time
+ * (dtmaxwell4_b200.window steps a grid larger than the device that way). */
+int  dtmx_park(dtmx_ctx* ctx);
+int  dtmx_unpark(dtmx_ctx* ctx);
 
 /* Tile height (y rows) of the single-sweep engine: 16 (default) or 8 (more
  * CTAs for grids of a few million cells; 0 restores 16).  The reference's
