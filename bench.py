@@ -51,6 +51,13 @@ def parse():
     ap.add_argument("--no-gyro", action="store_true", help="skip the gyrotropic / Purcell measurement")
     ap.add_argument("--gyro-only", action="store_true", help="with --extras-only: only the gyrotropic measurement")
     ap.add_argument("--no-purcell", action="store_true", help="gyrotropic measurement without the Purcell spectrum")
+    ap.add_argument("--no-ooc", action="store_true", help="skip the out-of-core (parked slabs) measurement")
+    ap.add_argument("--ooc-only", action="store_true", help="with --extras-only: only the out-of-core measurement")
+    ap.add_argument("--ooc-n", type=int, nargs=3, default=[1024, 512, 512])
+    ap.add_argument("--ooc-slabs", type=int, default=4)
+    ap.add_argument("--ooc-k", type=int, default=32, help="time steps per slab turn")
+    ap.add_argument("--ooc-resident", type=int, default=2, help="slabs on the device at once")
+    ap.add_argument("--ooc-steps", type=int, default=64)
     return ap.parse_args()
 
 
@@ -397,6 +404,63 @@ def run_point_dipole(args):
             "note": "50 MB of fields: L2-resident, issue/latency-bound (ncu capture of the field kernels on this grid)"}
 
 
+def run_out_of_core(args):
+    """A grid stepped as x slabs that take turns on the device (parked in
+    pinned host memory between turns, K steps per turn): rate against the
+    same grid in core, and whether the fields after the same steps are
+    identical.  Wall clock around the public-API calls, host-synchronised."""
+    import numpy as np
+    import torch
+    from dtmaxwell4_b200 import Simulation, scenarios
+    from dtmaxwell4_b200.window import OutOfCoreSimulation, parkable_simulation
+    nx, ny, nz = args.ooc_n
+    K, steps = args.ooc_k, args.ooc_steps
+    sc = scenarios.point_dipole_sphere(n=(nx, ny, nz), steps=K + steps, pml=10, nprobes=4)
+    cells = nx * ny * nz
+
+    def make(c):
+        s = parkable_simulation(c)
+        s.set_engine(3, 0)
+        return s
+    w = OutOfCoreSimulation(sc["cfg"], args.ooc_slabs, steps_per_turn=K, make_local=make, resident=args.ooc_resident)
+    scenarios.apply(w, sc)
+    w.step(K)                                   # builds the slabs, one warm-up turn
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    w.step(steps)
+    t_ooc = time.perf_counter() - t0
+    free_ooc = torch.cuda.mem_get_info()[0]
+    ez_ooc = w.get_field(2)
+    tr_ooc = w.read_probes()
+    w.close()
+    g = Simulation(sc["cfg"])
+    scenarios.apply(g, sc)
+    g.set_engine(3, 0)
+    g.step(K)
+    g.sync()
+    free_in = torch.cuda.mem_get_info()[0]
+    stream = torch.cuda.ExternalStream(g.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    g.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    t_in = e0.elapsed_time(e1) * 1e-3
+    same = bool(np.array_equal(ez_ooc, g.get_field(2)) and np.array_equal(tr_ooc, g.read_probes().astype(np.float64)))
+    g.close()
+    pl = w.plans
+    ghost = sum(p.nxl for p in pl) / nx - 1.0
+    return {"workload": sc["desc"] + ", %d timed steps" % steps,
+            "slabs": args.ooc_slabs, "steps_per_turn": K, "resident_slabs": args.ooc_resident,
+            "ghost_overhead": round(ghost, 3),
+            "gcell_per_s": round(cells * steps / t_ooc / 1e9, 3),
+            "in_core_gcell_per_s": round(cells * steps / t_in / 1e9, 3),
+            "device_bytes_free_out_of_core": int(free_ooc), "device_bytes_free_in_core": int(free_in),
+            "identical_to_in_core": same,
+            "note": "engine 3 in both; each turn unparks a slab (H2D of its state), writes its neighbours' "
+                    "edge planes, steps K times, reads its edge planes and parks it (D2H)"}
+
+
 def run_batched(args):
     """Independent design-block instances (edges from {64..256}, 8 blocks,
     one dipole, 10-cell CPML): one-at-a-time forward+adjoint loop against the
@@ -595,9 +659,14 @@ def main():
     import torch
     if args.extras_only:
         if rank == 0:
+            if args.ooc_only:
+                print(json.dumps({"out_of_core": run_out_of_core(args)}))
+                return 0
             ex = {} if args.gyro_only else {"point_dipole": None if args.no_point_dipole else run_point_dipole(args),
                                             "adjoint": run_adjoint(args),
                                             "batched": run_batched(args)}
+            if not args.no_ooc and not args.gyro_only:
+                ex["out_of_core"] = run_out_of_core(args)
             if not args.no_gyro:
                 ex["gyro_purcell"] = run_gyro_purcell(args)
             print(json.dumps(ex))
@@ -619,6 +688,8 @@ def main():
             extras["point_dipole"] = run_point_dipole(args)
         extras["adjoint"] = run_adjoint(args)
         extras["batched"] = run_batched(args)
+        if not args.no_ooc:
+            extras["out_of_core"] = run_out_of_core(args)
         if not args.no_gyro:
             extras["gyro_purcell"] = run_gyro_purcell(args)
     if world > 1:

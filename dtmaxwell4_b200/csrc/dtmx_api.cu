@@ -55,6 +55,7 @@ struct VmmBlock {
   size_t size = 0;
   CUmemGenericAllocationHandle h = 0;
   void* host = nullptr;       // pinned copy while parked
+  bool dead = false;          // parked without a copy: refilled with zeros on unpark
 };
 
 struct dtmx_ctx {
@@ -2288,9 +2289,17 @@ extern "C" int dtmx_park(dtmx_ctx* ctx) {
   CK(cudaStreamSynchronize(ctx->stream));
   const VmmApi& A = vmm_api();
   for (auto& b : ctx->vmm) {
+    // the single sweep's output buffers hold nothing between steps: every
+    // node they carry is written by the next step (zero where no step writes)
+    b.dead = false;
+    for (int comp = 0; comp < 6; comp++) b.dead = b.dead || b.va == (CUdeviceptr)ctx->f_alt[comp];
+    for (int a = 0; a < 3; a++)
+      for (int q = 0; q < 2; q++) b.dead = b.dead || b.va == (CUdeviceptr)ctx->hax_alt[a][q];
+    if (b.dead) continue;
     if (!b.host) CK(cudaMallocHost(&b.host, b.size));
-    CK(cudaMemcpy(b.host, (void*)b.va, b.size, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(b.host, (void*)b.va, b.size, cudaMemcpyDeviceToHost, ctx->stream));
   }
+  CK(cudaStreamSynchronize(ctx->stream));
   for (auto& b : ctx->vmm) {
     if (A.unmap(b.va, b.size) != CUDA_SUCCESS || A.release(b.h) != CUDA_SUCCESS)
       return fail(ctx, DTMX_ERR_CUDA, "releasing the device memory of a parked context");
@@ -2313,10 +2322,107 @@ extern "C" int dtmx_unpark(dtmx_ctx* ctx) {
       return fail(ctx, DTMX_ERR_OOM, "device memory for an unparked context");
     }
   }
-  for (auto& b : ctx->vmm) CK(cudaMemcpyAsync((void*)b.va, b.host, b.size, cudaMemcpyHostToDevice, ctx->stream));
+  for (auto& b : ctx->vmm) {
+    if (b.dead) CK(cudaMemsetAsync((void*)b.va, 0, b.size, ctx->stream));
+    else CK(cudaMemcpyAsync((void*)b.va, b.host, b.size, cudaMemcpyHostToDevice, ctx->stream));
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   ctx->parked = false;
   return DTMX_OK;
+}
+
+// ---- plane state: fields, y/z CPML auxiliaries and ADE state of x planes,
+// section-major in a dense host layout (the same for every context with the
+// same y/z configuration and material table, whatever its ADE box).
+static int plane_poles(const dtmx_ctx* ctx) {
+  int p = 0;
+  for (int m = 0; m < ctx->nmat; m++) p = std::max(p, ctx->mats[m].npoles);
+  return p;
+}
+
+static size_t plane_floats(const dtmx_ctx* ctx) {
+  const dtmx_config& c = ctx->cfg;
+  const size_t nyz = (size_t)c.ny * c.nz;
+  size_t n = 6 * nyz;
+  if (ctx->P.ab.aux[1][0]) n += 4 * (size_t)(ctx->P.ab.L[1][0] + ctx->P.ab.L[1][1]) * c.nz;
+  if (ctx->P.ab.aux[2][0]) n += 4 * (size_t)c.ny * (ctx->P.ab.L[2][0] + ctx->P.ab.L[2][1]);
+  return n + (size_t)3 * (1 + 2 * plane_poles(ctx)) * nyz;
+}
+
+static int plane_refusal(dtmx_ctx* ctx) {
+  if (ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
+  if (ctx->cfg.geometry != DTMX_GEOM_BOX || ctx->cfg.absorber == DTMX_ABS_SPLIT_PML)
+    return fail(ctx, DTMX_ERR_UNSUPPORTED, "plane state: box geometry with a CPML or no absorber only");
+  if (ctx->has_gyro || ctx->has_tfsf || ctx->P.des_on)
+    return fail(ctx, DTMX_ERR_UNSUPPORTED, "plane state: gyrotropic materials, TF/SF and design regions are not per plane");
+  return DTMX_OK;
+}
+
+static int plane_copy(dtmx_ctx* ctx, int x0, int np, float* host, bool read) {
+  if (!ctx) return DTMX_ERR_INVALID;
+  if (int rc = plane_refusal(ctx)) return rc;
+  const dtmx_config& c = ctx->cfg;
+  if (!host || np < 0 || x0 < 0 || x0 + np > c.nx) return fail(ctx, DTMX_ERR_INVALID, "planes outside the grid");
+  const int xl = ctx->P.ab.aux[0][0] ? ctx->P.ab.L[0][0] : 0, xh = ctx->P.ab.aux[0][0] ? ctx->P.ab.L[0][1] : 0;
+  if (np > 0 && (x0 < xl || x0 + np > c.nx - xh))
+    return fail(ctx, DTMX_ERR_UNSUPPORTED, "planes inside an x absorber slab");
+  if (np == 0) return DTMX_OK;
+  const cudaMemcpyKind kind = read ? cudaMemcpyDeviceToHost : cudaMemcpyHostToDevice;
+  const size_t nyz = (size_t)c.ny * c.nz;
+  float* h = host;
+  for (int comp = 0; comp < 6; comp++) {
+    float* d = ctx->P.f[comp] + (size_t)x0 * ctx->P.g.sx;
+    if (read) CK(cudaMemcpy2DAsync(h, (size_t)c.nz * 4, d, (size_t)ctx->nzp * 4, (size_t)c.nz * 4, (size_t)np * c.ny, kind, ctx->stream));
+    else CK(cudaMemcpy2DAsync(d, (size_t)ctx->nzp * 4, h, (size_t)c.nz * 4, (size_t)c.nz * 4, (size_t)np * c.ny, kind, ctx->stream));
+    h += (size_t)np * nyz;
+  }
+  for (int a = 1; a < 3; a++) {
+    if (!ctx->P.ab.aux[a][0]) continue;
+    const size_t th = (size_t)(ctx->P.ab.L[a][0] + ctx->P.ab.L[a][1]);
+    const size_t pp = a == 1 ? th * c.nz : (size_t)c.ny * th;     // slab_index: x-major in both
+    for (int q = 0; q < 4; q++) {
+      float* d = ctx->P.ab.aux[a][q] + (size_t)x0 * pp;
+      CK(cudaMemcpyAsync(read ? (void*)h : (void*)d, read ? (const void*)d : (const void*)h, (size_t)np * pp * 4, kind, ctx->stream));
+      h += (size_t)np * pp;
+    }
+  }
+  const Ade& A = ctx->P.ade;
+  const int P = plane_poles(ctx);
+  const int b0 = std::max(x0, A.lo[0]), b1 = std::min(x0 + np, A.lo[0] + A.n[0]);
+  for (int comp = 0; comp < 3; comp++)
+    for (int s = 0; s < 1 + 2 * P; s++) {
+      float* arr = s == 0 ? A.Em[comp] : s <= P ? A.Jp[comp][s - 1] : A.Jm[comp][s - 1 - P];
+      if (read) memset(h, 0, (size_t)np * nyz * 4);      // zero off the dispersive box
+      if (arr && b0 < b1) {
+        cudaMemcpy3DParms m = {};
+        const cudaPitchedPtr dev = make_cudaPitchedPtr(arr, (size_t)A.n[2] * 4, A.n[2], A.n[1]);
+        const cudaPitchedPtr hst = make_cudaPitchedPtr(h, (size_t)c.nz * 4, c.nz, c.ny);
+        const cudaPos pd = make_cudaPos(0, 0, b0 - A.lo[0]), ph = make_cudaPos((size_t)A.lo[2] * 4, A.lo[1], b0 - x0);
+        if (read) { m.srcPtr = dev; m.srcPos = pd; m.dstPtr = hst; m.dstPos = ph; }
+        else { m.srcPtr = hst; m.srcPos = ph; m.dstPtr = dev; m.dstPos = pd; }
+        m.extent = make_cudaExtent((size_t)A.n[2] * 4, A.n[1], b1 - b0);
+        m.kind = kind;
+        CK(cudaMemcpy3DAsync(&m, ctx->stream));
+      }
+      h += (size_t)np * nyz;
+    }
+  CK(cudaStreamSynchronize(ctx->stream));
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_plane_state_floats(dtmx_ctx* ctx, size_t* floats_per_plane) {
+  if (!ctx || !floats_per_plane) return fail(ctx, DTMX_ERR_INVALID, "bad plane state request");
+  if (int rc = plane_refusal(ctx)) return rc;
+  *floats_per_plane = plane_floats(ctx);
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_read_planes(dtmx_ctx* ctx, int x0, int nplanes, float* host) {
+  return plane_copy(ctx, x0, nplanes, host, true);
+}
+
+extern "C" int dtmx_write_planes(dtmx_ctx* ctx, int x0, int nplanes, const float* host) {
+  return plane_copy(ctx, x0, nplanes, const_cast<float*>(host), false);
 }
 
 extern "C" int dtmx_set_tile_rows(dtmx_ctx* ctx, int rows) {

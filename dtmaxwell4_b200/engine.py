@@ -20,7 +20,7 @@ EXPORTS = (
     "dtmx_set_materials", "dtmx_add_point_source", "dtmx_set_tfsf", "dtmx_add_probe",
     "dtmx_read_probes", "dtmx_add_dft_plane", "dtmx_read_dft", "dtmx_step", "dtmx_sync",
     "dtmx_get_step", "dtmx_get_field", "dtmx_set_field", "dtmx_field_device_ptr",
-    "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_set_xchunk", "dtmx_park", "dtmx_unpark", "dtmx_set_tile_rows", "dtmx_get_engine", "dtmx_get_stream",
+    "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_set_xchunk", "dtmx_park", "dtmx_unpark", "dtmx_plane_state_floats", "dtmx_read_planes", "dtmx_write_planes", "dtmx_set_tile_rows", "dtmx_get_engine", "dtmx_get_stream",
     "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
     "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
     "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
@@ -77,6 +77,9 @@ def load():
     L.dtmx_set_engine.argtypes = [vp, ip, ip]
     L.dtmx_set_xchunk.argtypes = [vp, ip]
     L.dtmx_park.argtypes = [vp]
+    L.dtmx_plane_state_floats.argtypes = [vp, C.POINTER(C.c_size_t)]
+    L.dtmx_read_planes.argtypes = [vp, ip, ip, vp]
+    L.dtmx_write_planes.argtypes = [vp, ip, ip, vp]
     L.dtmx_unpark.argtypes = [vp]
     L.dtmx_set_tile_rows.argtypes = [vp, ip]
     L.dtmx_get_engine.argtypes = [vp, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), C.POINTER(ip)]
@@ -243,6 +246,31 @@ class Simulation:
     def unpark(self):
         """Bring a parked context's state back to the device."""
         self._ck(self._L.dtmx_unpark(self._h))
+
+    def plane_state_floats(self):
+        """Floats of time-stepping state per x plane (dtmx_plane_state_floats)."""
+        n = C.c_size_t(0)
+        self._ck(self._L.dtmx_plane_state_floats(self._h, C.byref(n)))
+        return n.value
+
+    def read_planes(self, x0, nplanes, out=None):
+        """The state of planes [x0, x0 + nplanes) as one float32 array
+        (section-major, dtmx_read_planes); out: a buffer to fill (pinned
+        memory makes the copies asynchronous to the host)."""
+        n = self.plane_state_floats() * int(nplanes)
+        if out is None:
+            out = np.empty(n, dtype=np.float32)
+        if out.dtype != np.float32 or out.size < n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float32 array of %d values" % n)
+        self._ck(self._L.dtmx_read_planes(self._h, int(x0), int(nplanes), out.ctypes.data))
+        return out[:n]
+
+    def write_planes(self, x0, nplanes, state):
+        """Store a read_planes array back into planes [x0, x0 + nplanes)."""
+        a = np.ascontiguousarray(state, dtype=np.float32)
+        if a.size != self.plane_state_floats() * int(nplanes):
+            raise ValueError("plane state of the wrong size")
+        self._ck(self._L.dtmx_write_planes(self._h, int(x0), int(nplanes), a.ctypes.data))
 
     def set_xchunk(self, planes):
         """Planes of the x walk per CTA (0: automatic)."""

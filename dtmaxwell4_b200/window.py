@@ -1,0 +1,276 @@
+"""Out-of-core runs: a grid larger than the device, stepped as x slabs that
+take turns on one GPU, several time steps per turn.
+
+The reference keeps its domain in pinned host memory and streams it through
+the device window by window, Ntime time steps per pass (window.hpp:177-267,
+params.h:12, params.h:50-52).  Here the grid is cut into x slabs (the split
+of sharded.slab_bounds); each slab is a context created parkable (dtmx_park /
+dtmx_unpark move its arrays to pinned host memory and back at the same device
+addresses) whose local grid carries K + 1 ghost planes on each side that has
+a neighbour.  One turn of slab r at time n:
+
+  unpark; write the neighbours' edge planes of time n into the ghost planes
+  (the full plane state: fields, y/z CPML auxiliaries, ADE currents --
+  dtmx_write_planes); step k <= K times; read the slab's own first and last
+  K + 1 owned planes (dtmx_read_planes); park.
+
+Why it is exact: a local order-2 step is wrong only next to the local grid's
+faces (one plane at each cut face per step), so after k <= K steps the planes
+from the second ghost plane inward still equal the single-domain run's, bit
+for bit -- the owned planes and one plane beyond them at every step of the
+turn (which probes and DFT planes of the owned planes may read).  Point
+sources act in every slab whose local grid holds them, ghost planes
+included; probes and DFT planes in the slab that owns their plane.
+
+Only `resident` slabs' state is on the device at a time (one by default), so
+the grid may be as large as host memory allows; a turn moves the slab's state
+across the host link twice, once per K time steps (the reference's cadence is
+Ntime = NS - 3).
+Restrictions: order 2, box geometry with a CPML or no absorber, no TF/SF
+source, gyrotropic material or design region, and ghost planes outside the
+x absorber slabs.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from .sharded import slab_bounds
+
+
+class WindowSlab:
+    """One slab of an out-of-core run: owned planes [x0, x1), local grid
+    [lx0, lx0 + nxl) with halo ghost planes toward each neighbour."""
+
+    def __init__(self, cfg, nslabs, rank, halo):
+        if cfg.order != 2:
+            raise ValueError("out-of-core runs support the order-2 stencil only")
+        if cfg.geometry != abi.GEOM_BOX or cfg.absorber == abi.ABS_SPLIT_PML:
+            raise ValueError("out-of-core runs support the box geometry with a CPML or no absorber")
+        if halo < 1:
+            raise ValueError("halo must be >= 1")
+        self.rank, self.nslabs, self.halo = rank, nslabs, halo
+        self.x0, self.x1 = slab_bounds(cfg.nx, nslabs, rank)
+        self.glo = halo if rank > 0 else 0
+        self.ghi = halo if rank < nslabs - 1 else 0
+        self.lx0 = self.x0 - self.glo
+        self.nxl = self.x1 - self.x0 + self.glo + self.ghi
+        pml = (0, 0) if cfg.absorber == abi.ABS_NONE else tuple(cfg.pml[0])
+        if nslabs > 1 and self.x1 - self.x0 < halo:
+            raise ValueError("slab %d owns %d planes: it needs at least the halo (%d)" % (rank, self.x1 - self.x0, halo))
+        if (self.glo and self.lx0 < pml[0]) or (self.ghi and self.x1 + self.ghi > cfg.nx - pml[1]):
+            raise ValueError("slab %d: ghost planes inside an x absorber slab" % rank)
+        lc = abi.Config()
+        C.memmove(C.byref(lc), C.byref(cfg), C.sizeof(abi.Config))
+        lc.nx = self.nxl
+        lc.pml[0][0] = pml[0] if rank == 0 else 0
+        lc.pml[0][1] = pml[1] if rank == nslabs - 1 else 0
+        self.cfg = lc
+
+    def owns(self, i):
+        return self.x0 <= i < self.x1
+
+    def holds(self, i):
+        return self.lx0 <= i < self.lx0 + self.nxl
+
+    def local(self, i):
+        return i - self.lx0
+
+    def owned_local(self):
+        return self.glo, self.glo + self.x1 - self.x0
+
+
+def parkable_simulation(cfg):
+    """A GPU Simulation of cfg created parkable."""
+    from .engine import Simulation
+    lc = abi.Config()
+    C.memmove(C.byref(lc), C.byref(cfg), C.sizeof(abi.Config))
+    lc.parkable = 1
+    return Simulation(lc)
+
+
+class OutOfCoreSimulation:
+    """One grid stepped as nslabs x slabs that take turns on the device,
+    steps_per_turn time steps per turn.
+
+    Set-up calls take the global arrays and coordinates; they are applied to
+    the slabs when the slabs are built (at the first step or read-back).
+    make_local(cfg) builds a slab's simulation (default: a parkable GPU
+    Simulation); it must offer read_planes / write_planes.  park(local) /
+    unpark(local) move it off and onto the device (defaults: the
+    Simulation's park / unpark when make_local is the default, else no-ops).
+    """
+
+    def __init__(self, cfg, nslabs, steps_per_turn=8, make_local=None, park=None, unpark=None, resident=1):
+        self.K = int(steps_per_turn)
+        if self.K < 1:
+            raise ValueError("steps_per_turn must be >= 1")
+        self.resident = max(1, int(resident))
+        self._pool = None
+        self.plans = [WindowSlab(cfg, nslabs, r, self.K + 1) for r in range(nslabs)]
+        self.gcfg = cfg
+        if make_local is None:
+            make_local = parkable_simulation
+            park = park or (lambda s: s.park())
+            unpark = unpark or (lambda s: s.unpark())
+        self._make = make_local
+        self._park = park or (lambda s: None)
+        self._unpark = unpark or (lambda s: None)
+        self._ops = []            # set-up calls, replayed on each slab when it is built
+        self._fields = {}         # initial global fields by component
+        self._probes = []         # (slab, global id) in each slab's local order
+        self._nprobes = 0
+        self._dfts = []           # (slab, local id)
+        self.slabs = None
+        self._edges = None        # per slab: state of its first and last halo owned planes, last turn
+        self.turns = 0
+
+    # ---- set-up (recorded)
+    def set_materials(self, table, idx_x, idx_y=None, idx_z=None):
+        for m in table:
+            if m.gyro_wp > 0:
+                raise ValueError("out-of-core slabs do not carry gyrotropic materials")
+        self._ops.append(("mat", (table, idx_x, idx_y, idx_z)))
+
+    def add_point_source(self, src):
+        self._ops.append(("src", src))
+
+    def set_tfsf(self, t):
+        raise ValueError("out-of-core slabs do not carry TF/SF sources")
+
+    def set_design(self, lo, eps):
+        raise ValueError("out-of-core slabs do not carry design regions")
+
+    def add_probe(self, comp, i, j, k, mode=abi.PROBE_NODE):
+        gid = self._nprobes
+        self._nprobes += 1
+        self._ops.append(("probe", (gid, comp, i, j, k, mode)))
+        return gid
+
+    def add_dft_plane(self, axis, index, comp_mask, omegas):
+        if axis != 0:
+            raise ValueError("out-of-core slabs record DFT planes normal to x")
+        did = len(self._dfts)
+        self._dfts.append(None)
+        self._ops.append(("dft", (did, index, comp_mask, omegas)))
+        return did
+
+    def set_field(self, comp, arr):
+        if self.slabs is not None:
+            raise ValueError("fields are set before the first step")
+        self._fields[comp] = np.asarray(arr, dtype=np.float32)
+
+    # ---- slabs
+    def _read_edges(self, s, pl):
+        lo, hi = pl.owned_local()
+        h = pl.halo
+        return (s.read_planes(lo, h) if pl.rank > 0 else None,
+                s.read_planes(hi - h, h) if pl.rank < pl.nslabs - 1 else None)
+
+    def _build(self):
+        self.slabs, self._edges = [], []
+        for r, pl in enumerate(self.plans):
+            s = self._make(pl.cfg)
+            a, b = pl.lx0, pl.lx0 + pl.nxl
+            for kind, v in self._ops:
+                if kind == "mat":
+                    table, ix, iy, iz = v
+                    s.set_materials(table, *[None if q is None else np.ascontiguousarray(np.asarray(q, np.uint8)[a:b])
+                                             for q in (ix, iy, iz)])
+                elif kind == "src" and pl.holds(v.i):
+                    q = abi.PointSource()
+                    C.memmove(C.byref(q), C.byref(v), C.sizeof(abi.PointSource))
+                    q.i = pl.local(v.i)
+                    s.add_point_source(q)
+                elif kind == "probe" and pl.owns(v[2]):
+                    gid, comp, i, j, k, mode = v
+                    s.add_probe(comp, pl.local(i), j, k, mode)
+                    self._probes.append((r, gid))
+                elif kind == "dft" and pl.owns(v[1]):
+                    did, index, mask, om = v
+                    self._dfts[did] = (r, s.add_dft_plane(0, pl.local(index), mask, om))
+            for comp, arr in self._fields.items():
+                s.set_field(comp, np.ascontiguousarray(arr[a:b]))
+            self._edges.append(self._read_edges(s, pl))
+            self._park(s)
+            self.slabs.append(s)
+
+    def _turn(self, r, k):
+        """One turn of slab r: k steps from the edges of the last turn."""
+        s, pl = self.slabs[r], self.plans[r]
+        self._unpark(s)
+        if r > 0:
+            s.write_planes(0, pl.halo, self._edges[r - 1][1])
+        if r < len(self.slabs) - 1:
+            s.write_planes(pl.nxl - pl.halo, pl.halo, self._edges[r + 1][0])
+        s.step(k)
+        e = self._read_edges(s, pl)
+        self._park(s)
+        return e
+
+    def step(self, n):
+        """Advance every slab by n time steps, K per turn.  The turns of one
+        sweep read only the edges of the previous sweep, so with resident > 1
+        that many slabs take their turns at once (one host thread each, each
+        slab on its own stream: one slab's copies overlap another's steps)."""
+        if self.slabs is None:
+            self._build()
+        n = int(n)
+        while n > 0:
+            k = min(n, self.K)
+            if self.resident > 1:
+                if self._pool is None:
+                    from concurrent.futures import ThreadPoolExecutor
+                    self._pool = ThreadPoolExecutor(max_workers=self.resident)
+                new = list(self._pool.map(lambda r: self._turn(r, k), range(len(self.slabs))))
+            else:
+                new = [self._turn(r, k) for r in range(len(self.slabs))]
+            self._edges = new
+            self.turns += 1
+            n -= k
+
+    # ---- results
+    def get_field(self, comp):
+        if self.slabs is None:
+            self._build()
+        parts = []
+        for s, pl in zip(self.slabs, self.plans):
+            self._unpark(s)
+            lo, hi = pl.owned_local()
+            parts.append(np.asarray(s.get_field(comp))[lo:hi].copy())
+            self._park(s)
+        return np.concatenate(parts, axis=0)
+
+    def read_probes(self):
+        out, ns = {}, 0
+        for r, s in enumerate(self.slabs or []):
+            ids = [gid for (q, gid) in self._probes if q == r]
+            if not ids:
+                continue
+            self._unpark(s)
+            tr = np.asarray(s.read_probes())
+            self._park(s)
+            for q, gid in enumerate(ids):
+                out[gid] = tr[q]
+            ns = max(ns, tr.shape[1])
+        res = np.zeros((self._nprobes, ns), dtype=np.float64)
+        for gid, t in out.items():
+            res[gid, :t.shape[0]] = t
+        return res
+
+    def read_dft(self, did):
+        r, ld = self._dfts[did]
+        s = self.slabs[r]
+        self._unpark(s)
+        out = s.read_dft(ld)
+        self._park(s)
+        return out
+
+    def close(self):
+        if self._pool is not None:
+            self._pool.shutdown()
+            self._pool = None
+        for s in self.slabs or []:
+            if hasattr(s, "close"):
+                s.close()
+        self.slabs = None

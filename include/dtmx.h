@@ -449,6 +449,25 @@ int  dtmx_set_xchunk(dtmx_ctx* ctx, int planes);
 int  dtmx_park(dtmx_ctx* ctx);
 int  dtmx_unpark(dtmx_ctx* ctx);
 
+/* The time-stepping state of a run of x planes, handed between contexts of
+ * the same y/z configuration (the reference's window hands x slices of its
+ * domain between host and device, window.hpp:203-241; here a slab context
+ * receives its neighbours' planes).  dtmx_plane_state_floats gives the floats
+ * per plane: the six fields (ny*nz each), the four CPML auxiliaries of the y
+ * and z absorber slabs (4*(Ly0+Ly1)*nz and 4*ny*(Lz0+Lz1)), and, when the
+ * material table has poles (P = most poles of one material), Em, Jp[P] and
+ * Jm[P] of the three E components as dense ny*nz planes (zero off the
+ * dispersive nodes).  The host buffer is section-major: section s of plane p
+ * starts at (section offset)*nplanes + p*(section plane size).
+ * dtmx_read_planes fills it for planes [x0, x0+nplanes), dtmx_write_planes
+ * stores it back.  Refused (DTMX_ERR_UNSUPPORTED): planes inside an x
+ * absorber slab, gyrotropic materials, TF/SF sources and design regions
+ * (their state is not per plane); DTMX_ERR_INVALID for planes outside the
+ * grid.  Both wait for the context's stream. */
+int  dtmx_plane_state_floats(dtmx_ctx* ctx, size_t* floats_per_plane);
+int  dtmx_read_planes(dtmx_ctx* ctx, int x0, int nplanes, float* host);
+int  dtmx_write_planes(dtmx_ctx* ctx, int x0, int nplanes, const float* host);
+
 /* Tile height (y rows) of the single-sweep engine: 16 (default) or 8 (more
  * CTAs for grids of a few million cells; 0 restores 16).  The reference's
  * block shape is a per-build parameter (params.h:50-52); dtmx_autotune

@@ -932,6 +932,66 @@ int PFX(set_field)(void* h, int comp, const double* in) {
   return DTMX_OK;
 }
 
+/* State of x planes in the library's dtmx_read_planes layout (dtmx.h):
+ * section-major -- six fields, the four CPML auxiliaries of the y and z
+ * slabs, then Em, Jp[P], Jm[P] of the three E components as dense planes
+ * (zero off the ADE box), P the most poles of one material of the table.
+ * Used by the tests' out-of-core runs with the oracle as the slab engine. */
+static int plane_poles(const osim* s) {
+  int p = 0;
+  for (int m = 0; m < s->nmat; m++) if (s->mat[m].npoles > p) p = s->mat[m].npoles;
+  return p;
+}
+
+size_t PFX(plane_state_floats)(void* h) {
+  osim* s = h;
+  size_t nyz = (size_t)s->ny * s->nz, n = 6 * nyz;
+  if (s->aux[1][0]) n += 4 * (size_t)(s->L[1][0] + s->L[1][1]) * s->nz;
+  if (s->aux[2][0]) n += 4 * (size_t)s->ny * (s->L[2][0] + s->L[2][1]);
+  return n + (size_t)3 * (1 + 2 * plane_poles(s)) * nyz;
+}
+
+static int plane_copy(osim* s, int x0, int np, double* buf, int rd) {
+  if (x0 < 0 || np < 0 || x0 + np > s->nx) return DTMX_ERR_INVALID;
+  if (s->has_gyro || s->has_tfsf || s->des_on || s->cfg.geometry != DTMX_GEOM_BOX) return DTMX_ERR_UNSUPPORTED;
+  if (s->aux[0][0] && np > 0 && (x0 < s->L[0][0] || x0 + np > s->nx - s->L[0][1])) return DTMX_ERR_UNSUPPORTED;
+  size_t nyz = (size_t)s->ny * s->nz;
+  double* b = buf;
+  for (int c = 0; c < 6; c++) {
+    real* f = s->f[c] + (size_t)x0 * nyz;
+    for (size_t q = 0; q < (size_t)np * nyz; q++) { if (rd) b[q] = f[q]; else f[q] = (real)b[q]; }
+    b += (size_t)np * nyz;
+  }
+  for (int a = 1; a < 3; a++) {
+    if (!s->aux[a][0]) continue;
+    size_t th = (size_t)(s->L[a][0] + s->L[a][1]);
+    size_t pp = a == 1 ? th * s->nz : (size_t)s->ny * th;
+    for (int q = 0; q < 4; q++) {
+      real* f = s->aux[a][q] + (size_t)x0 * pp;
+      for (size_t u = 0; u < (size_t)np * pp; u++) { if (rd) b[u] = f[u]; else f[u] = (real)b[u]; }
+      b += (size_t)np * pp;
+    }
+  }
+  int P = plane_poles(s);
+  for (int c = 0; c < 3; c++)
+    for (int sec = 0; sec < 1 + 2 * P; sec++) {
+      real* arr = sec == 0 ? s->Em[c] : sec <= P ? s->Jp[c][sec - 1] : s->Jm[c][sec - 1 - P];
+      for (int p = 0; p < np; p++)
+        for (int j = 0; j < s->ny; j++)
+          for (int k = 0; k < s->nz; k++) {
+            double* v = b + ((size_t)p * s->ny + j) * s->nz + k;
+            long ai = arr ? ade_index(s, x0 + p, j, k) : -1;
+            if (rd) *v = ai >= 0 ? arr[ai] : 0.0;
+            else if (ai >= 0) arr[ai] = (real)*v;
+          }
+      b += (size_t)np * nyz;
+    }
+  return DTMX_OK;
+}
+
+int PFX(read_planes)(void* h, int x0, int np, double* out) { return plane_copy(h, x0, np, out, 1); }
+int PFX(write_planes)(void* h, int x0, int np, const double* in) { return plane_copy(h, x0, np, (double*)in, 0); }
+
 int PFX(read_probes)(void* h, double* out, int max_samples, int* ns) {
   osim* s = h;
   int n = s->nsamples < max_samples ? s->nsamples : max_samples;

@@ -42,6 +42,10 @@ def lib():
             g("read_probes").argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
             g("read_dft").argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
             g("set_design").argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p]
+            g("plane_state_floats").restype = C.c_size_t
+            g("plane_state_floats").argtypes = [C.c_void_p]
+            g("read_planes").argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+            g("write_planes").argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
             g("forward_adjoint").argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.POINTER(C.c_double),
                                              C.c_void_p]
         _lib = L
@@ -136,6 +140,24 @@ class OracleSim:
     def set_field(self, comp, arr):
         a = np.ascontiguousarray(arr, dtype=np.float64)
         self._f("set_field")(self._h, comp, a.ctypes.data)
+
+    def plane_state_floats(self):
+        return int(self._f("plane_state_floats")(self._h))
+
+    def read_planes(self, x0, nplanes, out=None):
+        out = np.empty(self.plane_state_floats() * int(nplanes), dtype=np.float64)
+        rc = self._f("read_planes")(self._h, int(x0), int(nplanes), out.ctypes.data)
+        if rc:
+            raise ValueError("read_planes rc=%d" % rc)
+        return out
+
+    def write_planes(self, x0, nplanes, state):
+        a = np.ascontiguousarray(state, dtype=np.float64)
+        if a.size != self.plane_state_floats() * int(nplanes):
+            raise ValueError("plane state of the wrong size")
+        rc = self._f("write_planes")(self._h, int(x0), int(nplanes), a.ctypes.data)
+        if rc:
+            raise ValueError("write_planes rc=%d" % rc)
 
     def read_probes(self, max_samples=100000):
         out = np.zeros((max(self._nprobes, 1), max_samples), dtype=np.float64)

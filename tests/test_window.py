@@ -1,0 +1,216 @@
+"""Out-of-core runs (dtmaxwell4_b200.window): a grid stepped as x slabs that
+take turns on the device, each slab parked in host memory between its turns.
+
+CPU: the slab walk with the FP32 oracle as the slab engine (its
+read_planes / write_planes restate the library's plane-state layout; parking
+is a no-op there) against one single-domain FP32 oracle run -- fields, probe
+traces and an x-normal DFT plane bit for bit, for 2 and 3 slabs and 1 to 5
+time steps per turn (a Drude block crosses a slab face, the dipole sits in a
+neighbour's ghost planes).
+GPU: dtmx_park / dtmx_unpark keep the state bit for bit and free the device
+memory while parked, a parked context refuses its calls, dtmx_read_planes /
+dtmx_write_planes round-trip and match the oracle's layout, and a 3-slab
+out-of-core run equals the plain in-core run bit for bit on both field
+engines.
+"""
+import numpy as np
+import pytest
+
+from test_sharded import NX, NY, NZ, STEPS, _scenario
+
+
+def _apply(sim, mats, idx, src, probes, fields):
+    from dtmaxwell4_b200 import abi
+    sim.set_materials(mats, idx, idx, idx)
+    sim.add_point_source(src)
+    for (c, i, j, k) in probes:
+        sim.add_probe(c, i, j, k)
+    d0 = sim.add_dft_plane(0, 16, (1 << abi.EY) | (1 << abi.HZ), [0.5, 0.8])
+    for c in range(6):
+        sim.set_field(c, fields[c])
+    return d0
+
+
+@pytest.mark.parametrize("nslabs,K,resident", [(2, 4, 1), (3, 1, 1), (3, 5, 2)])
+def test_window_equals_single_domain(nslabs, K, resident):
+    import pyoracle
+    from dtmaxwell4_b200.window import OutOfCoreSimulation
+    cfg, mats, idx, src, probes, fields = _scenario()
+    parked = []
+    w = OutOfCoreSimulation(cfg, nslabs, steps_per_turn=K, make_local=lambda c: pyoracle.OracleSim(c, "f32"),
+                            park=lambda s: parked.append(s), unpark=lambda s: None, resident=resident)
+    d0 = _apply(w, mats, idx, src, probes, fields)
+    w.step(STEPS)
+    turns = -(-STEPS // K)
+    assert w.turns == turns
+    assert len(parked) == nslabs * (turns + 1)        # every slab parked after set-up and after each turn
+    o = pyoracle.OracleSim(cfg, "f32")
+    do = _apply(o, mats, idx, src, probes, fields)
+    o.step(STEPS)
+    for c in range(6):
+        want = o.get_field(c)
+        assert np.abs(want).max() > 1e-4
+        assert np.array_equal(w.get_field(c), want), c
+    assert np.array_equal(w.read_probes(), o.read_probes(STEPS + 8))
+    assert np.array_equal(w.read_dft(d0), o.read_dft(do))
+    o.close()
+    w.close()
+
+
+def test_window_refusals():
+    from dtmaxwell4_b200 import abi
+    from dtmaxwell4_b200.window import OutOfCoreSimulation
+    cfg = _scenario()[0]
+    w = OutOfCoreSimulation(cfg, 2, make_local=lambda c: None)
+    with pytest.raises(ValueError):
+        w.set_tfsf(None)
+    with pytest.raises(ValueError):
+        w.set_design((0, 0, 0), None)
+    with pytest.raises(ValueError):
+        w.add_dft_plane(1, 3, 1, [0.5])
+    gyro = abi.make_material(1.0, eps_inf=1.0, gyro=(0.3, 0.01, 0.2))
+    with pytest.raises(ValueError):
+        w.set_materials([gyro], np.zeros((NX, NY, NZ), np.uint8))
+    with pytest.raises(ValueError):                   # 6 owned planes, a 9-plane halo
+        OutOfCoreSimulation(abi.make_config(12, 8, 8, pml=2), 2, steps_per_turn=8, make_local=lambda c: None)
+    with pytest.raises(ValueError):                   # slab 1's ghost planes reach the 6-plane x absorber
+        OutOfCoreSimulation(abi.make_config(40, 8, 8, pml=6), 3, steps_per_turn=8, make_local=lambda c: None)
+    OutOfCoreSimulation(abi.make_config(40, 8, 8, pml=6), 3, steps_per_turn=4, make_local=lambda c: None)
+    with pytest.raises(ValueError):
+        OutOfCoreSimulation(abi.make_config(40, 8, 8, order=4, courant=0.4), 2, make_local=lambda c: None)
+
+
+def test_oracle_plane_state_round_trip():
+    """The oracle's plane state: sizes per section, fields as get_field,
+    zero ADE sections off the dispersive box, write then read is identity."""
+    import pyoracle
+    cfg, mats, idx, src, probes, fields = _scenario()
+    o = pyoracle.OracleSim(cfg, "f32")
+    _apply(o, mats, idx, src, probes, fields)
+    o.step(7)
+    nyz = NY * NZ
+    L = 4                                             # CPML cells per face
+    assert o.plane_state_floats() == 6 * nyz + 4 * 2 * L * NZ + 4 * NY * 2 * L + 3 * (1 + 2 * 1) * nyz
+    st = o.read_planes(8, 5)
+    f = st[:6 * 5 * nyz].reshape(6, 5, NY, NZ)
+    for c in range(6):
+        assert np.array_equal(f[c], o.get_field(c)[8:13])
+    ade = st[-3 * 3 * 5 * nyz:].reshape(3, 3, 5, NY, NZ)
+    assert not ade.any()                              # planes 8..12 hold no Drude node
+    st2 = o.read_planes(19, 4)
+    assert st2[-3 * 3 * 4 * nyz:].any()               # the Drude block 20..23 has current after 7 steps
+    p = o.read_planes(4, 3)
+    q = p * 1.5
+    o.write_planes(4, 3, q)
+    assert np.array_equal(o.read_planes(4, 3), q.astype(np.float32).astype(np.float64))
+    with pytest.raises(ValueError):
+        o.read_planes(2, 3)                           # inside the x absorber slab
+    o.close()
+
+
+@pytest.mark.gpu
+def test_park_round_trip_frees_device_memory():
+    import torch
+    from dtmaxwell4_b200 import Simulation, abi
+    from dtmaxwell4_b200.engine import DtmxError
+    cfg, mats, idx, src, probes, fields = _scenario()
+    pc = abi.make_config(NX, NY, NZ, dx=1.0, courant=0.5, order=2, absorber=abi.ABS_CPML, pml=4,
+                         probe_capacity=STEPS + 8, parkable=True)
+    a, b = Simulation(pc), Simulation(cfg)
+    da, db = _apply(a, mats, idx, src, probes, fields), _apply(b, mats, idx, src, probes, fields)
+    a.step(STEPS // 2)
+    b.step(STEPS // 2)
+    a.park()
+    with pytest.raises(DtmxError):
+        a.step(1)
+    with pytest.raises(DtmxError):
+        a.get_field(abi.EX)
+    a.park()                                            # parking twice is a no-op
+    a.unpark()
+    a.unpark()
+    a.step(STEPS - STEPS // 2)
+    b.step(STEPS - STEPS // 2)
+    for c in range(6):
+        assert np.array_equal(a.get_field(c), b.get_field(c)), c
+    assert np.array_equal(a.read_probes(), b.read_probes())
+    assert np.array_equal(a.read_dft(da), b.read_dft(db))
+    with pytest.raises(DtmxError):
+        b.park()                                        # not created parkable
+    a.close()
+    b.close()
+    # a 256^3 context: its arrays leave the device while parked
+    big = Simulation(abi.make_config(256, 256, 256, pml=8, parkable=True))
+    big.step(2)
+    big.sync()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.mem_get_info()[0]
+    big.park()
+    f1 = torch.cuda.mem_get_info()[0]
+    big.unpark()
+    f2 = torch.cuda.mem_get_info()[0]
+    assert f1 - f0 >= 6 * 256 ** 3 * 4, (f0, f1)
+    assert abs(f2 - f0) < 64 << 20, (f0, f2)
+    big.step(1)
+    assert big.check_finite()
+    big.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine,resident", [(1, 1), (3, 1), (3, 2)])
+def test_window_equals_in_core_run(engine, resident):
+    from dtmaxwell4_b200 import Simulation, abi
+    from dtmaxwell4_b200.window import OutOfCoreSimulation
+    cfg, mats, idx, src, probes, fields = _scenario()
+
+    def make(c):
+        from dtmaxwell4_b200.window import parkable_simulation
+        s = parkable_simulation(c)
+        s.set_engine(engine, 0)
+        return s
+    w = OutOfCoreSimulation(cfg, 3, steps_per_turn=5, make_local=make, park=lambda s: s.park(),
+                            unpark=lambda s: s.unpark(), resident=resident)
+    b = Simulation(cfg)
+    b.set_engine(engine, 0)
+    dw, db = _apply(w, mats, idx, src, probes, fields), _apply(b, mats, idx, src, probes, fields)
+    w.step(STEPS)
+    b.step(STEPS)
+    for c in range(6):
+        want = b.get_field(c)
+        assert np.abs(want).max() > 1e-4
+        assert np.array_equal(w.get_field(c), want), c
+    assert np.array_equal(w.read_probes(), b.read_probes().astype(np.float64))
+    assert np.array_equal(w.read_dft(dw), b.read_dft(db))
+    w.close()
+    b.close()
+
+
+@pytest.mark.gpu
+def test_gpu_plane_state_layout():
+    """dtmx_read_planes: the oracle's section sizes, fields as dtmx_get_field,
+    ADE sections zero off the Drude block and nonzero on it; a written state
+    reads back unchanged (pinned output buffer too)."""
+    import pyoracle
+    import torch
+    from dtmaxwell4_b200 import Simulation
+    cfg, mats, idx, src, probes, fields = _scenario()
+    g = Simulation(cfg)
+    o = pyoracle.OracleSim(cfg, "f32")
+    _apply(g, mats, idx, src, probes, fields)
+    _apply(o, mats, idx, src, probes, fields)
+    g.step(7)
+    nyz = NY * NZ
+    assert g.plane_state_floats() == o.plane_state_floats()
+    st = g.read_planes(8, 5)
+    f = st[:6 * 5 * nyz].reshape(6, 5, NY, NZ)
+    for c in range(6):
+        assert np.array_equal(f[c], g.get_field(c)[8:13])
+    assert not st[-9 * 5 * nyz:].any()
+    assert g.read_planes(19, 4)[-9 * 4 * nyz:].any()
+    pinned = torch.empty(g.plane_state_floats() * 4, dtype=torch.float32).pin_memory().numpy()
+    p = g.read_planes(19, 4, out=pinned).copy()
+    q = (p * 1.5).astype(np.float32)
+    g.write_planes(19, 4, q)
+    assert np.array_equal(g.read_planes(19, 4), q)
+    g.write_planes(19, 4, p)
+    g.close()
+    o.close()
