@@ -55,9 +55,9 @@ def parse():
     ap.add_argument("--ooc-only", action="store_true", help="with --extras-only: only the out-of-core measurement")
     ap.add_argument("--ooc-n", type=int, nargs=3, default=[1024, 512, 512])
     ap.add_argument("--ooc-slabs", type=int, default=4)
-    ap.add_argument("--ooc-k", type=int, default=32, help="time steps per slab turn")
-    ap.add_argument("--ooc-resident", type=int, default=2, help="slabs on the device at once")
-    ap.add_argument("--ooc-steps", type=int, default=64)
+    ap.add_argument("--ooc-k", type=int, default=64, help="time steps per slab turn")
+    ap.add_argument("--ooc-resident", type=int, default=3, help="slabs on the device at once")
+    ap.add_argument("--ooc-steps", type=int, default=128)
     return ap.parse_args()
 
 

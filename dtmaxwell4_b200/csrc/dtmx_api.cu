@@ -56,6 +56,8 @@ struct VmmBlock {
   CUmemGenericAllocationHandle h = 0;
   void* host = nullptr;       // pinned copy while parked
   bool dead = false;          // parked without a copy: refilled with zeros on unpark
+  bool fixed = false;         // constant once the context has stepped (materials, tables)
+  bool saved_prepared = false;  // the host copy was taken after the context first stepped
 };
 
 struct dtmx_ctx {
@@ -220,7 +222,7 @@ static CUresult vmm_back(int dev, VmmBlock& b) {
 }
 
 template <class T>
-static int dalloc(dtmx_ctx* ctx, T** p, size_t count) {
+static int dalloc(dtmx_ctx* ctx, T** p, size_t count, bool fixed = false) {
   if (ctx->cfg.parkable) {
     const VmmApi& A = vmm_api();
     if (!A.ok) return fail(ctx, DTMX_ERR_CUDA, "CUDA virtual memory management is unavailable");
@@ -233,6 +235,7 @@ static int dalloc(dtmx_ctx* ctx, T** p, size_t count) {
     b.size = (bytes + g - 1) / g * g;
     if (A.reserve(&b.va, b.size, 0, 0, 0) != CUDA_SUCCESS) return fail(ctx, DTMX_ERR_OOM, "address reservation");
     if (vmm_back(ctx->dev, b) != CUDA_SUCCESS) { A.vfree(b.va, b.size); return fail(ctx, DTMX_ERR_OOM, "device memory"); }
+    b.fixed = fixed;
     ctx->vmm.push_back(b);
     CK(cudaMemsetAsync((void*)b.va, 0, b.size, ctx->stream));
     *p = (T*)b.va;
@@ -449,7 +452,7 @@ static int setup_absorber(dtmx_ctx* ctx) {
     const int H = 2 * n[a] + 2;
     float* q[3];
     for (int t = 0; t < 3; t++) {
-      int rc = dalloc(ctx, &q[t], H);
+      int rc = dalloc(ctx, &q[t], H, true);
       if (rc) return rc;
     }
     CK(cudaMemcpyAsync(q[0], t0[a].data(), H * 4, cudaMemcpyHostToDevice, ctx->stream));
@@ -517,15 +520,15 @@ extern "C" int dtmx_create(const dtmx_config* cfg, dtmx_ctx** out) {
   // 64 floats of slack: aligned 16-byte tile rows may read up to 3 floats past the last node
   for (int comp = 0; comp < 6 && !rc; comp++) rc = dalloc(ctx, &ctx->P.f[comp], ctx->nstore + 64);
   if (!rc) rc = setup_absorber(ctx);
-  if (!rc) rc = dalloc(ctx, &ctx->d_mt, 1);
+  if (!rc) rc = dalloc(ctx, &ctx->d_mt, 1, true);
   if (!rc) rc = dalloc(ctx, &ctx->d_step, 1);
   if (!rc) rc = dalloc(ctx, &ctx->d_flag, 1);
   if (!rc) rc = dalloc(ctx, &ctx->d_err, 1);
-  for (int comp = 0; comp < 3 && !rc; comp++) rc = dalloc(ctx, &ctx->d_mat[comp], ctx->nstore + 64);
+  for (int comp = 0; comp < 3 && !rc; comp++) rc = dalloc(ctx, &ctx->d_mat[comp], ctx->nstore + 64, true);
   if (!rc) rc = build_maps(ctx);
   ctx->P.ntz = (c.nz + TZ - 1) / TZ;
   ctx->P.nty = (c.ny + TYT - 1) / TYT;
-  if (!rc) rc = dalloc(ctx, &ctx->d_umat, (size_t)c.nx * ctx->P.nty * ctx->P.ntz);   // zeros: material 0 everywhere
+  if (!rc) rc = dalloc(ctx, &ctx->d_umat, (size_t)c.nx * ctx->P.nty * ctx->P.ntz, true);   // zeros: material 0 everywhere
   if (rc) { *out = ctx; return rc; }
   ctx->P.umat = ctx->d_umat;
   ctx->P.err = ctx->d_err;
@@ -1166,11 +1169,11 @@ static int prepare(dtmx_ctx* ctx) {
   if (ctx->prepared) return DTMX_OK;
   int rc;
   if (!ctx->psrc.empty()) {
-    if ((rc = dalloc(ctx, &ctx->d_psrc, ctx->psrc.size()))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_psrc, ctx->psrc.size(), true))) return rc;
     CK(cudaMemcpyAsync(ctx->d_psrc, ctx->psrc.data(), ctx->psrc.size() * sizeof(PointSrcDev), cudaMemcpyHostToDevice, ctx->stream));
   }
   if (!ctx->probes.empty()) {
-    if ((rc = dalloc(ctx, &ctx->d_probes, ctx->probes.size()))) return rc;
+    if ((rc = dalloc(ctx, &ctx->d_probes, ctx->probes.size(), true))) return rc;
     CK(cudaMemcpyAsync(ctx->d_probes, ctx->probes.data(), ctx->probes.size() * sizeof(ProbeDev), cudaMemcpyHostToDevice, ctx->stream));
     if ((rc = dalloc(ctx, &ctx->d_traces, ctx->probes.size() * (size_t)ctx->probe_cap))) return rc;
   }
@@ -2296,8 +2299,11 @@ extern "C" int dtmx_park(dtmx_ctx* ctx) {
     for (int a = 0; a < 3; a++)
       for (int q = 0; q < 2; q++) b.dead = b.dead || b.va == (CUdeviceptr)ctx->hax_alt[a][q];
     if (b.dead) continue;
+    // arrays fixed once the context has stepped keep the host copy of an earlier park
+    if (b.fixed && b.host && ctx->prepared && b.saved_prepared) continue;
     if (!b.host) CK(cudaMallocHost(&b.host, b.size));
     CK(cudaMemcpyAsync(b.host, (void*)b.va, b.size, cudaMemcpyDeviceToHost, ctx->stream));
+    b.saved_prepared = ctx->prepared;
   }
   CK(cudaStreamSynchronize(ctx->stream));
   for (auto& b : ctx->vmm) {

@@ -97,8 +97,10 @@ class OutOfCoreSimulation:
     the slabs when the slabs are built (at the first step or read-back).
     make_local(cfg) builds a slab's simulation (default: a parkable GPU
     Simulation); it must offer read_planes / write_planes.  park(local) /
-    unpark(local) move it off and onto the device (defaults: the
-    Simulation's park / unpark when make_local is the default, else no-ops).
+    unpark(local) move it off and onto the device (defaults: its park /
+    unpark methods where it has them, else nothing).  Edge planes of GPU
+    slabs pass through pinned host buffers (two per side, alternating
+    between sweeps), so their copies run at the host link's rate.
     """
 
     def __init__(self, cfg, nslabs, steps_per_turn=8, make_local=None, park=None, unpark=None, resident=1):
@@ -109,13 +111,11 @@ class OutOfCoreSimulation:
         self._pool = None
         self.plans = [WindowSlab(cfg, nslabs, r, self.K + 1) for r in range(nslabs)]
         self.gcfg = cfg
-        if make_local is None:
-            make_local = parkable_simulation
-            park = park or (lambda s: s.park())
-            unpark = unpark or (lambda s: s.unpark())
-        self._make = make_local
-        self._park = park or (lambda s: None)
-        self._unpark = unpark or (lambda s: None)
+        self._make = make_local or parkable_simulation
+        self._park = park or (lambda s: s.park() if hasattr(s, "park") else None)
+        self._unpark = unpark or (lambda s: s.unpark() if hasattr(s, "unpark") else None)
+        self._pins = None         # per slab, per parity, per side: pinned edge buffers (GPU slabs)
+        self._parity = 0
         self._ops = []            # set-up calls, replayed on each slab when it is built
         self._fields = {}         # initial global fields by component
         self._probes = []         # (slab, global id) in each slab's local order
@@ -161,11 +161,22 @@ class OutOfCoreSimulation:
         self._fields[comp] = np.asarray(arr, dtype=np.float32)
 
     # ---- slabs
-    def _read_edges(self, s, pl):
+    def _read_edges(self, s, pl, parity):
         lo, hi = pl.owned_local()
         h = pl.halo
-        return (s.read_planes(lo, h) if pl.rank > 0 else None,
-                s.read_planes(hi - h, h) if pl.rank < pl.nslabs - 1 else None)
+        pins = self._pins[pl.rank] if self._pins else None
+        pin = pins[parity] if pins else (None, None)
+        return (s.read_planes(lo, h, out=pin[0]) if pl.rank > 0 else None,
+                s.read_planes(hi - h, h, out=pin[1]) if pl.rank < pl.nslabs - 1 else None)
+
+    def _pin_buffers(self, s, pl):
+        """Two pinned float32 buffers per side for a GPU slab's edge planes."""
+        from .engine import Simulation
+        if not isinstance(s, Simulation):
+            return None
+        import torch
+        n = s.plane_state_floats() * pl.halo
+        return [[torch.empty(n, dtype=torch.float32).pin_memory().numpy() for _ in range(2)] for _ in range(2)]
 
     def _build(self):
         self.slabs, self._edges = [], []
@@ -191,7 +202,11 @@ class OutOfCoreSimulation:
                     self._dfts[did] = (r, s.add_dft_plane(0, pl.local(index), mask, om))
             for comp, arr in self._fields.items():
                 s.set_field(comp, np.ascontiguousarray(arr[a:b]))
-            self._edges.append(self._read_edges(s, pl))
+            pins = self._pin_buffers(s, pl)
+            if pins is not None:
+                self._pins = self._pins or [None] * len(self.plans)
+                self._pins[r] = pins
+            self._edges.append(self._read_edges(s, pl, 0))
             self._park(s)
             self.slabs.append(s)
 
@@ -204,7 +219,7 @@ class OutOfCoreSimulation:
         if r < len(self.slabs) - 1:
             s.write_planes(pl.nxl - pl.halo, pl.halo, self._edges[r + 1][0])
         s.step(k)
-        e = self._read_edges(s, pl)
+        e = self._read_edges(s, pl, self._parity ^ 1)
         self._park(s)
         return e
 
@@ -226,6 +241,7 @@ class OutOfCoreSimulation:
             else:
                 new = [self._turn(r, k) for r in range(len(self.slabs))]
             self._edges = new
+            self._parity ^= 1
             self.turns += 1
             n -= k
 
