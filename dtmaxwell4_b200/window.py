@@ -115,14 +115,13 @@ class OutOfCoreSimulation:
         self._park = park or (lambda s: s.park() if hasattr(s, "park") else None)
         self._unpark = unpark or (lambda s: s.unpark() if hasattr(s, "unpark") else None)
         self._pins = None         # per slab, per parity, per side: pinned edge buffers (GPU slabs)
-        self._parity = 0
         self._ops = []            # set-up calls, replayed on each slab when it is built
         self._fields = {}         # initial global fields by component
         self._probes = []         # (slab, global id) in each slab's local order
         self._nprobes = 0
         self._dfts = []           # (slab, local id)
         self.slabs = None
-        self._edges = None        # per slab: state of its first and last halo owned planes, last turn
+        self._edges = None        # [turn parity][slab]: state of its first and last halo owned planes
         self.turns = 0
 
     # ---- set-up (recorded)
@@ -179,7 +178,8 @@ class OutOfCoreSimulation:
         return [[torch.empty(n, dtype=torch.float32).pin_memory().numpy() for _ in range(2)] for _ in range(2)]
 
     def _build(self):
-        self.slabs, self._edges = [], []
+        self.slabs = []
+        self._edges = [[None] * len(self.plans), [None] * len(self.plans)]   # by turn parity
         for r, pl in enumerate(self.plans):
             s = self._make(pl.cfg)
             a, b = pl.lx0, pl.lx0 + pl.nxl
@@ -206,44 +206,66 @@ class OutOfCoreSimulation:
             if pins is not None:
                 self._pins = self._pins or [None] * len(self.plans)
                 self._pins[r] = pins
-            self._edges.append(self._read_edges(s, pl, 0))
+            self._edges[1][r] = self._read_edges(s, pl, 1)          # turn -1
             self._park(s)
             self.slabs.append(s)
 
-    def _turn(self, r, k):
-        """One turn of slab r: k steps from the edges of the last turn."""
+    def _turn(self, r, t, k):
+        """Turn t of slab r: k steps from the edges its neighbours left in
+        turn t - 1; its own edges of turn t go to the buffers of parity t % 2."""
         s, pl = self.slabs[r], self.plans[r]
+        old = self._edges[(t - 1) % 2]
         self._unpark(s)
         if r > 0:
-            s.write_planes(0, pl.halo, self._edges[r - 1][1])
+            s.write_planes(0, pl.halo, old[r - 1][1])
         if r < len(self.slabs) - 1:
-            s.write_planes(pl.nxl - pl.halo, pl.halo, self._edges[r + 1][0])
+            s.write_planes(pl.nxl - pl.halo, pl.halo, old[r + 1][0])
         s.step(k)
-        e = self._read_edges(s, pl, self._parity ^ 1)
+        self._edges[t % 2][r] = self._read_edges(s, pl, t % 2)
         self._park(s)
-        return e
+
+    def _turn_after(self, deps, r, t, k):
+        for d in deps:
+            d.result()
+        self._turn(r, t, k)
 
     def step(self, n):
-        """Advance every slab by n time steps, K per turn.  The turns of one
-        sweep read only the edges of the previous sweep, so with resident > 1
-        that many slabs take their turns at once (one host thread each, each
-        slab on its own stream: one slab's copies overlap another's steps)."""
+        """Advance every slab by n time steps, K per turn.
+
+        Turn t of slab r needs only turn t - 1 of slabs r - 1, r and r + 1
+        (whose completion also frees the edge buffers it overwrites), so with
+        resident > 1 the turns run as a dataflow on that many host threads,
+        each slab on its own stream: copies of one slab overlap the steps of
+        another, and a slab starts its next turn without waiting for the far
+        end of the grid."""
         if self.slabs is None:
             self._build()
+        ks = []
         n = int(n)
         while n > 0:
-            k = min(n, self.K)
-            if self.resident > 1:
-                if self._pool is None:
-                    from concurrent.futures import ThreadPoolExecutor
-                    self._pool = ThreadPoolExecutor(max_workers=self.resident)
-                new = list(self._pool.map(lambda r: self._turn(r, k), range(len(self.slabs))))
-            else:
-                new = [self._turn(r, k) for r in range(len(self.slabs))]
-            self._edges = new
-            self._parity ^= 1
-            self.turns += 1
-            n -= k
+            ks.append(min(n, self.K))
+            n -= ks[-1]
+        S, t0 = len(self.slabs), self.turns
+        if self.resident == 1:
+            for q, k in enumerate(ks):
+                for r in range(S):
+                    self._turn(r, t0 + q, k)
+                self.turns += 1
+            return
+        if self._pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(max_workers=self.resident)
+        futs = {}
+        for q, k in enumerate(ks):
+            t = t0 + q
+            for r in range(S):
+                deps = [futs[(x, t - 1)] for x in (r - 1, r, r + 1) if (x, t - 1) in futs]
+                futs[(r, t)] = self._pool.submit(self._turn_after, deps, r, t, k)
+        try:
+            for f in futs.values():
+                f.result()
+        finally:
+            self.turns = t0 + len(ks)
 
     # ---- results
     def get_field(self, comp):
