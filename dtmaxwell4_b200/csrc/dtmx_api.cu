@@ -11,6 +11,7 @@
 #include <vector>
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <tuple>
 
 #include <cudaTypedefs.h>
@@ -206,12 +207,46 @@ static CUmemAllocationProp vmm_prop(int dev) {
   prop.location.id = dev;
   return prop;
 }
+// Physical allocations released by dtmx_park, kept per device for the next
+// dtmx_unpark of a block of the same size (up to a byte limit, 0 by default:
+// released at once).  Creating and releasing physical memory costs more than
+// mapping it, so contexts that take turns on a device reuse each other's.
+struct HandlePool {
+  std::mutex mu;
+  std::multimap<size_t, CUmemGenericAllocationHandle> free;
+  size_t bytes = 0;
+  long long limit = 0;          // < 0: unlimited
+};
+constexpr int kPoolDevices = 64;
+static HandlePool& handle_pool(int dev) {
+  static HandlePool pools[kPoolDevices];
+  return pools[dev >= 0 && dev < kPoolDevices ? dev : 0];
+}
+static bool pool_take(int dev, size_t size, CUmemGenericAllocationHandle* h) {
+  HandlePool& P = handle_pool(dev);
+  std::lock_guard<std::mutex> lk(P.mu);
+  auto it = P.free.find(size);
+  if (it == P.free.end()) return false;
+  *h = it->second;
+  P.free.erase(it);
+  P.bytes -= size;
+  return true;
+}
+// keeps the handle (true) or leaves it to the caller to release (false)
+static bool pool_put(int dev, size_t size, CUmemGenericAllocationHandle h) {
+  HandlePool& P = handle_pool(dev);
+  std::lock_guard<std::mutex> lk(P.mu);
+  if (P.limit >= 0 && P.bytes + size > (size_t)P.limit) return false;
+  P.free.insert({size, h});
+  P.bytes += size;
+  return true;
+}
 // physical memory for block b, mapped read-write at its reserved address
 static CUresult vmm_back(int dev, VmmBlock& b) {
   const VmmApi& A = vmm_api();
   const CUmemAllocationProp prop = vmm_prop(dev);
-  CUresult r = A.create(&b.h, b.size, &prop, 0);
-  if (r != CUDA_SUCCESS) return r;
+  CUresult r = CUDA_SUCCESS;
+  if (!pool_take(dev, b.size, &b.h) && (r = A.create(&b.h, b.size, &prop, 0)) != CUDA_SUCCESS) return r;
   if ((r = A.map(b.va, b.size, 0, b.h, 0)) != CUDA_SUCCESS) { A.release(b.h); return r; }
   CUmemAccessDesc acc{};
   acc.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
@@ -2307,11 +2342,27 @@ extern "C" int dtmx_park(dtmx_ctx* ctx) {
   }
   CK(cudaStreamSynchronize(ctx->stream));
   for (auto& b : ctx->vmm) {
-    if (A.unmap(b.va, b.size) != CUDA_SUCCESS || A.release(b.h) != CUDA_SUCCESS)
+    if (A.unmap(b.va, b.size) != CUDA_SUCCESS || (!pool_put(ctx->dev, b.size, b.h) && A.release(b.h) != CUDA_SUCCESS))
       return fail(ctx, DTMX_ERR_CUDA, "releasing the device memory of a parked context");
     b.h = 0;
   }
   ctx->parked = true;
+  return DTMX_OK;
+}
+
+extern "C" int dtmx_set_park_pool(int device, int64_t bytes) {
+  if (device < 0 || device >= kPoolDevices) return DTMX_ERR_INVALID;
+  const VmmApi& A = vmm_api();
+  HandlePool& P = handle_pool(device);
+  std::lock_guard<std::mutex> lk(P.mu);
+  P.limit = bytes < 0 ? -1 : bytes;
+  // release what the new limit does not hold, largest first
+  while (P.limit >= 0 && P.bytes > (size_t)P.limit && !P.free.empty()) {
+    auto it = std::prev(P.free.end());
+    if (A.ok) A.release(it->second);
+    P.bytes -= it->first;
+    P.free.erase(it);
+  }
   return DTMX_OK;
 }
 

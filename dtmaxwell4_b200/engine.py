@@ -20,7 +20,7 @@ EXPORTS = (
     "dtmx_set_materials", "dtmx_add_point_source", "dtmx_set_tfsf", "dtmx_add_probe",
     "dtmx_read_probes", "dtmx_add_dft_plane", "dtmx_read_dft", "dtmx_step", "dtmx_sync",
     "dtmx_get_step", "dtmx_get_field", "dtmx_set_field", "dtmx_field_device_ptr",
-    "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_set_xchunk", "dtmx_park", "dtmx_unpark", "dtmx_plane_state_floats", "dtmx_read_planes", "dtmx_write_planes", "dtmx_set_tile_rows", "dtmx_get_engine", "dtmx_get_stream",
+    "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_set_xchunk", "dtmx_park", "dtmx_unpark", "dtmx_set_park_pool", "dtmx_plane_state_floats", "dtmx_read_planes", "dtmx_write_planes", "dtmx_set_tile_rows", "dtmx_get_engine", "dtmx_get_stream",
     "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
     "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
     "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
@@ -77,6 +77,7 @@ def load():
     L.dtmx_set_engine.argtypes = [vp, ip, ip]
     L.dtmx_set_xchunk.argtypes = [vp, ip]
     L.dtmx_park.argtypes = [vp]
+    L.dtmx_set_park_pool.argtypes = [ip, C.c_int64]
     L.dtmx_plane_state_floats.argtypes = [vp, C.POINTER(C.c_size_t)]
     L.dtmx_read_planes.argtypes = [vp, ip, ip, vp]
     L.dtmx_write_planes.argtypes = [vp, ip, ip, vp]
@@ -401,6 +402,16 @@ class Simulation:
         a, b, n = C.c_double(), C.c_double(), C.c_int64()
         self._ck(self._L.dtmx_read_profile(self._h, C.byref(a), C.byref(b), C.byref(n)))
         return a.value, b.value, n.value
+
+
+def set_park_pool(nbytes, device=0):
+    """Keep up to nbytes (< 0: no limit, 0: none) of the device memory that
+    parking releases on CUDA device `device`, for the next unpark of a block
+    of the same size (dtmx_set_park_pool)."""
+    L = load()
+    rc = L.dtmx_set_park_pool(int(device), int(nbytes))
+    if rc:
+        raise DtmxError(rc, "dtmx_set_park_pool")
 
 
 def batch_forward_adjoint(sims, nsteps, plane_x, omega, checkpoint_every=100):

@@ -115,6 +115,7 @@ class OutOfCoreSimulation:
         self._park = park or (lambda s: s.park() if hasattr(s, "park") else None)
         self._unpark = unpark or (lambda s: s.unpark() if hasattr(s, "unpark") else None)
         self._pins = None         # per slab, per parity, per side: pinned edge buffers (GPU slabs)
+        self._pool_dev = None     # device whose park pool this run opened
         self._ops = []            # set-up calls, replayed on each slab when it is built
         self._fields = {}         # initial global fields by component
         self._probes = []         # (slab, global id) in each slab's local order
@@ -169,11 +170,16 @@ class OutOfCoreSimulation:
                 s.read_planes(hi - h, h, out=pin[1]) if pl.rank < pl.nslabs - 1 else None)
 
     def _pin_buffers(self, s, pl):
-        """Two pinned float32 buffers per side for a GPU slab's edge planes."""
-        from .engine import Simulation
+        """Two pinned float32 buffers per side for a GPU slab's edge planes;
+        the first GPU slab also lets parking keep device memory for the
+        slabs that follow (released again by close)."""
+        from .engine import Simulation, set_park_pool
         if not isinstance(s, Simulation):
             return None
         import torch
+        if self._pool_dev is None:
+            self._pool_dev = torch.cuda.current_device()
+            set_park_pool(-1, self._pool_dev)
         n = s.plane_state_floats() * pl.halo
         return [[torch.empty(n, dtype=torch.float32).pin_memory().numpy() for _ in range(2)] for _ in range(2)]
 
@@ -312,3 +318,7 @@ class OutOfCoreSimulation:
             if hasattr(s, "close"):
                 s.close()
         self.slabs = None
+        if self._pool_dev is not None:
+            from .engine import set_park_pool
+            set_park_pool(0, self._pool_dev)
+            self._pool_dev = None

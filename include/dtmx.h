@@ -448,6 +448,12 @@ int  dtmx_set_xchunk(dtmx_ctx* ctx, int planes);
  * (dtmaxwell4_b200.window steps a grid larger than the device that way). */
 int  dtmx_park(dtmx_ctx* ctx);
 int  dtmx_unpark(dtmx_ctx* ctx);
+/* Device memory that dtmx_park releases on CUDA device `device` is kept, up to
+ * `bytes` (< 0: no limit; 0, the default: none), for the next dtmx_unpark of a
+ * block of the same size, instead of being returned to the driver; lowering
+ * the limit releases what it no longer holds.  For contexts that take turns
+ * on one device. */
+int  dtmx_set_park_pool(int device, int64_t bytes);
 
 /* The time-stepping state of a run of x planes, handed between contexts of
  * the same y/z configuration (the reference's window hands x slices of its

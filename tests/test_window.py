@@ -214,3 +214,37 @@ def test_gpu_plane_state_layout():
     g.write_planes(19, 4, p)
     g.close()
     o.close()
+
+
+@pytest.mark.gpu
+def test_park_pool_keeps_and_releases_memory():
+    """dtmx_set_park_pool: parked memory stays with the process up to the
+    limit and serves the next unpark; lowering the limit releases it."""
+    import torch
+    from dtmaxwell4_b200 import Simulation, abi, engine
+    dev = torch.cuda.current_device()
+    s = Simulation(abi.make_config(256, 256, 256, pml=8, parkable=True))
+    s.step(2)
+    s.sync()
+    a = np.asarray(s.get_field(abi.EZ)).copy()
+    engine.set_park_pool(-1, dev)
+    try:
+        torch.cuda.synchronize()
+        f0 = torch.cuda.mem_get_info()[0]
+        s.park()
+        f1 = torch.cuda.mem_get_info()[0]
+        assert abs(f1 - f0) < 64 << 20, (f0, f1)           # kept in the pool
+        s.unpark()
+        f2 = torch.cuda.mem_get_info()[0]
+        assert abs(f2 - f0) < 64 << 20, (f0, f2)           # served from the pool
+        assert np.array_equal(s.get_field(abi.EZ), a)
+        s.park()
+        engine.set_park_pool(0, dev)
+        f3 = torch.cuda.mem_get_info()[0]
+        assert f3 - f0 >= 6 * 256 ** 3 * 4, (f0, f3)       # released
+        s.unpark()
+        s.step(1)
+        assert s.check_finite()
+    finally:
+        engine.set_park_pool(0, dev)
+        s.close()
