@@ -689,7 +689,10 @@ def main():
         extras["adjoint"] = run_adjoint(args)
         extras["batched"] = run_batched(args)
         if not args.no_ooc:
-            extras["out_of_core"] = run_out_of_core(args)
+            try:
+                extras["out_of_core"] = run_out_of_core(args)
+            except Exception as e:                 # e.g. pinned host memory refused on this host
+                extras["out_of_core"] = {"error": "%s: %s" % (type(e).__name__, e)}
         if not args.no_gyro:
             extras["gyro_purcell"] = run_gyro_purcell(args)
     if world > 1:
