@@ -71,7 +71,8 @@ class TFSF(C.Structure):
         ("tstop", C.c_double),
         ("ntime", C.c_int),
         ("amp", C.c_double), ("f0", C.c_double), ("tau", C.c_double), ("t0", C.c_double),
-        ("reserved", C.c_double * 4),
+        ("x_origin", C.c_double), ("x_cells", C.c_double),
+        ("reserved", C.c_double * 2),
     ]
 
 

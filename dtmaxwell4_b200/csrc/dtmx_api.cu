@@ -87,6 +87,7 @@ struct dtmx_ctx {
   int has_tfsf = 0;
   dtmx_tfsf tfsf{};
   TfsfDev T{};
+  int line_cap = 0;              // cells of line_e / line_h
   double* line_e = nullptr;
   double* line_h = nullptr;
   int line_src = 0;
@@ -782,21 +783,30 @@ extern "C" int dtmx_set_tfsf(dtmx_ctx* ctx, const dtmx_tfsf* s) {
   if (!ctx || !s || (s->kind != DTMX_TFSF_DIPOLE && s->kind != DTMX_TFSF_PLANE_X)) return fail(ctx, DTMX_ERR_INVALID, "bad TF/SF source");
   if (ctx->prepared) return fail(ctx, DTMX_ERR_STATE, "TF/SF source must be set before the first step");
   const dtmx_config& c = ctx->cfg;
+  // a slab of a larger grid: plane 0 is whole-grid cell xo of gnx
+  const int xo = (int)s->x_origin;
+  const int gnx = s->x_cells > 0 ? (int)s->x_cells : c.nx;
+  if ((double)xo != s->x_origin || (s->x_cells > 0 && (double)gnx != s->x_cells) || xo < 0 || xo + c.nx > gnx ||
+      (c.geometry != DTMX_GEOM_BOX && (xo != 0 || gnx != c.nx)))
+    return fail(ctx, DTMX_ERR_INVALID, "TF/SF x_origin / x_cells do not place this grid inside a whole grid");
   TfsfDev& T = ctx->T;
   T = TfsfDev{};
+  T.xo = xo;
   const double d[3] = {c.dx, c.dy, c.dz};
   const int n[3] = {c.nx, c.ny, c.nz};
   for (int a = 0; a < 3; a++) {
-    sf_range(d[a], s->box_lo[a], s->box_hi[a], 2 * n[a], &T.lo[a], &T.hi[a]);
+    sf_range(d[a], s->box_lo[a], s->box_hi[a], 2 * (a == 0 ? gnx : n[a]), &T.lo[a], &T.hi[a]);
     if (T.lo[a] > T.hi[a]) return fail(ctx, DTMX_ERR_INVALID, "TF/SF box contains no node");
+    if (a == 0) { T.lo[0] -= 2 * xo; T.hi[0] -= 2 * xo; }
     // the correction shell (3 half cells around the surface) must stay inside the
-    // live domain and clear of the absorber
+    // live domain and clear of the absorber (along x: at the grid's uncut ends)
     const int clo = (T.lo[a] - 4) / 2 - 1, chi = (T.hi[a] + 4) / 2 + 1;
     const int alo = c.absorber == DTMX_ABS_NONE ? 0 : ctx->P.ab.L[a][0];
     const int ahi = c.absorber == DTMX_ABS_NONE ? 0 : ctx->P.ab.L[a][1];
     int llo = 0, lhi = n[a] - 1;
     for (int comp = 0; comp < 6; comp++) { llo = std::max(llo, ctx->P.g.live_lo[comp][a]); lhi = std::min(lhi, ctx->P.g.live_hi[comp][a]); }
-    if (clo < std::max(alo, llo) + 1 || chi > std::min(n[a] - 1 - ahi, lhi) - 1)
+    const bool lo_end = a != 0 || xo == 0, hi_end = a != 0 || xo + c.nx == gnx;
+    if ((lo_end && clo < std::max(alo, llo) + 1) || (hi_end && chi > std::min(n[a] - 1 - ahi, lhi) - 1))
       return fail(ctx, DTMX_ERR_INVALID, "TF/SF box too close to the boundary or absorber");
   }
   T.active_cfg = 1;
@@ -854,15 +864,20 @@ extern "C" int dtmx_set_tfsf(dtmx_ctx* ctx, const dtmx_tfsf* s) {
     }
   }
   if (s->kind == DTMX_TFSF_PLANE_X) {
-    T.line_M = 4096;
-    T.line_n = c.nx + 2 * T.line_M;
+    // the 1-D line spans the whole grid with 4096 cells beyond each end; plane 0
+    // of this grid reads line cell xo + 4096, the source sits 10 cells before
+    // the box's lower x face
+    constexpr int kLinePad = 4096;
+    T.line_M = kLinePad + xo;
+    T.line_n = gnx + 2 * kLinePad;
     int rc;
-    if (!ctx->line_e) {
+    if (ctx->line_cap < T.line_n) {
       if ((rc = dalloc(ctx, &ctx->line_e, T.line_n))) return rc;
       if ((rc = dalloc(ctx, &ctx->line_h, T.line_n))) return rc;
+      ctx->line_cap = T.line_n;
     }
     T.line_e = ctx->line_e; T.line_h = ctx->line_h;
-    ctx->line_src = (T.lo[0] - 1) / 2 - 10 + T.line_M;
+    ctx->line_src = (T.lo[0] + 2 * xo - 1) / 2 - 10 + kLinePad;
   }
   ctx->tfsf = *s;
   ctx->has_tfsf = 1;
@@ -2410,8 +2425,9 @@ static int plane_refusal(dtmx_ctx* ctx) {
   if (ctx->parked) return fail(ctx, DTMX_ERR_STATE, "the context is parked (dtmx_unpark first)");
   if (ctx->cfg.geometry != DTMX_GEOM_BOX || ctx->cfg.absorber == DTMX_ABS_SPLIT_PML)
     return fail(ctx, DTMX_ERR_UNSUPPORTED, "plane state: box geometry with a CPML or no absorber only");
-  if (ctx->has_gyro || ctx->has_tfsf || ctx->P.des_on)
-    return fail(ctx, DTMX_ERR_UNSUPPORTED, "plane state: gyrotropic materials, TF/SF and design regions are not per plane");
+  // (a TF/SF line is not per plane either, but every slab integrates the same one)
+  if (ctx->has_gyro || ctx->P.des_on)
+    return fail(ctx, DTMX_ERR_UNSUPPORTED, "plane state: gyrotropic materials and design regions are not per plane");
   return DTMX_OK;
 }
 

@@ -19,7 +19,8 @@ struct TfsfDev {
   int active_cfg;            // a TF/SF source is configured
   int kind;                  // 0 dipole, 1 plane +x
   int lo[3], hi[3];          // inside-box half-coordinate ranges (inclusive)
-  double ctr[3];             // dipole position (box centre, physical)
+  double ctr[3];             // dipole position (box centre, physical, whole-grid coordinates)
+  int xo;                    // whole-grid cell index of plane 0 (x slabs; 0 for a whole grid)
   double hd[3];              // half cell sizes dx/2, dy/2, dz/2
   double dt, c, w, kenv, tstop;
   int ntime;
@@ -41,7 +42,7 @@ __device__ __forceinline__ bool in_box(const TfsfDev& t, int X, int Y, int Z) {
 // Field of a z-oriented Hertzian dipole with a Hann-windowed sine moment,
 // reference DipoleTFSF (signal.hpp:51-97), evaluated in double precision.
 __device__ double dipole_field(const TfsfDev& t, int comp, int X, int Y, int Z, double tt) {
-  const double nx = X * t.hd[0] - t.ctr[0], ny = Y * t.hd[1] - t.ctr[1], nz = Z * t.hd[2] - t.ctr[2];
+  const double nx = (X + 2 * t.xo) * t.hd[0] - t.ctr[0], ny = Y * t.hd[1] - t.ctr[1], nz = Z * t.hd[2] - t.ctr[2];
   const double R = sqrt(nx * nx + ny * ny + nz * nz);
   const double time = tt * t.dt, c = t.c, w = t.w, ke = t.kenv;
   const double ph = w * time - w / c * R;

@@ -26,11 +26,13 @@ stream; gloo on the host).  No collective is issued inside a step.
 The CPML slabs of the x faces belong to the first and last ranks (each must
 own more planes than its slab, so that no ghost plane lies in one); the y
 and z slabs are the same on every rank.
-Sources and probes act on the rank that owns their plane; DFT planes normal
-to x are recorded by their owner, planes normal to y or z by every rank over
-its owned rows.  Refused (DTMX_ERR_UNSUPPORTED semantics, raised as
-ValueError): order 4 (its stencil needs more ghost planes), TF/SF sources,
-gyrotropic materials (their current couples x neighbours) and design regions.
+Sources and probes act on the rank that owns their plane; a TF/SF source on
+every rank, with its box and plane-wave line in whole-grid coordinates
+(dtmx_tfsf.x_origin); DFT planes normal to x are recorded by their owner,
+planes normal to y or z by every rank over its owned rows.  Refused
+(DTMX_ERR_UNSUPPORTED semantics, raised as ValueError): order 4 (its stencil
+needs more ghost planes), gyrotropic materials (their current couples x
+neighbours) and design regions.
 """
 import ctypes as C
 
@@ -161,7 +163,12 @@ class ShardedSimulation:
             self.local.add_point_source(s)
 
     def set_tfsf(self, t):
-        raise ValueError("slab sharding does not carry TF/SF sources")
+        """The whole grid's TF/SF source (box in whole-grid coordinates), taken
+        by every rank with its slab's x origin (dtmx_tfsf.x_origin)."""
+        q = abi.TFSF()
+        C.memmove(C.byref(q), C.byref(t), C.sizeof(abi.TFSF))
+        q.x_origin, q.x_cells = float(self.plan.lx0), float(self.gcfg.nx)
+        self.local.set_tfsf(q)
 
     def set_design(self, lo, eps):
         raise ValueError("slab sharding does not carry design regions")

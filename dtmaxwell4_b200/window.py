@@ -20,15 +20,17 @@ from the second ghost plane inward still equal the single-domain run's, bit
 for bit -- the owned planes and one plane beyond them at every step of the
 turn (which probes and DFT planes of the owned planes may read).  Point
 sources act in every slab whose local grid holds them, ghost planes
-included; probes and DFT planes in the slab that owns their plane.
+included, and a TF/SF source in every slab (its box and its plane wave's 1-D
+line in whole-grid coordinates, dtmx_tfsf.x_origin); probes and DFT planes in
+the slab that owns their plane.
 
 Only `resident` slabs' state is on the device at a time (one by default), so
 the grid may be as large as host memory allows; a turn moves the slab's state
 across the host link twice, once per K time steps (the reference's cadence is
 Ntime = NS - 3).
-Restrictions: order 2, box geometry with a CPML or no absorber, no TF/SF
-source, gyrotropic material or design region, and ghost planes outside the
-x absorber slabs.
+Restrictions: order 2, box geometry with a CPML or no absorber, no
+gyrotropic material or design region, and ghost planes outside the x
+absorber slabs.
 """
 import ctypes as C
 
@@ -136,7 +138,10 @@ class OutOfCoreSimulation:
         self._ops.append(("src", src))
 
     def set_tfsf(self, t):
-        raise ValueError("out-of-core slabs do not carry TF/SF sources")
+        """The TF/SF source of the whole grid (box in whole-grid coordinates):
+        every slab takes it with its x origin, so the plane wave's 1-D line
+        and the dipole's position are the whole grid's."""
+        self._ops.append(("tfsf", t))
 
     def set_design(self, lo, eps):
         raise ValueError("out-of-core slabs do not carry design regions")
@@ -194,6 +199,11 @@ class OutOfCoreSimulation:
                     table, ix, iy, iz = v
                     s.set_materials(table, *[None if q is None else np.ascontiguousarray(np.asarray(q, np.uint8)[a:b])
                                              for q in (ix, iy, iz)])
+                elif kind == "tfsf":
+                    q = abi.TFSF()
+                    C.memmove(C.byref(q), C.byref(v), C.sizeof(abi.TFSF))
+                    q.x_origin, q.x_cells = float(pl.lx0), float(self.gcfg.nx)
+                    s.set_tfsf(q)
                 elif kind == "src" and pl.holds(v.i):
                     q = abi.PointSource()
                     C.memmove(C.byref(q), C.byref(v), C.sizeof(abi.PointSource))

@@ -164,7 +164,15 @@ typedef struct dtmx_tfsf {
   /* Plane wave (kind DTMX_TFSF_PLANE_X): Ez_inc(x,t) from a 1-D line driven by
    * amp*sin(2*pi*f0*(t-t0))*exp(-((t-t0)/tau)^2) at the line's left end. */
   double amp, f0, tau, t0;
-  double reserved[4];
+  /* Slab of a larger grid (x slabs of dtmaxwell4_b200.window): x_origin is
+   * the whole grid's cell index of this grid's plane 0 and x_cells the whole
+   * grid's cells along x (both 0 for a whole grid).  box_lo/box_hi stay in
+   * the whole grid's coordinates: the dipole sits at its global position and
+   * the plane wave's 1-D line spans the whole grid, so every slab integrates
+   * the same line.  Box faces outside this grid are left to the slabs that
+   * hold them; the boundary checks apply to the grid's uncut x ends only. */
+  double x_origin, x_cells;
+  double reserved[2];
 } dtmx_tfsf;
 
 /* ---- probes ---------------------------------------------------------------- */

@@ -105,6 +105,7 @@ typedef struct {
   dtmx_point_source psrc[64]; int npsrc;
   int has_tfsf; dtmx_tfsf tfsf;
   int sf_lo[3], sf_hi[3];       /* inclusive half-coordinate range inside the box */
+  int sf_xo;                    /* whole-grid cell index of plane 0 (x slabs) */
   int line_M, line_n; double* line_e; double* line_h; int line_src;
   /* monitors */
   probe_t probes[4096]; int nprobes;
@@ -321,7 +322,7 @@ static int in_sf(const osim* s, int X, int Y, int Z) {
 /* reference DipoleTFSF (signal.hpp:51-97), evaluated in double */
 static double dipole_inc(const osim* s, int comp, int X, int Y, int Z, double tt) {
   const dtmx_tfsf* p = &s->tfsf;
-  double x = X * 0.5 * s->cfg.dx, y = Y * 0.5 * s->cfg.dy, z = Z * 0.5 * s->cfg.dz;
+  double x = (X + 2 * s->sf_xo) * 0.5 * s->cfg.dx, y = Y * 0.5 * s->cfg.dy, z = Z * 0.5 * s->cfg.dz;
   double t = tt * s->cfg.dt;
   double xd = (p->box_lo[0] + p->box_hi[0]) * 0.5, yd = (p->box_lo[1] + p->box_hi[1]) * 0.5,
          zd = (p->box_lo[2] + p->box_hi[2]) * 0.5;
@@ -808,16 +809,23 @@ int PFX(add_point_source)(void* h, const dtmx_point_source* p) {
 
 int PFX(set_tfsf)(void* h, const dtmx_tfsf* p) {
   osim* s = h;
+  /* a slab of a larger grid (dtmx.h, dtmx_tfsf.x_origin / x_cells): box and
+   * line in whole-grid coordinates, half-coordinate ranges shifted to this grid */
+  int xo = (int)p->x_origin, gnx = p->x_cells > 0 ? (int)p->x_cells : s->nx;
+  if ((double)xo != p->x_origin || xo < 0 || xo + s->nx > gnx) return DTMX_ERR_INVALID;
   s->tfsf = *p; s->has_tfsf = 1;
+  s->sf_xo = xo;
   double d[3] = {s->cfg.dx, s->cfg.dy, s->cfg.dz};
-  for (int a = 0; a < 3; a++) sf_range(d[a], p->box_lo[a], p->box_hi[a], half_max(s, a), &s->sf_lo[a], &s->sf_hi[a]);
+  for (int a = 0; a < 3; a++)
+    sf_range(d[a], p->box_lo[a], p->box_hi[a], a == 0 ? 2 * gnx : half_max(s, a), &s->sf_lo[a], &s->sf_hi[a]);
+  s->sf_lo[0] -= 2 * xo; s->sf_hi[0] -= 2 * xo;
   if (p->kind == DTMX_TFSF_PLANE_X) {
-    s->line_M = 4096;
-    s->line_n = s->nx + 2 * s->line_M;
+    s->line_M = 4096 + xo;
+    s->line_n = gnx + 2 * 4096;
     free(s->line_e); free(s->line_h);
     s->line_e = calloc(s->line_n, sizeof(double)); s->line_h = calloc(s->line_n, sizeof(double));
     /* source point 10 cells before the box's lower x face */
-    s->line_src = (s->sf_lo[0] - 1) / 2 - 10 + s->line_M;
+    s->line_src = (s->sf_lo[0] + 2 * xo - 1) / 2 - 10 + 4096;
   }
   return DTMX_OK;
 }
@@ -953,7 +961,7 @@ size_t PFX(plane_state_floats)(void* h) {
 
 static int plane_copy(osim* s, int x0, int np, double* buf, int rd) {
   if (x0 < 0 || np < 0 || x0 + np > s->nx) return DTMX_ERR_INVALID;
-  if (s->has_gyro || s->has_tfsf || s->des_on || s->cfg.geometry != DTMX_GEOM_BOX) return DTMX_ERR_UNSUPPORTED;
+  if (s->has_gyro || s->des_on || s->cfg.geometry != DTMX_GEOM_BOX) return DTMX_ERR_UNSUPPORTED;
   if (s->aux[0][0] && np > 0 && (x0 < s->L[0][0] || x0 + np > s->nx - s->L[0][1])) return DTMX_ERR_UNSUPPORTED;
   size_t nyz = (size_t)s->ny * s->nz;
   double* b = buf;

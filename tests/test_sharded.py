@@ -2,7 +2,8 @@
 2 and 3 over gloo, each rank stepping its slab with the FP32 oracle as the
 local engine and exchanging E planes with its neighbours every step, against
 one single-domain FP32 oracle run of the whole grid: fields, probe traces and
-DFT planes (normal to x and to y) bit for bit.  The partition rules and the
+DFT planes (normal to x and to y) bit for bit, with point sources and with a
+plane-wave TF/SF source.  The partition rules and the
 refused configurations are checked without processes."""
 import os
 import socket
@@ -58,14 +59,16 @@ class _OraclePlanes:
 
     def recv(self, comp, i):
         import torch
-        buf = torch.empty(NY * NZ, dtype=torch.float64)
+        ny, nz = self.sim.shape[1:]
+        buf = torch.empty(ny * nz, dtype=torch.float64)
         self.pending.append((comp, i, buf))
         return buf
 
     def commit(self):
+        ny, nz = self.sim.shape[1:]
         for comp, i, buf in self.pending:
             a = self.sim.get_field(comp)
-            a[i] = buf.numpy().reshape(NY, NZ)
+            a[i] = buf.numpy().reshape(ny, nz)
             self.sim.set_field(comp, a)
         self.pending = []
 
@@ -94,6 +97,41 @@ def _rank_main(rank, world, port, out_dir):
         dist.destroy_process_group()
 
 
+def _rank_main_tfsf(rank, world, port, out_dir):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for p in (root, os.path.join(root, "oracle")):
+        sys.path.insert(0, p)
+    import torch.distributed as dist
+    import pyoracle
+    from dtmaxwell4_b200 import scenarios
+    from dtmaxwell4_b200.sharded import ShardedSimulation
+    os.environ["OMP_NUM_THREADS"] = "1"
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=rank, world_size=world)
+    try:
+        sc = _tfsf_plane()
+        s = ShardedSimulation(sc["cfg"], make_local=lambda c: pyoracle.OracleSim(c, "f32"), planes=_OraclePlanes)
+        ids = scenarios.apply(s, sc)
+        s.step(TFSF_STEPS)
+        res = dict(fields=np.stack([s.get_field(c) for c in range(6)]), dft=s.read_dft(ids[0]))
+        if rank == 0:
+            np.savez(os.path.join(out_dir, "t%d.npz" % world), **res)
+        s.close()
+    finally:
+        dist.destroy_process_group()
+
+
+TFSF_STEPS = 60
+
+
+def _tfsf_plane():
+    """Plane-wave TF/SF Drude sphere, 40 cells along x (box faces near x = 12
+    and 28), x-normal DFT plane."""
+    from dtmaxwell4_b200 import scenarios
+    return scenarios.drude_sphere_tfsf(n=(40, 36, 40), steps=TFSF_STEPS, pml=6, inset=6, radius=4, lambda0=10.0,
+                                       nfreq=2)
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -118,6 +156,28 @@ def test_sharded_equals_single_domain(world, tmp_path):
     assert np.array_equal(got["probes"], o.read_probes(STEPS + 8))
     assert np.array_equal(got["dft0"], o.read_dft(d0))
     assert np.array_equal(got["dft1"], o.read_dft(d1))
+    o.close()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_tfsf_equals_single_domain(world, tmp_path):
+    """A plane-wave TF/SF source across the ranks' slab faces: every rank
+    takes the whole grid's box and 1-D line; bit for bit with one domain."""
+    import torch.multiprocessing as mp
+    import pyoracle
+    from dtmaxwell4_b200 import scenarios
+    pyoracle.lib()
+    mp.start_processes(_rank_main_tfsf, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    got = np.load(os.path.join(str(tmp_path), "t%d.npz" % world))
+    sc = _tfsf_plane()
+    o = pyoracle.OracleSim(sc["cfg"], "f32")
+    ids = scenarios.apply(o, sc)
+    o.step(TFSF_STEPS)
+    want = np.stack([o.get_field(c) for c in range(6)])
+    assert np.abs(want).max() > 1e-4                  # the pulse's leading edge has entered the box
+    assert np.array_equal(got["fields"], want)
+    assert np.array_equal(got["dft"], o.read_dft(ids[0]))
     o.close()
 
 

@@ -63,8 +63,6 @@ def test_window_refusals():
     cfg = _scenario()[0]
     w = OutOfCoreSimulation(cfg, 2, make_local=lambda c: None)
     with pytest.raises(ValueError):
-        w.set_tfsf(None)
-    with pytest.raises(ValueError):
         w.set_design((0, 0, 0), None)
     with pytest.raises(ValueError):
         w.add_dft_plane(1, 3, 1, [0.5])
@@ -248,3 +246,100 @@ def test_park_pool_keeps_and_releases_memory():
     finally:
         engine.set_park_pool(0, dev)
         s.close()
+
+
+def _tfsf_scenario(kind):
+    """A plane-wave TF/SF Drude sphere with an x-normal DFT plane, or a
+    dipole TF/SF box over a dielectric layer; 40-48 cells along x, 6-cell CPML."""
+    from dtmaxwell4_b200 import abi, scenarios
+    if kind == "plane":
+        sc = scenarios.drude_sphere_tfsf(n=(40, 36, 40), steps=70, pml=6, inset=6, radius=4, lambda0=10.0, nfreq=2)
+        sc["probes"] = [(abi.EZ, 20, 18, 16, abi.PROBE_NODE), (abi.HY, 13, 17, 15, abi.PROBE_NODE),
+                        (abi.EZ, 29, 18, 16, abi.PROBE_NODE)]
+        return sc, 70
+    cfg = abi.make_config(48, 45, 40, dx=1.0, courant=0.5, order=2, pml=6, probe_capacity=100)
+    t = abi.TFSF()
+    t.kind = abi.TFSF_DIPOLE
+    t.box_lo[:] = [18.3, 17.4, 15.2]
+    t.box_hi[:] = [28.6, 27.9, 24.7]
+    t.c, t.w, t.kenv, t.tstop, t.ntime = 1.0, 2 * np.pi / 10, 0.3, 0.0, 1
+    layer = np.zeros((48, 45, 40), np.uint8)
+    layer[:, :, :10] = 1
+    sc = dict(cfg=cfg, materials=([abi.make_material(1.0), abi.make_material(2.25)], [layer] * 3), tfsf=t,
+              probes=[(abi.EZ, 23, 22, 20, abi.PROBE_NODE), (abi.HX, 30, 22, 12, abi.PROBE_NODE)],
+              dft=[(0, 33, (1 << abi.EZ) | (1 << abi.HY), [0.5])], point_sources=[])
+    return sc, 60
+
+
+@pytest.mark.parametrize("kind,K,resident", [("plane", 3, 1), ("plane", 2, 2), ("dipole", 3, 2)])
+def test_window_tfsf_equals_single_domain(kind, K, resident):
+    """TF/SF sources across slab faces (the box's x faces fall in owned and
+    ghost planes of different slabs): bit for bit with one domain."""
+    import pyoracle
+    from dtmaxwell4_b200 import scenarios
+    from dtmaxwell4_b200.window import OutOfCoreSimulation
+    sc, steps = _tfsf_scenario(kind)
+    w = OutOfCoreSimulation(sc["cfg"], 3, steps_per_turn=K, make_local=lambda c: pyoracle.OracleSim(c, "f32"),
+                            resident=resident)
+    dw = scenarios.apply(w, sc)
+    w.step(steps)
+    o = pyoracle.OracleSim(sc["cfg"], "f32")
+    do = scenarios.apply(o, sc)
+    o.step(steps)
+    for c in range(6):
+        want = o.get_field(c)
+        assert np.array_equal(w.get_field(c), want), c
+    assert np.abs(o.get_field(2)).max() > 1e-4
+    assert np.array_equal(w.read_probes(), o.read_probes(100000))
+    for a, b in zip(dw, do):
+        assert np.array_equal(w.read_dft(a), o.read_dft(b))
+    o.close()
+    w.close()
+
+
+def test_tfsf_x_origin_checks():
+    """A slab takes the whole grid's TF/SF box; bad origins are refused, and
+    the boundary check applies at the grid's uncut x ends only."""
+    import pyoracle
+    from dtmaxwell4_b200 import abi
+    sc, _ = _tfsf_scenario("dipole")
+    t = sc["tfsf"]
+    lc = abi.make_config(20, 45, 40, dx=1.0, courant=0.5, order=2, pml=((0, 0), (6, 6), (6, 6)))
+    o = pyoracle.OracleSim(lc, "f32")
+    q = abi.TFSF()
+    C = __import__("ctypes")
+    C.memmove(C.byref(q), C.byref(t), C.sizeof(abi.TFSF))
+    q.x_origin, q.x_cells = 40.0, 48.0                # 40 + 20 > 48
+    assert o._f("set_tfsf")(o._h, C.byref(q)) != 0
+    q.x_origin = 14.5
+    assert o._f("set_tfsf")(o._h, C.byref(q)) != 0
+    q.x_origin = 14.0
+    assert o._f("set_tfsf")(o._h, C.byref(q)) == 0
+    o.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind,engine", [("plane", 3), ("plane", 1), ("dipole", 3)])
+def test_window_tfsf_equals_in_core_run(kind, engine):
+    from dtmaxwell4_b200 import Simulation, abi, scenarios
+    from dtmaxwell4_b200.window import OutOfCoreSimulation, parkable_simulation
+    sc, steps = _tfsf_scenario(kind)
+
+    def make(c):
+        s = parkable_simulation(c)
+        s.set_engine(engine, 0)
+        return s
+    w = OutOfCoreSimulation(sc["cfg"], 3, steps_per_turn=3, make_local=make, resident=2)
+    b = Simulation(sc["cfg"])
+    b.set_engine(engine, 0)
+    dw, db = scenarios.apply(w, sc), scenarios.apply(b, sc)
+    w.step(steps)
+    b.step(steps)
+    for c in range(6):
+        assert np.array_equal(w.get_field(c), b.get_field(c)), c
+    assert np.abs(b.get_field(abi.EZ)).max() > 1e-4
+    assert np.array_equal(w.read_probes(), b.read_probes().astype(np.float64))
+    for x, y in zip(dw, db):
+        assert np.array_equal(w.read_dft(x), b.read_dft(y))
+    w.close()
+    b.close()
