@@ -57,6 +57,27 @@ def test_window_equals_single_domain(nslabs, K, resident):
     w.close()
 
 
+def test_window_single_slab_and_short_turns():
+    """One slab (no ghost planes) and a run shorter than one turn are the
+    single-domain run."""
+    import pyoracle
+    from dtmaxwell4_b200.window import OutOfCoreSimulation
+    cfg, mats, idx, src, probes, fields = _scenario()
+    o = pyoracle.OracleSim(cfg, "f32")
+    _apply(o, mats, idx, src, probes, fields)
+    o.step(7)
+    for nslabs, K in ((1, 4), (2, 8)):
+        w = OutOfCoreSimulation(cfg, nslabs, steps_per_turn=K, make_local=lambda c: pyoracle.OracleSim(c, "f32"))
+        _apply(w, mats, idx, src, probes, fields)
+        w.step(3)
+        w.step(4)
+        assert w.turns == 2                           # one turn per call: 3 and 4 steps
+        for c in range(6):
+            assert np.array_equal(w.get_field(c), o.get_field(c)), (nslabs, K, c)
+        w.close()
+    o.close()
+
+
 def test_window_refusals():
     from dtmaxwell4_b200 import abi
     from dtmaxwell4_b200.window import OutOfCoreSimulation
