@@ -21,8 +21,9 @@ for bit -- the owned planes and one plane beyond them at every step of the
 turn (which probes and DFT planes of the owned planes may read).  Point
 sources act in every slab whose local grid holds them, ghost planes
 included, and a TF/SF source in every slab (its box and its plane wave's 1-D
-line in whole-grid coordinates, dtmx_tfsf.x_origin); probes and DFT planes in
-the slab that owns their plane.
+line in whole-grid coordinates, dtmx_tfsf.x_origin); probes and x-normal DFT
+planes in the slab that owns their plane, y- and z-normal DFT planes in every
+slab over its own rows.
 
 Only `resident` slabs' state is on the device at a time (one by default), so
 the grid may be as large as host memory allows; a turn moves the slab's state
@@ -153,11 +154,12 @@ class OutOfCoreSimulation:
         return gid
 
     def add_dft_plane(self, axis, index, comp_mask, omegas):
-        if axis != 0:
-            raise ValueError("out-of-core slabs record DFT planes normal to x")
+        """A DFT plane of the whole grid: normal to x, recorded by the slab
+        that owns it; normal to y or z, recorded by every slab over its local
+        rows and read back as the owned rows of each."""
         did = len(self._dfts)
         self._dfts.append(None)
-        self._ops.append(("dft", (did, index, comp_mask, omegas)))
+        self._ops.append(("dft", (did, axis, index, comp_mask, omegas)))
         return did
 
     def set_field(self, comp, arr):
@@ -213,9 +215,14 @@ class OutOfCoreSimulation:
                     gid, comp, i, j, k, mode = v
                     s.add_probe(comp, pl.local(i), j, k, mode)
                     self._probes.append((r, gid))
-                elif kind == "dft" and pl.owns(v[1]):
-                    did, index, mask, om = v
-                    self._dfts[did] = (r, s.add_dft_plane(0, pl.local(index), mask, om))
+                elif kind == "dft":
+                    did, axis, index, mask, om = v
+                    if axis == 0 and pl.owns(index):
+                        self._dfts[did] = (0, r, s.add_dft_plane(0, pl.local(index), mask, om))
+                    elif axis != 0:
+                        if self._dfts[did] is None:
+                            self._dfts[did] = (axis, [None] * len(self.plans))
+                        self._dfts[did][1][r] = s.add_dft_plane(axis, index, mask, om)
             for comp, arr in self._fields.items():
                 s.set_field(comp, np.ascontiguousarray(arr[a:b]))
             pins = self._pin_buffers(s, pl)
@@ -313,12 +320,22 @@ class OutOfCoreSimulation:
         return res
 
     def read_dft(self, did):
-        r, ld = self._dfts[did]
-        s = self.slabs[r]
-        self._unpark(s)
-        out = s.read_dft(ld)
-        self._park(s)
-        return out
+        d = self._dfts[did]
+        if d[0] == 0:
+            _, r, ld = d
+            s = self.slabs[r]
+            self._unpark(s)
+            out = s.read_dft(ld)
+            self._park(s)
+            return out
+        # normal to y or z: the plane's first in-plane axis is x; keep each slab's owned rows
+        parts = []
+        for s, pl, ld in zip(self.slabs, self.plans, d[1]):
+            self._unpark(s)
+            lo, hi = pl.owned_local()
+            parts.append(np.asarray(s.read_dft(ld))[:, :, lo:hi].copy())
+            self._park(s)
+        return np.concatenate(parts, axis=2)
 
     def close(self):
         if self._pool is not None:

@@ -7,6 +7,7 @@ is a no-op there) against one single-domain FP32 oracle run -- fields, probe
 traces and an x-normal DFT plane bit for bit, for 2 and 3 slabs and 1 to 5
 time steps per turn (a Drude block crosses a slab face, the dipole sits in a
 neighbour's ghost planes).
+DFT planes normal to x (one owner) and to y (every slab's own rows).
 GPU: dtmx_park / dtmx_unpark keep the state bit for bit and free the device
 memory while parked, a parked context refuses its calls, dtmx_read_planes /
 dtmx_write_planes round-trip and match the oracle's layout, and a 3-slab
@@ -26,9 +27,10 @@ def _apply(sim, mats, idx, src, probes, fields):
     for (c, i, j, k) in probes:
         sim.add_probe(c, i, j, k)
     d0 = sim.add_dft_plane(0, 16, (1 << abi.EY) | (1 << abi.HZ), [0.5, 0.8])
+    d1 = sim.add_dft_plane(1, 9, (1 << abi.EX) | (1 << abi.HX), [0.5, 0.8])
     for c in range(6):
         sim.set_field(c, fields[c])
-    return d0
+    return d0, d1
 
 
 @pytest.mark.parametrize("nslabs,K,resident", [(2, 4, 1), (3, 1, 1), (3, 5, 2)])
@@ -52,7 +54,8 @@ def test_window_equals_single_domain(nslabs, K, resident):
         assert np.abs(want).max() > 1e-4
         assert np.array_equal(w.get_field(c), want), c
     assert np.array_equal(w.read_probes(), o.read_probes(STEPS + 8))
-    assert np.array_equal(w.read_dft(d0), o.read_dft(do))
+    for a, b in zip(d0, do):                          # x-normal (owner) and y-normal (every slab's rows)
+        assert np.array_equal(w.read_dft(a), o.read_dft(b))
     o.close()
     w.close()
 
@@ -85,8 +88,6 @@ def test_window_refusals():
     w = OutOfCoreSimulation(cfg, 2, make_local=lambda c: None)
     with pytest.raises(ValueError):
         w.set_design((0, 0, 0), None)
-    with pytest.raises(ValueError):
-        w.add_dft_plane(1, 3, 1, [0.5])
     gyro = abi.make_material(1.0, eps_inf=1.0, gyro=(0.3, 0.01, 0.2))
     with pytest.raises(ValueError):
         w.set_materials([gyro], np.zeros((NX, NY, NZ), np.uint8))
@@ -152,7 +153,8 @@ def test_park_round_trip_frees_device_memory():
     for c in range(6):
         assert np.array_equal(a.get_field(c), b.get_field(c)), c
     assert np.array_equal(a.read_probes(), b.read_probes())
-    assert np.array_equal(a.read_dft(da), b.read_dft(db))
+    for x, y in zip(da, db):
+        assert np.array_equal(a.read_dft(x), b.read_dft(y))
     with pytest.raises(DtmxError):
         b.park()                                        # not created parkable
     a.close()
@@ -198,7 +200,8 @@ def test_window_equals_in_core_run(engine, resident):
         assert np.abs(want).max() > 1e-4
         assert np.array_equal(w.get_field(c), want), c
     assert np.array_equal(w.read_probes(), b.read_probes().astype(np.float64))
-    assert np.array_equal(w.read_dft(dw), b.read_dft(db))
+    for x, y in zip(dw, db):
+        assert np.array_equal(w.read_dft(x), b.read_dft(y))
     w.close()
     b.close()
 
