@@ -463,15 +463,15 @@ def run_out_of_core(args):
 
 def run_out_of_core_headline(args):
     """The headline workload (384^3 Drude sphere, plane-wave TF/SF, 16-frequency
-    DFT plane) stepped out of core: 4 x slabs parked in host memory, 32 steps
-    per turn, one resident (at this size concurrent turns measured slower),
-    against the same run in core; fields and DFT compared bit for bit.  Wall
-    clock around the public-API calls."""
+    DFT plane) stepped out of core: 2 x slabs parked in host memory, 64 steps
+    per turn, one resident (at this size more slabs and concurrent turns
+    measured slower), against the same run in core; fields and DFT compared
+    bit for bit.  Wall clock around the public-API calls."""
     import numpy as np
     import torch
     from dtmaxwell4_b200 import Simulation, scenarios
     from dtmaxwell4_b200.window import OutOfCoreSimulation, parkable_simulation
-    K, steps, nsl = 32, 128, 4
+    K, steps, nsl = 64, 128, 2
     sc = scenarios.drude_sphere_tfsf(n=args.n, steps=K + steps)
     cells = args.n ** 3
 
