@@ -278,6 +278,9 @@ class OutOfCoreSimulation:
         if self._pool is None:
             from concurrent.futures import ThreadPoolExecutor
             self._pool = ThreadPoolExecutor(max_workers=self.resident)
+        # Turns are submitted in (turn, slab) order and the pool's threads take
+        # them first in, first out, so every turn a thread waits for was taken
+        # by a thread before it: the earliest unfinished turn always runs.
         futs = {}
         for q, k in enumerate(ks):
             t = t0 + q
