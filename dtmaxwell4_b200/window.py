@@ -11,8 +11,11 @@ a neighbour.  One turn of slab r at time n:
 
   unpark; write the neighbours' edge planes of time n into the ghost planes
   (the full plane state: fields, y/z CPML auxiliaries, ADE currents --
-  dtmx_write_planes); step k <= K times; read the slab's own first and last
-  K + 1 owned planes (dtmx_read_planes); park.
+  dtmx_write_planes); read its own last K + 1 owned planes (time n, for slab
+  r + 1 later in the same sweep, dtmx_read_planes); step k <= K times; read
+  its own first K + 1 owned planes (time n + k, for slab r - 1 in the next
+  sweep); park.  The slabs take their turns in order, so each edge needs one
+  host buffer.
 
 Why it is exact: a local order-2 step is wrong only next to the local grid's
 faces (one plane at each cut face per step), so after k <= K steps the planes
@@ -102,8 +105,8 @@ class OutOfCoreSimulation:
     Simulation); it must offer read_planes / write_planes.  park(local) /
     unpark(local) move it off and onto the device (defaults: its park /
     unpark methods where it has them, else nothing).  Edge planes of GPU
-    slabs pass through pinned host buffers (two per side, alternating
-    between sweeps), so their copies run at the host link's rate.
+    slabs pass through pinned host buffers (one per side), so their copies
+    run at the host link's rate.
     """
 
     def __init__(self, cfg, nslabs, steps_per_turn=8, make_local=None, park=None, unpark=None, resident=1):
@@ -117,7 +120,7 @@ class OutOfCoreSimulation:
         self._make = make_local or parkable_simulation
         self._park = park or (lambda s: s.park() if hasattr(s, "park") else None)
         self._unpark = unpark or (lambda s: s.unpark() if hasattr(s, "unpark") else None)
-        self._pins = None         # per slab, per parity, per side: pinned edge buffers (GPU slabs)
+        self._pins = None         # per slab: pinned buffers of its upper and lower edge planes (GPU slabs)
         self._pool_dev = None     # device whose park pool this run opened
         self._ops = []            # set-up calls, replayed on each slab when it is built
         self._fields = {}         # initial global fields by component
@@ -125,7 +128,7 @@ class OutOfCoreSimulation:
         self._nprobes = 0
         self._dfts = []           # (slab, local id)
         self.slabs = None
-        self._edges = None        # [turn parity][slab]: state of its first and last halo owned planes
+        self._up = self._down = None   # per slab: its upper / lower owned halo planes (see _read_upper)
         self.turns = 0
 
     # ---- set-up (recorded)
@@ -168,16 +171,23 @@ class OutOfCoreSimulation:
         self._fields[comp] = np.asarray(arr, dtype=np.float32)
 
     # ---- slabs
-    def _read_edges(self, s, pl, parity):
+    # Edge planes: U[r], slab r's upper owned halo planes, read at the start of
+    # its turn (time n, before it steps) for slab r + 1's lower ghosts in the
+    # same sweep; D[r], its lower owned halo planes, read at the end of its
+    # turn (time n + k) for slab r - 1's upper ghosts in the next sweep.  One
+    # buffer per side: turn t of slab r runs after turn t of slab r - 1 (U[r-1]
+    # of this sweep) and after turn t - 1 of slab r + 1 (D[r+1] of the last),
+    # which also keeps every buffer until its reader is done.
+    def _read_upper(self, s, pl):
         lo, hi = pl.owned_local()
-        h = pl.halo
-        pins = self._pins[pl.rank] if self._pins else None
-        pin = pins[parity] if pins else (None, None)
-        return (s.read_planes(lo, h, out=pin[0]) if pl.rank > 0 else None,
-                s.read_planes(hi - h, h, out=pin[1]) if pl.rank < pl.nslabs - 1 else None)
+        return s.read_planes(hi - pl.halo, pl.halo, out=self._pins[pl.rank][0] if self._pins else None)
+
+    def _read_lower(self, s, pl):
+        lo, hi = pl.owned_local()
+        return s.read_planes(lo, pl.halo, out=self._pins[pl.rank][1] if self._pins else None)
 
     def _pin_buffers(self, s, pl):
-        """Two pinned float32 buffers per side for a GPU slab's edge planes;
+        """One pinned float32 buffer per side for a GPU slab's edge planes;
         the first GPU slab also lets parking keep device memory for the
         slabs that follow (released again by close)."""
         from .engine import Simulation, set_park_pool
@@ -188,11 +198,12 @@ class OutOfCoreSimulation:
             self._pool_dev = torch.cuda.current_device()
             set_park_pool(-1, self._pool_dev)
         n = s.plane_state_floats() * pl.halo
-        return [[torch.empty(n, dtype=torch.float32).pin_memory().numpy() for _ in range(2)] for _ in range(2)]
+        return [torch.empty(n, dtype=torch.float32).pin_memory().numpy() for _ in range(2)]
 
     def _build(self):
         self.slabs = []
-        self._edges = [[None] * len(self.plans), [None] * len(self.plans)]   # by turn parity
+        S = len(self.plans)
+        self._up, self._down = [None] * S, [None] * S
         for r, pl in enumerate(self.plans):
             s = self._make(pl.cfg)
             a, b = pl.lx0, pl.lx0 + pl.nxl
@@ -221,30 +232,33 @@ class OutOfCoreSimulation:
                         self._dfts[did] = (0, r, s.add_dft_plane(0, pl.local(index), mask, om))
                     elif axis != 0:
                         if self._dfts[did] is None:
-                            self._dfts[did] = (axis, [None] * len(self.plans))
+                            self._dfts[did] = (axis, [None] * S)
                         self._dfts[did][1][r] = s.add_dft_plane(axis, index, mask, om)
             for comp, arr in self._fields.items():
                 s.set_field(comp, np.ascontiguousarray(arr[a:b]))
             pins = self._pin_buffers(s, pl)
             if pins is not None:
-                self._pins = self._pins or [None] * len(self.plans)
+                self._pins = self._pins or [None] * S
                 self._pins[r] = pins
-            self._edges[1][r] = self._read_edges(s, pl, 1)          # turn -1
+            if r > 0:
+                self._down[r] = self._read_lower(s, pl)              # for slab r - 1's first turn
             self._park(s)
             self.slabs.append(s)
 
     def _turn(self, r, t, k):
-        """Turn t of slab r: k steps from the edges its neighbours left in
-        turn t - 1; its own edges of turn t go to the buffers of parity t % 2."""
+        """Turn t of slab r: k steps from time n, its ghost planes from U[r-1]
+        (this sweep) and D[r+1] (the last)."""
         s, pl = self.slabs[r], self.plans[r]
-        old = self._edges[(t - 1) % 2]
+        last = len(self.slabs) - 1
         self._unpark(s)
         if r > 0:
-            s.write_planes(0, pl.halo, old[r - 1][1])
-        if r < len(self.slabs) - 1:
-            s.write_planes(pl.nxl - pl.halo, pl.halo, old[r + 1][0])
+            s.write_planes(0, pl.halo, self._up[r - 1])
+        if r < last:
+            s.write_planes(pl.nxl - pl.halo, pl.halo, self._down[r + 1])
+            self._up[r] = self._read_upper(s, pl)
         s.step(k)
-        self._edges[t % 2][r] = self._read_edges(s, pl, t % 2)
+        if r > 0:
+            self._down[r] = self._read_lower(s, pl)
         self._park(s)
 
     def _turn_after(self, deps, r, t, k):
@@ -255,12 +269,11 @@ class OutOfCoreSimulation:
     def step(self, n):
         """Advance every slab by n time steps, K per turn.
 
-        Turn t of slab r needs only turn t - 1 of slabs r - 1, r and r + 1
-        (whose completion also frees the edge buffers it overwrites), so with
-        resident > 1 the turns run as a dataflow on that many host threads,
-        each slab on its own stream: copies of one slab overlap the steps of
-        another, and a slab starts its next turn without waiting for the far
-        end of the grid."""
+        Turn t of slab r needs turn t of slab r - 1 and turn t - 1 of slabs r
+        and r + 1, so with resident > 1 the turns run as a dataflow on that
+        many host threads (a wavefront: slab r at turn t beside slab r + 2 at
+        turn t - 1), each slab on its own stream, one slab's copies overlapping
+        another's steps."""
         if self.slabs is None:
             self._build()
         ks = []
@@ -285,7 +298,7 @@ class OutOfCoreSimulation:
         for q, k in enumerate(ks):
             t = t0 + q
             for r in range(S):
-                deps = [futs[(x, t - 1)] for x in (r - 1, r, r + 1) if (x, t - 1) in futs]
+                deps = [futs[x] for x in ((r - 1, t), (r, t - 1), (r + 1, t - 1)) if x in futs]
                 futs[(r, t)] = self._pool.submit(self._turn_after, deps, r, t, k)
         try:
             for f in futs.values():
