@@ -2483,6 +2483,101 @@ static int plane_copy(dtmx_ctx* ctx, int x0, int np, float* host, bool read) {
   return DTMX_OK;
 }
 
+// Where array arr of ctx lives now: its device address, or while the context is
+// parked, the same offset in its block's pinned host copy (nullptr if that block
+// has no copy).  `bytes` from arr must lie inside the block.
+static char* array_home(dtmx_ctx* ctx, const void* arr, size_t bytes) {
+  if (!ctx->parked) return (char*)arr;
+  const CUdeviceptr a = (CUdeviceptr)arr;
+  for (const VmmBlock& b : ctx->vmm)
+    if (a >= b.va && a + bytes <= b.va + b.size) return (b.host && !b.dead) ? (char*)b.host + (a - b.va) : nullptr;
+  return nullptr;
+}
+
+// Plane state of planes [src_x0, src_x0 + n) of src into planes [dst_x0, ...)
+// of dst, either of them parked (then its pinned host copy is read or written).
+extern "C" int dtmx_copy_planes(dtmx_ctx* dst, int dst_x0, dtmx_ctx* src, int src_x0, int nplanes) {
+  if (!dst || !src || dst == src) return fail(dst, DTMX_ERR_INVALID, "copy_planes needs two contexts");
+  for (dtmx_ctx* x : {dst, src}) {
+    if (x->cfg.geometry != DTMX_GEOM_BOX || x->cfg.absorber == DTMX_ABS_SPLIT_PML)
+      return fail(dst, DTMX_ERR_UNSUPPORTED, "plane state: box geometry with a CPML or no absorber only");
+    if (x->has_gyro || x->P.des_on)
+      return fail(dst, DTMX_ERR_UNSUPPORTED, "plane state: gyrotropic materials and design regions are not per plane");
+  }
+  const dtmx_config &cd = dst->cfg, &cs = src->cfg;
+  if (cd.ny != cs.ny || cd.nz != cs.nz || dst->nzp != src->nzp || plane_poles(dst) != plane_poles(src) ||
+      plane_floats(dst) != plane_floats(src))
+    return fail(dst, DTMX_ERR_INVALID, "copy_planes: contexts of different y/z configurations or material tables");
+  for (int a = 1; a < 3; a++)
+    if ((dst->P.ab.aux[a][0] != nullptr) != (src->P.ab.aux[a][0] != nullptr) || dst->P.ab.L[a][0] != src->P.ab.L[a][0] ||
+        dst->P.ab.L[a][1] != src->P.ab.L[a][1])
+      return fail(dst, DTMX_ERR_INVALID, "copy_planes: different y/z absorber slabs");
+  const int np = nplanes;
+  if (np < 0 || dst_x0 < 0 || src_x0 < 0 || dst_x0 + np > cd.nx || src_x0 + np > cs.nx)
+    return fail(dst, DTMX_ERR_INVALID, "planes outside the grid");
+  for (dtmx_ctx* x : {dst, src}) {
+    const int x0 = x == dst ? dst_x0 : src_x0;
+    const int xl = x->P.ab.aux[0][0] ? x->P.ab.L[0][0] : 0, xh = x->P.ab.aux[0][0] ? x->P.ab.L[0][1] : 0;
+    if (np > 0 && (x0 < xl || x0 + np > x->cfg.nx - xh)) return fail(dst, DTMX_ERR_UNSUPPORTED, "planes inside an x absorber slab");
+  }
+  if (np == 0) return DTMX_OK;
+  dtmx_ctx* ctx = dst;                          // errors of the copies are reported on dst
+  CK(cudaStreamSynchronize(src->stream));
+  cudaStream_t st = dst->stream;
+  auto span = [&](dtmx_ctx* x, const float* arr, size_t off, size_t cnt) -> char* {
+    // cnt floats from arr + off, inside the array's block
+    return array_home(x, arr + off, cnt * 4);
+  };
+  // fields and y/z auxiliaries: the same per-plane layout in both contexts
+  const size_t sx = (size_t)src->P.g.sx;
+  for (int comp = 0; comp < 6; comp++) {
+    char* d = span(dst, dst->P.f[comp], (size_t)dst_x0 * sx, (size_t)np * sx);
+    char* h = span(src, src->P.f[comp], (size_t)src_x0 * sx, (size_t)np * sx);
+    if (!d || !h) return fail(dst, DTMX_ERR_STATE, "copy_planes: a parked array has no host copy");
+    CK(cudaMemcpyAsync(d, h, (size_t)np * sx * 4, cudaMemcpyDefault, st));
+  }
+  for (int a = 1; a < 3; a++) {
+    if (!src->P.ab.aux[a][0]) continue;
+    const size_t th = (size_t)(src->P.ab.L[a][0] + src->P.ab.L[a][1]);
+    const size_t pp = a == 1 ? th * cs.nz : (size_t)cs.ny * th;
+    for (int q = 0; q < 4; q++) {
+      char* d = span(dst, dst->P.ab.aux[a][q], (size_t)dst_x0 * pp, (size_t)np * pp);
+      char* h = span(src, src->P.ab.aux[a][q], (size_t)src_x0 * pp, (size_t)np * pp);
+      if (!d || !h) return fail(dst, DTMX_ERR_STATE, "copy_planes: a parked array has no host copy");
+      CK(cudaMemcpyAsync(d, h, (size_t)np * pp * 4, cudaMemcpyDefault, st));
+    }
+  }
+  // ADE state over the intersection of the two boxes (a dispersive node of
+  // the copied planes lies in both; the rest of either box holds zeros there)
+  const Ade &As = src->P.ade, &Ad = dst->P.ade;
+  const int P = plane_poles(src);
+  const int p0 = std::max(std::max(0, As.lo[0] - src_x0), Ad.lo[0] - dst_x0);
+  const int p1 = std::min(std::min(np, As.lo[0] + As.n[0] - src_x0), Ad.lo[0] + Ad.n[0] - dst_x0);
+  const int y0 = std::max(As.lo[1], Ad.lo[1]), y1 = std::min(As.lo[1] + As.n[1], Ad.lo[1] + Ad.n[1]);
+  const int z0 = std::max(As.lo[2], Ad.lo[2]), z1 = std::min(As.lo[2] + As.n[2], Ad.lo[2] + Ad.n[2]);
+  for (int comp = 0; comp < 3; comp++)
+    for (int q = 0; q < 1 + 2 * P; q++) {
+      float* as = q == 0 ? As.Em[comp] : q <= P ? As.Jp[comp][q - 1] : As.Jm[comp][q - 1 - P];
+      float* ad = q == 0 ? Ad.Em[comp] : q <= P ? Ad.Jp[comp][q - 1] : Ad.Jm[comp][q - 1 - P];
+      if (!as || p0 >= p1 || y0 >= y1 || z0 >= z1) continue;       // nothing dispersive in the copied planes
+      if (!ad) return fail(dst, DTMX_ERR_INVALID, "copy_planes: dispersive nodes the destination does not hold");
+      const size_t ns = (size_t)As.n[0] * As.n[1] * As.n[2], nd = (size_t)Ad.n[0] * Ad.n[1] * Ad.n[2];
+      char* hs = array_home(src, as, ns * 4);
+      char* hd = array_home(dst, ad, nd * 4);
+      if (!hs || !hd) return fail(dst, DTMX_ERR_STATE, "copy_planes: a parked array has no host copy");
+      cudaMemcpy3DParms m = {};
+      m.srcPtr = make_cudaPitchedPtr(hs, (size_t)As.n[2] * 4, As.n[2], As.n[1]);
+      m.srcPos = make_cudaPos((size_t)(z0 - As.lo[2]) * 4, y0 - As.lo[1], src_x0 + p0 - As.lo[0]);
+      m.dstPtr = make_cudaPitchedPtr(hd, (size_t)Ad.n[2] * 4, Ad.n[2], Ad.n[1]);
+      m.dstPos = make_cudaPos((size_t)(z0 - Ad.lo[2]) * 4, y0 - Ad.lo[1], dst_x0 + p0 - Ad.lo[0]);
+      m.extent = make_cudaExtent((size_t)(z1 - z0) * 4, y1 - y0, p1 - p0);
+      m.kind = cudaMemcpyDefault;
+      CK(cudaMemcpy3DAsync(&m, st));
+    }
+  CK(cudaStreamSynchronize(st));
+  return DTMX_OK;
+}
+
 extern "C" int dtmx_plane_state_floats(dtmx_ctx* ctx, size_t* floats_per_plane) {
   if (!ctx || !floats_per_plane) return fail(ctx, DTMX_ERR_INVALID, "bad plane state request");
   if (int rc = plane_refusal(ctx)) return rc;

@@ -20,7 +20,7 @@ EXPORTS = (
     "dtmx_set_materials", "dtmx_add_point_source", "dtmx_set_tfsf", "dtmx_add_probe",
     "dtmx_read_probes", "dtmx_add_dft_plane", "dtmx_read_dft", "dtmx_step", "dtmx_sync",
     "dtmx_get_step", "dtmx_get_field", "dtmx_set_field", "dtmx_field_device_ptr",
-    "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_set_xchunk", "dtmx_park", "dtmx_unpark", "dtmx_set_park_pool", "dtmx_plane_state_floats", "dtmx_read_planes", "dtmx_write_planes", "dtmx_set_tile_rows", "dtmx_get_engine", "dtmx_get_stream",
+    "dtmx_check_finite", "dtmx_kernel_launches", "dtmx_set_engine", "dtmx_set_xchunk", "dtmx_park", "dtmx_unpark", "dtmx_set_park_pool", "dtmx_plane_state_floats", "dtmx_read_planes", "dtmx_write_planes", "dtmx_copy_planes", "dtmx_set_tile_rows", "dtmx_get_engine", "dtmx_get_stream",
     "dtmx_set_profiling", "dtmx_read_profile", "dtmx_abi_sizes", "dtmx_count_nonfinite_noalloc",
     "dtmx_tfsfsrc_set", "dtmx_ref_main", "dtmx_ref_materials", "dtmx_ref_material_table",
     "dtmx_set_design", "dtmx_forward_adjoint", "dtmx_batch_forward_adjoint", "dtmx_autotune",
@@ -81,6 +81,7 @@ def load():
     L.dtmx_plane_state_floats.argtypes = [vp, C.POINTER(C.c_size_t)]
     L.dtmx_read_planes.argtypes = [vp, ip, ip, vp]
     L.dtmx_write_planes.argtypes = [vp, ip, ip, vp]
+    L.dtmx_copy_planes.argtypes = [vp, ip, vp, ip, ip]
     L.dtmx_unpark.argtypes = [vp]
     L.dtmx_set_tile_rows.argtypes = [vp, ip]
     L.dtmx_get_engine.argtypes = [vp, C.POINTER(ip), C.POINTER(ip), C.POINTER(ip), C.POINTER(ip)]
@@ -272,6 +273,11 @@ class Simulation:
         if a.size != self.plane_state_floats() * int(nplanes):
             raise ValueError("plane state of the wrong size")
         self._ck(self._L.dtmx_write_planes(self._h, int(x0), int(nplanes), a.ctypes.data))
+
+    def copy_planes(self, x0, src, src_x0, nplanes):
+        """Planes [src_x0, src_x0 + nplanes) of Simulation src into planes
+        [x0, ...) of this one, either of them parked (dtmx_copy_planes)."""
+        self._ck(self._L.dtmx_copy_planes(self._h, int(x0), src._h, int(src_x0), int(nplanes)))
 
     def set_xchunk(self, planes):
         """Planes of the x walk per CTA (0: automatic)."""

@@ -9,13 +9,13 @@ dtmx_unpark move its arrays to pinned host memory and back at the same device
 addresses) whose local grid carries K + 1 ghost planes on each side that has
 a neighbour.  One turn of slab r at time n:
 
-  unpark; write the neighbours' edge planes of time n into the ghost planes
-  (the full plane state: fields, y/z CPML auxiliaries, ADE currents --
-  dtmx_write_planes); read its own last K + 1 owned planes (time n, for slab
-  r + 1 later in the same sweep, dtmx_read_planes); step k <= K times; read
-  its own first K + 1 owned planes (time n + k, for slab r - 1 in the next
-  sweep); park.  The slabs take their turns in order, so each edge needs one
-  host buffer.
+  unpark (its lower ghost planes already hold slab r - 1's last owned planes
+  of time n, left in its parked state by r - 1's turn); copy slab r + 1's
+  first owned planes into its upper ghost planes and its own last owned
+  planes into slab r + 1's lower ghost planes, straight between the device
+  and r + 1's parked host copy (the full plane state: fields, y/z CPML
+  auxiliaries, ADE currents -- dtmx_copy_planes); step k <= K times; park.
+  No edge buffers, one copy of K + 1 planes each way per turn.
 
 Why it is exact: a local order-2 step is wrong only next to the local grid's
 faces (one plane at each cut face per step), so after k <= K steps the planes
@@ -102,11 +102,10 @@ class OutOfCoreSimulation:
     Set-up calls take the global arrays and coordinates; they are applied to
     the slabs when the slabs are built (at the first step or read-back).
     make_local(cfg) builds a slab's simulation (default: a parkable GPU
-    Simulation); it must offer read_planes / write_planes.  park(local) /
+    Simulation); it must offer copy_planes or read_planes / write_planes.  park(local) /
     unpark(local) move it off and onto the device (defaults: its park /
-    unpark methods where it has them, else nothing).  Edge planes of GPU
-    slabs pass through pinned host buffers (one per side), so their copies
-    run at the host link's rate.
+    unpark methods where it has them, else nothing).  Slabs without
+    copy_planes (a CPU engine) exchange edges by read_planes / write_planes.
     """
 
     def __init__(self, cfg, nslabs, steps_per_turn=8, make_local=None, park=None, unpark=None, resident=1):
@@ -120,7 +119,6 @@ class OutOfCoreSimulation:
         self._make = make_local or parkable_simulation
         self._park = park or (lambda s: s.park() if hasattr(s, "park") else None)
         self._unpark = unpark or (lambda s: s.unpark() if hasattr(s, "unpark") else None)
-        self._pins = None         # per slab: pinned buffers of its upper and lower edge planes (GPU slabs)
         self._pool_dev = None     # device whose park pool this run opened
         self._ops = []            # set-up calls, replayed on each slab when it is built
         self._fields = {}         # initial global fields by component
@@ -128,7 +126,6 @@ class OutOfCoreSimulation:
         self._nprobes = 0
         self._dfts = []           # (slab, local id)
         self.slabs = None
-        self._up = self._down = None   # per slab: its upper / lower owned halo planes (see _read_upper)
         self.turns = 0
 
     # ---- set-up (recorded)
@@ -171,39 +168,32 @@ class OutOfCoreSimulation:
         self._fields[comp] = np.asarray(arr, dtype=np.float32)
 
     # ---- slabs
-    # Edge planes: U[r], slab r's upper owned halo planes, read at the start of
-    # its turn (time n, before it steps) for slab r + 1's lower ghosts in the
-    # same sweep; D[r], its lower owned halo planes, read at the end of its
-    # turn (time n + k) for slab r - 1's upper ghosts in the next sweep.  One
-    # buffer per side: turn t of slab r runs after turn t of slab r - 1 (U[r-1]
-    # of this sweep) and after turn t - 1 of slab r + 1 (D[r+1] of the last),
-    # which also keeps every buffer until its reader is done.
-    def _read_upper(self, s, pl):
-        lo, hi = pl.owned_local()
-        return s.read_planes(hi - pl.halo, pl.halo, out=self._pins[pl.rank][0] if self._pins else None)
+    # Edge planes move between neighbours directly (dtmx_copy_planes, the
+    # parked neighbour's host copy read or written in place): at the start of
+    # its turn, slab r takes its upper ghost planes from slab r + 1's first
+    # owned planes and leaves its own last owned planes in slab r + 1's lower
+    # ghost planes, both at time n, before it steps.  Turn t of slab r runs
+    # after turn t of slab r - 1 (which left r's lower ghosts) and after turn
+    # t - 1 of slab r + 1, and before turn t of slab r + 1.
+    @staticmethod
+    def _copy(dst, x0, src, src_x0, n):
+        if hasattr(dst, "copy_planes"):
+            dst.copy_planes(x0, src, src_x0, n)
+        else:
+            dst.write_planes(x0, n, src.read_planes(src_x0, n))
 
-    def _read_lower(self, s, pl):
-        lo, hi = pl.owned_local()
-        return s.read_planes(lo, pl.halo, out=self._pins[pl.rank][1] if self._pins else None)
-
-    def _pin_buffers(self, s, pl):
-        """One pinned float32 buffer per side for a GPU slab's edge planes;
-        the first GPU slab also lets parking keep device memory for the
-        slabs that follow (released again by close)."""
+    def _open_pool(self, s):
+        """The first GPU slab lets parking keep device memory for the slabs
+        that follow (released again by close)."""
         from .engine import Simulation, set_park_pool
-        if not isinstance(s, Simulation):
-            return None
-        import torch
-        if self._pool_dev is None:
+        if self._pool_dev is None and isinstance(s, Simulation):
+            import torch
             self._pool_dev = torch.cuda.current_device()
             set_park_pool(-1, self._pool_dev)
-        n = s.plane_state_floats() * pl.halo
-        return [torch.empty(n, dtype=torch.float32).pin_memory().numpy() for _ in range(2)]
 
     def _build(self):
         self.slabs = []
         S = len(self.plans)
-        self._up, self._down = [None] * S, [None] * S
         for r, pl in enumerate(self.plans):
             s = self._make(pl.cfg)
             a, b = pl.lx0, pl.lx0 + pl.nxl
@@ -236,29 +226,21 @@ class OutOfCoreSimulation:
                         self._dfts[did][1][r] = s.add_dft_plane(axis, index, mask, om)
             for comp, arr in self._fields.items():
                 s.set_field(comp, np.ascontiguousarray(arr[a:b]))
-            pins = self._pin_buffers(s, pl)
-            if pins is not None:
-                self._pins = self._pins or [None] * S
-                self._pins[r] = pins
-            if r > 0:
-                self._down[r] = self._read_lower(s, pl)              # for slab r - 1's first turn
+            self._open_pool(s)
             self._park(s)
             self.slabs.append(s)
 
     def _turn(self, r, t, k):
-        """Turn t of slab r: k steps from time n, its ghost planes from U[r-1]
-        (this sweep) and D[r+1] (the last)."""
+        """Turn t of slab r: exchange edge planes with the parked slab r + 1
+        (time n), then k steps."""
         s, pl = self.slabs[r], self.plans[r]
-        last = len(self.slabs) - 1
         self._unpark(s)
-        if r > 0:
-            s.write_planes(0, pl.halo, self._up[r - 1])
-        if r < last:
-            s.write_planes(pl.nxl - pl.halo, pl.halo, self._down[r + 1])
-            self._up[r] = self._read_upper(s, pl)
+        if r < len(self.slabs) - 1:
+            nb, npl = self.slabs[r + 1], self.plans[r + 1]
+            lo, hi = pl.owned_local()
+            self._copy(s, pl.nxl - pl.halo, nb, npl.owned_local()[0], pl.halo)
+            self._copy(nb, 0, s, hi - pl.halo, pl.halo)
         s.step(k)
-        if r > 0:
-            self._down[r] = self._read_lower(s, pl)
         self._park(s)
 
     def _turn_after(self, deps, r, t, k):

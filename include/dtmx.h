@@ -481,6 +481,13 @@ int  dtmx_set_park_pool(int device, int64_t bytes);
 int  dtmx_plane_state_floats(dtmx_ctx* ctx, size_t* floats_per_plane);
 int  dtmx_read_planes(dtmx_ctx* ctx, int x0, int nplanes, float* host);
 int  dtmx_write_planes(dtmx_ctx* ctx, int x0, int nplanes, const float* host);
+/* The same state of planes [src_x0, src_x0 + nplanes) of src copied straight
+ * into planes [dst_x0, ...) of dst (same y/z configuration and material
+ * table), either context parked or not: a parked context's pinned host copy
+ * is read or written, so a slab can take its neighbour's edge planes from,
+ * or leave its own in, the neighbour's parked state without a staging
+ * buffer.  Same refusals as dtmx_read_planes; waits for both streams. */
+int  dtmx_copy_planes(dtmx_ctx* dst, int dst_x0, dtmx_ctx* src, int src_x0, int nplanes);
 
 /* Tile height (y rows) of the single-sweep engine: 16 (default) or 8 (more
  * CTAs for grids of a few million cells; 0 restores 16).  The reference's

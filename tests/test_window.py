@@ -367,3 +367,33 @@ def test_window_tfsf_equals_in_core_run(kind, engine):
         assert np.array_equal(w.read_dft(x), b.read_dft(y))
     w.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_copy_planes_between_parked_and_live_contexts():
+    """dtmx_copy_planes gives the planes dtmx_read_planes / dtmx_write_planes
+    would move, whether the source or the destination is parked."""
+    from dtmaxwell4_b200 import Simulation, abi
+    cfg, mats, idx, src, probes, fields = _scenario()
+    pc = abi.make_config(NX, NY, NZ, dx=1.0, courant=0.5, order=2, absorber=abi.ABS_CPML, pml=4,
+                         probe_capacity=STEPS + 8, parkable=True)
+    a, b = Simulation(pc), Simulation(pc)
+    _apply(a, mats, idx, src, probes, fields)
+    _apply(b, mats, idx, src, probes, fields)
+    a.step(11)
+    b.step(5)
+    # the same planes of both grids (the same materials there, as for two slabs' shared planes)
+    want = a.read_planes(18, 4)                      # planes 18..21: dielectric, Drude nodes, CPML rows
+    assert not np.array_equal(b.read_planes(18, 4), want)
+    b.park()
+    b.copy_planes(18, a, 18, 4)                      # live source, parked destination
+    b.unpark()
+    assert np.array_equal(b.read_planes(18, 4), want)
+    b.step(2)
+    a.park()
+    b.copy_planes(18, a, 18, 4)                      # parked source, live destination
+    assert np.array_equal(b.read_planes(18, 4), want)
+    a.unpark()
+    assert np.array_equal(a.read_planes(18, 4), want)
+    a.close()
+    b.close()
