@@ -457,8 +457,8 @@ def run_out_of_core(args):
             "in_core_gcell_per_s": round(cells * steps / t_in / 1e9, 3),
             "device_bytes_free_out_of_core": int(free_ooc), "device_bytes_free_in_core": int(free_in),
             "identical_to_in_core": same,
-            "note": "engine 3 in both; each turn unparks a slab (H2D of its state), writes its neighbours' "
-                    "edge planes, steps K times, reads its edge planes and parks it (D2H)"}
+            "note": "engine 3 in both; each turn unparks a slab (H2D of its state), exchanges K+1 edge planes "
+                    "with the parked next slab's host copy, steps K times and parks it (D2H)"}
 
 
 def run_out_of_core_headline(args):
